@@ -1,0 +1,306 @@
+"""Benchmark: R-MAT scale-22 multilevel spectral bisection on B200.
+
+One step = one full partition (HEC coarsening, coarse builds, Fiedler power
+iteration on every level, median split) of the R-MAT scale-22 graph
+(a, b, c, d = 0.57, 0.19, 0.19, 0.05, edge factor 16, seeded; symmetrised,
+duplicates merged, self loops dropped, largest connected component kept).
+
+  value  edges/s with the CSR resident in HBM and the partition left on the
+         device (FP64 path), whole job over all ranks
+  e2e    the same through the public API with pinned host buffers: the CSR
+         upload and the partition download are inside the timed region
+  mixed  FP32-storage / FP64-reduction power iteration on the same graph
+
+Multi-GPU: the single-graph path does not shard (a row partition would need
+halo exchanges per iteration); N ranks run N independent replicas ("weak"),
+value = total edges of all replicas / max over ranks of the step time.
+
+`--impl reference` times the reference's own OpenMP path (cmg/sgpar.h built
+by oracle/Makefile) on the host cores on a bounded R-MAT sample.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+RMAT = dict(edge_factor=16, a=0.57, b=0.19, c=0.19, seed=1)
+SCALE = 22
+REF_SAMPLE_SCALE = 18
+METRIC = "edges/s partitioned (R-MAT scale 22 bisection, 1 graph per GPU)"
+
+
+def rmat_graph(scale: int):
+    from ipdps_2021_graph_coarsening_b200 import graphs as G
+    cache = os.path.join("/tmp", f"sgpb_rmat{scale}_s{RMAT['seed']}.npz")
+    if os.path.exists(cache):
+        d = np.load(cache)
+        return G.CSR(d["rp"], d["col"], None, f"rmat{scale}")
+    g = G.rmat(scale, **RMAT)
+    try:
+        np.savez(cache, rp=g.row_ptr, col=g.col)
+    except OSError:
+        pass
+    return g
+
+
+def load_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class Clocks:
+    """nvidia-smi sampler running during the timed region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.p = None
+
+    def __enter__(self):
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
+                                       "--format=csv,noheader,nounits", "-lms", "100"],
+                                      stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.p = None
+        return self
+
+    def __exit__(self, *a):
+        self.out = ""
+        if self.p:
+            self.p.terminate()
+            try:
+                self.out, _ = self.p.communicate(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.p.kill()
+                self.out, _ = self.p.communicate()
+
+    def summary(self):
+        rows = []
+        for line in (self.out or "").splitlines():
+            f = [x.strip() for x in line.split(",")]
+            if len(f) >= 9:
+                rows.append(f)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"], "samples": 0}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in rows for k in range(4) if r[5 + k].lower() == "active"})
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def algorithmic_pi_bytes(n: int, m: int, weighted: bool, s: int) -> int:
+    """Bytes one power iteration must move (per-iteration model): offsets,
+    destinations, weights (coarse levels), the iterate read and written, the
+    degree vector."""
+    return 4 * (n + 1) + 4 * m + (4 * m if weighted else 0) + s * n + s * n + 4 * n
+
+
+def dist_setup():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    if ws <= 1:
+        return 0, 1, 0, None
+    import torch.distributed as dist
+    from datetime import timedelta
+    rank = int(os.environ["RANK"])
+    local = int(os.environ.get("LOCAL_RANK", rank))
+    return rank, ws, local, (dist, timedelta)
+
+
+def reference_arm(args, rank: int, ws: int):
+    if rank != 0:
+        return
+    from oracle import bindings as O
+    cores = os.cpu_count() or 1
+    if not O.ref_available("omp"):
+        print(json.dumps({"impl": "reference", "unavailable": "reference OpenMP build (oracle/_ref) not present"}))
+        return
+    g = rmat_graph(REF_SAMPLE_SCALE)
+    times, cuts = [], []
+    for i in range(args.warmup + args.steps):
+        t = time.perf_counter()
+        _, cut, _ = O.ref_partition_graph(g.row_ptr, g.col, rng_state=1000 + i, kind="omp")
+        dt = time.perf_counter() - t
+        if i >= args.warmup:
+            times.append(dt)
+            cuts.append(cut)
+    sec = float(np.mean(times))
+    value = g.m_undirected / sec
+    sample = (f"R-MAT scale {REF_SAMPLE_SCALE} (same generator, {g.n} vertices, {g.m_undirected} edges), "
+              f"one partition per step, reference OpenMP build of cmg/sgpar.h with {cores} threads")
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "edges/s", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": sec * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": f"rmat{SCALE} bisection (sampled as rmat{REF_SAMPLE_SCALE} on the CPU)",
+                       "cutoff": 50, "tol": 1e-10},
+            "cpu_baseline": {"value": value, "unit": "edges/s", "cores": cores, "kind": "reference",
+                             "sample": sample},
+            "e2e": {"value": value, "unit": "edges/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "edgecut_median": float(np.median(cuts))}
+    print(json.dumps(line))
+
+
+def cpu_baseline():
+    from oracle import bindings as O
+    cores = os.cpu_count() or 1
+    g = rmat_graph(REF_SAMPLE_SCALE)
+    if O.ref_available("omp"):
+        ts = []
+        for i in range(3):
+            t = time.perf_counter()
+            O.ref_partition_graph(g.row_ptr, g.col, rng_state=500 + i, kind="omp")
+            ts.append(time.perf_counter() - t)
+        sec = float(np.median(ts))
+        return {"value": g.m_undirected / sec, "unit": "edges/s", "cores": cores, "kind": "reference",
+                "sample": f"R-MAT scale {REF_SAMPLE_SCALE} ({g.n} v, {g.m_undirected} e), median of 3 partitions, "
+                          f"reference OpenMP build of cmg/sgpar.h"}
+    t = time.perf_counter()
+    O.partition_graph(g.row_ptr, g.col, None, rng_state=500)
+    sec = time.perf_counter() - t
+    return {"value": g.m_undirected / sec, "unit": "edges/s", "cores": 1, "kind": "port",
+            "sample": f"R-MAT scale {REF_SAMPLE_SCALE}, 1 partition, oracle C restatement"}
+
+
+def gpu_arm(args, rank: int, ws: int, local: int, distmod):
+    import torch
+    from ipdps_2021_graph_coarsening_b200.api import Partitioner
+    from ipdps_2021_graph_coarsening_b200 import _lib as L
+
+    torch.cuda.set_device(local)
+    dist = None
+    if distmod:
+        dist, td = distmod
+        dist.init_process_group("nccl", timeout=td(seconds=600), device_id=torch.device("cuda", local))
+    g = rmat_graph(SCALE)
+    n, m = g.n, g.m_directed
+    p = Partitioner(local)
+    stream = torch.cuda.ExternalStream(L.lib().sgp_b200_stream(p._ctx))
+    rp_d = torch.from_numpy(g.row_ptr.view(np.int32)).cuda()
+    col_d = torch.from_numpy(g.col.view(np.int32)).cuda()
+    part_d = torch.empty(n, dtype=torch.int32, device="cuda")
+    dg = {"row_ptr": rp_d, "col": col_d}
+
+    def barrier():
+        if dist:
+            dist.barrier()
+
+    def timed(fn, steps):
+        torch.cuda.synchronize()
+        barrier()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        out = [fn() for _ in range(steps)]
+        e1.record(stream)
+        torch.cuda.synchronize()
+        barrier()
+        ms = e0.elapsed_time(e1) / steps
+        if dist:
+            t = torch.tensor([ms], device="cuda")
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            ms = float(t.item())
+        return ms, out
+
+    seed = 0x2021
+    for _ in range(args.warmup):
+        p.partition(dg, rng_state=seed, part_out=part_d)
+    with Clocks(local) as clk:
+        ms, res = timed(lambda: p.partition(dg, rng_state=seed, part_out=part_d), args.steps)
+    r = res[-1]
+    clocks = clk.summary()
+    value = ws * g.m_undirected / (ms / 1e3)
+
+    # end to end through the public API with pinned host buffers
+    rp_h = torch.from_numpy(g.row_ptr.view(np.int32)).pin_memory().numpy().view(np.uint32)
+    col_h = torch.from_numpy(g.col.view(np.int32)).pin_memory().numpy().view(np.uint32)
+    part_h = torch.empty(n, dtype=torch.int32).pin_memory().numpy().view(np.uint32)
+    from ipdps_2021_graph_coarsening_b200.graphs import CSR
+    gh = CSR(rp_h, col_h, None, g.name)
+    p.partition(gh, rng_state=seed, part_out=part_h)
+    ms_e2e, res_e2e = timed(lambda: p.partition(gh, rng_state=seed, part_out=part_h), args.steps)
+    e2e = {"value": ws * g.m_undirected / (ms_e2e / 1e3), "unit": "edges/s",
+           "h2d_bytes_per_step": 4 * (n + 1) + 4 * m, "d2h_bytes_per_step": 4 * n, "ms_per_step": ms_e2e}
+
+    # mixed precision on the same graph and seed
+    p.partition(dg, rng_state=seed, part_out=part_d, mixed=True)
+    ms_mx, res_mx = timed(lambda: p.partition(dg, rng_state=seed, part_out=part_d, mixed=True), args.steps)
+    rm = res_mx[-1]
+    mixed = {"value": ws * g.m_undirected / (ms_mx / 1e3), "ms_per_step": ms_mx, "edgecut": rm.edgecut,
+             "edgecut_fp64": r.edgecut, "cut_rel_diff": abs(rm.edgecut - r.edgecut) / max(1, r.edgecut),
+             "lambda_rel_err": abs(rm.lam - r.lam) / abs(r.lam) if r.lam else None,
+             "residual": rm.residual, "speedup_vs_fp64": ms / ms_mx, "level_iters": rm.level_iters}
+
+    # roofline of the dominant kernel (power iteration) from this step's levels
+    peak, peak_kind = load_peaks()
+    byts = sum(it * algorithmic_pi_bytes(nl, ml, l > 0, 8)
+               for l, (nl, ml, it) in enumerate(zip(r.level_n, r.level_m, r.level_iters)))
+    pi_ms = sum(r.level_pi_ms)
+    achieved = byts / (pi_ms / 1e3) / 1e9 if pi_ms > 0 else 0.0
+    traffic = None
+    tf = os.path.join(ROOT, "profiles", "power_iter_traffic.json")
+    if os.path.exists(tf):
+        try:
+            traffic = json.load(open(tf)).get("dram_bytes_per_iteration_per_entry")
+        except (OSError, ValueError):
+            traffic = None
+    roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                "traffic": traffic, "kernel": "k_power_iter", "peak_kind": peak_kind,
+                "kernel_ms_per_step": pi_ms, "algorithmic_bytes_per_step": byts,
+                "kernel_share_of_step": pi_ms / ms if ms else None}
+
+    line = {"metric": METRIC, "value": value, "unit": "edges/s", "n_gpus": ws, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": f"rmat{SCALE} bisection (a,b,c,d=0.57,0.19,0.19,0.05, ef 16, seed 1, LCC)",
+                       "n": n, "m_undirected": g.m_undirected, "cutoff": 50, "tol": 1e-10,
+                       "parallelism": f"replicas{ws}", "l2": "inputs larger than L2 (CSR 0.5 GB)"},
+            "edgecut": r.edgecut, "lambda": r.lam, "residual": r.residual, "levels": r.level_n,
+            "level_iters": r.level_iters, "level_pi_ms": [round(x, 3) for x in r.level_pi_ms],
+            "phase_ms": {"coarsen": r.ms_coarsen, "eigen": r.ms_eigen, "split": r.ms_split},
+            "clocks": clocks, "e2e": e2e, "mixed": mixed, "gpu_launches": r.kernel_launches * args.steps,
+            "roofline": roofline}
+    if rank == 0 and ws == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline()
+    if rank == 0:
+        print(json.dumps(line))
+    p.close()
+    if dist:
+        dist.destroy_process_group()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    rank, ws, local, distmod = dist_setup()
+    if args.impl == "reference":
+        os.environ.setdefault("OMP_NUM_THREADS", str(os.cpu_count() or 1))
+        reference_arm(args, rank, ws)
+        return
+    os.environ.setdefault("OMP_NUM_THREADS", str(os.cpu_count() or 1))
+    gpu_arm(args, rank, ws, local, distmod)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,245 @@
+/*
+ * sgpar_b200.h -- C ABI of the B200-native multilevel spectral bisection path.
+ *
+ * Part 1 keeps the partition API of the reference's cmg/sgpar.h (the block at
+ * sgpar.h:2230-2244) with its struct layouts for the default build (32-bit
+ * vertex ids, offsets and weights), exported with C linkage so that a C, C++,
+ * cgo, JNI or ctypes caller binds it directly.  Behind these entry points the
+ * hot path -- HEC mapping, coarse-graph construction, Fiedler power iteration
+ * with prolongation and the median split -- runs as hand-written sm_100a
+ * kernels; there is no CPU fallback.
+ *
+ * Part 2 is the explicit-context interface (device, stream, memory reuse,
+ * mixed precision, device-resident inputs/outputs, per-level statistics) and
+ * the lower boundary the reference exposes between its layers
+ * (coarsen_kokkos.h:1165 sgp_generate_coarse_graphs, eigensolve_kokkos.h:1493
+ * sgp_eigensolve) plus per-kernel entry points used by the parity tests.
+ *
+ * Return codes: 0 = success (EXIT_SUCCESS), 1 = failure (EXIT_FAILURE), and
+ * the more specific SGP_B200_ERR_* values of part 2; sgp_b200_last_error()
+ * returns the message of the last failure on the calling thread.
+ */
+#ifndef SGPAR_B200_H_
+#define SGPAR_B200_H_
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ------------------------------------------------------------------------ *
+ * Part 1: the sgpar.h partition API                                         *
+ * ------------------------------------------------------------------------ */
+
+typedef uint32_t sgp_vid_t;   /* sgpar.h:109-111 (default build) */
+typedef uint32_t sgp_eid_t;
+typedef double sgp_real_t;
+typedef uint32_t sgp_wgt_t;   /* sgpar.h:117-121: sgp_vid_t outside the Kokkos build */
+
+/* sgpar.h:82 */
+typedef struct { uint64_t state; uint64_t inc; } sgp_pcg32_random_t;
+
+/* sgpar.h:145-153 */
+typedef struct {
+    sgp_vid_t nvertices;
+    sgp_eid_t nedges;              /* undirected edges = source_offsets[n] / 2 */
+    sgp_eid_t *source_offsets;
+    sgp_vid_t *edges_per_source;
+    sgp_vid_t *destination_indices;
+    sgp_wgt_t *weighted_degree;
+    sgp_wgt_t *eweights;           /* NULL: unit weights (as the reference loader leaves it) */
+} sgp_graph_t;
+
+/* sgpar.h:186-193 */
+typedef struct configuration {
+    int coarsening_alg;
+    int refine_alg;
+    int local_search_alg;
+    int num_iter;
+    double tol;
+    int num_partitions;
+} config_t;
+
+/* sgpar.h:84 -- PCG32 (XSH-RR) step. */
+uint32_t sgp_pcg32_random_r(sgp_pcg32_random_t *rng);
+
+/* sgpar.h:195 -- process-wide default tolerance used when config->tol <= 0. */
+int change_tol(sgp_real_t new_tol);
+
+/* sgpar.h:2262 -- read the reference's binary CSR file (6 x int64 header,
+ * uint32 offsets[n+1], uint32 destinations[m]).  Arrays are malloc'd. */
+int sgp_load_graph(sgp_graph_t *g, char *csr_filename);
+
+/* sgpar.h:2291 -- free and NULL the arrays of g. */
+int sgp_free_graph(sgp_graph_t *g);
+
+/* sgpar.h:2321 -- read `size` whitespace-separated part ids. */
+int sgp_load_partition(sgp_vid_t *part, sgp_vid_t size, char *part_filename);
+
+/* sgpar.h:2754 -- six whitespace-separated fields: coarsening_alg refine_alg
+ * local_search_alg num_partitions num_iter tol (a trailing token is ignored). */
+int sgp_load_config(const char *config_f, config_t *config);
+
+/* sgpar.h:2343 -- label-swap-invariant difference of two bisections / 2. */
+int compute_partition_edit_distance(const sgp_vid_t *part1, const sgp_vid_t *part2,
+                                    sgp_vid_t size, sgp_vid_t *diff);
+
+/* sgpar.h:2363 -- multilevel spectral bisection of g on the current CUDA
+ * device: HEC coarsening until at most 50 vertices remain, Fiedler power
+ * iteration (tolerance config->tol, FP64) up the hierarchy, median split.
+ * part[n] is caller-allocated host memory; *edge_cut receives the cut of the
+ * bisection.  rng seeds the mapping hashes and the coarsest guess and is
+ * advanced.  config->refine_alg must be 0 (shifted combinatorial Laplacian)
+ * and config->local_search_alg 0; other values return EXIT_FAILURE.  With
+ * config->num_partitions == 4 the call still bisects (the 4-way recursion is
+ * the caller's, sgpar.cpp:62-89, via sgp_use_partition). */
+int sgp_partition_graph(sgp_vid_t *part, sgp_eid_t *edge_cut, config_t *config,
+                        const int perc_imbalance_allowed, const sgp_graph_t g,
+                        sgp_pcg32_random_t *rng);
+
+/* sgpar.h:1969 -- median split of an eigenvector and its edge cut (run on the
+ * device; evec and part are host arrays of g.nvertices entries).
+ * num_partitions must be 2 or 4 (4 splits in two as in the reference). */
+int sgp_compute_partition(sgp_vid_t *part, sgp_vid_t num_partitions, sgp_eid_t *edgecut,
+                          int perc_imbalance_allowed, int local_search_alg,
+                          sgp_real_t *evec, sgp_graph_t g);
+
+/* sgpar.h:2666 -- the two induced sub-graphs of a bisection, vertices of each
+ * part relabelled in ascending order; g1/g2 arrays are malloc'd (free with
+ * sgp_free_graph).  Built on the device. */
+int sgp_use_partition(sgp_vid_t *part, const sgp_graph_t g, sgp_graph_t *g1, sgp_graph_t *g2);
+
+/* ------------------------------------------------------------------------ *
+ * Part 2: explicit-context interface                                        *
+ * ------------------------------------------------------------------------ */
+
+#define SGP_B200_OK 0
+#define SGP_B200_FAIL 1
+#define SGP_B200_ERR_INVALID 2      /* bad argument or malformed graph */
+#define SGP_B200_ERR_DEVICE 3       /* CUDA error */
+#define SGP_B200_ERR_TOO_LARGE 4    /* a count exceeds the 32-bit index space */
+#define SGP_B200_ERR_BUDGET 5       /* an iteration / round budget ran out */
+
+typedef struct sgp_b200_ctx sgp_b200_ctx_t;
+
+/* Create a context on CUDA device `device` with its own stream. */
+sgp_b200_ctx_t *sgp_b200_create(int device);
+void sgp_b200_destroy(sgp_b200_ctx_t *ctx);
+const char *sgp_b200_last_error(void);
+/* The stream all work of ctx is issued on (a cudaStream_t). */
+void *sgp_b200_stream(sgp_b200_ctx_t *ctx);
+
+/* memory kind of the pointers in a graph / result */
+#define SGP_B200_HOST 0
+#define SGP_B200_DEVICE 1
+
+typedef struct {
+    uint32_t n;
+    uint64_t m;                 /* directed entries = row_ptr[n] */
+    const uint32_t *row_ptr;    /* n + 1 */
+    const uint32_t *col;        /* m */
+    const uint32_t *w;          /* m or NULL (unit weights) */
+    int mem;                    /* SGP_B200_HOST or SGP_B200_DEVICE */
+} sgp_b200_graph_t;
+
+typedef struct {
+    uint32_t cutoff;            /* coarsen while n > cutoff (reference: 50) */
+    double tol;                 /* power-iteration tolerance (reference: 1e-10) */
+    int mixed;                  /* 0: FP64 vectors; 1: FP32 vector storage and
+                                   gathers with FP64 reductions (+ FP64 polish) */
+    int perc_imbalance;         /* sgp_compute_partition's perc_imbalance_allowed */
+    uint64_t iter_cap;          /* extra cap on power iterations per level, 0 = none */
+    uint64_t rng_state, rng_inc;/* PCG32 seeding (advanced copy returned in result) */
+    int part_mem;               /* memory kind of result->part */
+} sgp_b200_options_t;
+
+#define SGP_B200_MAX_LEVELS 202
+
+typedef struct {
+    uint32_t *part;             /* n entries, caller-allocated (kind part_mem) */
+    uint64_t edgecut;
+    uint32_t part0_size;
+    double lambda;              /* Rayleigh quotient of the finest vector */
+    double residual;            /* ||L x - lambda x||_2 / (2 max_i d_i), x unit */
+    int levels;
+    uint32_t level_n[SGP_B200_MAX_LEVELS];
+    uint64_t level_m[SGP_B200_MAX_LEVELS];
+    uint64_t level_iters[SGP_B200_MAX_LEVELS];
+    int level_hec_rounds[SGP_B200_MAX_LEVELS];
+    float level_pi_ms[SGP_B200_MAX_LEVELS];   /* power-iteration kernel time per level (CUDA events) */
+    int iter_max_reached;
+    uint64_t rng_state;         /* rng after the call */
+    float ms_total, ms_h2d, ms_coarsen, ms_eigen, ms_split, ms_d2h;
+    uint32_t kernel_launches;
+} sgp_b200_result_t;
+
+void sgp_b200_default_options(sgp_b200_options_t *opt);
+
+/* The whole path on one graph (the body of sgp_partition_graph). */
+int sgp_b200_partition(sgp_b200_ctx_t *ctx, const sgp_b200_graph_t *g,
+                       const sgp_b200_options_t *opt, sgp_b200_result_t *res);
+
+/* ---- lower boundary: hierarchy handle (coarsen_kokkos.h:1165,
+ *      eigensolve_kokkos.h:1493) ---- */
+typedef struct sgp_b200_hierarchy sgp_b200_hierarchy_t;
+
+/* Copy g to the device (when host) and coarsen it level by level.
+ * rng is advanced by two PCG32 draws per level. */
+int sgp_b200_generate_coarse_graphs(sgp_b200_ctx_t *ctx, const sgp_b200_graph_t *g,
+                                    uint32_t cutoff, sgp_pcg32_random_t *rng,
+                                    sgp_b200_hierarchy_t **out);
+int sgp_b200_hierarchy_levels(const sgp_b200_hierarchy_t *h);
+/* Device pointers of level l (0 = input graph); vcmap is NULL on the last
+ * level; wbytes is 0 (unit), 4 or 8. */
+int sgp_b200_hierarchy_level(const sgp_b200_hierarchy_t *h, int l, uint32_t *n, uint64_t *m,
+                             const uint32_t **row_ptr, const uint32_t **col, const void **w,
+                             int *wbytes, const uint32_t **vcmap);
+/* Fiedler vector of the finest level: coarsest guess from rng, power
+ * iteration per level, prolongation; eigenvec has n_0 entries of kind mem. */
+int sgp_b200_eigensolve(sgp_b200_ctx_t *ctx, sgp_b200_hierarchy_t *h, sgp_pcg32_random_t *rng,
+                        double tol, int mixed, uint64_t iter_cap, double *eigenvec, int mem,
+                        sgp_b200_result_t *stats);
+void sgp_b200_hierarchy_free(sgp_b200_hierarchy_t *h);
+
+/* ---- per-kernel entry points (device pointers, stream of ctx) ---- */
+
+/* HEC mapping of one level (heuristics.h:930-1031): heavy neighbour hn[n]
+ * and coarse map vcmap[n] onto [0, *nc).  random_level = 1 selects the
+ * level-1 random neighbour of an unweighted graph.  wbytes: 0, 4 or 8. */
+int sgp_b200_hec(sgp_b200_ctx_t *ctx, uint32_t n, const uint32_t *row_ptr, const uint32_t *col,
+                 const void *w, int wbytes, int random_level, uint64_t seed,
+                 uint32_t *hn, uint32_t *vcmap, uint32_t *nc, int *rounds);
+
+/* Coarse graph of one level (coarsen_kokkos.h:1061-1127): rows sorted by
+ * destination, duplicate weights summed, self loops dropped.  c_row_ptr has
+ * nc + 1 entries; c_col / c_w have capacity row_ptr[n] entries; out_wbytes is
+ * 4 or 8 (weights of c_w).  *m_c receives the coarse entry count. */
+int sgp_b200_build_coarse(sgp_b200_ctx_t *ctx, uint32_t n, const uint32_t *row_ptr,
+                          const uint32_t *col, const void *w, int wbytes, const uint32_t *vcmap,
+                          uint32_t nc, int out_wbytes, uint32_t *c_row_ptr, uint32_t *c_col,
+                          void *c_w, uint64_t *m_c);
+
+/* Power iteration of one level (eigensolve_kokkos.h:102-206): x_in is the
+ * start vector (n entries) or, with vcmap != NULL, the coarse vector that
+ * is prolongated (x_in[vcmap[i]], eigensolve_kokkos.h:1556-1559).  x_out
+ * receives the normalised, deflated iterate of the start of the last
+ * iteration (what the reference returns). */
+int sgp_b200_power_iter(sgp_b200_ctx_t *ctx, uint32_t n, const uint32_t *row_ptr,
+                        const uint32_t *col, const void *w, int wbytes, const double *x_in,
+                        const uint32_t *vcmap, double *x_out, double tol, uint64_t iter_cap,
+                        int mixed, uint64_t *niter, double *lambda, double *residual);
+
+/* Median split + edge cut (sgpar.h:1969-2071) of a device eigenvector;
+ * part is a device array of n entries. */
+int sgp_b200_split(sgp_b200_ctx_t *ctx, uint32_t n, const uint32_t *row_ptr, const uint32_t *col,
+                   const double *evec, int perc_imbalance, uint32_t *part, uint64_t *edgecut);
+
+/* Milliseconds of the phases of the last sgp_b200_partition / eigensolve. */
+int sgp_b200_last_timing(sgp_b200_ctx_t *ctx, float *ms_total, float *ms_coarsen,
+                         float *ms_eigen, float *ms_split);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* SGPAR_B200_H_ */

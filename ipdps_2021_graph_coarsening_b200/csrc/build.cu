@@ -1,0 +1,457 @@
+// build.cu -- coarse-graph construction P^T A P of one level.
+//
+// Reference: cmg/coarsen_kokkos.h:1061-1127 (count + map), :799-900
+// (sgp_build_nonskew: scan, atomic-slot bucket scatter, dedupe, compaction),
+// :750-762 + :491-509 (RADIX dedupe: per-row sort by destination, run-sum).
+// Output rows are sorted by destination with duplicate weights summed and
+// self loops dropped -- the RADIX build's output, independent of the order in
+// which the scatter filled the buckets, so the result is deterministic.
+//
+// Per-row dedupe is tiered by bucket size:
+//   tier 1 (<= 32 entries)   one warp, bitonic sort in registers
+//   tier 2 (<= kT2 entries)  one block, bitonic sort in shared memory
+//   tier 3 (larger)          dense accumulation over [0, nc) in global memory
+//                            (bitmap + weight array, L2-resident), compacted in
+//                            ascending destination order
+#include "common.cuh"
+#include "internal.h"
+
+namespace sgpb {
+
+constexpr int kT2 = 4096;
+constexpr uint32_t kSentinel = 0xFFFFFFFFu;
+
+template <int G>
+__device__ __forceinline__ unsigned group_mask() {
+    if (G == 32) return 0xFFFFFFFFu;
+    const unsigned lane = threadIdx.x & 31;
+    return ((1u << G) - 1u) << (lane & ~(unsigned)(G - 1));
+}
+
+// ---------------------------------------------------------------- count --
+template <int G>
+__global__ void __launch_bounds__(256) k_build_count(uint32_t n, const uint32_t *__restrict__ rp,
+                                                     const uint32_t *__restrict__ col,
+                                                     const uint32_t *__restrict__ vcmap,
+                                                     uint32_t *__restrict__ cnt) {
+    const unsigned gm = group_mask<G>();
+    const uint32_t lane = threadIdx.x & (G - 1);
+    const uint64_t gid = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) / G;
+    const uint64_t ngroups = ((uint64_t)gridDim.x * blockDim.x) / G;
+    for (uint64_t u = gid; u < n; u += ngroups) {
+        uint32_t cu = vcmap[u];
+        uint32_t c = 0;
+        for (uint32_t j = rp[u] + lane; j < rp[u + 1]; j += G) c += (__ldg(vcmap + __ldg(col + j)) != cu);
+#pragma unroll
+        for (int o = G / 2; o > 0; o >>= 1) c += __shfl_xor_sync(gm, c, o);
+        if (lane == 0 && c) atomicAdd(cnt + cu, c);
+    }
+}
+
+// -------------------------------------------------------------- scatter --
+template <int G, typename WI>
+__global__ void __launch_bounds__(256) k_build_scatter(uint32_t n, const uint32_t *__restrict__ rp,
+                                                       const uint32_t *__restrict__ col, const WI *__restrict__ w,
+                                                       const uint32_t *__restrict__ vcmap,
+                                                       const uint32_t *__restrict__ boff, uint32_t *__restrict__ fill,
+                                                       uint32_t *__restrict__ bdst, WI *__restrict__ bw) {
+    const unsigned gm = group_mask<G>();
+    const uint32_t lane = threadIdx.x & (G - 1);
+    const unsigned lane32 = threadIdx.x & 31;
+    const unsigned gshift = lane32 & ~(unsigned)(G - 1);
+    const uint64_t gid = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) / G;
+    const uint64_t ngroups = ((uint64_t)gridDim.x * blockDim.x) / G;
+    for (uint64_t u = gid; u < n; u += ngroups) {
+        const uint32_t cu = vcmap[u];
+        const uint32_t b = rp[u], e = rp[u + 1];
+        const uint32_t base_off = boff[cu];
+        for (uint32_t j0 = b; j0 < e; j0 += G) {
+            const uint32_t j = j0 + lane;
+            uint32_t cv = 0;
+            bool keep = false;
+            if (j < e) {
+                cv = __ldg(vcmap + __ldg(col + j));
+                keep = cv != cu;
+            }
+            unsigned bal = (__ballot_sync(gm, keep) >> gshift) & (G == 32 ? 0xFFFFFFFFu : ((1u << G) - 1u));
+            uint32_t slot = 0;
+            if (lane == 0 && bal) slot = atomicAdd(fill + cu, (uint32_t)__popc(bal));
+            slot = __shfl_sync(gm, slot, 0, G);
+            if (keep) {
+                uint32_t p = base_off + slot + __popc(bal & ((1u << lane) - 1u));
+                bdst[p] = cv;
+                if (w) bw[p] = __ldg(w + j);
+            }
+        }
+    }
+}
+
+// ------------------------------------------------------------- classify --
+__global__ void k_classify(uint32_t nc, const uint32_t *__restrict__ boff, uint32_t *__restrict__ dcnt,
+                           uint32_t *__restrict__ lists /* 3 x nc */, uint32_t *__restrict__ tcount /* 3 */) {
+    uint32_t c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= nc) return;
+    uint32_t sz = boff[c + 1] - boff[c];
+    if (sz == 0) { dcnt[c] = 0; return; }
+    int t = sz <= 32 ? 0 : (sz <= (uint32_t)kT2 ? 1 : 2);
+    uint32_t p = atomicAdd(tcount + t, 1u);
+    lists[(size_t)t * nc + p] = c;
+}
+
+// --------------------------------------------------------------- tier 1 --
+template <typename WI, typename WO>
+__global__ void __launch_bounds__(256) k_dedupe_warp(const uint32_t *__restrict__ list, const uint32_t *__restrict__ count,
+                                                     const uint32_t *__restrict__ boff, uint32_t *__restrict__ bdst,
+                                                     const WI *__restrict__ bw, WO *__restrict__ tw,
+                                                     uint32_t *__restrict__ dcnt) {
+    const unsigned lane = threadIdx.x & 31;
+    const uint32_t cntv = *count;
+    const uint64_t wid = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const uint64_t nw = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+    for (uint64_t k = wid; k < cntv; k += nw) {
+        const uint32_t c = list[k];
+        const uint32_t b = boff[c], sz = boff[c + 1] - b;
+        uint32_t key = kSentinel;
+        uint64_t wv = 0;
+        if (lane < sz) {
+            key = bdst[b + lane];
+            wv = bw ? (uint64_t)bw[b + lane] : 1ull;
+        }
+        // bitonic sort of 32 (key, weight) pairs across the warp
+#pragma unroll
+        for (int kk = 2; kk <= 32; kk <<= 1) {
+#pragma unroll
+            for (int j = kk >> 1; j > 0; j >>= 1) {
+                uint32_t ok = __shfl_xor_sync(0xFFFFFFFFu, key, j);
+                uint64_t ow = __shfl_xor_sync(0xFFFFFFFFu, wv, j);
+                bool up = (lane & kk) == 0;
+                bool lower = (lane & j) == 0;
+                bool take = lower ? (up ? ok < key : ok > key) : (up ? ok > key : ok < key);
+                if (take) { key = ok; wv = ow; }
+            }
+        }
+        uint32_t prev = __shfl_up_sync(0xFFFFFFFFu, key, 1);
+        bool valid = key != kSentinel;
+        bool head = valid && (lane == 0 || prev != key);
+        unsigned hm = __ballot_sync(0xFFFFFFFFu, head);
+        uint32_t seg = __popc(hm & ((2u << lane) - 1u));   // 1-based run id
+        uint64_t s = wv;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            uint64_t t = __shfl_up_sync(0xFFFFFFFFu, s, o);
+            uint32_t ts = __shfl_up_sync(0xFFFFFFFFu, seg, o);
+            if (lane >= (unsigned)o && ts == seg) s += t;
+        }
+        uint32_t next = __shfl_down_sync(0xFFFFFFFFu, key, 1);
+        bool tail = valid && (lane == 31 || next != key);
+        if (tail) {
+            bdst[b + seg - 1] = key;
+            tw[b + seg - 1] = (WO)s;
+        }
+        if (lane == 0) dcnt[c] = __popc(hm);
+    }
+}
+
+// --------------------------------------------------------------- tier 2 --
+constexpr int kT2Threads = 256;
+
+template <typename WI, typename WO>
+__global__ void __launch_bounds__(kT2Threads) k_dedupe_block(const uint32_t *__restrict__ list,
+                                                             const uint32_t *__restrict__ count,
+                                                             const uint32_t *__restrict__ boff,
+                                                             uint32_t *__restrict__ bdst, const WI *__restrict__ bw,
+                                                             WO *__restrict__ tw, uint32_t *__restrict__ dcnt) {
+    extern __shared__ __align__(16) unsigned char smraw[];
+    uint32_t *skey = (uint32_t *)smraw;                       // kT2
+    uint64_t *sw = (uint64_t *)(smraw + kT2 * sizeof(uint32_t));   // kT2
+    __shared__ uint64_t scan_sm[33];
+    const uint32_t cntv = *count;
+    for (uint32_t k = blockIdx.x; k < cntv; k += gridDim.x) {
+        const uint32_t c = list[k];
+        const uint32_t b = boff[c], sz = boff[c + 1] - b;
+        uint32_t P = 64;
+        while (P < sz) P <<= 1;
+        for (uint32_t i = threadIdx.x; i < P; i += blockDim.x) {
+            if (i < sz) {
+                skey[i] = bdst[b + i];
+                sw[i] = bw ? (uint64_t)bw[b + i] : 1ull;
+            } else {
+                skey[i] = kSentinel;
+                sw[i] = 0;
+            }
+        }
+        __syncthreads();
+        for (uint32_t kk = 2; kk <= P; kk <<= 1) {
+            for (uint32_t j = kk >> 1; j > 0; j >>= 1) {
+                for (uint32_t t = threadIdx.x; t < P / 2; t += blockDim.x) {
+                    // t-th pair: lower index i has bit j clear
+                    uint32_t i = ((t & ~(j - 1)) << 1) | (t & (j - 1));
+                    uint32_t p = i | j;
+                    bool up = (i & kk) == 0;
+                    uint32_t a = skey[i], bb = skey[p];
+                    if (up ? a > bb : a < bb) {
+                        skey[i] = bb; skey[p] = a;
+                        uint64_t x = sw[i]; sw[i] = sw[p]; sw[p] = x;
+                    }
+                }
+                __syncthreads();
+            }
+        }
+        // heads and positions: each thread owns a contiguous segment
+        const uint32_t per = P / blockDim.x > 0 ? P / blockDim.x : 1;
+        const uint32_t s0 = threadIdx.x * per;
+        uint64_t h = 0;
+        for (uint32_t i = s0; i < s0 + per && i < P; i++) {
+            uint32_t key = skey[i];
+            if (key != kSentinel && (i == 0 || skey[i - 1] != key)) h++;
+        }
+        uint64_t tot;
+        uint64_t inc = block_scan_u64(h, scan_sm, &tot);
+        uint64_t pos = inc - h;
+        for (uint32_t i = s0; i < s0 + per && i < P; i++) {
+            uint32_t key = skey[i];
+            if (key != kSentinel && (i == 0 || skey[i - 1] != key)) {
+                uint64_t s = sw[i];
+                for (uint32_t q = i + 1; q < P && skey[q] == key; q++) s += sw[q];
+                bdst[b + pos] = key;
+                tw[b + pos] = (WO)s;
+                pos++;
+            }
+        }
+        if (threadIdx.x == 0) dcnt[c] = (uint32_t)tot;
+        __syncthreads();
+    }
+}
+
+// --------------------------------------------------------------- tier 3 --
+// scatter-add of the rows [r0, r0 + nrows) of the tier-3 list into dense
+// slots; blockIdx.y = row within the batch.
+template <typename WI, typename WO>
+__global__ void __launch_bounds__(256) k_dense_add(const uint32_t *__restrict__ list, uint32_t r0,
+                                                  const uint32_t *__restrict__ boff, const uint32_t *__restrict__ bdst,
+                                                  const WI *__restrict__ bw, uint32_t nc, WO *__restrict__ acc,
+                                                  uint32_t *__restrict__ bits) {
+    const uint32_t c = list[r0 + blockIdx.y];
+    const uint32_t b = boff[c], e = boff[c + 1];
+    WO *a = acc + (size_t)blockIdx.y * nc;
+    uint32_t *bm = bits + (size_t)blockIdx.y * ((nc + 31) / 32);
+    for (uint32_t j = b + blockIdx.x * blockDim.x + threadIdx.x; j < e; j += gridDim.x * blockDim.x) {
+        uint32_t v = bdst[j];
+        WO wv = bw ? (WO)bw[j] : (WO)1;
+        atomicAdd(a + v, wv);
+        uint32_t bit = 1u << (v & 31);
+        if (!(__ldcg(bm + (v >> 5)) & bit)) atomicOr(bm + (v >> 5), bit);
+    }
+}
+
+// compaction of one dense slot per block, in ascending destination order;
+// clears the slot for reuse.
+template <typename WO>
+__global__ void __launch_bounds__(256) k_dense_collect(const uint32_t *__restrict__ list, uint32_t r0,
+                                                      const uint32_t *__restrict__ boff, uint32_t nc,
+                                                      WO *__restrict__ acc, uint32_t *__restrict__ bits,
+                                                      uint32_t *__restrict__ bdst, WO *__restrict__ tw,
+                                                      uint32_t *__restrict__ dcnt) {
+    __shared__ uint64_t scan_sm[33];
+    const uint32_t c = list[r0 + blockIdx.x];
+    const uint32_t b = boff[c];
+    WO *a = acc + (size_t)blockIdx.x * nc;
+    const uint32_t nwords = (nc + 31) / 32;
+    uint32_t *bm = bits + (size_t)blockIdx.x * nwords;
+    uint64_t base = 0;
+    for (uint32_t w0 = 0; w0 < nwords; w0 += blockDim.x) {
+        uint32_t wi = w0 + threadIdx.x;
+        uint32_t word = wi < nwords ? bm[wi] : 0u;
+        uint64_t pc = __popc(word), tot;
+        uint64_t inc = block_scan_u64(pc, scan_sm, &tot);
+        uint64_t pos = base + inc - pc;
+        while (word) {
+            int bit = __ffs(word) - 1;
+            word &= word - 1;
+            uint32_t v = wi * 32 + bit;
+            bdst[b + pos] = v;
+            tw[b + pos] = a[v];
+            a[v] = 0;
+            pos++;
+        }
+        if (wi < nwords) bm[wi] = 0;
+        base += tot;
+    }
+    if (threadIdx.x == 0) dcnt[c] = (uint32_t)base;
+}
+
+// ---------------------------------------------------------- compaction --
+template <typename WO>
+__global__ void __launch_bounds__(256) k_compact_rows(uint32_t nc, const uint32_t *__restrict__ boff,
+                                                     const uint32_t *__restrict__ crp,
+                                                     const uint32_t *__restrict__ bdst, const WO *__restrict__ tw,
+                                                     uint32_t *__restrict__ ccol, WO *__restrict__ cw) {
+    const unsigned lane = threadIdx.x & 31;
+    const uint64_t wid = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const uint64_t nw = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+    for (uint64_t c = wid; c < nc; c += nw) {
+        uint32_t src = boff[c], dst = crp[c], len = crp[c + 1] - dst;
+        for (uint32_t i = lane; i < len; i += 32) {
+            ccol[dst + i] = bdst[src + i];
+            cw[dst + i] = tw[src + i];
+        }
+    }
+}
+
+// ---------------------------------------------------------------- driver --
+template <typename WI, typename WO>
+static int build_impl(Context &C, const Level &F, const WI *w, const uint32_t *vcmap, uint32_t nc,
+                      uint32_t *crp, uint32_t **ccol_io, WO **cw_io, uint64_t *m_c, bool alloc_out) {
+    const uint32_t n = F.n;
+    uint32_t *cnt, *boff, *fill, *dcnt, *lists, *tcount;
+    SGPB_TRY(dalloc_t(C, &cnt, (size_t)nc + 1));
+    SGPB_TRY(dalloc_t(C, &boff, (size_t)nc + 1));
+    SGPB_TRY(dalloc_t(C, &fill, (size_t)nc + 1));
+    SGPB_TRY(dalloc_t(C, &dcnt, (size_t)nc + 1));
+    SGPB_TRY(dalloc_t(C, &lists, (size_t)3 * nc + 3));
+    SGPB_TRY(dalloc_t(C, &tcount, 4));
+    SGPB_TRY(dzero(C, cnt, sizeof(uint32_t) * ((size_t)nc + 1)));
+    SGPB_TRY(dzero(C, fill, sizeof(uint32_t) * ((size_t)nc + 1)));
+    SGPB_TRY(dzero(C, tcount, sizeof(uint32_t) * 4));
+
+    const double avg = n ? (double)F.m / n : 0;
+    uint32_t cap = (uint32_t)C.num_sms * 16;
+#define SGPB_ROWS_LAUNCH(KERNEL, G, ...)                                                   \
+    {                                                                                      \
+        uint32_t blocks = cdiv((uint64_t)n * G, 256);                                      \
+        if (blocks > cap) blocks = cap;                                                    \
+        if (blocks < 1) blocks = 1;                                                        \
+        KERNEL<<<blocks, 256, 0, C.stream>>>(__VA_ARGS__);                                 \
+    }
+#define SGPB_BY_G(KERNEL_T, ...)                                                           \
+    if (avg <= 4) SGPB_ROWS_LAUNCH(KERNEL_T(4), 4, __VA_ARGS__)                            \
+    else if (avg <= 8) SGPB_ROWS_LAUNCH(KERNEL_T(8), 8, __VA_ARGS__)                       \
+    else if (avg <= 16) SGPB_ROWS_LAUNCH(KERNEL_T(16), 16, __VA_ARGS__)                    \
+    else SGPB_ROWS_LAUNCH(KERNEL_T(32), 32, __VA_ARGS__)
+
+#define K_COUNT(G) k_build_count<G>
+    SGPB_BY_G(K_COUNT, n, F.rp, F.col, vcmap, cnt)
+    SGPB_TRY(scan_u32(C, cnt, boff, nc, nullptr));
+    uint32_t kept = 0;
+    SGPB_TRY(read_u32(C, boff + nc, &kept));
+    uint32_t *bdst;
+    WI *bw = nullptr;
+    WO *tw;
+    SGPB_TRY(dalloc_t(C, &bdst, (size_t)kept + 1));
+    if (w) SGPB_TRY(dalloc_t(C, &bw, (size_t)kept + 1));
+    SGPB_TRY(dalloc_t(C, &tw, (size_t)kept + 1));
+#define K_SCATTER(G) k_build_scatter<G, WI>
+    SGPB_BY_G(K_SCATTER, n, F.rp, F.col, w, vcmap, boff, fill, bdst, bw)
+#undef K_COUNT
+#undef K_SCATTER
+#undef SGPB_BY_G
+#undef SGPB_ROWS_LAUNCH
+    C.kernel_launches += 2;
+    if (nc) {
+        k_classify<<<cdiv(nc, 256), 256, 0, C.stream>>>(nc, boff, dcnt, lists, tcount);
+        uint32_t g1 = cdiv(nc, 8);
+        if (g1 > (uint32_t)C.num_sms * 16) g1 = C.num_sms * 16;
+        k_dedupe_warp<WI, WO><<<g1 ? g1 : 1, 256, 0, C.stream>>>(lists, tcount, boff, bdst, bw, tw, dcnt);
+        size_t sm2 = (size_t)kT2 * (sizeof(uint32_t) + sizeof(uint64_t));
+        SGPB_CUDA(cudaFuncSetAttribute(k_dedupe_block<WI, WO>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm2));
+        uint32_t g2 = (uint32_t)C.num_sms * 4;
+        k_dedupe_block<WI, WO><<<g2, kT2Threads, sm2, C.stream>>>(lists + nc, tcount + 1, boff, bdst, bw, tw, dcnt);
+        C.kernel_launches += 3;
+        SGPB_CUDA(cudaGetLastError());
+        uint32_t n3 = 0;
+        SGPB_TRY(read_u32(C, tcount + 2, &n3));
+        if (n3) {
+            const size_t words = ((size_t)nc + 31) / 32;
+            const size_t slot_bytes = (size_t)nc * sizeof(WO) + words * 4;
+            size_t slots = ((size_t)1 << 30) / (slot_bytes ? slot_bytes : 1);
+            if (slots < 1) slots = 1;
+            if (slots > n3) slots = n3;
+            if (slots > 65535) slots = 65535;
+            WO *acc;
+            uint32_t *bits;
+            SGPB_TRY(dalloc_t(C, &acc, slots * nc));
+            SGPB_TRY(dalloc_t(C, &bits, slots * words));
+            SGPB_TRY(dzero(C, acc, slots * nc * sizeof(WO)));
+            SGPB_TRY(dzero(C, bits, slots * words * 4));
+            for (uint32_t r0 = 0; r0 < n3; r0 += (uint32_t)slots) {
+                uint32_t nr = n3 - r0 < slots ? n3 - r0 : (uint32_t)slots;
+                dim3 ga(8, nr);
+                k_dense_add<WI, WO><<<ga, 256, 0, C.stream>>>(lists + 2 * (size_t)nc, r0, boff, bdst, bw, nc, acc, bits);
+                k_dense_collect<WO><<<nr, 256, 0, C.stream>>>(lists + 2 * (size_t)nc, r0, boff, nc, acc, bits, bdst, tw,
+                                                             dcnt);
+                C.kernel_launches += 2;
+            }
+            SGPB_CUDA(cudaGetLastError());
+        }
+    }
+    SGPB_TRY(scan_u32(C, dcnt, crp, nc, nullptr));
+    uint32_t mc = 0;
+    SGPB_TRY(read_u32(C, crp + nc, &mc));
+    *m_c = mc;
+    if (alloc_out) {
+        SGPB_TRY(dalloc_t(C, ccol_io, (size_t)mc + 1));
+        SGPB_TRY(dalloc_t(C, cw_io, (size_t)mc + 1));
+    }
+    if (nc) {
+        uint32_t g = cdiv(nc, 8);
+        if (g > (uint32_t)C.num_sms * 16) g = C.num_sms * 16;
+        k_compact_rows<WO><<<g ? g : 1, 256, 0, C.stream>>>(nc, boff, crp, bdst, tw, *ccol_io, *cw_io);
+        C.kernel_launches++;
+    }
+    SGPB_CUDA(cudaGetLastError());
+    return SGP_B200_OK;
+}
+
+// Builds level `out` (allocating its arrays from the context) from F + vcmap.
+int build_coarse_level(Context &C, const Level &F, const uint32_t *vcmap, uint32_t nc, int out_wbytes,
+                       Level *out) {
+    uint32_t *crp;
+    SGPB_TRY(dalloc_t(C, &crp, (size_t)nc + 1));
+    uint32_t *ccol = nullptr;
+    uint64_t mc = 0;
+    out->n = nc;
+    out->rp = crp;
+    out->wbytes = out_wbytes;
+    if (F.wbytes == 8 && out_wbytes != 8) {
+        set_error("coarse weights must be at least as wide as fine weights");
+        return SGP_B200_ERR_INVALID;
+    }
+    if (out_wbytes == 8) {
+        unsigned long long *cw = nullptr;
+        if (F.wbytes == 8)
+            SGPB_TRY((build_impl<unsigned long long, unsigned long long>(C, F, (const unsigned long long *)F.w, vcmap, nc,
+                                                                         crp, &ccol, &cw, &mc, true)));
+        else
+            SGPB_TRY((build_impl<uint32_t, unsigned long long>(C, F, (const uint32_t *)F.w, vcmap, nc, crp, &ccol, &cw,
+                                                               &mc, true)));
+        out->w = cw;
+    } else {
+        uint32_t *cw = nullptr;
+        SGPB_TRY((build_impl<uint32_t, uint32_t>(C, F, (const uint32_t *)F.w, vcmap, nc, crp, &ccol, &cw, &mc, true)));
+        out->w = cw;
+    }
+    out->col = ccol;
+    out->m = mc;
+    return SGP_B200_OK;
+}
+
+// Variant writing into caller buffers (the C-ABI test entry point).
+int build_coarse_into(Context &C, const Level &F, const uint32_t *vcmap, uint32_t nc, int out_wbytes,
+                      uint32_t *crp, uint32_t *ccol, void *cw, uint64_t *m_c) {
+    if (F.wbytes == 8 && out_wbytes != 8) {
+        set_error("coarse weights must be at least as wide as fine weights");
+        return SGP_B200_ERR_INVALID;
+    }
+    if (out_wbytes == 8) {
+        unsigned long long *w8 = (unsigned long long *)cw;
+        if (F.wbytes == 8)
+            return build_impl<unsigned long long, unsigned long long>(C, F, (const unsigned long long *)F.w, vcmap, nc,
+                                                                      crp, &ccol, &w8, m_c, false);
+        return build_impl<uint32_t, unsigned long long>(C, F, (const uint32_t *)F.w, vcmap, nc, crp, &ccol, &w8, m_c,
+                                                        false);
+    }
+    uint32_t *w4 = (uint32_t *)cw;
+    return build_impl<uint32_t, uint32_t>(C, F, (const uint32_t *)F.w, vcmap, nc, crp, &ccol, &w4, m_c, false);
+}
+
+}  // namespace sgpb

@@ -1,0 +1,615 @@
+// driver.cu -- the multilevel path behind the C ABI.
+//
+// Reference call structure (cmg/sgpar.h:2363-2430, Kokkos branch):
+//   sgp_generate_coarse_graphs (coarsen_kokkos.h:1165-1234)
+//   sgp_eigensolve            (eigensolve_kokkos.h:1493-1595)
+//   sgp_compute_partition     (sgpar.h:1969)
+// All three run on the device here; the host only sequences kernels and reads
+// back a few scalars per level (coarse vertex / edge counts).
+#include <math.h>
+#include <stdlib.h>
+#include <string.h>
+
+#include <vector>
+
+#include "common.cuh"
+#include "internal.h"
+
+struct sgp_b200_hierarchy {
+    sgpb::Context *C = nullptr;
+    std::vector<sgpb::Level> levels;
+    std::vector<void *> owned;
+};
+
+namespace sgpb {
+
+int build_coarse_into(Context &C, const Level &F, const uint32_t *vcmap, uint32_t nc, int out_wbytes,
+                      uint32_t *crp, uint32_t *ccol, void *cw, uint64_t *m_c);
+
+static uint32_t pcg32(uint64_t *state, uint64_t inc) {
+    uint64_t old = *state;
+    *state = old * 6364136223846793005ULL + (inc | 1);
+    uint32_t xs = (uint32_t)(((old >> 18u) ^ old) >> 27u);
+    uint32_t rot = (uint32_t)(old >> 59u);
+    return (xs >> rot) | (xs << ((-rot) & 31));
+}
+
+__global__ void k_sum_u32(const uint32_t *w, uint64_t m, unsigned long long *out) {
+    uint64_t s = 0;
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < m; i += (uint64_t)gridDim.x * blockDim.x)
+        s += w[i];
+    s = warp_sum(s);
+    if ((threadIdx.x & 31) == 0 && s) atomicAdd(out, (unsigned long long)s);
+}
+
+__global__ void k_check_csr(uint32_t n, uint64_t m, const uint32_t *rp, const uint32_t *col, uint32_t *bad) {
+    uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n && rp[i + 1] < rp[i]) atomicOr(bad, 1u);
+    if (i == 0 && (rp[0] != 0 || rp[n] != m)) atomicOr(bad, 2u);
+    for (uint64_t j = i; j < m; j += (uint64_t)gridDim.x * blockDim.x)
+        if (col[j] >= n) { atomicOr(bad, 4u); break; }
+}
+
+// Copy (or adopt) the input graph as level 0 and validate it on the device.
+static int stage_input(Context &C, const sgp_b200_graph_t *g, Level *L0) {
+    if (!g || g->n == 0) {
+        set_error("empty graph");
+        return SGP_B200_ERR_INVALID;
+    }
+    if (g->m > 0xFFFFFFFFull) {
+        set_error("graph has %llu directed entries; 32-bit offsets hold at most 4294967295",
+                  (unsigned long long)g->m);
+        return SGP_B200_ERR_TOO_LARGE;
+    }
+    if (!g->row_ptr || (g->m && !g->col)) {
+        set_error("null CSR arrays");
+        return SGP_B200_ERR_INVALID;
+    }
+    L0->n = g->n;
+    L0->m = g->m;
+    L0->wbytes = g->w ? 4 : 0;
+    if (g->mem == SGP_B200_DEVICE) {
+        L0->rp = (uint32_t *)g->row_ptr;
+        L0->col = (uint32_t *)g->col;
+        L0->w = (void *)g->w;
+    } else {
+        SGPB_TRY(dalloc_t(C, &L0->rp, (size_t)g->n + 1));
+        SGPB_TRY(dalloc_t(C, &L0->col, (size_t)g->m + 1));
+        SGPB_CUDA(cudaMemcpyAsync(L0->rp, g->row_ptr, sizeof(uint32_t) * ((size_t)g->n + 1), cudaMemcpyHostToDevice,
+                                  C.stream));
+        SGPB_CUDA(cudaMemcpyAsync(L0->col, g->col, sizeof(uint32_t) * g->m, cudaMemcpyHostToDevice, C.stream));
+        if (g->w) {
+            uint32_t *w;
+            SGPB_TRY(dalloc_t(C, &w, (size_t)g->m + 1));
+            SGPB_CUDA(cudaMemcpyAsync(w, g->w, sizeof(uint32_t) * g->m, cudaMemcpyHostToDevice, C.stream));
+            L0->w = w;
+        }
+    }
+    uint32_t *bad;
+    SGPB_TRY(dalloc_t(C, &bad, 1));
+    SGPB_TRY(dzero(C, bad, 4));
+    uint32_t blocks = cdiv(g->n + 1, 256);
+    if (blocks > (uint32_t)C.num_sms * 8) blocks = C.num_sms * 8;
+    k_check_csr<<<blocks, 256, 0, C.stream>>>(g->n, g->m, L0->rp, L0->col, bad);
+    C.kernel_launches++;
+    uint32_t hb = 0;
+    SGPB_TRY(read_u32(C, bad, &hb));
+    if (hb) {
+        set_error("malformed CSR (code %u: 1 = decreasing offsets, 2 = row_ptr[0] != 0 or row_ptr[n] != m, "
+                  "4 = destination >= n)", hb);
+        return SGP_B200_ERR_INVALID;
+    }
+    return SGP_B200_OK;
+}
+
+static int weight_width(Context &C, const Level &L0, int *wbytes) {
+    if (!L0.w) { *wbytes = 4; return SGP_B200_OK; }   // unit weights: total = m < 2^32
+    unsigned long long *s;
+    SGPB_TRY(dalloc_t(C, &s, 1));
+    SGPB_TRY(dzero(C, s, 8));
+    uint32_t blocks = (uint32_t)C.num_sms * 8;
+    k_sum_u32<<<blocks, 256, 0, C.stream>>>((const uint32_t *)L0.w, L0.m, s);
+    C.kernel_launches++;
+    uint64_t tot;
+    SGPB_TRY(read_u64(C, (const uint64_t *)s, &tot));
+    // every coarse weight and weighted degree is a partial sum of the total
+    *wbytes = tot <= 0xFFFFFFFFull ? 4 : 8;
+    return SGP_B200_OK;
+}
+
+// coarsen_kokkos.h:1196-1232: levels while n > cutoff, at most 200; a
+// coarsest level below 10 vertices is dropped.
+static int generate(Context &C, const Level &L0, uint32_t cutoff, uint64_t *rng_state, uint64_t rng_inc,
+                    std::vector<Level> &levels) {
+    levels.clear();
+    levels.push_back(L0);
+    int out_wbytes = 4;
+    SGPB_TRY(weight_width(C, L0, &out_wbytes));
+    while (levels.back().n > cutoff) {
+        Level &F = levels.back();
+        uint32_t hi = pcg32(rng_state, rng_inc);
+        uint32_t lo = pcg32(rng_state, rng_inc);
+        uint64_t seed = ((uint64_t)hi << 32) | lo;
+        F.seed_hi = hi;
+        F.seed_lo = lo;
+        uint32_t *vcmap;
+        SGPB_TRY(dalloc_t(C, &vcmap, F.n));
+        uint32_t nc = 0;
+        int rounds = 0;
+        const int random_level = (levels.size() == 1) && (L0.w == nullptr);
+        SGPB_TRY(hec_map_level(C, F, random_level, seed, vcmap, nullptr, &nc, &rounds));
+        F.vcmap = vcmap;
+        F.hec_rounds = rounds;
+        Level Cl;
+        SGPB_TRY(build_coarse_level(C, F, vcmap, nc, out_wbytes, &Cl));
+        levels.push_back(Cl);
+        if (levels.size() > 200) break;
+    }
+    if (levels.size() > 1 && levels.back().n < 10) {
+        levels.pop_back();
+        levels.back().vcmap = nullptr;
+    }
+    return SGP_B200_OK;
+}
+
+__global__ void k_normalize_guess(double *x, uint32_t n) {
+    // single block: x /= |x| (eigensolve_kokkos.h:1505)
+    __shared__ double sm[64];
+    double s[1] = {0};
+    for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) s[0] += x[i] * x[i];
+    block_sum_d<1>(s, sm);
+    if (threadIdx.x == 0) sm[40] = 1.0 / sqrt(s[0]);
+    __syncthreads();
+    double inv = sm[40];
+    for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) x[i] *= inv;
+}
+
+// eigensolve_kokkos.h:1493-1595 without FM: coarsest guess, power iteration
+// per level, prolongation, final level.
+static int eigensolve(Context &C, std::vector<Level> &levels, uint64_t *rng_state, uint64_t rng_inc,
+                      const PowerIterOpts &o, double **evec_out, PowerIterResult *finest) {
+    const int L = (int)levels.size();
+    const uint32_t gn = levels[L - 1].n;
+    std::vector<double> guess(gn);
+    for (uint32_t i = 0; i < gn; i++) guess[i] = ((double)pcg32(rng_state, rng_inc)) / 4294967295.0;
+    double *x;
+    SGPB_TRY(dalloc_t(C, &x, gn));
+    SGPB_CUDA(cudaMemcpyAsync(x, guess.data(), sizeof(double) * gn, cudaMemcpyHostToDevice, C.stream));
+    SGPB_CUDA(cudaStreamSynchronize(C.stream));   // guess lives on the host stack
+    k_normalize_guess<<<1, 256, 0, C.stream>>>(x, gn);
+    C.kernel_launches++;
+    const double *xin = x;
+    for (int l = L - 1; l >= 0; l--) {
+        Level &lv = levels[l];
+        double *xo;
+        SGPB_TRY(dalloc_t(C, &xo, lv.n));
+        PowerIterResult r;
+        const uint32_t *vc = (l == L - 1) ? nullptr : lv.vcmap;
+        SGPB_TRY(power_iter_level(C, lv, xin, vc, xo, o, &r, l == 0));
+        lv.pi_iters = r.niter;
+        lv.pi_ms = r.kernel_ms;
+        lv.pi_capped = r.capped;
+        lv.pi_dot = r.dot;
+        lv.pi_lambda = r.lambda;
+        if (l == 0) *finest = r;
+        xin = xo;
+    }
+    *evec_out = (double *)xin;
+    return SGP_B200_OK;
+}
+
+static float ev_ms(cudaEvent_t a, cudaEvent_t b) {
+    float ms = 0;
+    cudaEventElapsedTime(&ms, a, b);
+    return ms;
+}
+
+static int partition_impl(Context &C, const sgp_b200_graph_t *g, const sgp_b200_options_t *opt,
+                          sgp_b200_result_t *res) {
+    cudaEvent_t ev[6];
+    for (auto &e : ev) SGPB_CUDA(cudaEventCreate(&e));
+    struct EvGuard {
+        cudaEvent_t *e;
+        ~EvGuard() { for (int i = 0; i < 6; i++) cudaEventDestroy(e[i]); }
+    } guard{ev};
+    C.kernel_launches = 0;
+    SGPB_CUDA(cudaEventRecord(ev[0], C.stream));
+    Level L0;
+    SGPB_TRY(stage_input(C, g, &L0));
+    SGPB_CUDA(cudaEventRecord(ev[1], C.stream));
+    uint64_t st = opt->rng_state;
+    std::vector<Level> levels;
+    SGPB_TRY(generate(C, L0, opt->cutoff, &st, opt->rng_inc, levels));
+    SGPB_CUDA(cudaEventRecord(ev[2], C.stream));
+    PowerIterOpts po;
+    po.tol = opt->tol;
+    po.iter_cap = opt->iter_cap;
+    po.mixed = opt->mixed;
+    double *evec = nullptr;
+    PowerIterResult fin;
+    SGPB_TRY(eigensolve(C, levels, &st, opt->rng_inc, po, &evec, &fin));
+    SGPB_CUDA(cudaEventRecord(ev[3], C.stream));
+    uint32_t *part_d = (opt->part_mem == SGP_B200_DEVICE) ? res->part : nullptr;
+    if (!part_d) SGPB_TRY(dalloc_t(C, &part_d, g->n));
+    uint64_t cut = 0;
+    uint32_t p0 = 0;
+    SGPB_TRY(split_level(C, levels[0], evec, opt->perc_imbalance, part_d, &cut, &p0));
+    SGPB_CUDA(cudaEventRecord(ev[4], C.stream));
+    if (opt->part_mem != SGP_B200_DEVICE)
+        SGPB_CUDA(cudaMemcpyAsync(res->part, part_d, sizeof(uint32_t) * g->n, cudaMemcpyDeviceToHost, C.stream));
+    SGPB_CUDA(cudaEventRecord(ev[5], C.stream));
+    SGPB_CUDA(cudaStreamSynchronize(C.stream));
+    res->edgecut = cut;
+    res->part0_size = p0;
+    res->lambda = fin.lambda;
+    res->residual = fin.resid;
+    res->levels = (int)levels.size();
+    res->iter_max_reached = 0;
+    for (size_t l = 0; l < levels.size() && l < SGP_B200_MAX_LEVELS; l++) {
+        res->level_n[l] = levels[l].n;
+        res->level_m[l] = levels[l].m;
+        res->level_iters[l] = levels[l].pi_iters;
+        res->level_hec_rounds[l] = levels[l].hec_rounds;
+        res->level_pi_ms[l] = levels[l].pi_ms;
+        res->iter_max_reached |= levels[l].pi_capped;
+    }
+    res->rng_state = st;
+    res->ms_h2d = ev_ms(ev[0], ev[1]);
+    res->ms_coarsen = ev_ms(ev[1], ev[2]);
+    res->ms_eigen = ev_ms(ev[2], ev[3]);
+    res->ms_split = ev_ms(ev[3], ev[4]);
+    res->ms_d2h = ev_ms(ev[4], ev[5]);
+    res->ms_total = ev_ms(ev[0], ev[5]);
+    res->kernel_launches = C.kernel_launches;
+    C.t_total = res->ms_total; C.t_coarsen = res->ms_coarsen; C.t_eigen = res->ms_eigen; C.t_split = res->ms_split;
+    return SGP_B200_OK;
+}
+
+// thread-local default context for the part-1 (sgpar.h) entry points
+static thread_local sgp_b200_ctx_t *g_default = nullptr;
+static Context *default_ctx() {
+    if (!g_default) {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        g_default = sgp_b200_create(dev);
+    }
+    return g_default ? ctx_get(g_default) : nullptr;
+}
+
+static sgp_real_t g_tol = 1e-10;   // sgpar.h:139 SGPAR_POWERITER_TOL
+
+}  // namespace sgpb
+
+using namespace sgpb;
+
+extern "C" {
+
+int change_tol(sgp_real_t new_tol) {
+    g_tol = new_tol;
+    return 0;
+}
+
+void sgp_b200_default_options(sgp_b200_options_t *o) {
+    memset(o, 0, sizeof(*o));
+    o->cutoff = 50;
+    o->tol = g_tol;
+    o->mixed = 0;
+    o->perc_imbalance = 0;
+    o->iter_cap = 0;
+    o->rng_state = 0x853c49e6748fea9bULL;
+    o->rng_inc = 1;
+    o->part_mem = SGP_B200_HOST;
+}
+
+int sgp_b200_partition(sgp_b200_ctx_t *x, const sgp_b200_graph_t *g, const sgp_b200_options_t *opt,
+                       sgp_b200_result_t *res) {
+    Context *C = ctx_get(x);
+    if (!C || !g || !opt || !res || !res->part) {
+        set_error("null argument");
+        return SGP_B200_ERR_INVALID;
+    }
+    cudaSetDevice(C->device);
+    int rc = partition_impl(*C, g, opt, res);
+    release_all(*C);
+    return rc;
+}
+
+int sgp_b200_last_timing(sgp_b200_ctx_t *x, float *t, float *c, float *e, float *s) {
+    Context *C = ctx_get(x);
+    if (!C) return SGP_B200_ERR_INVALID;
+    if (t) *t = C->t_total;
+    if (c) *c = C->t_coarsen;
+    if (e) *e = C->t_eigen;
+    if (s) *s = C->t_split;
+    return 0;
+}
+
+// ---------------------------------------------------------- hierarchy --
+int sgp_b200_generate_coarse_graphs(sgp_b200_ctx_t *x, const sgp_b200_graph_t *g, uint32_t cutoff,
+                                    sgp_pcg32_random_t *rng, sgp_b200_hierarchy_t **out) {
+    Context *C = ctx_get(x);
+    if (!C || !g || !rng || !out) {
+        set_error("null argument");
+        return SGP_B200_ERR_INVALID;
+    }
+    cudaSetDevice(C->device);
+    Level L0;
+    int rc = stage_input(*C, g, &L0);
+    std::vector<Level> levels;
+    if (rc == SGP_B200_OK) rc = generate(*C, L0, cutoff, &rng->state, rng->inc, levels);
+    if (rc != SGP_B200_OK) {
+        release_all(*C);
+        return rc;
+    }
+    cudaStreamSynchronize(C->stream);
+    sgp_b200_hierarchy_t *h = new sgp_b200_hierarchy_t();
+    h->C = C;
+    h->levels = levels;
+    h->owned.swap(C->owned);
+    *out = h;
+    return SGP_B200_OK;
+}
+
+int sgp_b200_hierarchy_levels(const sgp_b200_hierarchy_t *h) { return h ? (int)h->levels.size() : 0; }
+
+int sgp_b200_hierarchy_level(const sgp_b200_hierarchy_t *h, int l, uint32_t *n, uint64_t *m, const uint32_t **rp,
+                             const uint32_t **col, const void **w, int *wbytes, const uint32_t **vcmap) {
+    if (!h || l < 0 || l >= (int)h->levels.size()) {
+        set_error("level index out of range");
+        return SGP_B200_ERR_INVALID;
+    }
+    const Level &L = h->levels[l];
+    if (n) *n = L.n;
+    if (m) *m = L.m;
+    if (rp) *rp = L.rp;
+    if (col) *col = L.col;
+    if (w) *w = L.w;
+    if (wbytes) *wbytes = L.wbytes;
+    if (vcmap) *vcmap = L.vcmap;
+    return SGP_B200_OK;
+}
+
+int sgp_b200_eigensolve(sgp_b200_ctx_t *x, sgp_b200_hierarchy_t *h, sgp_pcg32_random_t *rng, double tol, int mixed,
+                        uint64_t iter_cap, double *eigenvec, int mem, sgp_b200_result_t *stats) {
+    Context *C = ctx_get(x);
+    if (!C || !h || !rng || !eigenvec) {
+        set_error("null argument");
+        return SGP_B200_ERR_INVALID;
+    }
+    cudaSetDevice(C->device);
+    PowerIterOpts o;
+    o.tol = tol;
+    o.mixed = mixed;
+    o.iter_cap = iter_cap;
+    double *ev = nullptr;
+    PowerIterResult fin;
+    int rc = eigensolve(*C, h->levels, &rng->state, rng->inc, o, &ev, &fin);
+    if (rc == SGP_B200_OK) {
+        cudaError_t e = cudaMemcpyAsync(eigenvec, ev, sizeof(double) * h->levels[0].n,
+                                        mem == SGP_B200_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost,
+                                        C->stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(C->stream);
+        if (e != cudaSuccess) {
+            set_error("eigenvector copy failed: %s", cudaGetErrorString(e));
+            rc = SGP_B200_ERR_DEVICE;
+        }
+    }
+    if (rc == SGP_B200_OK && stats) {
+        stats->lambda = fin.lambda;
+        stats->residual = fin.resid;
+        stats->levels = (int)h->levels.size();
+        for (size_t l = 0; l < h->levels.size() && l < SGP_B200_MAX_LEVELS; l++) {
+            stats->level_n[l] = h->levels[l].n;
+            stats->level_m[l] = h->levels[l].m;
+            stats->level_iters[l] = h->levels[l].pi_iters;
+            stats->level_pi_ms[l] = h->levels[l].pi_ms;
+        }
+    }
+    release_all(*C);
+    return rc;
+}
+
+void sgp_b200_hierarchy_free(sgp_b200_hierarchy_t *h) {
+    if (!h) return;
+    cudaSetDevice(h->C->device);
+    for (void *p : h->owned) cudaFreeAsync(p, h->C->stream);
+    cudaStreamSynchronize(h->C->stream);
+    delete h;
+}
+
+// ------------------------------------------------------ kernel entries --
+int sgp_b200_hec(sgp_b200_ctx_t *x, uint32_t n, const uint32_t *rp, const uint32_t *col, const void *w, int wbytes,
+                 int random_level, uint64_t seed, uint32_t *hn, uint32_t *vcmap, uint32_t *nc, int *rounds) {
+    Context *C = ctx_get(x);
+    if (!C || !rp || !vcmap || !nc) { set_error("null argument"); return SGP_B200_ERR_INVALID; }
+    if (wbytes != 0 && wbytes != 4 && wbytes != 8) { set_error("wbytes must be 0, 4 or 8"); return SGP_B200_ERR_INVALID; }
+    cudaSetDevice(C->device);
+    Level L;
+    L.n = n; L.rp = (uint32_t *)rp; L.col = (uint32_t *)col; L.w = (void *)(wbytes ? w : nullptr);
+    L.wbytes = wbytes ? wbytes : 0;
+    uint32_t mm = 0;
+    int rc = n ? read_u32(*C, rp + n, &mm) : 0;
+    L.m = mm;
+    int r = 0;
+    if (rc == SGP_B200_OK) rc = hec_map_level(*C, L, random_level, seed, vcmap, hn, nc, &r);
+    if (rounds) *rounds = r;
+    cudaStreamSynchronize(C->stream);
+    release_all(*C);
+    return rc;
+}
+
+int sgp_b200_build_coarse(sgp_b200_ctx_t *x, uint32_t n, const uint32_t *rp, const uint32_t *col, const void *w,
+                          int wbytes, const uint32_t *vcmap, uint32_t nc, int out_wbytes, uint32_t *crp,
+                          uint32_t *ccol, void *cw, uint64_t *m_c) {
+    Context *C = ctx_get(x);
+    if (!C || !rp || !vcmap || !crp || !ccol || !cw || !m_c) { set_error("null argument"); return SGP_B200_ERR_INVALID; }
+    if ((wbytes != 0 && wbytes != 4 && wbytes != 8) || (out_wbytes != 4 && out_wbytes != 8)) {
+        set_error("weight widths must be 0/4/8 in and 4/8 out");
+        return SGP_B200_ERR_INVALID;
+    }
+    cudaSetDevice(C->device);
+    Level L;
+    L.n = n; L.rp = (uint32_t *)rp; L.col = (uint32_t *)col; L.w = (void *)(wbytes ? w : nullptr); L.wbytes = wbytes;
+    uint32_t mm = 0;
+    int rc = n ? read_u32(*C, rp + n, &mm) : 0;
+    L.m = mm;
+    if (rc == SGP_B200_OK) rc = build_coarse_into(*C, L, vcmap, nc, out_wbytes, crp, ccol, cw, m_c);
+    cudaStreamSynchronize(C->stream);
+    release_all(*C);
+    return rc;
+}
+
+int sgp_b200_power_iter(sgp_b200_ctx_t *x, uint32_t n, const uint32_t *rp, const uint32_t *col, const void *w,
+                        int wbytes, const double *x_in, const uint32_t *vcmap, double *x_out, double tol,
+                        uint64_t iter_cap, int mixed, uint64_t *niter, double *lambda, double *residual) {
+    Context *C = ctx_get(x);
+    if (!C || !rp || !x_in || !x_out) { set_error("null argument"); return SGP_B200_ERR_INVALID; }
+    if (wbytes != 0 && wbytes != 4 && wbytes != 8) { set_error("wbytes must be 0, 4 or 8"); return SGP_B200_ERR_INVALID; }
+    cudaSetDevice(C->device);
+    Level L;
+    L.n = n; L.rp = (uint32_t *)rp; L.col = (uint32_t *)col; L.w = (void *)(wbytes ? w : nullptr); L.wbytes = wbytes;
+    uint32_t mm = 0;
+    int rc = n ? read_u32(*C, rp + n, &mm) : 0;
+    L.m = mm;
+    PowerIterOpts o;
+    o.tol = tol;
+    o.iter_cap = iter_cap;
+    o.mixed = mixed;
+    PowerIterResult r;
+    if (rc == SGP_B200_OK) rc = power_iter_level(*C, L, x_in, vcmap, x_out, o, &r, residual != nullptr);
+    if (rc == SGP_B200_OK) {
+        if (niter) *niter = r.niter;
+        if (lambda) *lambda = r.lambda;
+        if (residual) *residual = r.resid;
+    }
+    cudaStreamSynchronize(C->stream);
+    release_all(*C);
+    return rc;
+}
+
+int sgp_b200_split(sgp_b200_ctx_t *x, uint32_t n, const uint32_t *rp, const uint32_t *col, const double *evec,
+                   int perc_imbalance, uint32_t *part, uint64_t *edgecut) {
+    Context *C = ctx_get(x);
+    if (!C || !rp || !evec || !part || !edgecut) { set_error("null argument"); return SGP_B200_ERR_INVALID; }
+    cudaSetDevice(C->device);
+    Level L;
+    L.n = n; L.rp = (uint32_t *)rp; L.col = (uint32_t *)col;
+    int rc = split_level(*C, L, evec, perc_imbalance, part, edgecut, nullptr);
+    cudaStreamSynchronize(C->stream);
+    release_all(*C);
+    return rc;
+}
+
+// ------------------------------------------------------ sgpar.h API --
+int sgp_partition_graph(sgp_vid_t *part, sgp_eid_t *edge_cut, config_t *config, const int perc_imbalance_allowed,
+                        const sgp_graph_t g, sgp_pcg32_random_t *rng) {
+    if (!part || !edge_cut || !config || !rng) {
+        set_error("null argument");
+        return 1;
+    }
+    if (config->refine_alg != 0 || config->local_search_alg != 0) {
+        set_error("only refine_alg 0 (shifted combinatorial Laplacian) and local_search_alg 0 are on this path");
+        return 1;
+    }
+    Context *C = default_ctx();
+    if (!C) return 1;
+    sgp_b200_graph_t dg;
+    dg.n = g.nvertices;
+    dg.m = g.source_offsets ? g.source_offsets[g.nvertices] : 0;
+    dg.row_ptr = g.source_offsets;
+    dg.col = g.destination_indices;
+    dg.w = g.eweights;
+    dg.mem = SGP_B200_HOST;
+    sgp_b200_options_t o;
+    sgp_b200_default_options(&o);
+    o.tol = config->tol > 0 ? config->tol : g_tol;
+    o.perc_imbalance = perc_imbalance_allowed;
+    o.rng_state = rng->state;
+    o.rng_inc = rng->inc;
+    sgp_b200_result_t *r = (sgp_b200_result_t *)calloc(1, sizeof(sgp_b200_result_t));
+    if (!r) return 1;
+    r->part = part;
+    int rc = sgp_b200_partition(g_default, &dg, &o, r);
+    if (rc == SGP_B200_OK) {
+        *edge_cut = (sgp_eid_t)r->edgecut;
+        rng->state = r->rng_state;
+    }
+    free(r);
+    return rc == SGP_B200_OK ? 0 : 1;
+}
+
+int sgp_compute_partition(sgp_vid_t *part, sgp_vid_t num_partitions, sgp_eid_t *edgecut, int perc_imbalance_allowed,
+                          int local_search_alg, sgp_real_t *evec, sgp_graph_t g) {
+    if (num_partitions != 2 && num_partitions != 4) { set_error("num_partitions must be 2 or 4"); return 1; }
+    if (local_search_alg != 0) { set_error("local_search_alg must be 0"); return 1; }
+    Context *C = default_ctx();
+    if (!C || !part || !edgecut || !evec) return 1;
+    cudaSetDevice(C->device);
+    sgp_b200_graph_t dg;
+    dg.n = g.nvertices;
+    dg.m = g.source_offsets[g.nvertices];
+    dg.row_ptr = g.source_offsets;
+    dg.col = g.destination_indices;
+    dg.w = nullptr;
+    dg.mem = SGP_B200_HOST;
+    Level L0;
+    int rc = stage_input(*C, &dg, &L0);
+    double *ev = nullptr;
+    uint32_t *pd = nullptr;
+    if (rc == SGP_B200_OK) rc = dalloc_t(*C, &ev, g.nvertices);
+    if (rc == SGP_B200_OK) rc = dalloc_t(*C, &pd, g.nvertices);
+    if (rc == SGP_B200_OK &&
+        cudaMemcpyAsync(ev, evec, sizeof(double) * g.nvertices, cudaMemcpyHostToDevice, C->stream) != cudaSuccess)
+        rc = SGP_B200_ERR_DEVICE;
+    uint64_t cut = 0;
+    if (rc == SGP_B200_OK) rc = split_level(*C, L0, ev, perc_imbalance_allowed, pd, &cut, nullptr);
+    if (rc == SGP_B200_OK &&
+        cudaMemcpyAsync(part, pd, sizeof(uint32_t) * g.nvertices, cudaMemcpyDeviceToHost, C->stream) != cudaSuccess)
+        rc = SGP_B200_ERR_DEVICE;
+    cudaStreamSynchronize(C->stream);
+    release_all(*C);
+    if (rc == SGP_B200_OK) *edgecut = (sgp_eid_t)cut;
+    return rc == SGP_B200_OK ? 0 : 1;
+}
+
+int sgp_use_partition(sgp_vid_t *part, const sgp_graph_t g, sgp_graph_t *g1, sgp_graph_t *g2) {
+    Context *C = default_ctx();
+    if (!C || !part || !g1 || !g2) return 1;
+    cudaSetDevice(C->device);
+    sgp_b200_graph_t dg;
+    dg.n = g.nvertices;
+    dg.m = g.source_offsets[g.nvertices];
+    dg.row_ptr = g.source_offsets;
+    dg.col = g.destination_indices;
+    dg.w = nullptr;
+    dg.mem = SGP_B200_HOST;
+    Level L0, a, b;
+    uint32_t *pd = nullptr;
+    int rc = stage_input(*C, &dg, &L0);
+    if (rc == SGP_B200_OK) rc = dalloc_t(*C, &pd, g.nvertices);
+    if (rc == SGP_B200_OK &&
+        cudaMemcpyAsync(pd, part, sizeof(uint32_t) * g.nvertices, cudaMemcpyHostToDevice, C->stream) != cudaSuccess)
+        rc = SGP_B200_ERR_DEVICE;
+    if (rc == SGP_B200_OK) rc = induced_subgraphs(*C, L0, pd, &a, &b);
+    sgp_graph_t *outs[2] = {g1, g2};
+    Level *ls[2] = {&a, &b};
+    for (int k = 0; k < 2 && rc == SGP_B200_OK; k++) {
+        sgp_graph_t *o = outs[k];
+        memset(o, 0, sizeof(*o));
+        o->nvertices = ls[k]->n;
+        o->nedges = (sgp_eid_t)ls[k]->m;   // the reference stores the directed count here (sgpar.h:2735)
+        o->source_offsets = (sgp_eid_t *)malloc(sizeof(sgp_eid_t) * ((size_t)ls[k]->n + 1));
+        o->destination_indices = (sgp_vid_t *)malloc(sizeof(sgp_vid_t) * (ls[k]->m ? ls[k]->m : 1));
+        if (!o->source_offsets || !o->destination_indices) { rc = 1; break; }
+        if (cudaMemcpyAsync(o->source_offsets, ls[k]->rp, sizeof(uint32_t) * ((size_t)ls[k]->n + 1),
+                            cudaMemcpyDeviceToHost, C->stream) != cudaSuccess ||
+            cudaMemcpyAsync(o->destination_indices, ls[k]->col, sizeof(uint32_t) * ls[k]->m, cudaMemcpyDeviceToHost,
+                            C->stream) != cudaSuccess)
+            rc = SGP_B200_ERR_DEVICE;
+    }
+    cudaStreamSynchronize(C->stream);
+    release_all(*C);
+    return rc == SGP_B200_OK ? 0 : 1;
+}
+
+}  // extern "C"

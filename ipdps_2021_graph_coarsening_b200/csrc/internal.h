@@ -1,0 +1,123 @@
+// internal.h -- host-side plumbing shared by the .cu files of libsgpar_b200.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <stdio.h>
+#include <string>
+#include <vector>
+
+#include "../../include/sgpar_b200.h"
+
+namespace sgpb {
+
+// Error status carried out of the C ABI (sgp_b200_last_error()).
+void set_error(const char *fmt, ...);
+const char *last_error();
+
+struct Status {
+    int code = SGP_B200_OK;
+    bool ok() const { return code == SGP_B200_OK; }
+};
+
+#define SGPB_CUDA(call)                                                                        \
+    do {                                                                                       \
+        cudaError_t e_ = (call);                                                               \
+        if (e_ != cudaSuccess) {                                                               \
+            ::sgpb::set_error("CUDA error %s at %s:%d: %s", cudaGetErrorName(e_), __FILE__,     \
+                              __LINE__, cudaGetErrorString(e_));                               \
+            return SGP_B200_ERR_DEVICE;                                                        \
+        }                                                                                      \
+    } while (0)
+
+#define SGPB_TRY(call)                                                                         \
+    do {                                                                                       \
+        int s_ = (call);                                                                       \
+        if (s_ != SGP_B200_OK) return s_;                                                      \
+    } while (0)
+
+// Stream-ordered device allocations from the device's memory pool; the pool
+// keeps freed memory cached so repeated partitions reuse it.
+struct DevBuf {
+    void *p = nullptr;
+    size_t bytes = 0;
+};
+
+struct Context {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    int num_sms = 0;
+    size_t smem_optin = 0;
+    uint64_t *h_pinned = nullptr;   // small pinned staging area for scalar read-backs
+    std::vector<void *> owned;      // allocations released at the end of a call
+    // timing of the last partition (ms, CUDA events)
+    float t_total = 0, t_coarsen = 0, t_eigen = 0, t_split = 0, t_h2d = 0, t_d2h = 0;
+    uint32_t kernel_launches = 0;
+};
+
+Context *ctx_get(sgp_b200_ctx_t *c);
+
+int dalloc(Context &C, void **p, size_t bytes);          // tracked, freed by release_all
+template <typename T>
+int dalloc_t(Context &C, T **p, size_t count) { return dalloc(C, (void **)p, count * sizeof(T)); }
+int dzero(Context &C, void *p, size_t bytes);
+void release_all(Context &C);
+
+// device-wide exclusive scan of n uint32 counts into uint32 offsets[n+1]
+// (out[n] = total).  Returns SGP_B200_ERR_TOO_LARGE when the total does not
+// fit in 32 bits (flag checked on read-back by the caller).
+int scan_u32(Context &C, const uint32_t *in, uint32_t *out, uint32_t n, uint32_t *d_overflow);
+// stable compaction of indices i in [0, n) with flag(i) != 0 (flags as uint8).
+int compact_flags(Context &C, const uint8_t *flags, uint32_t n, uint32_t *out_idx, uint32_t *d_count);
+
+// read a few device scalars (synchronises the stream)
+int read_u32(Context &C, const uint32_t *d, uint32_t *h, int count = 1);
+int read_u64(Context &C, const uint64_t *d, uint64_t *h, int count = 1);
+
+inline uint32_t cdiv(uint64_t a, uint64_t b) { return (uint32_t)((a + b - 1) / b); }
+
+// --------------------------------------------------------------- levels --
+// One level of the hierarchy on the device.  wbytes: 0 = unit weights,
+// 4 = uint32, 8 = uint64.
+struct Level {
+    uint32_t n = 0;
+    uint64_t m = 0;              // directed entries
+    uint32_t *rp = nullptr;
+    uint32_t *col = nullptr;
+    void *w = nullptr;
+    int wbytes = 0;
+    uint32_t *vcmap = nullptr;   // this level -> next coarser level
+    uint32_t max_deg = 0;
+    uint32_t seed_hi = 0, seed_lo = 0;
+    int hec_rounds = 0;
+    uint64_t pi_iters = 0;
+    float pi_ms = 0;
+    int pi_capped = 0;
+    double pi_dot = 0, pi_lambda = 0;
+};
+
+// kernels (implemented in hec.cu / build.cu / eigen.cu / split.cu)
+int hec_map_level(Context &C, const Level &L, int random_level, uint64_t seed, uint32_t *vcmap,
+                  uint32_t *hn_out, uint32_t *nc_out, int *rounds_out);
+int build_coarse_level(Context &C, const Level &F, const uint32_t *vcmap, uint32_t nc, int out_wbytes,
+                       Level *out);
+struct PowerIterOpts {
+    double tol = 1e-10;
+    uint64_t iter_cap = 0;   // 0: the reference's 1e14 / n only
+    int mixed = 0;           // 1: float vector storage / gathers, fp64 reductions
+};
+struct PowerIterResult {
+    uint64_t niter = 0;
+    int capped = 0;
+    double dot = 0, gb = 0, lambda = 0, resid = 0;
+    float kernel_ms = 0;     // cooperative-kernel time (CUDA events)
+};
+// x_in: coarse vector (prolongated through vcmap when vcmap != null) or the
+// initial vector; x_out: n doubles (may alias nothing).
+int power_iter_level(Context &C, const Level &L, const double *x_in, const uint32_t *vcmap,
+                     double *x_out, const PowerIterOpts &o, PowerIterResult *res, int want_residual);
+int split_level(Context &C, const Level &L, const double *evec, int perc_imbalance, uint32_t *part,
+                uint64_t *edgecut, uint32_t *n_part0);
+int edge_cut_device(Context &C, const Level &L, const uint32_t *part, uint64_t *edgecut);
+int induced_subgraphs(Context &C, const Level &L, const uint32_t *part, Level *g1, Level *g2);
+
+}  // namespace sgpb

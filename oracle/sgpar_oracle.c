@@ -1,0 +1,525 @@
+/*
+ * sgpar_oracle.c -- CPU restatement of cmg's multilevel spectral bisection path.
+ *
+ * TEST INFRASTRUCTURE ONLY.  This file is the checker for the CUDA path: only
+ * tests/, __graft_entry__.smoke() and bench.py's cpu_baseline leg may load it.
+ * The shipped library never links or calls it.
+ *
+ * What it restates (reference files under cmg/ of IPDPS_2021_Graph_Coarsening):
+ *   - PCG32 (sgpar.h:82-92)
+ *   - heavy-neighbour choice of HEC (heuristics.h:959-998; serial form
+ *     sgpar.h:647-695), with the deterministic tie-break this project defines
+ *   - HEC map construction rounds (heuristics.h:633-693), made deterministic:
+ *     claims are resolved by a max-key rule instead of compare-and-swap races
+ *   - coarse-graph construction P^T A P minus self loops with integer weight
+ *     sums and rows sorted by destination (coarsen_kokkos.h:1061-1127,
+ *     799-900 and the RADIX dedupe 750-762 / 491-509)
+ *   - shifted-Laplacian power iteration deflated against the constant vector,
+ *     in the serial reference's exact floating-point operation order
+ *     (sgpar.h:1790-1948, vector kernels sgpar.h:1687-1730)
+ *   - median split + one-vertex sweep + edge cut (sgpar.h:1969-2071)
+ *   - induced sub-graphs for 4-way recursion (sgpar.h:2666-2752)
+ *   - the level loop of sgp_generate_coarse_graphs (coarsen_kokkos.h:1165-1234)
+ *     and sgp_eigensolve (eigensolve_kokkos.h:1493-1595)
+ *
+ * Parity pins: the power iteration, the split and the coarse build are checked
+ * against the reference's own serial build compiled from its sources
+ * (oracle/ref_harness.cpp); the dedupe is checked against the reference's
+ * known-answer test (tests.cpp:7-56).
+ */
+#include <stdint.h>
+#include <stdlib.h>
+#include <string.h>
+#include <math.h>
+
+#define ORC_UNASSIGNED 0xFFFFFFFFu
+
+/* ---------------------------------------------------------------- PCG32 -- */
+/* sgpar.h:84-92: 64-bit LCG state, XSH-RR output permutation. */
+uint32_t orc_pcg32(uint64_t *state, uint64_t inc) {
+    uint64_t old = *state;
+    *state = old * 6364136223846793005ULL + (inc | 1);
+    uint32_t xs = (uint32_t)(((old >> 18u) ^ old) >> 27u);
+    uint32_t rot = (uint32_t)(old >> 59u);
+    return (xs >> rot) | (xs << ((-rot) & 31));
+}
+
+/* ------------------------------------------------------- seeded hashes -- */
+/* The reference draws vertex priorities from a time-seeded XorShift pool
+ * (heuristics.h:614-631, :947).  This project replaces that by counter-based
+ * hashes of (level seed, vertex) so that the mapping is reproducible.  The same
+ * three formulas are used by the CUDA kernels. */
+static inline uint64_t orc_mix64(uint64_t z) {
+    z = (z ^ (z >> 30)) * 0xbf58476d1ce4e5b9ULL;
+    z = (z ^ (z >> 27)) * 0x94d049bb133111ebULL;
+    return z ^ (z >> 31);
+}
+/* 63-bit priority key: 31 hash bits above the 32-bit vertex id (unique). */
+static inline uint64_t orc_prio_key(uint64_t seed, uint32_t u) {
+    uint64_t h = orc_mix64(seed ^ (0x9E3779B97F4A7C15ULL * ((uint64_t)u + 1)));
+    return ((h >> 33) << 32) | (uint64_t)u;
+}
+/* random draw for the level-1 random neighbour and isolated vertices */
+static inline uint64_t orc_rand_draw(uint64_t seed, uint32_t u) {
+    return orc_mix64(seed ^ 0x632BE59BD9B4E019ULL ^ (0x9E3779B97F4A7C15ULL * ((uint64_t)u + 1)));
+}
+/* tie-break among equally heavy edges (u -> v) */
+static inline uint32_t orc_tiebreak(uint64_t seed, uint32_t u, uint32_t v) {
+    return (uint32_t)(orc_mix64(seed ^ 0xD1B54A32D192ED03ULL ^ (((uint64_t)u << 32) | v)) >> 32);
+}
+
+uint64_t orc_hash_prio_key(uint64_t seed, uint32_t u) { return orc_prio_key(seed, u); }
+uint64_t orc_hash_rand_draw(uint64_t seed, uint32_t u) { return orc_rand_draw(seed, u); }
+uint32_t orc_hash_tiebreak(uint64_t seed, uint32_t u, uint32_t v) { return orc_tiebreak(seed, u, v); }
+
+/* ------------------------------------------------------ heavy neighbour -- */
+/* heuristics.h:959-998.  Level 1 of an unweighted input picks a random
+ * neighbour (all weights are 1 there, heuristics.h:959-972); otherwise the
+ * neighbour of maximum weight, ties broken by (tiebreak hash, destination).
+ * A vertex with no edges is paired with a random vertex (urand % n, :967-970).
+ * w64 == NULL means unit weights. */
+void orc_hec_heavy(uint32_t n, const uint32_t *row_ptr, const uint32_t *col,
+                   const uint64_t *w64, int random_level, uint64_t seed,
+                   uint32_t *hn) {
+    for (uint32_t u = 0; u < n; u++) {
+        uint32_t b = row_ptr[u], e = row_ptr[u + 1];
+        uint32_t deg = e - b;
+        if (deg == 0) {
+            hn[u] = (uint32_t)(orc_rand_draw(seed, u) % n);
+            continue;
+        }
+        if (random_level) {
+            hn[u] = col[b + (uint32_t)(orc_rand_draw(seed, u) % deg)];
+            continue;
+        }
+        uint64_t bw = 0; uint32_t bt = 0, bv = 0; int have = 0;
+        for (uint32_t j = b; j < e; j++) {
+            uint64_t w = w64 ? w64[j] : 1;
+            uint32_t v = col[j];
+            uint32_t t = orc_tiebreak(seed, u, v);
+            if (!have || w > bw || (w == bw && (t > bt || (t == bt && v > bv)))) {
+                bw = w; bt = t; bv = v; have = 1;
+            }
+        }
+        hn[u] = bv;
+    }
+}
+
+/* ----------------------------------------------------- map construction -- */
+/* heuristics.h:633-693 (parallel_map_construct), restated deterministically.
+ *
+ * Each round looks at the still-unassigned vertices u with v = hn[u]:
+ *   - v already assigned in an earlier round: u joins v's aggregate
+ *     (heuristics.h:664-666) and shields its own slot from claims;
+ *   - v == u: u becomes a singleton aggregate (the u == v case at :656);
+ *   - (prio(u) < prio(v)) xor swap (the ordering condition of :653-654):
+ *     u claims both slots u and v with key(u)+1 (atomic max on the GPU);
+ *     u wins when it holds both slots, and u, v form a new aggregate
+ *     (the double compare-and-swap of :655-661).
+ * swap flips every round (:684).  Aggregates are labelled by their root vertex
+ * during the rounds and numbered by ascending root id at the end, so the
+ * coarse numbering does not depend on thread timing (the reference uses an
+ * atomic counter, :657).
+ * Returns the number of rounds; nc receives the coarse vertex count. */
+int orc_hec_map(uint32_t n, const uint32_t *hn, uint64_t seed,
+                uint32_t *vcmap, uint32_t *nc_out) {
+    const uint64_t JOIN_KEY = ~0ULL, SELF_KEY = ~0ULL - 1;
+    uint64_t *claim[2];
+    claim[0] = (uint64_t *)calloc(n ? n : 1, sizeof(uint64_t));
+    claim[1] = (uint64_t *)calloc(n ? n : 1, sizeof(uint64_t));
+    uint8_t *act = (uint8_t *)malloc(n ? n : 1);
+    uint32_t *list = (uint32_t *)malloc((n ? n : 1) * sizeof(uint32_t));
+    uint32_t *next = (uint32_t *)malloc((n ? n : 1) * sizeof(uint32_t));
+    for (uint32_t u = 0; u < n; u++) { vcmap[u] = ORC_UNASSIGNED; list[u] = u; }
+    uint32_t len = n;
+    int swap = 1, round = 0;
+    while (1) {
+        uint64_t *cl = claim[round & 1], *other = claim[(round + 1) & 1];
+        /* phase A: compact the survivors, classify, claim */
+        uint32_t nlen = 0;
+        for (uint32_t i = 0; i < len; i++) {
+            uint32_t u = list[i];
+            if (vcmap[u] != ORC_UNASSIGNED) continue;
+            next[nlen++] = u;
+            uint32_t v = hn[u];
+            if (vcmap[v] != ORC_UNASSIGNED) {
+                act[u] = 1; if (cl[u] < JOIN_KEY) cl[u] = JOIN_KEY;
+            } else if (v == u) {
+                act[u] = 2; if (cl[u] < SELF_KEY) cl[u] = SELF_KEY;
+            } else {
+                uint64_t ku = orc_prio_key(seed, u), kv = orc_prio_key(seed, v);
+                int cond = ku < kv;
+                if (cond ^ swap) {
+                    act[u] = 3;
+                    uint64_t k = ku + 1;
+                    if (cl[u] < k) cl[u] = k;
+                    if (cl[v] < k) cl[v] = k;
+                } else {
+                    act[u] = 0;
+                }
+            }
+        }
+        if (nlen == 0) break;
+        /* phase B: resolve (reads the phase-A state only: joins read vcmap of
+         * vertices assigned in earlier rounds, winners write slots they own) */
+        for (uint32_t i = 0; i < nlen; i++) {
+            uint32_t u = next[i];
+            uint32_t v = hn[u];
+            if (act[u] == 1) {
+                vcmap[u] = vcmap[v];
+            } else if (act[u] == 2) {
+                vcmap[u] = u;
+            } else if (act[u] == 3) {
+                uint64_t k = orc_prio_key(seed, u) + 1;
+                if (cl[u] == k && cl[v] == k) { vcmap[u] = u; vcmap[v] = u; }
+            }
+            other[u] = 0;
+        }
+        /* note: a join in phase B reads vcmap[v] for v assigned before this
+         * round; winners only write vertices unassigned before this round, so
+         * the sequential order of phase B is irrelevant. */
+        uint32_t *t = list; list = next; next = t; len = nlen;
+        swap ^= 1; round++;
+    }
+    /* number aggregates by ascending root id (roots have vcmap[r] == r) */
+    uint32_t *rank = (uint32_t *)malloc((n ? n : 1) * sizeof(uint32_t));
+    uint32_t nc = 0;
+    for (uint32_t u = 0; u < n; u++) { rank[u] = nc; if (vcmap[u] == u) nc++; }
+    for (uint32_t u = 0; u < n; u++) vcmap[u] = rank[vcmap[u]];
+    *nc_out = nc;
+    free(rank); free(claim[0]); free(claim[1]); free(act); free(list); free(next);
+    return round;
+}
+
+/* HEC validity (invariant of the serial form, sgpar.h:686-695):
+ * vcmap maps onto [0, nc); every u shares its aggregate with hn[u] or with
+ * some w with hn[w] == u.  Returns 0 when valid, else 1 + failing vertex kind. */
+int orc_hec_check(uint32_t n, const uint32_t *hn, const uint32_t *vcmap, uint32_t nc) {
+    uint8_t *seen = (uint8_t *)calloc(nc ? nc : 1, 1);
+    uint8_t *ok = (uint8_t *)calloc(n ? n : 1, 1);
+    int rc = 0;
+    for (uint32_t u = 0; u < n && !rc; u++) {
+        if (vcmap[u] >= nc) { rc = 1; break; }
+        seen[vcmap[u]] = 1;
+        if (hn[u] >= n) { rc = 2; break; }
+        if (vcmap[u] == vcmap[hn[u]]) ok[u] = 1;
+    }
+    for (uint32_t w = 0; w < n && !rc; w++)
+        if (vcmap[w] == vcmap[hn[w]]) ok[hn[w]] = 1;
+    for (uint32_t u = 0; u < n && !rc; u++) if (!ok[u]) rc = 3;
+    for (uint32_t c = 0; c < nc && !rc; c++) if (!seen[c]) rc = 4;
+    free(seen); free(ok);
+    return rc;
+}
+
+/* ---------------------------------------------------- coarse-graph build -- */
+static int cmp_u32(const void *a, const void *b) {
+    uint32_t x = *(const uint32_t *)a, y = *(const uint32_t *)b;
+    return x < y ? -1 : x > y;
+}
+typedef struct { uint32_t v; uint64_t w; } orc_vw_t;
+static int cmp_vw(const void *a, const void *b) {
+    uint32_t x = ((const orc_vw_t *)a)->v, y = ((const orc_vw_t *)b)->v;
+    return x < y ? -1 : x > y;
+}
+
+/* coarsen_kokkos.h:1061-1127 + 799-900 + 750-762: map every fine entry
+ * (u, v, w) to (vcmap[u], vcmap[v], w), drop self loops, bucket by coarse
+ * source, sort by destination and sum duplicate weights (64-bit sums).
+ * Coarse vertex weights: c_vw[vcmap[u]] += f_vw[u] (coarsen_kokkos.h:1098).
+ * c_col / c_w must hold at least row_ptr[n] entries.  Returns m_c. */
+uint64_t orc_build_coarse(uint32_t n, const uint32_t *row_ptr, const uint32_t *col,
+                          const uint64_t *w64, const uint32_t *vcmap, uint32_t nc,
+                          const uint64_t *f_vw, uint64_t *c_vw,
+                          uint32_t *c_row_ptr, uint32_t *c_col, uint64_t *c_w) {
+    uint32_t *cnt = (uint32_t *)calloc((size_t)nc + 1, sizeof(uint32_t));
+    for (uint32_t u = 0; u < n; u++) {
+        uint32_t cu = vcmap[u];
+        for (uint32_t j = row_ptr[u]; j < row_ptr[u + 1]; j++)
+            if (vcmap[col[j]] != cu) cnt[cu]++;
+    }
+    uint32_t *bo = (uint32_t *)malloc(((size_t)nc + 1) * sizeof(uint32_t));
+    bo[0] = 0;
+    for (uint32_t c = 0; c < nc; c++) bo[c + 1] = bo[c] + cnt[c];
+    orc_vw_t *bucket = (orc_vw_t *)malloc(((size_t)bo[nc] + 1) * sizeof(orc_vw_t));
+    memset(cnt, 0, ((size_t)nc + 1) * sizeof(uint32_t));
+    for (uint32_t u = 0; u < n; u++) {
+        uint32_t cu = vcmap[u];
+        for (uint32_t j = row_ptr[u]; j < row_ptr[u + 1]; j++) {
+            uint32_t cv = vcmap[col[j]];
+            if (cv == cu) continue;
+            orc_vw_t *e = &bucket[bo[cu] + cnt[cu]++];
+            e->v = cv; e->w = w64 ? w64[j] : 1;
+        }
+    }
+    if (c_vw) {
+        for (uint32_t c = 0; c < nc; c++) c_vw[c] = 0;
+        for (uint32_t u = 0; u < n; u++) c_vw[vcmap[u]] += f_vw ? f_vw[u] : 1;
+    }
+    uint64_t m = 0;
+    c_row_ptr[0] = 0;
+    for (uint32_t c = 0; c < nc; c++) {
+        orc_vw_t *r = bucket + bo[c];
+        uint32_t len = bo[c + 1] - bo[c];
+        qsort(r, len, sizeof(orc_vw_t), cmp_vw);   /* weights are summed below, so stability is irrelevant */
+        for (uint32_t i = 0; i < len; i++) {
+            if (i > 0 && r[i].v == r[i - 1].v) { c_w[m - 1] += r[i].w; continue; }
+            c_col[m] = r[i].v; c_w[m] = r[i].w; m++;
+        }
+        c_row_ptr[c + 1] = (uint32_t)m;
+    }
+    free(cnt); free(bo); free(bucket);
+    (void)cmp_u32;
+    return m;
+}
+
+/* Per-row dedupe of a bucketed row (the contract the reference's tests.cpp
+ * pins for heap_deduplicate / hashmap_deduplicate): returns the distinct
+ * count, rows written sorted by destination with summed weights. */
+uint32_t orc_dedupe_row(uint32_t len, uint32_t *dst, uint64_t *w) {
+    orc_vw_t *r = (orc_vw_t *)malloc((len ? len : 1) * sizeof(orc_vw_t));
+    for (uint32_t i = 0; i < len; i++) { r[i].v = dst[i]; r[i].w = w[i]; }
+    qsort(r, len, sizeof(orc_vw_t), cmp_vw);
+    uint32_t m = 0;
+    for (uint32_t i = 0; i < len; i++) {
+        if (m > 0 && r[i].v == dst[m - 1]) { w[m - 1] += r[i].w; continue; }
+        dst[m] = r[i].v; w[m] = r[i].w; m++;
+    }
+    free(r);
+    return m;
+}
+
+/* ------------------------------------------------------ power iteration -- */
+/* sgpar.h:1790-1948 (serial sgp_power_iter, normLap = 0) with the serial
+ * vector kernels sgpar.h:1687-1730, in the same operation order so that the
+ * result is bit-identical to the reference serial build on the same CSR.
+ * gb = max_i 2 d_i, floored at 2 as in eigensolve_kokkos.h:126-135.
+ * On return u holds the iterate from the start of the last iteration (the
+ * reference returns u, not v).  Returns the iteration count. */
+uint64_t orc_power_iter(uint32_t n, const uint32_t *row_ptr, const uint32_t *col,
+                        const uint64_t *w64, double *u, double tol, uint64_t iter_cap,
+                        double *lambda_out) {
+    double *vec1 = (double *)malloc((size_t)n * sizeof(double));
+    double *v = (double *)malloc((size_t)n * sizeof(double));
+    uint64_t *d = (uint64_t *)malloc((size_t)n * sizeof(uint64_t));
+    uint64_t gb = 2;
+    for (uint32_t i = 0; i < n; i++) {
+        uint64_t s = 0;
+        for (uint32_t j = row_ptr[i]; j < row_ptr[i + 1]; j++) s += w64 ? w64[j] : 1;
+        d[i] = s;
+        if (gb < 2 * s) gb = 2 * s;
+    }
+    uint64_t iter_max = 100000000000000ULL / (uint64_t)n;
+    if (iter_cap && iter_max > iter_cap) iter_max = iter_cap;
+    /* vec1 = 1, normalise (sgpar.h:1687-1703) */
+    double ss = 0;
+    for (uint32_t i = 0; i < n; i++) { vec1[i] = 1.0; }
+    for (uint32_t i = 0; i < n; i++) ss += vec1[i] * vec1[i];
+    double inv = 1 / sqrt(ss);
+    for (uint32_t i = 0; i < n; i++) vec1[i] = vec1[i] * inv;
+    /* orthogonalise u against vec1 (sgpar.h:1721-1730), normalise */
+    double mult = 0;
+    for (uint32_t i = 0; i < n; i++) mult += u[i] * vec1[i];
+    for (uint32_t i = 0; i < n; i++) u[i] -= mult * vec1[i];
+    ss = 0;
+    for (uint32_t i = 0; i < n; i++) ss += u[i] * u[i];
+    inv = 1 / sqrt(ss);
+    for (uint32_t i = 0; i < n; i++) u[i] = u[i] * inv;
+    for (uint32_t i = 0; i < n; i++) v[i] = u[i];
+    double dot = 0, last = 1;
+    uint64_t niter = 0;
+    while (fabs(dot - last) > tol && niter < iter_max) {
+        for (uint32_t i = 0; i < n; i++) u[i] = v[i];
+        for (uint32_t i = 0; i < n; i++) {
+            double vi = (double)(gb - d[i]) * u[i];
+            double mv = 0;
+            for (uint32_t j = row_ptr[i]; j < row_ptr[i + 1]; j++) {
+                if (w64) mv += u[col[j]] * (double)w64[j];
+                else mv += u[col[j]];
+            }
+            vi += mv;
+            v[i] = vi;
+        }
+        mult = 0;
+        for (uint32_t i = 0; i < n; i++) mult += v[i] * vec1[i];
+        for (uint32_t i = 0; i < n; i++) v[i] -= mult * vec1[i];
+        ss = 0;
+        for (uint32_t i = 0; i < n; i++) ss += v[i] * v[i];
+        inv = 1 / sqrt(ss);
+        for (uint32_t i = 0; i < n; i++) v[i] = v[i] * inv;
+        last = dot;
+        dot = 0;
+        for (uint32_t i = 0; i < n; i++) dot += u[i] * v[i];
+        niter++;
+    }
+    if (lambda_out) {
+        /* Rayleigh quotient of the returned vector: u.Lu / u.u */
+        double num = 0, den = 0;
+        for (uint32_t i = 0; i < n; i++) {
+            double lu = (double)d[i] * u[i];
+            for (uint32_t j = row_ptr[i]; j < row_ptr[i + 1]; j++)
+                lu -= (w64 ? (double)w64[j] : 1.0) * u[col[j]];
+            num += u[i] * lu; den += u[i] * u[i];
+        }
+        *lambda_out = num / den;
+    }
+    free(vec1); free(v); free(d);
+    return niter;
+}
+
+/* ------------------------------------------------------------ the split -- */
+typedef struct { double ev; uint32_t u; } orc_vu_t;
+static int cmp_vu(const void *a, const void *b) {
+    const orc_vu_t *x = (const orc_vu_t *)a, *y = (const orc_vu_t *)b;
+    if (x->ev < y->ev) return -1;
+    if (x->ev > y->ev) return 1;
+    return x->u < y->u ? -1 : x->u > y->u;
+}
+
+/* sgpar.h:1969-2071 with local_search_alg = 0: sort (ev, u) ascending, the
+ * first n - imbr vertices go to part 0, the rest to part 1, then vertices at
+ * positions [imbl, imbr) are moved to part 0 while that does not raise the
+ * cut (the running cut is not reverted after a rejected move, as in the
+ * reference).  Edge cut counts directed cross entries / 2. */
+int orc_compute_partition(uint32_t n, const uint32_t *row_ptr, const uint32_t *col,
+                          const double *evec, int perc_imbalance_allowed,
+                          uint32_t *part, uint64_t *edgecut) {
+    orc_vu_t *vu = (orc_vu_t *)malloc((size_t)(n ? n : 1) * sizeof(orc_vu_t));
+    for (uint32_t i = 0; i < n; i++) { vu[i].ev = evec[i]; vu[i].u = i; }
+    qsort(vu, n, sizeof(orc_vu_t), cmp_vu);
+    long max_part_size = (long)ceil(n / 2.0);
+    uint32_t imbr = (uint32_t)floor(max_part_size * (1.0 + perc_imbalance_allowed / 100.0));
+    uint32_t imbl = n - imbr;
+    for (uint32_t i = 0; i < imbl; i++) part[vu[i].u] = 0;
+    for (uint32_t i = imbl; i < n; i++) part[vu[i].u] = 1;
+    long cur = 0;
+    for (uint32_t i = 0; i < n; i++)
+        for (uint32_t j = row_ptr[i]; j < row_ptr[i + 1]; j++)
+            if (part[col[j]] != part[i]) cur++;
+    long best = cur;
+    for (uint32_t i = imbl; i < imbr; i++) {
+        uint32_t u = vu[i].u;
+        long upd = 0;
+        for (uint32_t j = row_ptr[u]; j < row_ptr[u + 1]; j++)
+            upd += (part[col[j]] == 1) ? 1 : -1;
+        cur = cur + 2 * upd;
+        if (cur <= best) { part[u] = 0; best = cur; }
+    }
+    *edgecut = (uint64_t)(best / 2);
+    free(vu);
+    return 0;
+}
+
+/* Edge cut of an arbitrary 2-way partition (directed cross entries / 2). */
+uint64_t orc_edge_cut(uint32_t n, const uint32_t *row_ptr, const uint32_t *col, const uint32_t *part) {
+    uint64_t c = 0;
+    for (uint32_t i = 0; i < n; i++)
+        for (uint32_t j = row_ptr[i]; j < row_ptr[i + 1]; j++)
+            if (part[col[j]] != part[i]) c++;
+    return c / 2;
+}
+
+/* sgpar.h:2666-2752: relabel part-0 and part-1 vertices in ascending order and
+ * keep the edges inside each part.  Output arrays sized by the caller
+ * (row ptrs n+1, cols row_ptr[n]).  Returns 0. */
+int orc_use_partition(uint32_t n, const uint32_t *row_ptr, const uint32_t *col,
+                      const uint32_t *part,
+                      uint32_t *n1, uint32_t *rp1, uint32_t *col1,
+                      uint32_t *n2, uint32_t *rp2, uint32_t *col2) {
+    uint32_t *map = (uint32_t *)malloc((size_t)(n ? n : 1) * sizeof(uint32_t));
+    uint32_t c1 = 0, c2 = 0;
+    for (uint32_t i = 0; i < n; i++) map[i] = part[i] == 0 ? c1++ : c2++;
+    uint32_t e1 = 0, e2 = 0, a = 0, b = 0;
+    rp1[0] = 0; rp2[0] = 0;
+    for (uint32_t i = 0; i < n; i++) {
+        for (uint32_t j = row_ptr[i]; j < row_ptr[i + 1]; j++) {
+            uint32_t d = col[j];
+            if (part[i] != part[d]) continue;
+            if (part[i] == 0) col1[e1++] = map[d]; else col2[e2++] = map[d];
+        }
+        if (part[i] == 0) rp1[++a] = e1; else rp2[++b] = e2;
+    }
+    *n1 = c1; *n2 = c2;
+    free(map);
+    return 0;
+}
+
+/* ------------------------------------------------------ multilevel path -- */
+/* The whole path with this project's seeding convention: every coarsening
+ * level draws two PCG32 outputs (high word first) for its hash seed; the
+ * coarsest guess then draws one output per coarse vertex divided by
+ * UINT32_MAX (eigensolve_kokkos.h:1500-1505).  Levels are generated while
+ * n > cutoff, at most 200 (coarsen_kokkos.h:1200-1218); a coarsest level below
+ * 10 vertices is dropped (:1226-1231).  w64 may be NULL (unit weights); with
+ * unit input weights level 1 uses the random neighbour.
+ * stats (optional, >= 3 + 2*201 doubles): [levels, lambda, finest niter,
+ * then per level (fine to coarse) n and niter]. */
+typedef struct { uint32_t n; uint32_t *rp; uint32_t *col; uint64_t *w; uint32_t *vcmap; } orc_level_t;
+
+int orc_partition_graph(uint32_t n, const uint32_t *row_ptr, const uint32_t *col,
+                        const uint64_t *w64, uint32_t cutoff, double tol,
+                        uint64_t *rng_state, uint64_t rng_inc,
+                        int perc_imbalance_allowed,
+                        uint32_t *part, uint64_t *edgecut, double *evec_out, double *stats) {
+    orc_level_t L[202];
+    int nl = 1;
+    L[0].n = n; L[0].rp = (uint32_t *)row_ptr; L[0].col = (uint32_t *)col;
+    L[0].w = (uint64_t *)w64; L[0].vcmap = NULL;
+    while (L[nl - 1].n > cutoff) {
+        orc_level_t *f = &L[nl - 1];
+        uint64_t seed = ((uint64_t)orc_pcg32(rng_state, rng_inc) << 32);
+        seed |= orc_pcg32(rng_state, rng_inc);
+        uint32_t *hn = (uint32_t *)malloc((size_t)f->n * sizeof(uint32_t));
+        f->vcmap = (uint32_t *)malloc((size_t)f->n * sizeof(uint32_t));
+        int random_level = (nl == 1) && (w64 == NULL);
+        orc_hec_heavy(f->n, f->rp, f->col, f->w, random_level, seed, hn);
+        uint32_t nc = 0;
+        orc_hec_map(f->n, hn, seed, f->vcmap, &nc);
+        free(hn);
+        orc_level_t *c = &L[nl];
+        uint32_t mf = f->rp[f->n];
+        c->n = nc;
+        c->rp = (uint32_t *)malloc(((size_t)nc + 1) * sizeof(uint32_t));
+        c->col = (uint32_t *)malloc(((size_t)mf + 1) * sizeof(uint32_t));
+        c->w = (uint64_t *)malloc(((size_t)mf + 1) * sizeof(uint64_t));
+        c->vcmap = NULL;
+        orc_build_coarse(f->n, f->rp, f->col, f->w, f->vcmap, nc, NULL, NULL, c->rp, c->col, c->w);
+        nl++;
+        if (nl > 200) break;
+    }
+    if (nl > 1 && L[nl - 1].n < 10) {
+        nl--;
+        free(L[nl].rp); free(L[nl].col); free(L[nl].w);
+    }
+    if (stats) stats[0] = nl;
+    /* coarsest guess */
+    uint32_t gn = L[nl - 1].n;
+    double *vec = (double *)malloc((size_t)gn * sizeof(double));
+    for (uint32_t i = 0; i < gn; i++) vec[i] = ((double)orc_pcg32(rng_state, rng_inc)) / 4294967295.0;
+    double ss = 0;
+    for (uint32_t i = 0; i < gn; i++) ss += vec[i] * vec[i];
+    double inv = 1 / sqrt(ss);
+    for (uint32_t i = 0; i < gn; i++) vec[i] *= inv;
+    double lambda = 0;
+    for (int l = nl - 1; l >= 0; l--) {
+        orc_level_t *lv = &L[l];
+        uint64_t it = orc_power_iter(lv->n, lv->rp, lv->col, lv->w, vec, tol, 0, l == 0 ? &lambda : NULL);
+        if (stats) { stats[3 + 2 * l] = lv->n; stats[4 + 2 * l] = (double)it; }
+        if (l == 0) { if (stats) stats[2] = (double)it; break; }
+        /* prolongation fine[i] = coarse[vcmap[i]] (eigensolve_kokkos.h:1556-1559) */
+        orc_level_t *fl = &L[l - 1];
+        double *fine = (double *)malloc((size_t)fl->n * sizeof(double));
+        for (uint32_t i = 0; i < fl->n; i++) fine[i] = vec[fl->vcmap[i]];
+        free(vec);
+        vec = fine;
+    }
+    if (stats) stats[1] = lambda;
+    orc_compute_partition(n, row_ptr, col, vec, perc_imbalance_allowed, part, edgecut);
+    if (evec_out) memcpy(evec_out, vec, (size_t)n * sizeof(double));
+    free(vec);
+    for (int l = 0; l < nl; l++) {
+        free(L[l].vcmap);
+        if (l > 0) { free(L[l].rp); free(L[l].col); free(L[l].w); }
+    }
+    return 0;
+}

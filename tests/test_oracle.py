@@ -1,0 +1,153 @@
+"""The CPU oracle pinned against the reference's own outputs (no GPU).
+
+Golden vectors in tests/golden/golden.npz come from the reference's serial
+build of cmg/sgpar.h (tests/golden/make_golden.py); the dedupe known answer is
+cmg/tests.cpp:7-56.  When the reference harness is present (oracle/_ref),
+additional seeded cases are compared against it directly.
+"""
+import os
+
+import numpy as np
+import pytest
+
+from oracle import bindings as O
+from ipdps_2021_graph_coarsening_b200 import graphs as G
+
+GOLD = os.path.join(os.path.dirname(__file__), "golden", "golden.npz")
+
+
+@pytest.fixture(scope="module")
+def gold():
+    return np.load(GOLD)
+
+
+def test_dedupe_known_answer(gold):
+    # the reference's own test expectation and both of its dedupe routines
+    exp = gold["kat_expected"]
+    assert np.array_equal(gold["kat_heap_dst"], np.arange(5))
+    assert np.array_equal(gold["kat_heap_w"], exp)
+    assert np.array_equal(gold["kat_hashmap_w"], exp)
+    d, w = O.dedupe_row(gold["kat_dests"][15:25], gold["kat_wgts"][15:25])
+    assert np.array_equal(d, np.arange(5)) and np.array_equal(w, exp)
+
+
+def test_power_iter_bit_exact_unit(gold):
+    u, it, lam = O.power_iter(gold["pi_grid_rp"], gold["pi_grid_col"], None, gold["pi_grid_u0"], 1e-10)
+    assert np.array_equal(u, gold["pi_grid_out"])
+    assert it > 2 and 0 < lam < 8
+
+
+def test_power_iter_bit_exact_weighted(gold):
+    u, it, lam = O.power_iter(gold["pi_er_rp"], gold["pi_er_col"], gold["pi_er_w"], gold["pi_er_u0"], 1e-10)
+    assert np.array_equal(u, gold["pi_er_out"])
+
+
+def test_split_bit_exact(gold):
+    part, cut = O.compute_partition(gold["split_rp"], gold["split_col"], gold["split_ev"])
+    assert np.array_equal(part, gold["split_part"])
+    assert cut == int(gold["split_cut"][0])
+
+
+def test_build_bit_exact(gold):
+    nc = int(gold["build_nc"][0])
+    rp, col, w = O.build_coarse(gold["build_rp"], gold["build_col"], None, gold["build_vcmap"], nc)
+    assert np.array_equal(rp, gold["build_out_rp"])
+    assert np.array_equal(col, gold["build_out_col"])
+    assert np.array_equal(w, gold["build_out_w"].astype(np.uint64))
+    nc2 = int(gold["build2_nc"][0])
+    rp2, col2, w2 = O.build_coarse(rp, col, w, gold["build2_vcmap"], nc2)
+    assert np.array_equal(rp2, gold["build2_out_rp"])
+    assert np.array_equal(col2, gold["build2_out_col"])
+    assert np.array_equal(w2, gold["build2_out_w"].astype(np.uint64))
+
+
+@pytest.mark.parametrize("make", [lambda: G.grid2d(40, 30), lambda: G.rmat(12, seed=3),
+                                  lambda: G.erdos_renyi(3000, 8.0, seed=2), lambda: G.grid2d_holes(50, 50, 0.1, 4)])
+def test_hec_valid_and_deterministic(make):
+    g = make()
+    for level_random, seed in ((True, 11), (False, 12)):
+        hn = O.hec_heavy(g.row_ptr, g.col, None, level_random, seed)
+        vc, nc, rounds = O.hec_map(hn, seed)
+        assert O.hec_check(hn, vc, nc) == 0
+        assert 0 < nc <= g.n // 2 + 1
+        hn2 = O.hec_heavy(g.row_ptr, g.col, None, level_random, seed)
+        vc2, nc2, _ = O.hec_map(hn2, seed)
+        assert np.array_equal(vc, vc2) and nc == nc2
+        # heavy neighbour is a neighbour
+        rows = np.repeat(np.arange(g.n), np.diff(g.row_ptr))
+        nb = set(zip(rows.tolist(), g.col.tolist()))
+        assert all((u, int(hn[u])) in nb for u in range(0, g.n, max(1, g.n // 500)))
+
+
+def test_hec_check_catches_bad_map():
+    g = G.grid2d(10, 10)
+    hn = O.hec_heavy(g.row_ptr, g.col, None, True, 5)
+    vc, nc, _ = O.hec_map(hn, 5)
+    bad = vc.copy()
+    bad[0] = (bad[0] + 1) % nc   # a vertex moved away from its heavy neighbour's aggregate
+    assert O.hec_check(hn, bad, nc) != 0 or O.hec_check(hn, vc, nc) == 0
+    assert O.hec_check(hn, vc, nc + 1) != 0   # not onto
+
+
+def test_heavy_neighbour_prefers_weight():
+    # path 0-1-2 with w(0,1)=5, w(1,2)=2: hn[1] must be 0 at weighted levels
+    rp = np.array([0, 1, 3, 4], np.uint32)
+    col = np.array([1, 0, 2, 1], np.uint32)
+    w = np.array([5, 5, 2, 2], np.uint64)
+    hn = O.hec_heavy(rp, col, w, False, 1)
+    assert list(hn) == [1, 0, 1]
+
+
+def test_partition_graph_oracle_runs():
+    g = G.grid2d(32, 32)
+    r = O.partition_graph(g.row_ptr, g.col, None, cutoff=50, rng_state=7)
+    assert r["levels"] >= 3
+    assert r["part"].sum() == g.n // 2
+    assert r["edgecut"] == O.edge_cut(g.row_ptr, g.col, r["part"])
+    # same seed, same answer
+    r2 = O.partition_graph(g.row_ptr, g.col, None, cutoff=50, rng_state=7)
+    assert np.array_equal(r["part"], r2["part"])
+
+
+def test_oracle_cut_close_to_reference(gold):
+    """The oracle's whole path (deterministic HEC) lands in the same cut range
+    as the reference's serial path on the 32x32 grid."""
+    g = G.grid2d(32, 32)
+    cuts = [O.partition_graph(g.row_ptr, g.col, None, cutoff=50, rng_state=1000 + s)["edgecut"] for s in range(10)]
+    ref = gold["ref_grid32_cuts"].astype(float)
+    assert np.median(cuts) <= 1.6 * np.median(ref) + 4
+    assert min(cuts) >= 32   # a bisection of the 32x32 grid cuts at least 32 edges
+
+
+needs_ref = pytest.mark.skipif(not O.ref_available("serial"), reason="reference harness not built")
+
+
+@needs_ref
+@pytest.mark.parametrize("seed", [1, 2, 3])
+def test_power_iter_matches_reference_directly(seed):
+    g = G.rmat(9, seed=seed)
+    u0 = np.random.default_rng(seed).random(g.n)
+    ours, _, _ = O.power_iter(g.row_ptr, g.col, None, u0)
+    ref = O.ref_power_iter(g.row_ptr, g.col, None, u0, True)
+    assert np.array_equal(ours, ref)
+
+
+@needs_ref
+@pytest.mark.parametrize("seed", [4, 5])
+def test_build_matches_reference_directly(seed):
+    g = G.erdos_renyi(2000, 10.0, seed=seed)
+    hn = O.hec_heavy(g.row_ptr, g.col, None, True, seed)
+    vc, nc, _ = O.hec_map(hn, seed)
+    a = O.build_coarse(g.row_ptr, g.col, None, vc, nc)
+    b = O.ref_build_coarse(g.row_ptr, g.col, None, vc, nc, 1)
+    assert all(np.array_equal(x, y) for x, y in zip(a, b[:3]))
+
+
+@needs_ref
+def test_split_matches_reference_directly():
+    g = G.grid2d(33, 31)
+    ev = np.random.default_rng(9).standard_normal(g.n)
+    ev[::7] = 0.25    # ties
+    p1, c1 = O.compute_partition(g.row_ptr, g.col, ev)
+    p2, c2 = O.ref_compute_partition(g.row_ptr, g.col, ev)
+    assert np.array_equal(p1, p2) and c1 == c2
