@@ -187,9 +187,20 @@ def gpu_arm(args, rank: int, ws: int, local: int, distmod):
     if distmod:
         dist, td = distmod
         dist.init_process_group("nccl", timeout=td(seconds=600), device_id=torch.device("cuda", local))
-    g = rmat_graph(SCALE)
+    g = rmat_graph(args.scale)
     n, m = g.n, g.m_directed
     p = Partitioner(local)
+    if args.single:
+        # one partition of the chosen case (used for profiler captures)
+        rp_d = torch.from_numpy(g.row_ptr.view(np.int32)).cuda()
+        col_d = torch.from_numpy(g.col.view(np.int32)).cuda()
+        r = p.partition({"row_ptr": rp_d, "col": col_d}, rng_state=0x2021, mixed=args.mixed)
+        print(json.dumps({"case": f"rmat{args.scale}", "n": n, "m_undirected": g.m_undirected,
+                          "ms": r.ms_total, "levels": r.level_n, "level_m": r.level_m,
+                          "level_iters": r.level_iters, "level_pi_ms": r.level_pi_ms, "edgecut": r.edgecut,
+                          "phase_ms": [r.ms_coarsen, r.ms_eigen, r.ms_split]}))
+        p.close()
+        return
     stream = torch.cuda.ExternalStream(L.lib().sgp_b200_stream(p._ctx))
     rp_d = torch.from_numpy(g.row_ptr.view(np.int32)).cuda()
     col_d = torch.from_numpy(g.col.view(np.int32)).cuda()
@@ -270,6 +281,7 @@ def gpu_arm(args, rank: int, ws: int, local: int, distmod):
                        "n": n, "m_undirected": g.m_undirected, "cutoff": 50, "tol": 1e-10,
                        "parallelism": f"replicas{ws}", "l2": "inputs larger than L2 (CSR 0.5 GB)"},
             "edgecut": r.edgecut, "lambda": r.lam, "residual": r.residual, "levels": r.level_n,
+            "level_m": r.level_m,
             "level_iters": r.level_iters, "level_pi_ms": [round(x, 3) for x in r.level_pi_ms],
             "phase_ms": {"coarsen": r.ms_coarsen, "eigen": r.ms_eigen, "split": r.ms_split},
             "clocks": clocks, "e2e": e2e, "mixed": mixed, "gpu_launches": r.kernel_launches * args.steps,
@@ -290,6 +302,9 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--scale", type=int, default=SCALE, help="R-MAT scale (the benchmark is 22)")
+    ap.add_argument("--single", action="store_true", help="one partition of --scale and exit (profiling)")
+    ap.add_argument("--mixed", action="store_true", help="with --single: mixed-precision power iteration")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

@@ -95,6 +95,44 @@ __device__ __forceinline__ double row_degree_group(const PIArgs &a, uint32_t i, 
     return (double)s;
 }
 
+// acc += sum_j w_j src[col_j] and dsum += sum_j w_j over j = j0, j0 + s, ... < e.
+// Four entries per lane are in flight (destination loads, weight loads, then
+// the four gathers), so a warp keeps 4x the memory requests outstanding of a
+// one-at-a-time loop; the summation order is fixed for a given stride.
+template <typename W, typename V, typename ACC>
+__device__ __forceinline__ void row_accum(const uint32_t *__restrict__ col, const W *__restrict__ w, const V *src,
+                                          uint32_t j, uint32_t e, uint32_t s, ACC &acc, uint64_t &dsum) {
+    if (w) {
+        for (; j + 3 * s < e; j += 4 * s) {
+            const uint32_t c0 = __ldg(col + j), c1 = __ldg(col + j + s), c2 = __ldg(col + j + 2 * s),
+                           c3 = __ldg(col + j + 3 * s);
+            const W w0 = __ldg(w + j), w1 = __ldg(w + j + s), w2 = __ldg(w + j + 2 * s), w3 = __ldg(w + j + 3 * s);
+            const V x0 = src[c0], x1 = src[c1], x2 = src[c2], x3 = src[c3];
+            acc += (ACC)((V)w0 * x0);
+            acc += (ACC)((V)w1 * x1);
+            acc += (ACC)((V)w2 * x2);
+            acc += (ACC)((V)w3 * x3);
+            dsum += (uint64_t)w0 + (uint64_t)w1 + (uint64_t)w2 + (uint64_t)w3;
+        }
+        for (; j < e; j += s) {
+            const W wt = __ldg(w + j);
+            acc += (ACC)((V)wt * src[__ldg(col + j)]);
+            dsum += (uint64_t)wt;
+        }
+    } else {
+        for (; j + 3 * s < e; j += 4 * s) {
+            const uint32_t c0 = __ldg(col + j), c1 = __ldg(col + j + s), c2 = __ldg(col + j + 2 * s),
+                           c3 = __ldg(col + j + 3 * s);
+            const V x0 = src[c0], x1 = src[c1], x2 = src[c2], x3 = src[c3];
+            acc += (ACC)x0;
+            acc += (ACC)x1;
+            acc += (ACC)x2;
+            acc += (ACC)x3;
+        }
+        for (; j < e; j += s) acc += (ACC)src[__ldg(col + j)];
+    }
+}
+
 template <int G>
 __device__ __forceinline__ unsigned pi_group_mask() {
     if (G == 32) return 0xFFFFFFFFu;
@@ -237,16 +275,7 @@ __global__ void __launch_bounds__(kPIThreads) k_power_iter(PIArgs a) {
             if (e - b > T) continue;   // group-uniform
             V acc = 0;
             uint64_t dsum = 0;
-            for (uint32_t j = b + lane; j < e; j += G) {
-                const uint32_t c = __ldg(a.col + j);
-                if (w) {
-                    const W wt = __ldg(w + j);
-                    acc += (V)wt * src[c];
-                    dsum += (uint64_t)wt;
-                } else {
-                    acc += src[c];
-                }
-            }
+            row_accum<W, V, V>(a.col, w, src, b + lane, e, G, acc, dsum);
 #pragma unroll
             for (int o = G / 2; o > 0; o >>= 1) {
                 acc += __shfl_xor_sync(gm, acc, o);
@@ -266,17 +295,10 @@ __global__ void __launch_bounds__(kPIThreads) k_power_iter(PIArgs a) {
         for (uint32_t h = blockIdx.x; h < n_heavy; h += gridDim.x) {
             const uint32_t i = a.heavy[h];
             const uint32_t b = a.rp[i], e = a.rp[i + 1];
-            double acc = 0, dsum = 0;
-            for (uint32_t j = b + threadIdx.x; j < e; j += blockDim.x) {
-                const uint32_t c = __ldg(a.col + j);
-                if (w) {
-                    const double wt = (double)__ldg(w + j);
-                    acc += wt * (double)src[c];
-                    dsum += wt;
-                } else {
-                    acc += (double)src[c];
-                }
-            }
+            double acc = 0;
+            uint64_t dsum_i = 0;
+            row_accum<W, V, double>(a.col, w, src, b + threadIdx.x, e, blockDim.x, acc, dsum_i);
+            double dsum = (double)dsum_i;   // exact: weighted degrees stay below 2^53
             block_sum2(acc, dsum, sm);
             if (threadIdx.x == 0) {
                 const double d = w ? dsum : (double)(e - b);
@@ -480,20 +502,27 @@ int power_iter_level(Context &C, const Level &L, const double *x_in, const uint3
     double rh[6];
     float kms = 0;
     uint64_t total_iters = 0;
-    // mixed precision: FP32 storage until converged or stalled, then FP64
-    // iterations from the FP32 result down to the requested tolerance.
+    // Mixed precision: FP32 vector storage and gathers under the reference's
+    // stopping rule.  When |d dot| stops shrinking before reaching tol (the
+    // FP32 noise floor), the FP32 iterate seeds FP64 iterations that finish
+    // the level at the requested tolerance.  Levels below 4096 vertices are
+    // latency-bound and run in FP64 directly.
+    bool done = false;
     if (o.mixed && n >= 4096) {
         a.stall_factor = 0.5;
         a.stall_window = 64;
         SGPB_TRY(run_pi(C, L, a, 1, res_d, rh, &kms));
         total_iters += (uint64_t)rh[0];
+        done = rh[5] == 0.0;
         a.x_in = x_out;
         a.vcmap = nullptr;
         a.stall_factor = 0;
         a.iter_max = imax > total_iters ? imax - total_iters : 1;
     }
-    SGPB_TRY(run_pi(C, L, a, 0, res_d, rh, &kms));
-    total_iters += (uint64_t)rh[0];
+    if (!done) {
+        SGPB_TRY(run_pi(C, L, a, 0, res_d, rh, &kms));
+        total_iters += (uint64_t)rh[0];
+    }
     res->niter = total_iters;
     res->dot = rh[1];
     res->gb = rh[2];
