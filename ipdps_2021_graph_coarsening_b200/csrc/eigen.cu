@@ -39,6 +39,7 @@ struct PIArgs {
     const uint32_t *heavy;        // rows with degree > heavy_T, ascending
     const uint32_t *n_heavy_ptr;
     uint32_t heavy_T;
+    const uint32_t *cpre;         // [n+1] prefix of per-row cost (0 for heavy rows): warp row ranges
     const double *x_in;
     const uint32_t *vcmap;
     void *va;
@@ -102,35 +103,57 @@ __device__ __forceinline__ double row_degree_group(const PIArgs &a, uint32_t i, 
 template <typename W, typename V, typename ACC>
 __device__ __forceinline__ void row_accum(const uint32_t *__restrict__ col, const W *__restrict__ w, const V *src,
                                           uint32_t j, uint32_t e, uint32_t s, ACC &acc, uint64_t &dsum) {
+    // every trip issues up to four predicated entries, the last partial trip
+    // included, so a row costs ceil(len / 4s) dependent-load rounds
     if (w) {
-        for (; j + 3 * s < e; j += 4 * s) {
-            const uint32_t c0 = __ldg(col + j), c1 = __ldg(col + j + s), c2 = __ldg(col + j + 2 * s),
-                           c3 = __ldg(col + j + 3 * s);
-            const W w0 = __ldg(w + j), w1 = __ldg(w + j + s), w2 = __ldg(w + j + 2 * s), w3 = __ldg(w + j + 3 * s);
-            const V x0 = src[c0], x1 = src[c1], x2 = src[c2], x3 = src[c3];
+        for (; j < e; j += 4 * s) {
+            const bool p1 = j + s < e, p2 = j + 2 * s < e, p3 = j + 3 * s < e;
+            const uint32_t c0 = __ldg(col + j);
+            const uint32_t c1 = p1 ? __ldg(col + j + s) : 0u;
+            const uint32_t c2 = p2 ? __ldg(col + j + 2 * s) : 0u;
+            const uint32_t c3 = p3 ? __ldg(col + j + 3 * s) : 0u;
+            const W w0 = __ldg(w + j);
+            const W w1 = p1 ? __ldg(w + j + s) : (W)0;
+            const W w2 = p2 ? __ldg(w + j + 2 * s) : (W)0;
+            const W w3 = p3 ? __ldg(w + j + 3 * s) : (W)0;
+            const V x0 = src[c0];
+            const V x1 = p1 ? src[c1] : (V)0;
+            const V x2 = p2 ? src[c2] : (V)0;
+            const V x3 = p3 ? src[c3] : (V)0;
             acc += (ACC)((V)w0 * x0);
             acc += (ACC)((V)w1 * x1);
             acc += (ACC)((V)w2 * x2);
             acc += (ACC)((V)w3 * x3);
             dsum += (uint64_t)w0 + (uint64_t)w1 + (uint64_t)w2 + (uint64_t)w3;
         }
-        for (; j < e; j += s) {
-            const W wt = __ldg(w + j);
-            acc += (ACC)((V)wt * src[__ldg(col + j)]);
-            dsum += (uint64_t)wt;
-        }
     } else {
-        for (; j + 3 * s < e; j += 4 * s) {
-            const uint32_t c0 = __ldg(col + j), c1 = __ldg(col + j + s), c2 = __ldg(col + j + 2 * s),
-                           c3 = __ldg(col + j + 3 * s);
-            const V x0 = src[c0], x1 = src[c1], x2 = src[c2], x3 = src[c3];
+        for (; j < e; j += 4 * s) {
+            const bool p1 = j + s < e, p2 = j + 2 * s < e, p3 = j + 3 * s < e;
+            const uint32_t c0 = __ldg(col + j);
+            const uint32_t c1 = p1 ? __ldg(col + j + s) : 0u;
+            const uint32_t c2 = p2 ? __ldg(col + j + 2 * s) : 0u;
+            const uint32_t c3 = p3 ? __ldg(col + j + 3 * s) : 0u;
+            const V x0 = src[c0];
+            const V x1 = p1 ? src[c1] : (V)0;
+            const V x2 = p2 ? src[c2] : (V)0;
+            const V x3 = p3 ? src[c3] : (V)0;
             acc += (ACC)x0;
             acc += (ACC)x1;
             acc += (ACC)x2;
             acc += (ACC)x3;
         }
-        for (; j < e; j += s) acc += (ACC)src[__ldg(col + j)];
     }
+}
+
+// first index i in [0, n] with pre[i] >= t (pre non-decreasing, pre[n] total)
+__device__ __forceinline__ uint32_t lower_bound_u32(const uint32_t *pre, uint32_t n, uint64_t t) {
+    uint32_t lo = 0, hi = n;
+    while (lo < hi) {
+        uint32_t mid = lo + ((hi - lo) >> 1);
+        if ((uint64_t)pre[mid] < t) lo = mid + 1;
+        else hi = mid;
+    }
+    return lo;
 }
 
 template <int G>
@@ -152,7 +175,7 @@ __device__ __forceinline__ void block_sum2(double &x, double &y, double *sm) {
 }
 
 template <int G, typename W, typename V>
-__global__ void __launch_bounds__(kPIThreads) k_power_iter(PIArgs a) {
+__global__ void __launch_bounds__(kPIThreads, 2) k_power_iter(PIArgs a) {
     cg::grid_group grid = cg::this_grid();
     // [0, 160): block_sum_d scratch (5 x 32), [200, 202): broadcast, [210, 226): warp maxima
     __shared__ double sm[256];
@@ -164,6 +187,12 @@ __global__ void __launch_bounds__(kPIThreads) k_power_iter(PIArgs a) {
     const uint64_t ngroups = ((uint64_t)gridDim.x * blockDim.x) / G;
     const uint32_t n_heavy = *a.n_heavy_ptr;
     const uint32_t T = a.heavy_T;
+    // this warp's rows: equal shares of the total row cost
+    const uint32_t gwarp = (uint32_t)(((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+    const uint32_t nwarps = (uint32_t)(((uint64_t)gridDim.x * blockDim.x) >> 5);
+    const uint64_t ctot = a.cpre[n];
+    const uint32_t w_r0 = lower_bound_u32(a.cpre, n, ctot * gwarp / nwarps);
+    const uint32_t w_r1 = gwarp + 1 == nwarps ? n : lower_bound_u32(a.cpre, n, ctot * (gwarp + 1) / nwarps);
     V *va = (V *)a.va, *vb = (V *)a.vb;
     double *part0 = a.partials, *part1 = a.partials + (size_t)gridDim.x * kNP;
 
@@ -268,9 +297,8 @@ __global__ void __launch_bounds__(kPIThreads) k_power_iter(PIArgs a) {
         if (!(fabs(dot - last) > a.tol && niter < a.iter_max)) break;
         if (a.stall_factor > 0 && niter > 2 && niter - best_at > a.stall_window) { stalled = 1; break; }
         double P[kNP] = {0, 0, 0, 0, 0};
-        // normal rows
-        for (uint64_t i64 = gid; i64 < n; i64 += ngroups) {
-            const uint32_t i = (uint32_t)i64;
+        // normal rows: this warp's cost-balanced contiguous range, G lanes per row
+        for (uint32_t i = w_r0 + (threadIdx.x & 31) / G; i < w_r1; i += 32 / G) {
             const uint32_t b = a.rp[i], e = a.rp[i + 1];
             if (e - b > T) continue;   // group-uniform
             V acc = 0;
@@ -398,8 +426,26 @@ __global__ void k_heavy_flags(uint32_t n, const uint32_t *rp, uint32_t T, uint8_
     if (i < n) f[i] = (rp[i + 1] - rp[i]) > T ? 1 : 0;
 }
 
+// per-row cost used to give every warp an equal share: entries plus a fixed
+// row overhead; heavy rows (handled by whole blocks) cost nothing here
+__global__ void k_row_cost(uint32_t n, const uint32_t *rp, uint32_t T, uint32_t shift, uint32_t *cost) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    uint32_t len = rp[i + 1] - rp[i];
+    cost[i] = len > T ? 0u : ((len + 8u) >> shift) + 1u;
+}
+
+static int pi_lanes(double avg) { return avg <= 4 ? 4 : avg <= 8 ? 8 : avg <= 16 ? 16 : 32; }
+
+static uint32_t pi_grid(const Context &C, uint32_t n, int G) {
+    const uint64_t maxg = (uint64_t)2 * C.num_sms;   // two resident blocks per SM (launch bounds)
+    const uint64_t want = cdiv((uint64_t)n * G, kPIThreads * 4ull);
+    uint32_t grid = (uint32_t)(want < maxg ? want : maxg);
+    return grid < 1 ? 1 : grid;
+}
+
 template <int G, typename W, typename V>
-static int launch_pi(Context &C, PIArgs &a, uint32_t work_groups) {
+static int launch_pi(Context &C, PIArgs &a, uint32_t grid) {
     const void *k = (const void *)k_power_iter<G, W, V>;
     int per_sm = 0;
     SGPB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, kPIThreads, 0));
@@ -407,11 +453,7 @@ static int launch_pi(Context &C, PIArgs &a, uint32_t work_groups) {
         set_error("power-iteration kernel does not fit on an SM");
         return SGP_B200_ERR_DEVICE;
     }
-    if (per_sm > 2) per_sm = 2;   // fewer blocks: cheaper barrier and partial reduction
-    uint64_t maxg = (uint64_t)per_sm * C.num_sms;
-    uint64_t want = cdiv((uint64_t)work_groups * G, kPIThreads * 4ull);
-    uint32_t grid = (uint32_t)(want < maxg ? want : maxg);
-    if (grid < 1) grid = 1;
+    if ((uint64_t)grid > (uint64_t)per_sm * C.num_sms) grid = per_sm * C.num_sms;
     SGPB_TRY(dalloc_t(C, &a.partials, (size_t)2 * grid * kNP));
     void *args[] = {&a};
     SGPB_CUDA(cudaLaunchCooperativeKernel(k, dim3(grid), dim3(kPIThreads), args, 0, C.stream));
@@ -420,20 +462,16 @@ static int launch_pi(Context &C, PIArgs &a, uint32_t work_groups) {
 }
 
 template <typename W, typename V>
-static int launch_pi_w(Context &C, PIArgs &a, double avg) {
-    if (avg <= 4) return launch_pi<4, W, V>(C, a, a.n);
-    if (avg <= 8) return launch_pi<8, W, V>(C, a, a.n);
-    if (avg <= 16) return launch_pi<16, W, V>(C, a, a.n);
-    return launch_pi<32, W, V>(C, a, a.n);
-}
-
-static uint32_t heavy_threshold(double avg) {
-    int G = avg <= 4 ? 4 : avg <= 8 ? 8 : avg <= 16 ? 16 : 32;
-    return (uint32_t)G * 64u;
+static int launch_pi_w(Context &C, PIArgs &a, int G, uint32_t grid) {
+    if (G == 4) return launch_pi<4, W, V>(C, a, grid);
+    if (G == 8) return launch_pi<8, W, V>(C, a, grid);
+    if (G == 16) return launch_pi<16, W, V>(C, a, grid);
+    return launch_pi<32, W, V>(C, a, grid);
 }
 
 static int run_pi(Context &C, const Level &L, PIArgs a, int mixed, double *res_d, double res_h[6], float *ms) {
-    const double avg = L.n ? (double)L.m / L.n : 0;
+    const int G = pi_lanes(L.n ? (double)L.m / L.n : 0);
+    const uint32_t grid = pi_grid(C, L.n, G);
     a.res = res_d;
     int rc;
     cudaEvent_t e0, e1;
@@ -446,15 +484,15 @@ static int run_pi(Context &C, const Level &L, PIArgs a, int mixed, double *res_d
         SGPB_TRY(dalloc_t(C, &va, L.n));
         SGPB_TRY(dalloc_t(C, &vb, L.n));
         a.va = va; a.vb = vb;
-        if (L.wbytes == 8) rc = launch_pi_w<unsigned long long, float>(C, a, avg);
-        else rc = launch_pi_w<uint32_t, float>(C, a, avg);
+        if (L.wbytes == 8) rc = launch_pi_w<unsigned long long, float>(C, a, G, grid);
+        else rc = launch_pi_w<uint32_t, float>(C, a, G, grid);
     } else {
         double *va, *vb;
         SGPB_TRY(dalloc_t(C, &va, L.n));
         SGPB_TRY(dalloc_t(C, &vb, L.n));
         a.va = va; a.vb = vb;
-        if (L.wbytes == 8) rc = launch_pi_w<unsigned long long, double>(C, a, avg);
-        else rc = launch_pi_w<uint32_t, double>(C, a, avg);
+        if (L.wbytes == 8) rc = launch_pi_w<unsigned long long, double>(C, a, G, grid);
+        else rc = launch_pi_w<uint32_t, double>(C, a, G, grid);
     }
     cudaEventRecord(e1, C.stream);
     if (rc != SGP_B200_OK) { cudaEventDestroy(e0); cudaEventDestroy(e1); return rc; }
@@ -478,16 +516,29 @@ int power_iter_level(Context &C, const Level &L, const double *x_in, const uint3
     PIArgs a;
     memset(&a, 0, sizeof(a));
     a.n = n; a.rp = L.rp; a.col = L.col; a.w = L.w;
-    a.heavy_T = heavy_threshold(avg);
+    // Rows longer than one warp's share of the entries (and than 64 G) are
+    // processed by a whole block; the rest are split into cost-balanced
+    // contiguous ranges, one per warp.
+    const int G = pi_lanes(avg);
+    const uint64_t nwarps = (uint64_t)pi_grid(C, n, G) * (kPIThreads / 32);
+    uint64_t T = L.m / nwarps;
+    if (T < 64ull * G) T = 64ull * G;
+    if (T > 0xFFFFFFFFull) T = 0xFFFFFFFFull;
+    a.heavy_T = (uint32_t)T;
     uint8_t *flags;
-    uint32_t *heavy, *nh;
+    uint32_t *heavy, *nh, *cost, *cpre;
     SGPB_TRY(dalloc_t(C, &flags, n));
     SGPB_TRY(dalloc_t(C, &heavy, (size_t)n + 1));
     SGPB_TRY(dalloc_t(C, &nh, 1));
+    SGPB_TRY(dalloc_t(C, &cost, (size_t)n + 1));
+    SGPB_TRY(dalloc_t(C, &cpre, (size_t)n + 1));
     k_heavy_flags<<<cdiv(n, 256), 256, 0, C.stream>>>(n, L.rp, a.heavy_T, flags);
-    C.kernel_launches++;
+    const uint32_t shift = (L.m + 9ull * n < 0xFFFFFFF0ull) ? 0u : 4u;   // keep the cost total in 32 bits
+    k_row_cost<<<cdiv(n, 256), 256, 0, C.stream>>>(n, L.rp, a.heavy_T, shift, cost);
+    C.kernel_launches += 2;
     SGPB_TRY(compact_flags(C, flags, n, heavy, nh));
-    a.heavy = heavy; a.n_heavy_ptr = nh;
+    SGPB_TRY(scan_u32(C, cost, cpre, n, nullptr));
+    a.heavy = heavy; a.n_heavy_ptr = nh; a.cpre = cpre;
     a.x_in = x_in; a.vcmap = vcmap; a.out = x_out;
     // the reference's cap (eigensolve_kokkos.h:153) is 1e14 / n, unbounded in
     // practice for small levels; a default budget of 5e6 iterations turns a
