@@ -40,6 +40,7 @@ struct PIArgs {
     const uint32_t *n_heavy_ptr;
     uint32_t heavy_T;
     const uint32_t *cpre;         // [n+1] prefix of per-row cost (0 for heavy rows): warp row ranges
+    const uint32_t *cpre_all;     // [n+1] prefix of per-row cost of all rows: block row ranges
     const double *x_in;
     const uint32_t *vcmap;
     void *va;
@@ -145,9 +146,8 @@ __device__ __forceinline__ void row_accum(const uint32_t *__restrict__ col, cons
     }
 }
 
-// first index i in [0, n] with pre[i] >= t (pre non-decreasing, pre[n] total)
-__device__ __forceinline__ uint32_t lower_bound_u32(const uint32_t *pre, uint32_t n, uint64_t t) {
-    uint32_t lo = 0, hi = n;
+// first index i in [lo, hi] with pre[i] >= t (pre non-decreasing)
+__device__ __forceinline__ uint32_t lower_bound_u32(const uint32_t *pre, uint32_t lo, uint32_t hi, uint64_t t) {
     while (lo < hi) {
         uint32_t mid = lo + ((hi - lo) >> 1);
         if ((uint64_t)pre[mid] < t) lo = mid + 1;
@@ -187,12 +187,20 @@ __global__ void __launch_bounds__(kPIThreads, 2) k_power_iter(PIArgs a) {
     const uint64_t ngroups = ((uint64_t)gridDim.x * blockDim.x) / G;
     const uint32_t n_heavy = *a.n_heavy_ptr;
     const uint32_t T = a.heavy_T;
-    // this warp's rows: equal shares of the total row cost
-    const uint32_t gwarp = (uint32_t)(((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5);
-    const uint32_t nwarps = (uint32_t)(((uint64_t)gridDim.x * blockDim.x) >> 5);
-    const uint64_t ctot = a.cpre[n];
-    const uint32_t w_r0 = lower_bound_u32(a.cpre, n, ctot * gwarp / nwarps);
-    const uint32_t w_r1 = gwarp + 1 == nwarps ? n : lower_bound_u32(a.cpre, n, ctot * (gwarp + 1) / nwarps);
+    // Work split, fixed for the whole launch: block b owns the rows whose
+    // cost prefix (all rows) starts in the b-th equal share; inside the block,
+    // heavy rows are processed by all threads and the remaining rows are cut
+    // into equal-cost contiguous ranges, one per warp.
+    const uint64_t call = a.cpre_all[n];
+    const uint32_t B0 = lower_bound_u32(a.cpre_all, 0, n, call * blockIdx.x / gridDim.x);
+    const uint32_t B1 = blockIdx.x + 1 == gridDim.x ? n
+                                                    : lower_bound_u32(a.cpre_all, 0, n, call * (blockIdx.x + 1) / gridDim.x);
+    const uint32_t h0 = lower_bound_u32(a.heavy, 0, n_heavy, B0);
+    const uint32_t h1 = lower_bound_u32(a.heavy, 0, n_heavy, B1);
+    const uint32_t wk = threadIdx.x >> 5, nwk = blockDim.x >> 5;
+    const uint64_t clo = a.cpre[B0], chi = a.cpre[B1];
+    const uint32_t w_r0 = lower_bound_u32(a.cpre, B0, B1, clo + (chi - clo) * wk / nwk);
+    const uint32_t w_r1 = wk + 1 == nwk ? B1 : lower_bound_u32(a.cpre, B0, B1, clo + (chi - clo) * (wk + 1) / nwk);
     V *va = (V *)a.va, *vb = (V *)a.vb;
     double *part0 = a.partials, *part1 = a.partials + (size_t)gridDim.x * kNP;
 
@@ -319,8 +327,8 @@ __global__ void __launch_bounds__(kPIThreads, 2) k_power_iter(PIArgs a) {
                 P[0] += rd; P[1] += rd * rd; P[2] += ui * rd; P[3] += ui; P[4] += ui * ui;
             }
         }
-        // heavy rows: one block per row
-        for (uint32_t h = blockIdx.x; h < n_heavy; h += gridDim.x) {
+        // heavy rows of this block's range: all threads on one row
+        for (uint32_t h = h0; h < h1; h++) {
             const uint32_t i = a.heavy[h];
             const uint32_t b = a.rp[i], e = a.rp[i + 1];
             double acc = 0;
@@ -428,11 +436,14 @@ __global__ void k_heavy_flags(uint32_t n, const uint32_t *rp, uint32_t T, uint8_
 
 // per-row cost used to give every warp an equal share: entries plus a fixed
 // row overhead; heavy rows (handled by whole blocks) cost nothing here
-__global__ void k_row_cost(uint32_t n, const uint32_t *rp, uint32_t T, uint32_t shift, uint32_t *cost) {
+__global__ void k_row_cost(uint32_t n, const uint32_t *rp, uint32_t T, uint32_t shift, uint32_t *cost,
+                           uint32_t *cost_all) {
     uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     uint32_t len = rp[i + 1] - rp[i];
-    cost[i] = len > T ? 0u : ((len + 8u) >> shift) + 1u;
+    uint32_t c = ((len + 8u) >> shift) + 1u;
+    cost[i] = len > T ? 0u : c;
+    cost_all[i] = c;
 }
 
 static int pi_lanes(double avg) { return avg <= 4 ? 4 : avg <= 8 ? 8 : avg <= 16 ? 16 : 32; }
@@ -526,19 +537,22 @@ int power_iter_level(Context &C, const Level &L, const double *x_in, const uint3
     if (T > 0xFFFFFFFFull) T = 0xFFFFFFFFull;
     a.heavy_T = (uint32_t)T;
     uint8_t *flags;
-    uint32_t *heavy, *nh, *cost, *cpre;
+    uint32_t *heavy, *nh, *cost, *cpre, *cost_all, *cpre_all;
     SGPB_TRY(dalloc_t(C, &flags, n));
     SGPB_TRY(dalloc_t(C, &heavy, (size_t)n + 1));
     SGPB_TRY(dalloc_t(C, &nh, 1));
     SGPB_TRY(dalloc_t(C, &cost, (size_t)n + 1));
     SGPB_TRY(dalloc_t(C, &cpre, (size_t)n + 1));
+    SGPB_TRY(dalloc_t(C, &cost_all, (size_t)n + 1));
+    SGPB_TRY(dalloc_t(C, &cpre_all, (size_t)n + 1));
     k_heavy_flags<<<cdiv(n, 256), 256, 0, C.stream>>>(n, L.rp, a.heavy_T, flags);
     const uint32_t shift = (L.m + 9ull * n < 0xFFFFFFF0ull) ? 0u : 4u;   // keep the cost total in 32 bits
-    k_row_cost<<<cdiv(n, 256), 256, 0, C.stream>>>(n, L.rp, a.heavy_T, shift, cost);
+    k_row_cost<<<cdiv(n, 256), 256, 0, C.stream>>>(n, L.rp, a.heavy_T, shift, cost, cost_all);
     C.kernel_launches += 2;
     SGPB_TRY(compact_flags(C, flags, n, heavy, nh));
     SGPB_TRY(scan_u32(C, cost, cpre, n, nullptr));
-    a.heavy = heavy; a.n_heavy_ptr = nh; a.cpre = cpre;
+    SGPB_TRY(scan_u32(C, cost_all, cpre_all, n, nullptr));
+    a.heavy = heavy; a.n_heavy_ptr = nh; a.cpre = cpre; a.cpre_all = cpre_all;
     a.x_in = x_in; a.vcmap = vcmap; a.out = x_out;
     // the reference's cap (eigensolve_kokkos.h:153) is 1e14 / n, unbounded in
     // practice for small levels; a default budget of 5e6 iterations turns a
