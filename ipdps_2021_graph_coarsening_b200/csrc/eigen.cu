@@ -16,12 +16,24 @@
 // Per-block partial sums are combined in a fixed order, so results are
 // reproducible run to run.
 //
-// Rows are processed by groups of G lanes (G from the level's mean degree);
-// rows longer than the heavy threshold by a whole block.  V is the vector
-// storage type: double (plain FP64) or float (mixed precision: FP32 storage,
-// gathers and row sums; FP64 reductions, deflation and normalisation).
+// SpMV mapping.  Block b owns an equal share of the rows' cost (entries plus
+// a per-row overhead).  Inside the block, rows longer than one warp's share
+// (and empty rows) are processed by all threads; the other rows are cut into
+// equal-cost contiguous ranges, one per warp, and each warp streams its
+// entries in tiles of 128 (four consecutive entries per lane, 16-byte vector
+// loads of destinations and weights), recovers row ids from a window of row
+// offsets in shared memory, and combines rows across lanes with a segmented
+// warp scan.  Every lane carries four entries whatever the row lengths, so
+// short-row graphs (grids, the finest R-MAT level) stream as well as dense
+// coarse levels.
+//
+// V is the vector storage type: double (plain FP64) or float (mixed
+// precision: FP32 storage, gathers and row sums; FP64 reductions, deflation,
+// normalisation and stopping test).
 #include <math.h>
 #include <string.h>
+
+#include <type_traits>
 
 #include "common.cuh"
 #include "internal.h"
@@ -29,18 +41,24 @@
 namespace sgpb {
 
 constexpr int kPIThreads = 512;
+constexpr int kPIWarps = kPIThreads / 32;
 constexpr int kNP = 5;
+constexpr int kTile = 128;        // entries per warp tile
+constexpr int kWin = kTile + 1;   // row offsets per window
 
 struct PIArgs {
     uint32_t n;
+    uint64_t m;
     const uint32_t *rp;
     const uint32_t *col;
     const void *w;
-    const uint32_t *heavy;        // rows with degree > heavy_T, ascending
+    int vec_ok;                   // col / w 16-byte aligned: vector loads allowed
+    const uint32_t *heavy;        // rows handled block-wide (long or empty), ascending
     const uint32_t *n_heavy_ptr;
     uint32_t heavy_T;
-    const uint32_t *cpre;         // [n+1] prefix of per-row cost (0 for heavy rows): warp row ranges
-    const uint32_t *cpre_all;     // [n+1] prefix of per-row cost of all rows: block row ranges
+    const uint32_t *cpre;         // [n+1] prefix of per-row cost, heavy rows 0: warp ranges
+    const uint32_t *cpre_all;     // [n+1] prefix of per-row cost of all rows: block ranges
+    double *deg;                  // [n] weighted degree (written in phase 0)
     const double *x_in;
     const uint32_t *vcmap;
     void *va;
@@ -49,7 +67,7 @@ struct PIArgs {
     double *partials;             // [2][gridDim][kNP]
     double tol;
     uint64_t iter_max;
-    double stall_factor;          // > 0: stop when |d dot| has not improved by this factor in stall_window iterations
+    double stall_factor;          // > 0: stop when |d dot| has not halved within stall_window iterations
     uint32_t stall_window;
     double *res;                  // [0] niter [1] dot [2] gb [3] lambda [4] capped [5] stalled
 };
@@ -58,9 +76,6 @@ __device__ __forceinline__ void grid_barrier(cg::grid_group &g) {
     if (gridDim.x == 1) __syncthreads();
     else g.sync();
 }
-
-template <typename V>
-__device__ __forceinline__ double vld(const V *p, uint32_t i) { return (double)p[i]; }
 
 // reduce per-block partials (all blocks compute the same totals, same order)
 __device__ __forceinline__ void reduce_partials(const double *part, double (&S)[kNP], double *sm) {
@@ -84,66 +99,15 @@ __device__ __forceinline__ void reduce_partials(const double *part, double (&S)[
     __syncthreads();
 }
 
-// Weighted degree of row i (sum of weights; row length for unit weights).
-template <int G, typename W>
-__device__ __forceinline__ double row_degree_group(const PIArgs &a, uint32_t i, uint32_t lane, unsigned gm) {
-    const uint32_t b = a.rp[i], e = a.rp[i + 1];
-    const W *w = (const W *)a.w;
-    if (!w) return (double)(e - b);
-    uint64_t s = 0;
-    for (uint32_t j = b + lane; j < e; j += G) s += (uint64_t)__ldg(w + j);
-#pragma unroll
-    for (int o = G / 2; o > 0; o >>= 1) s += __shfl_xor_sync(gm, s, o);
-    return (double)s;
-}
-
-// acc += sum_j w_j src[col_j] and dsum += sum_j w_j over j = j0, j0 + s, ... < e.
-// Four entries per lane are in flight (destination loads, weight loads, then
-// the four gathers), so a warp keeps 4x the memory requests outstanding of a
-// one-at-a-time loop; the summation order is fixed for a given stride.
-template <typename W, typename V, typename ACC>
-__device__ __forceinline__ void row_accum(const uint32_t *__restrict__ col, const W *__restrict__ w, const V *src,
-                                          uint32_t j, uint32_t e, uint32_t s, ACC &acc, uint64_t &dsum) {
-    // every trip issues up to four predicated entries, the last partial trip
-    // included, so a row costs ceil(len / 4s) dependent-load rounds
-    if (w) {
-        for (; j < e; j += 4 * s) {
-            const bool p1 = j + s < e, p2 = j + 2 * s < e, p3 = j + 3 * s < e;
-            const uint32_t c0 = __ldg(col + j);
-            const uint32_t c1 = p1 ? __ldg(col + j + s) : 0u;
-            const uint32_t c2 = p2 ? __ldg(col + j + 2 * s) : 0u;
-            const uint32_t c3 = p3 ? __ldg(col + j + 3 * s) : 0u;
-            const W w0 = __ldg(w + j);
-            const W w1 = p1 ? __ldg(w + j + s) : (W)0;
-            const W w2 = p2 ? __ldg(w + j + 2 * s) : (W)0;
-            const W w3 = p3 ? __ldg(w + j + 3 * s) : (W)0;
-            const V x0 = src[c0];
-            const V x1 = p1 ? src[c1] : (V)0;
-            const V x2 = p2 ? src[c2] : (V)0;
-            const V x3 = p3 ? src[c3] : (V)0;
-            acc += (ACC)((V)w0 * x0);
-            acc += (ACC)((V)w1 * x1);
-            acc += (ACC)((V)w2 * x2);
-            acc += (ACC)((V)w3 * x3);
-            dsum += (uint64_t)w0 + (uint64_t)w1 + (uint64_t)w2 + (uint64_t)w3;
-        }
-    } else {
-        for (; j < e; j += 4 * s) {
-            const bool p1 = j + s < e, p2 = j + 2 * s < e, p3 = j + 3 * s < e;
-            const uint32_t c0 = __ldg(col + j);
-            const uint32_t c1 = p1 ? __ldg(col + j + s) : 0u;
-            const uint32_t c2 = p2 ? __ldg(col + j + 2 * s) : 0u;
-            const uint32_t c3 = p3 ? __ldg(col + j + 3 * s) : 0u;
-            const V x0 = src[c0];
-            const V x1 = p1 ? src[c1] : (V)0;
-            const V x2 = p2 ? src[c2] : (V)0;
-            const V x3 = p3 ? src[c3] : (V)0;
-            acc += (ACC)x0;
-            acc += (ACC)x1;
-            acc += (ACC)x2;
-            acc += (ACC)x3;
-        }
-    }
+// block-wide deterministic sum of two values, result broadcast to all threads
+__device__ __forceinline__ void block_sum2(double &x, double &y, double *sm) {
+    double v[2] = {x, y};
+    block_sum_d<2>(v, sm);
+    if (threadIdx.x == 0) { sm[200] = v[0]; sm[201] = v[1]; }
+    __syncthreads();
+    x = sm[200];
+    y = sm[201];
+    __syncthreads();
 }
 
 // first index i in [lo, hi] with pre[i] >= t (pre non-decreasing)
@@ -156,41 +120,216 @@ __device__ __forceinline__ uint32_t lower_bound_u32(const uint32_t *pre, uint32_
     return lo;
 }
 
-template <int G>
-__device__ __forceinline__ unsigned pi_group_mask() {
-    if (G == 32) return 0xFFFFFFFFu;
+// acc += sum_j w_j src[col_j] over j = j0, j0 + s, ... < e, four predicated
+// entries in flight per thread (used for block-wide rows).
+template <typename W, typename V, typename ACC>
+__device__ __forceinline__ void row_accum(const uint32_t *__restrict__ col, const W *__restrict__ w, const V *src,
+                                          uint32_t j, uint32_t e, uint32_t s, ACC &acc) {
+    for (; j < e; j += 4 * s) {
+        const bool p1 = j + s < e, p2 = j + 2 * s < e, p3 = j + 3 * s < e;
+        const uint32_t c0 = __ldg(col + j);
+        const uint32_t c1 = p1 ? __ldg(col + j + s) : 0u;
+        const uint32_t c2 = p2 ? __ldg(col + j + 2 * s) : 0u;
+        const uint32_t c3 = p3 ? __ldg(col + j + 3 * s) : 0u;
+        V x0 = src[c0];
+        V x1 = p1 ? src[c1] : (V)0;
+        V x2 = p2 ? src[c2] : (V)0;
+        V x3 = p3 ? src[c3] : (V)0;
+        if (w) {
+            x0 *= (V)__ldg(w + j);
+            if (p1) x1 *= (V)__ldg(w + j + s);
+            if (p2) x2 *= (V)__ldg(w + j + 2 * s);
+            if (p3) x3 *= (V)__ldg(w + j + 3 * s);
+        }
+        acc += (ACC)x0;
+        acc += (ACC)x1;
+        acc += (ACC)x2;
+        acc += (ACC)x3;
+    }
+}
+
+// four consecutive destinations (and weights) starting at p
+template <typename W>
+__device__ __forceinline__ void load4(const uint32_t *__restrict__ col, const W *__restrict__ w, uint32_t p,
+                                      uint64_t m, bool vec, uint32_t (&c)[4], W (&wt)[4]) {
+    if (vec && (uint64_t)p + 3 < m) {
+        const uint4 v = __ldg(reinterpret_cast<const uint4 *>(col + p));
+        c[0] = v.x; c[1] = v.y; c[2] = v.z; c[3] = v.w;
+        if (w) {
+            if (sizeof(W) == 4) {
+                const uint4 q = __ldg(reinterpret_cast<const uint4 *>(w + p));
+                wt[0] = (W)q.x; wt[1] = (W)q.y; wt[2] = (W)q.z; wt[3] = (W)q.w;
+            } else {
+                const ulonglong2 q0 = __ldg(reinterpret_cast<const ulonglong2 *>(w + p));
+                const ulonglong2 q1 = __ldg(reinterpret_cast<const ulonglong2 *>(w + p + 2));
+                wt[0] = (W)q0.x; wt[1] = (W)q0.y; wt[2] = (W)q1.x; wt[3] = (W)q1.y;
+            }
+        }
+    } else {
+#pragma unroll
+        for (int k = 0; k < 4; k++) {
+            const bool ok = (uint64_t)p + k < m;
+            c[k] = ok ? __ldg(col + p + k) : 0u;
+            if (w) wt[k] = ok ? __ldg(w + p + k) : (W)0;
+        }
+    }
+}
+
+// Stream the rows [ra, rb) (all non-empty, none block-wide) through one warp.
+// fin(i, sum, unit_degree) is called exactly once per row, by one lane.
+// win: this warp's kWin-entry shared-memory window of row offsets.
+template <typename W, typename V, typename ACC, typename Fin>
+__device__ __forceinline__ void warp_stream(const uint32_t *__restrict__ rp, const uint32_t *__restrict__ col,
+                                            const W *__restrict__ w, const V *src, uint64_t m, bool vec,
+                                            uint32_t ra, uint32_t rb, uint32_t *win, Fin &fin) {
     const unsigned lane = threadIdx.x & 31;
-    return ((1u << G) - 1u) << (lane & ~(unsigned)(G - 1));
+    if (ra >= rb) return;
+    const uint32_t Ea = rp[ra], Eb = rp[rb];
+    uint32_t cur = ra;   // row holding the first entry of the tile
+    ACC carry = 0;       // its partial sum from earlier tiles
+    for (uint32_t c = Ea & ~3u; c < Eb; c += kTile) {
+        // window: win[j] = rp[cur + j] (clamped at rb); rows are non-empty, so
+        // the <= 128 entries of a tile lie in rows cur .. cur + 127
+#pragma unroll
+        for (int q = 0; q < 4; q++) {
+            const uint32_t r = cur + lane * 4 + q;
+            win[lane * 4 + q] = rp[r < rb ? r : rb];
+        }
+        if (lane == 0) {
+            const uint32_t r = cur + kTile;
+            win[kTile] = rp[r < rb ? r : rb];
+        }
+        const uint32_t p = c + 4 * lane;
+        uint32_t cc[4];
+        W ww[4];
+        load4<W>(col, w, p, m, vec, cc, ww);
+        V prod[4];
+        bool valid[4];
+#pragma unroll
+        for (int k = 0; k < 4; k++) {
+            valid[k] = (p + k >= Ea) && (p + k < Eb);
+            V x = valid[k] ? src[cc[k]] : (V)0;
+            prod[k] = w ? (V)ww[k] * x : x;
+        }
+        __syncwarp();
+        const uint32_t first = (Ea > c ? Ea : c);
+        const unsigned lane_first = (first - c) >> 2;
+        // row slot (offset from cur) of each valid entry
+        uint32_t slot[4] = {0, 0, 0, 0};
+        int nvalid = 0;
+        {
+            uint32_t s = 0;
+            bool have = false;
+#pragma unroll
+            for (int k = 0; k < 4; k++) {
+                if (!valid[k]) continue;
+                const uint32_t q = p + k;
+                if (!have) {
+                    uint32_t lo = 0, hi = kTile;   // largest j with win[j] <= q
+                    while (lo < hi) {
+                        uint32_t mid = (lo + hi + 1) >> 1;
+                        if (win[mid] <= q) lo = mid;
+                        else hi = mid - 1;
+                    }
+                    s = lo;
+                    have = true;
+                } else {
+                    while (s < kTile && win[s + 1] <= q) s++;
+                }
+                slot[k] = s;
+                nvalid++;
+            }
+        }
+        // lane-local runs: A = first run, B = last run, middle runs complete here
+        ACC A = 0, B = 0, run = 0;
+        uint32_t s0 = 0, s3 = 0, rs = 0;
+        bool started = false, multi = false;
+#pragma unroll
+        for (int k = 0; k < 4; k++) {
+            if (!valid[k]) continue;
+            if (!started) {
+                started = true;
+                rs = slot[k];
+                s0 = rs;
+                run = (ACC)prod[k];
+            } else if (slot[k] != rs) {
+                if (!multi) {
+                    A = run;
+                    multi = true;
+                } else {
+                    fin(cur + rs, run, (double)(win[rs + 1] - win[rs]));   // middle run
+                }
+                rs = slot[k];
+                run = (ACC)prod[k];
+            } else {
+                run += (ACC)prod[k];
+            }
+        }
+        s3 = rs;
+        B = run;
+        if (!multi) A = B;
+        if (lane == lane_first && nvalid) {
+            A += carry;
+            if (!multi) B = A;
+        }
+        // segmented inclusive scan over lanes of the last-run sums
+        const bool lv = nvalid > 0;
+        const uint32_t prev_s3 = __shfl_up_sync(0xFFFFFFFFu, s3, 1);
+        const int prev_v = __shfl_up_sync(0xFFFFFFFFu, (int)lv, 1);
+        const bool cont_prev = lv && lane > 0 && prev_v && lane != lane_first && prev_s3 == s0;
+        ACC S = lv ? B : (ACC)0;
+        int F = (!lv || multi || !cont_prev) ? 1 : 0;
+#pragma unroll
+        for (int d = 1; d < 32; d <<= 1) {
+            const ACC t = __shfl_up_sync(0xFFFFFFFFu, S, d);
+            const int tf = __shfl_up_sync(0xFFFFFFFFu, F, d);
+            if (lane >= (unsigned)d) {
+                if (!F) S += t;
+                F |= tf;
+            }
+        }
+        const ACC S_prev = __shfl_up_sync(0xFFFFFFFFu, S, 1);
+        const uint32_t next_s0 = __shfl_down_sync(0xFFFFFFFFu, s0, 1);
+        const int next_v = __shfl_down_sync(0xFFFFFFFFu, (int)lv, 1);
+        // first run of a multi-run lane ends here
+        if (lv && multi) {
+            ACC tot = A + (cont_prev ? S_prev : (ACC)0);
+            fin(cur + s0, tot, (double)(win[s0 + 1] - win[s0]));
+        }
+        // last run: ends here unless the next lane or the next tile continues it
+        const bool next_cont = lane < 31 && next_v && next_s0 == s3;
+        const bool tile_cont = lane == 31 && lv && win[s3 + 1] > c + kTile;
+        if (lv && !next_cont && !tile_cont) fin(cur + s3, S, (double)(win[s3 + 1] - win[s3]));
+        // next tile starts in row cur + s3 of lane 31 (continued) or the row after
+        const int tc = __shfl_sync(0xFFFFFFFFu, (int)tile_cont, 31);
+        const uint32_t s31 = __shfl_sync(0xFFFFFFFFu, s3, 31);
+        const ACC S31 = __shfl_sync(0xFFFFFFFFu, S, 31);
+        __syncwarp();
+        if (tc) {
+            cur += s31;
+            carry = S31;
+        } else {
+            cur += s31 + 1;
+            carry = 0;
+        }
+    }
 }
 
-// block-wide deterministic sum of two values, result broadcast to all threads
-__device__ __forceinline__ void block_sum2(double &x, double &y, double *sm) {
-    double v[2] = {x, y};
-    block_sum_d<2>(v, sm);
-    if (threadIdx.x == 0) { sm[200] = v[0]; sm[201] = v[1]; }
-    __syncthreads();
-    x = sm[200];
-    y = sm[201];
-    __syncthreads();
-}
-
-template <int G, typename W, typename V>
+template <typename W, typename V>
 __global__ void __launch_bounds__(kPIThreads, 2) k_power_iter(PIArgs a) {
     cg::grid_group grid = cg::this_grid();
     // [0, 160): block_sum_d scratch (5 x 32), [200, 202): broadcast, [210, 226): warp maxima
     __shared__ double sm[256];
+    __shared__ uint32_t swin[kPIWarps][kWin + 3];
+    typedef typename std::conditional<sizeof(V) == 8, double, float>::type ACC;
     const uint32_t n = a.n;
     const W *w = (const W *)a.w;
-    const unsigned gm = pi_group_mask<G>();
-    const uint32_t lane = threadIdx.x & (G - 1);
-    const uint64_t gid = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) / G;
-    const uint64_t ngroups = ((uint64_t)gridDim.x * blockDim.x) / G;
+    const unsigned lane = threadIdx.x & 31;
     const uint32_t n_heavy = *a.n_heavy_ptr;
-    const uint32_t T = a.heavy_T;
     // Work split, fixed for the whole launch: block b owns the rows whose
     // cost prefix (all rows) starts in the b-th equal share; inside the block,
-    // heavy rows are processed by all threads and the remaining rows are cut
-    // into equal-cost contiguous ranges, one per warp.
+    // block-wide rows are processed by all threads and the remaining rows are
+    // cut into equal-cost contiguous ranges, one per warp.
     const uint64_t call = a.cpre_all[n];
     const uint32_t B0 = lower_bound_u32(a.cpre_all, 0, n, call * blockIdx.x / gridDim.x);
     const uint32_t B1 = blockIdx.x + 1 == gridDim.x ? n
@@ -201,37 +340,49 @@ __global__ void __launch_bounds__(kPIThreads, 2) k_power_iter(PIArgs a) {
     const uint64_t clo = a.cpre[B0], chi = a.cpre[B1];
     const uint32_t w_r0 = lower_bound_u32(a.cpre, B0, B1, clo + (chi - clo) * wk / nwk);
     const uint32_t w_r1 = wk + 1 == nwk ? B1 : lower_bound_u32(a.cpre, B0, B1, clo + (chi - clo) * (wk + 1) / nwk);
+    const uint32_t wh0 = lower_bound_u32(a.heavy, h0, h1, w_r0);
+    const uint32_t wh1 = lower_bound_u32(a.heavy, h0, h1, w_r1);
     V *va = (V *)a.va, *vb = (V *)a.vb;
     double *part0 = a.partials, *part1 = a.partials + (size_t)gridDim.x * kNP;
+    const uint64_t gwarp = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
 
     // ---- phase 0a: prolongate / load the start vector, weighted degrees
     double p_sum = 0, p_maxd = 0;
-    for (uint64_t i64 = gid; i64 < n; i64 += ngroups) {
+    for (uint64_t i64 = gwarp; i64 < n; i64 += nwarps) {
         const uint32_t i = (uint32_t)i64;
-        const uint32_t deg = a.rp[i + 1] - a.rp[i];
-        double d = deg > T ? 0.0 : row_degree_group<G, W>(a, i, lane, gm);
+        const uint32_t b = a.rp[i], e = a.rp[i + 1];
+        double d = (double)(e - b);
+        if (w && e - b <= a.heavy_T) {
+            uint64_t s = 0;
+            for (uint32_t j = b + lane; j < e; j += 32) s += (uint64_t)__ldg(w + j);
+            d = (double)warp_sum(s);
+        }
         if (lane == 0) {
-            double x = a.vcmap ? a.x_in[a.vcmap[i]] : a.x_in[i];
-            V xs = (V)x;
+            const double x = a.vcmap ? a.x_in[a.vcmap[i]] : a.x_in[i];
+            const V xs = (V)x;
             va[i] = xs;
             p_sum += (double)xs;
-            if (deg <= T && d > p_maxd) p_maxd = d;
+            if (!w || e - b <= a.heavy_T) {
+                a.deg[i] = d;
+                if (d > p_maxd) p_maxd = d;
+            }
         }
     }
-    for (uint32_t h = blockIdx.x; h < n_heavy; h += gridDim.x) {
-        const uint32_t i = a.heavy[h];
-        const uint32_t b = a.rp[i], e = a.rp[i + 1];
-        double d;
-        if (!w) {
-            d = (double)(e - b);
-        } else {
-            double s = 0;
-            for (uint32_t j = b + threadIdx.x; j < e; j += blockDim.x) s += (double)__ldg(w + j);
-            double z = 0;
-            block_sum2(s, z, sm);
-            d = s;
+    if (w) {
+        for (uint32_t h = blockIdx.x; h < n_heavy; h += gridDim.x) {
+            const uint32_t i = a.heavy[h];
+            const uint32_t b = a.rp[i], e = a.rp[i + 1];
+            if (e - b <= a.heavy_T) continue;   // empty rows were done above (block-uniform)
+            uint64_t s = 0;
+            for (uint32_t j = b + threadIdx.x; j < e; j += blockDim.x) s += (uint64_t)__ldg(w + j);
+            double sd = (double)s, z = 0;
+            block_sum2(sd, z, sm);
+            if (threadIdx.x == 0) {
+                a.deg[i] = sd;
+                if (sd > p_maxd) p_maxd = sd;
+            }
         }
-        if (threadIdx.x == 0 && d > p_maxd) p_maxd = d;
     }
     {
         double v2[2] = {p_sum, 0};
@@ -249,17 +400,16 @@ __global__ void __launch_bounds__(kPIThreads, 2) k_power_iter(PIArgs a) {
     grid_barrier(grid);
     double S1 = 0, maxd = 0;
     {
-        const int lane32 = threadIdx.x & 31;
         if (threadIdx.x < 32) {
             double s = 0, m = 0;
-            for (uint32_t b = lane32; b < gridDim.x; b += 32) {
+            for (uint32_t b = lane; b < gridDim.x; b += 32) {
                 s += part0[(size_t)b * kNP + 0];
                 double x = part0[(size_t)b * kNP + 1];
                 m = x > m ? x : m;
             }
             s = warp_sum(s);
             m = warp_max(m);
-            if (lane32 == 0) { sm[0] = s; sm[1] = m; }
+            if (lane == 0) { sm[0] = s; sm[1] = m; }
         }
         __syncthreads();
         S1 = sm[0];
@@ -299,45 +449,40 @@ __global__ void __launch_bounds__(kPIThreads, 2) k_power_iter(PIArgs a) {
     double best_delta = 1e300;
     uint64_t best_at = 0;
     uint64_t niter = 0;
-    int stalled = 0;
     V *src = va, *dst = vb;
+    uint32_t *win = swin[wk];
     while (true) {
-        if (!(fabs(dot - last) > a.tol && niter < a.iter_max)) break;
-        if (a.stall_factor > 0 && niter > 2 && niter - best_at > a.stall_window) { stalled = 1; break; }
         double P[kNP] = {0, 0, 0, 0, 0};
-        // normal rows: this warp's cost-balanced contiguous range, G lanes per row
-        for (uint32_t i = w_r0 + (threadIdx.x & 31) / G; i < w_r1; i += 32 / G) {
-            const uint32_t b = a.rp[i], e = a.rp[i + 1];
-            if (e - b > T) continue;   // group-uniform
-            V acc = 0;
-            uint64_t dsum = 0;
-            row_accum<W, V, V>(a.col, w, src, b + lane, e, G, acc, dsum);
-#pragma unroll
-            for (int o = G / 2; o > 0; o >>= 1) {
-                acc += __shfl_xor_sync(gm, acc, o);
-                if (w) dsum += __shfl_xor_sync(gm, dsum, o);
+        // finalise row i from its sum of w_ij * src_j
+        auto fin = [&](uint32_t i, ACC acc, double d_unit) {
+            const double d = w ? a.deg[i] : d_unit;
+            const double ui = ((double)src[i] - mu) * inv_nu;
+            const double r = (gb - d) * ui + ((double)acc - mu * d) * inv_nu;
+            const V rs = (V)r;
+            dst[i] = rs;
+            const double rd = (double)rs;
+            P[0] += rd; P[1] += rd * rd; P[2] += ui * rd; P[3] += ui; P[4] += ui * ui;
+        };
+        // this warp's rows, in segments between block-wide rows
+        {
+            uint32_t seg = w_r0;
+            for (uint32_t h = wh0; h < wh1; h++) {
+                const uint32_t hr = a.heavy[h];
+                warp_stream<W, V, ACC>(a.rp, a.col, w, src, a.m, a.vec_ok, seg, hr, win, fin);
+                seg = hr + 1;
             }
-            if (lane == 0) {
-                const double d = w ? (double)dsum : (double)(e - b);
-                const double ui = ((double)src[i] - mu) * inv_nu;
-                const double r = (gb - d) * ui + ((double)acc - mu * d) * inv_nu;
-                const V rs = (V)r;
-                dst[i] = rs;
-                const double rd = (double)rs;
-                P[0] += rd; P[1] += rd * rd; P[2] += ui * rd; P[3] += ui; P[4] += ui * ui;
-            }
+            warp_stream<W, V, ACC>(a.rp, a.col, w, src, a.m, a.vec_ok, seg, w_r1, win, fin);
         }
-        // heavy rows of this block's range: all threads on one row
+        // block-wide rows of this block's range
         for (uint32_t h = h0; h < h1; h++) {
             const uint32_t i = a.heavy[h];
             const uint32_t b = a.rp[i], e = a.rp[i + 1];
             double acc = 0;
-            uint64_t dsum_i = 0;
-            row_accum<W, V, double>(a.col, w, src, b + threadIdx.x, e, blockDim.x, acc, dsum_i);
-            double dsum = (double)dsum_i;   // exact: weighted degrees stay below 2^53
-            block_sum2(acc, dsum, sm);
+            row_accum<W, V, double>(a.col, w, src, b + threadIdx.x, e, blockDim.x, acc);
+            double z = 0;
+            block_sum2(acc, z, sm);
             if (threadIdx.x == 0) {
-                const double d = w ? dsum : (double)(e - b);
+                const double d = w ? (e > b ? a.deg[i] : 0.0) : (double)(e - b);
                 const double ui = ((double)src[i] - mu) * inv_nu;
                 const double r = (gb - d) * ui + (acc - mu * d) * inv_nu;
                 const V rs = (V)r;
@@ -362,8 +507,9 @@ __global__ void __launch_bounds__(kPIThreads, 2) k_power_iter(PIArgs a) {
         niter++;
         const double delta = fabs(dot - last);
         if (niter > 2 && delta < best_delta * a.stall_factor) { best_delta = delta; best_at = niter; }
-        if (!(fabs(dot - last) > a.tol && niter < a.iter_max) ||
-            (a.stall_factor > 0 && niter > 2 && niter - best_at > a.stall_window)) {
+        const bool converged = !(delta > a.tol && niter < a.iter_max);
+        const bool stalled = a.stall_factor > 0 && niter > 2 && niter - best_at > a.stall_window;
+        if (converged || stalled) {
             // the reference returns u of the last iteration: (src - mu) / nu
             for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
                  i += (uint64_t)gridDim.x * blockDim.x)
@@ -374,20 +520,13 @@ __global__ void __launch_bounds__(kPIThreads, 2) k_power_iter(PIArgs a) {
                 a.res[2] = gb;
                 a.res[3] = (gb * S[4] - S[2]) / S[4];
                 a.res[4] = niter >= a.iter_max ? 1.0 : 0.0;
-                a.res[5] = (fabs(dot - last) > a.tol && niter < a.iter_max) ? 1.0 : 0.0;
+                a.res[5] = converged ? 0.0 : 1.0;
             }
             return;
         }
         mu = mu_n;
         inv_nu = inv_nu_n;
         V *t = src; src = dst; dst = t;
-    }
-    // loop exit before any iteration (not reachable: |0 - 1| > tol)
-    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
-        a.out[i] = ((double)src[i] - mu) * inv_nu;
-    if (blockIdx.x == 0 && threadIdx.x == 0) {
-        a.res[0] = (double)niter; a.res[1] = dot; a.res[2] = gb; a.res[3] = 0; a.res[4] = 0;
-        a.res[5] = stalled;
     }
 }
 
@@ -429,35 +568,37 @@ __global__ void k_sum_pairs(const double *part, uint32_t nb, double *out) {
     }
 }
 
+// block-wide rows: longer than T, or empty
 __global__ void k_heavy_flags(uint32_t n, const uint32_t *rp, uint32_t T, uint8_t *f) {
     uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < n) f[i] = (rp[i + 1] - rp[i]) > T ? 1 : 0;
+    if (i < n) {
+        uint32_t len = rp[i + 1] - rp[i];
+        f[i] = (len > T || len == 0) ? 1 : 0;
+    }
 }
 
-// per-row cost used to give every warp an equal share: entries plus a fixed
-// row overhead; heavy rows (handled by whole blocks) cost nothing here
+// per-row cost used to give every block and warp an equal share: entries
+// plus a fixed row overhead; block-wide rows cost nothing in the warp prefix
 __global__ void k_row_cost(uint32_t n, const uint32_t *rp, uint32_t T, uint32_t shift, uint32_t *cost,
                            uint32_t *cost_all) {
     uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     uint32_t len = rp[i + 1] - rp[i];
     uint32_t c = ((len + 8u) >> shift) + 1u;
-    cost[i] = len > T ? 0u : c;
+    cost[i] = (len > T || len == 0) ? 0u : c;
     cost_all[i] = c;
 }
 
-static int pi_lanes(double avg) { return avg <= 4 ? 4 : avg <= 8 ? 8 : avg <= 16 ? 16 : 32; }
-
-static uint32_t pi_grid(const Context &C, uint32_t n, int G) {
+static uint32_t pi_grid(const Context &C, uint64_t n, uint64_t m) {
     const uint64_t maxg = (uint64_t)2 * C.num_sms;   // two resident blocks per SM (launch bounds)
-    const uint64_t want = cdiv((uint64_t)n * G, kPIThreads * 4ull);
-    uint32_t grid = (uint32_t)(want < maxg ? want : maxg);
-    return grid < 1 ? 1 : grid;
+    const uint64_t want = cdiv(m + 8 * n, (uint64_t)kPIThreads * 64);
+    uint64_t grid = want < maxg ? want : maxg;
+    return (uint32_t)(grid < 1 ? 1 : grid);
 }
 
-template <int G, typename W, typename V>
+template <typename W, typename V>
 static int launch_pi(Context &C, PIArgs &a, uint32_t grid) {
-    const void *k = (const void *)k_power_iter<G, W, V>;
+    const void *k = (const void *)k_power_iter<W, V>;
     int per_sm = 0;
     SGPB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, kPIThreads, 0));
     if (per_sm < 1) {
@@ -472,38 +613,30 @@ static int launch_pi(Context &C, PIArgs &a, uint32_t grid) {
     return SGP_B200_OK;
 }
 
-template <typename W, typename V>
-static int launch_pi_w(Context &C, PIArgs &a, int G, uint32_t grid) {
-    if (G == 4) return launch_pi<4, W, V>(C, a, grid);
-    if (G == 8) return launch_pi<8, W, V>(C, a, grid);
-    if (G == 16) return launch_pi<16, W, V>(C, a, grid);
-    return launch_pi<32, W, V>(C, a, grid);
-}
-
 static int run_pi(Context &C, const Level &L, PIArgs a, int mixed, double *res_d, double res_h[6], float *ms) {
-    const int G = pi_lanes(L.n ? (double)L.m / L.n : 0);
-    const uint32_t grid = pi_grid(C, L.n, G);
+    const uint32_t grid = pi_grid(C, L.n, L.m);
     a.res = res_d;
     int rc;
     cudaEvent_t e0, e1;
     SGPB_CUDA(cudaEventCreate(&e0));
     SGPB_CUDA(cudaEventCreate(&e1));
-    // partials are allocated inside launch_pi; the events bracket the launch only
-    SGPB_CUDA(cudaEventRecord(e0, C.stream));
     if (mixed) {
         float *va, *vb;
         SGPB_TRY(dalloc_t(C, &va, L.n));
         SGPB_TRY(dalloc_t(C, &vb, L.n));
         a.va = va; a.vb = vb;
-        if (L.wbytes == 8) rc = launch_pi_w<unsigned long long, float>(C, a, G, grid);
-        else rc = launch_pi_w<uint32_t, float>(C, a, G, grid);
+        // partials are allocated inside launch_pi; the events bracket the launch
+        SGPB_CUDA(cudaEventRecord(e0, C.stream));
+        if (L.wbytes == 8) rc = launch_pi<unsigned long long, float>(C, a, grid);
+        else rc = launch_pi<uint32_t, float>(C, a, grid);
     } else {
         double *va, *vb;
         SGPB_TRY(dalloc_t(C, &va, L.n));
         SGPB_TRY(dalloc_t(C, &vb, L.n));
         a.va = va; a.vb = vb;
-        if (L.wbytes == 8) rc = launch_pi_w<unsigned long long, double>(C, a, G, grid);
-        else rc = launch_pi_w<uint32_t, double>(C, a, G, grid);
+        SGPB_CUDA(cudaEventRecord(e0, C.stream));
+        if (L.wbytes == 8) rc = launch_pi<unsigned long long, double>(C, a, grid);
+        else rc = launch_pi<uint32_t, double>(C, a, grid);
     }
     cudaEventRecord(e1, C.stream);
     if (rc != SGP_B200_OK) { cudaEventDestroy(e0); cudaEventDestroy(e1); return rc; }
@@ -523,17 +656,14 @@ int power_iter_level(Context &C, const Level &L, const double *x_in, const uint3
                      const PowerIterOpts &o, PowerIterResult *res, int want_residual) {
     const uint32_t n = L.n;
     if (n == 0) { *res = PowerIterResult(); return SGP_B200_OK; }
-    const double avg = (double)L.m / n;
     PIArgs a;
     memset(&a, 0, sizeof(a));
-    a.n = n; a.rp = L.rp; a.col = L.col; a.w = L.w;
-    // Rows longer than one warp's share of the entries (and than 64 G) are
-    // processed by a whole block; the rest are split into cost-balanced
-    // contiguous ranges, one per warp.
-    const int G = pi_lanes(avg);
-    const uint64_t nwarps = (uint64_t)pi_grid(C, n, G) * (kPIThreads / 32);
-    uint64_t T = L.m / nwarps;
-    if (T < 64ull * G) T = 64ull * G;
+    a.n = n; a.m = L.m; a.rp = L.rp; a.col = L.col; a.w = L.w;
+    a.vec_ok = (((uintptr_t)L.col | (uintptr_t)L.w) & 15u) == 0;
+    // rows longer than one warp's share of the cost are processed block-wide
+    const uint64_t nwarps = (uint64_t)pi_grid(C, n, L.m) * kPIWarps;
+    uint64_t T = (L.m + 8ull * n) / nwarps;
+    if (T < 4ull * kTile) T = 4ull * kTile;
     if (T > 0xFFFFFFFFull) T = 0xFFFFFFFFull;
     a.heavy_T = (uint32_t)T;
     uint8_t *flags;
@@ -545,6 +675,7 @@ int power_iter_level(Context &C, const Level &L, const double *x_in, const uint3
     SGPB_TRY(dalloc_t(C, &cpre, (size_t)n + 1));
     SGPB_TRY(dalloc_t(C, &cost_all, (size_t)n + 1));
     SGPB_TRY(dalloc_t(C, &cpre_all, (size_t)n + 1));
+    SGPB_TRY(dalloc_t(C, &a.deg, (size_t)n + 1));
     k_heavy_flags<<<cdiv(n, 256), 256, 0, C.stream>>>(n, L.rp, a.heavy_T, flags);
     const uint32_t shift = (L.m + 9ull * n < 0xFFFFFFF0ull) ? 0u : 4u;   // keep the cost total in 32 bits
     k_row_cost<<<cdiv(n, 256), 256, 0, C.stream>>>(n, L.rp, a.heavy_T, shift, cost, cost_all);
