@@ -31,6 +31,7 @@
 // precision: FP32 storage, gathers and row sums; FP64 reductions, deflation,
 // normalisation and stopping test).
 #include <math.h>
+#include <stdlib.h>
 #include <string.h>
 
 #include <type_traits>
@@ -148,29 +149,92 @@ __device__ __forceinline__ void row_accum(const uint32_t *__restrict__ col, cons
     }
 }
 
+// Streaming loads of the matrix (destinations, weights): read-only and read
+// once per iteration, so they bypass L1 allocation and leave L1 to the
+// gathered vector entries (NA = true).
+template <bool NA>
+__device__ __forceinline__ uint32_t ld_stream(const uint32_t *p) {
+    if (NA) {
+        uint32_t v;
+        asm("ld.global.nc.L1::no_allocate.u32 %0, [%1];" : "=r"(v) : "l"(p));
+        return v;
+    }
+    return __ldg(p);
+}
+template <bool NA>
+__device__ __forceinline__ unsigned long long ld_stream(const unsigned long long *p) {
+    if (NA) {
+        unsigned long long v;
+        asm("ld.global.nc.L1::no_allocate.u64 %0, [%1];" : "=l"(v) : "l"(p));
+        return v;
+    }
+    return __ldg(p);
+}
+
+// acc += sum_j w_j src[col_j] over the row entries j = j0, j0 + 32, ... < e of
+// one warp (j0 = row start + lane): U predicated entries in flight per lane,
+// destinations and weights first, then the U gathers.
+template <int U, bool NA, typename W, typename V, typename ACC>
+__device__ __forceinline__ void warp_row_accum(const uint32_t *__restrict__ col, const W *__restrict__ w,
+                                               const V *src, uint32_t j, uint32_t e, ACC &acc) {
+    for (; j < e; j += 32 * U) {
+        uint32_t c[U];
+        V x[U];
+#pragma unroll
+        for (int k = 0; k < U; k++) c[k] = (j + 32 * k < e) ? ld_stream<NA>(col + j + 32 * k) : 0u;
+        if (w) {
+            W wt[U];
+#pragma unroll
+            for (int k = 0; k < U; k++) wt[k] = (j + 32 * k < e) ? ld_stream<NA>(w + j + 32 * k) : (W)0;
+#pragma unroll
+            for (int k = 0; k < U; k++) x[k] = (j + 32 * k < e) ? (V)wt[k] * src[c[k]] : (V)0;
+        } else {
+#pragma unroll
+            for (int k = 0; k < U; k++) x[k] = (j + 32 * k < e) ? src[c[k]] : (V)0;
+        }
+#pragma unroll
+        for (int k = 0; k < U; k++) acc += (ACC)x[k];
+    }
+}
+
 // four consecutive destinations (and weights) starting at p
-template <typename W>
+template <bool NA>
+__device__ __forceinline__ uint4 ld_stream4(const uint32_t *p) {
+    if (NA) {
+        uint4 v;
+        asm("ld.global.nc.L1::no_allocate.v4.u32 {%0, %1, %2, %3}, [%4];"
+                     : "=r"(v.x), "=r"(v.y), "=r"(v.z), "=r"(v.w)
+                     : "l"(p));
+        return v;
+    }
+    return __ldg(reinterpret_cast<const uint4 *>(p));
+}
+
+template <bool NA, typename W>
 __device__ __forceinline__ void load4(const uint32_t *__restrict__ col, const W *__restrict__ w, uint32_t p,
                                       uint64_t m, bool vec, uint32_t (&c)[4], W (&wt)[4]) {
     if (vec && (uint64_t)p + 3 < m) {
-        const uint4 v = __ldg(reinterpret_cast<const uint4 *>(col + p));
+        const uint4 v = ld_stream4<NA>(col + p);
         c[0] = v.x; c[1] = v.y; c[2] = v.z; c[3] = v.w;
         if (w) {
             if (sizeof(W) == 4) {
-                const uint4 q = __ldg(reinterpret_cast<const uint4 *>(w + p));
+                const uint4 q = ld_stream4<NA>(reinterpret_cast<const uint32_t *>(w + p));
                 wt[0] = (W)q.x; wt[1] = (W)q.y; wt[2] = (W)q.z; wt[3] = (W)q.w;
             } else {
-                const ulonglong2 q0 = __ldg(reinterpret_cast<const ulonglong2 *>(w + p));
-                const ulonglong2 q1 = __ldg(reinterpret_cast<const ulonglong2 *>(w + p + 2));
-                wt[0] = (W)q0.x; wt[1] = (W)q0.y; wt[2] = (W)q1.x; wt[3] = (W)q1.y;
+                const uint4 q0 = ld_stream4<NA>(reinterpret_cast<const uint32_t *>(w + p));
+                const uint4 q1 = ld_stream4<NA>(reinterpret_cast<const uint32_t *>(w + p + 2));
+                wt[0] = (W)(((unsigned long long)q0.y << 32) | q0.x);
+                wt[1] = (W)(((unsigned long long)q0.w << 32) | q0.z);
+                wt[2] = (W)(((unsigned long long)q1.y << 32) | q1.x);
+                wt[3] = (W)(((unsigned long long)q1.w << 32) | q1.z);
             }
         }
     } else {
 #pragma unroll
         for (int k = 0; k < 4; k++) {
             const bool ok = (uint64_t)p + k < m;
-            c[k] = ok ? __ldg(col + p + k) : 0u;
-            if (w) wt[k] = ok ? __ldg(w + p + k) : (W)0;
+            c[k] = ok ? ld_stream<NA>(col + p + k) : 0u;
+            if (w) wt[k] = ok ? ld_stream<NA>(w + p + k) : (W)0;
         }
     }
 }
@@ -178,10 +242,11 @@ __device__ __forceinline__ void load4(const uint32_t *__restrict__ col, const W 
 // Stream the rows [ra, rb) (all non-empty, none block-wide) through one warp.
 // fin(i, sum, unit_degree) is called exactly once per row, by one lane.
 // win: this warp's kWin-entry shared-memory window of row offsets.
-template <typename W, typename V, typename ACC, typename Fin>
+template <bool NA, typename W, typename V, typename ACC, typename Fin>
 __device__ __forceinline__ void warp_stream(const uint32_t *__restrict__ rp, const uint32_t *__restrict__ col,
                                             const W *__restrict__ w, const V *src, uint64_t m, bool vec,
-                                            uint32_t ra, uint32_t rb, uint32_t *win, Fin &fin) {
+                                            uint32_t ra, uint32_t rb, const double *deg, uint32_t *win, V *winx,
+                                            double *wind, Fin &fin) {
     const unsigned lane = threadIdx.x & 31;
     if (ra >= rb) return;
     const uint32_t Ea = rp[ra], Eb = rp[rb];
@@ -189,11 +254,16 @@ __device__ __forceinline__ void warp_stream(const uint32_t *__restrict__ rp, con
     ACC carry = 0;       // its partial sum from earlier tiles
     for (uint32_t c = Ea & ~3u; c < Eb; c += kTile) {
         // window: win[j] = rp[cur + j] (clamped at rb); rows are non-empty, so
-        // the <= 128 entries of a tile lie in rows cur .. cur + 127
+        // the <= 128 entries of a tile lie in rows cur .. cur + 127.  The rows'
+        // own iterate values (and weighted degrees) are staged alongside, so
+        // finalising a row needs no dependent global load.
 #pragma unroll
         for (int q = 0; q < 4; q++) {
             const uint32_t r = cur + lane * 4 + q;
             win[lane * 4 + q] = rp[r < rb ? r : rb];
+            const uint32_t rr = r < rb ? r : rb - 1;
+            winx[lane * 4 + q] = src[rr];
+            if (w) wind[lane * 4 + q] = deg[rr];
         }
         if (lane == 0) {
             const uint32_t r = cur + kTile;
@@ -202,7 +272,7 @@ __device__ __forceinline__ void warp_stream(const uint32_t *__restrict__ rp, con
         const uint32_t p = c + 4 * lane;
         uint32_t cc[4];
         W ww[4];
-        load4<W>(col, w, p, m, vec, cc, ww);
+        load4<NA, W>(col, w, p, m, vec, cc, ww);
         V prod[4];
         bool valid[4];
 #pragma unroll
@@ -240,6 +310,10 @@ __device__ __forceinline__ void warp_stream(const uint32_t *__restrict__ rp, con
                 nvalid++;
             }
         }
+        // row slot s of this tile is complete with sum t
+        auto done = [&](uint32_t s, ACC t) {
+            fin(cur + s, t, w ? wind[s] : (double)(win[s + 1] - win[s]), (double)winx[s]);
+        };
         // lane-local runs: A = first run, B = last run, middle runs complete here
         ACC A = 0, B = 0, run = 0;
         uint32_t s0 = 0, s3 = 0, rs = 0;
@@ -257,7 +331,7 @@ __device__ __forceinline__ void warp_stream(const uint32_t *__restrict__ rp, con
                     A = run;
                     multi = true;
                 } else {
-                    fin(cur + rs, run, (double)(win[rs + 1] - win[rs]));   // middle run
+                    done(rs, run);   // middle run
                 }
                 rs = slot[k];
                 run = (ACC)prod[k];
@@ -292,14 +366,11 @@ __device__ __forceinline__ void warp_stream(const uint32_t *__restrict__ rp, con
         const uint32_t next_s0 = __shfl_down_sync(0xFFFFFFFFu, s0, 1);
         const int next_v = __shfl_down_sync(0xFFFFFFFFu, (int)lv, 1);
         // first run of a multi-run lane ends here
-        if (lv && multi) {
-            ACC tot = A + (cont_prev ? S_prev : (ACC)0);
-            fin(cur + s0, tot, (double)(win[s0 + 1] - win[s0]));
-        }
+        if (lv && multi) done(s0, A + (cont_prev ? S_prev : (ACC)0));
         // last run: ends here unless the next lane or the next tile continues it
         const bool next_cont = lane < 31 && next_v && next_s0 == s3;
         const bool tile_cont = lane == 31 && lv && win[s3 + 1] > c + kTile;
-        if (lv && !next_cont && !tile_cont) fin(cur + s3, S, (double)(win[s3 + 1] - win[s3]));
+        if (lv && !next_cont && !tile_cont) done(s3, S);
         // next tile starts in row cur + s3 of lane 31 (continued) or the row after
         const int tc = __shfl_sync(0xFFFFFFFFu, (int)tile_cont, 31);
         const uint32_t s31 = __shfl_sync(0xFFFFFFFFu, s3, 31);
@@ -315,12 +386,19 @@ __device__ __forceinline__ void warp_stream(const uint32_t *__restrict__ rp, con
     }
 }
 
-template <typename W, typename V>
+// MODE 0: normal rows streamed in warp tiles (short-row levels); MODE 4 / 8:
+// one warp per row with 4 / 8 loads in flight per lane (dense levels).
+// NA: matrix loads bypass L1 allocation.
+template <typename W, typename V, int MODE, bool NA>
 __global__ void __launch_bounds__(kPIThreads, 2) k_power_iter(PIArgs a) {
+    constexpr bool STREAM = MODE == 0;
     cg::grid_group grid = cg::this_grid();
     // [0, 160): block_sum_d scratch (5 x 32), [200, 202): broadcast, [210, 226): warp maxima
     __shared__ double sm[256];
     __shared__ uint32_t swin[kPIWarps][kWin + 3];
+    // per-row staging of the stream windows (unused by the warp-row variants)
+    __shared__ V swinx[STREAM ? kPIWarps : 1][kTile];
+    __shared__ double swind[STREAM ? kPIWarps : 1][kTile];
     typedef typename std::conditional<sizeof(V) == 8, double, float>::type ACC;
     const uint32_t n = a.n;
     const W *w = (const W *)a.w;
@@ -451,27 +529,47 @@ __global__ void __launch_bounds__(kPIThreads, 2) k_power_iter(PIArgs a) {
     uint64_t niter = 0;
     V *src = va, *dst = vb;
     uint32_t *win = swin[wk];
+    V *winx = swinx[STREAM ? wk : 0];
+    double *wind = swind[STREAM ? wk : 0];
     while (true) {
         double P[kNP] = {0, 0, 0, 0, 0};
-        // finalise row i from its sum of w_ij * src_j
-        auto fin = [&](uint32_t i, ACC acc, double d_unit) {
-            const double d = w ? a.deg[i] : d_unit;
-            const double ui = ((double)src[i] - mu) * inv_nu;
+        // finalise row i from its sum of w_ij * src_j, its weighted degree d
+        // and its own raw iterate value xi
+        auto fin = [&](uint32_t i, ACC acc, double d, double xi) {
+            const double ui = (xi - mu) * inv_nu;
             const double r = (gb - d) * ui + ((double)acc - mu * d) * inv_nu;
             const V rs = (V)r;
             dst[i] = rs;
             const double rd = (double)rs;
             P[0] += rd; P[1] += rd * rd; P[2] += ui * rd; P[3] += ui; P[4] += ui * ui;
         };
-        // this warp's rows, in segments between block-wide rows
-        {
+        // this warp's rows
+        if (STREAM) {
+            // in segments between block-wide rows
             uint32_t seg = w_r0;
             for (uint32_t h = wh0; h < wh1; h++) {
                 const uint32_t hr = a.heavy[h];
-                warp_stream<W, V, ACC>(a.rp, a.col, w, src, a.m, a.vec_ok, seg, hr, win, fin);
+                warp_stream<NA, W, V, ACC>(a.rp, a.col, w, src, a.m, a.vec_ok, seg, hr, a.deg, win, winx, wind, fin);
                 seg = hr + 1;
             }
-            warp_stream<W, V, ACC>(a.rp, a.col, w, src, a.m, a.vec_ok, seg, w_r1, win, fin);
+            warp_stream<NA, W, V, ACC>(a.rp, a.col, w, src, a.m, a.vec_ok, seg, w_r1, a.deg, win, winx, wind, fin);
+        } else {
+            uint32_t e = w_r0 < w_r1 ? a.rp[w_r0] : 0;
+            for (uint32_t i = w_r0; i < w_r1; i++) {
+                const uint32_t b = e;
+                e = a.rp[i + 1];
+                if (e - b > a.heavy_T || e == b) continue;   // block-wide rows
+                // issue the row's own loads before its entries so their latency overlaps
+                double xi = 0, d = (double)(e - b);
+                if (lane == 0) {
+                    xi = (double)src[i];
+                    if (w) d = a.deg[i];
+                }
+                ACC acc = 0;
+                warp_row_accum<(MODE == 8 ? 8 : 4), NA, W, V, ACC>(a.col, w, src, b + lane, e, acc);
+                acc = warp_sum(acc);
+                if (lane == 0) fin(i, acc, d, xi);
+            }
         }
         // block-wide rows of this block's range
         for (uint32_t h = h0; h < h1; h++) {
@@ -596,9 +694,43 @@ static uint32_t pi_grid(const Context &C, uint64_t n, uint64_t m) {
     return (uint32_t)(grid < 1 ? 1 : grid);
 }
 
+// mean degree above which a level uses one warp per row
+constexpr double kStreamMaxAvgDegree = 64.0;
+
+// SpMV variant of a level: SGPB_PI_MODE = stream | row4 | row8 overrides the
+// degree rule, SGPB_PI_NA = 0 | 1 the L1 policy of the matrix stream.
+struct PIVariant {
+    int mode;   // 0 stream, 4 / 8 warp rows
+    bool na;
+};
+static PIVariant pi_variant(const PIArgs &a) {
+    PIVariant v;
+    v.mode = (a.n && (double)a.m / a.n <= kStreamMaxAvgDegree) ? 0 : 4;
+    v.na = true;
+    if (const char *s = getenv("SGPB_PI_MODE")) {
+        if (!strcmp(s, "stream")) v.mode = 0;
+        else if (!strcmp(s, "row4")) v.mode = 4;
+        else if (!strcmp(s, "row8")) v.mode = 8;
+    }
+    if (const char *s = getenv("SGPB_PI_NA")) v.na = atoi(s) != 0;
+    return v;
+}
+
+template <typename W, typename V>
+static const void *pi_kernel(const PIVariant &v) {
+    if (v.na) {
+        if (v.mode == 0) return (const void *)k_power_iter<W, V, 0, true>;
+        if (v.mode == 8) return (const void *)k_power_iter<W, V, 8, true>;
+        return (const void *)k_power_iter<W, V, 4, true>;
+    }
+    if (v.mode == 0) return (const void *)k_power_iter<W, V, 0, false>;
+    if (v.mode == 8) return (const void *)k_power_iter<W, V, 8, false>;
+    return (const void *)k_power_iter<W, V, 4, false>;
+}
+
 template <typename W, typename V>
 static int launch_pi(Context &C, PIArgs &a, uint32_t grid) {
-    const void *k = (const void *)k_power_iter<W, V>;
+    const void *k = pi_kernel<W, V>(pi_variant(a));
     int per_sm = 0;
     SGPB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, kPIThreads, 0));
     if (per_sm < 1) {

@@ -152,8 +152,17 @@ def test_split_bit_exact(partitioner, graph, ties):
 
 
 # ------------------------------------------------------ power iteration --
+@pytest.fixture(params=["auto", "stream", "row4", "row8"])
+def spmv_variant(request, monkeypatch):
+    """Every SpMV variant of the power-iteration kernel (the default picks one
+    per level by mean degree; the others are forced here)."""
+    if request.param != "auto":
+        monkeypatch.setenv("SGPB_PI_MODE", request.param)
+    return request.param
+
+
 @pytest.mark.parametrize("weighted", [False, True])
-def test_power_iter_matches_oracle(partitioner, graph, weighted):
+def test_power_iter_matches_oracle(partitioner, graph, weighted, spmv_variant):
     rp, col, w = graph.row_ptr, graph.col, None
     if weighted:
         hn = O.hec_heavy(rp, col, None, True, 5)
