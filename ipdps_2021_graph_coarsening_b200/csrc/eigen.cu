@@ -71,6 +71,24 @@ struct PIArgs {
     double stall_factor;          // > 0: stop when |d dot| has not halved within stall_window iterations
     uint32_t stall_window;
     double *res;                  // [0] niter [1] dot [2] gb [3] lambda [4] capped [5] stalled
+    const uint32_t *inv;          // relabelled copy: new id -> level vertex id (null: identity)
+    uint32_t kcache;              // leading iterate entries kept in shared memory
+    int cache_ok;                 // host: use the shared-memory cache for this level
+};
+
+// dynamic shared memory for the iterate cache, per block (two blocks per SM)
+constexpr size_t kCacheBytesRows = 96 * 1024;
+constexpr size_t kCacheBytesStream = 48 * 1024;
+
+// The iterate as the SpMV gathers it: entries below k come from the block's
+// shared-memory copy (the most referenced vertices after hub-first
+// relabelling, or the whole vector of a small level), the rest from global.
+template <typename V>
+struct XView {
+    const V *g;
+    const V *s;
+    uint32_t k;
+    __device__ __forceinline__ V operator[](uint32_t c) const { return c < k ? s[c] : g[c]; }
 };
 
 __device__ __forceinline__ void grid_barrier(cg::grid_group &g) {
@@ -124,7 +142,7 @@ __device__ __forceinline__ uint32_t lower_bound_u32(const uint32_t *pre, uint32_
 // acc += sum_j w_j src[col_j] over j = j0, j0 + s, ... < e, four predicated
 // entries in flight per thread (used for block-wide rows).
 template <typename W, typename V, typename ACC>
-__device__ __forceinline__ void row_accum(const uint32_t *__restrict__ col, const W *__restrict__ w, const V *src,
+__device__ __forceinline__ void row_accum(const uint32_t *__restrict__ col, const W *__restrict__ w, const XView<V> &src,
                                           uint32_t j, uint32_t e, uint32_t s, ACC &acc) {
     for (; j < e; j += 4 * s) {
         const bool p1 = j + s < e, p2 = j + 2 * s < e, p3 = j + 3 * s < e;
@@ -176,7 +194,7 @@ __device__ __forceinline__ unsigned long long ld_stream(const unsigned long long
 // destinations and weights first, then the U gathers.
 template <int U, bool NA, typename W, typename V, typename ACC>
 __device__ __forceinline__ void warp_row_accum(const uint32_t *__restrict__ col, const W *__restrict__ w,
-                                               const V *src, uint32_t j, uint32_t e, ACC &acc) {
+                                               const XView<V> &src, uint32_t j, uint32_t e, ACC &acc) {
     for (; j < e; j += 32 * U) {
         uint32_t c[U];
         V x[U];
@@ -194,6 +212,91 @@ __device__ __forceinline__ void warp_row_accum(const uint32_t *__restrict__ col,
         }
 #pragma unroll
         for (int k = 0; k < U; k++) acc += (ACC)x[k];
+    }
+}
+
+// One warp, rows [r0, r1) one after another, 128-entry trips (4 per lane),
+// software-pipelined: the destinations and weights of the next trip (in the
+// same row or the next processed row) are loaded before the gathers of the
+// current trip, so DRAM latency overlaps the L2 gathers; a row's own value
+// and weighted degree are loaded with its first trip.  Rows for which
+// skip(len) holds are left out.  fin(i, sum, d, xi) on lane 0 once per row.
+template <bool NA, typename W, typename V, typename ACC, typename Skip, typename Fin>
+__device__ __forceinline__ void warp_rows_pipelined(const uint32_t *__restrict__ rp, const uint32_t *__restrict__ col,
+                                                    const W *__restrict__ w, const XView<V> &src, const double *deg,
+                                                    uint32_t r0, uint32_t r1, Skip skip, Fin &fin) {
+    const unsigned lane = threadIdx.x & 31;
+    // find the first processed row at or after i; returns r1 when none
+    auto advance = [&](uint32_t i, uint32_t &b, uint32_t &e) -> uint32_t {
+        for (; i < r1; i++) {
+            b = rp[i];
+            e = rp[i + 1];
+            if (!skip(e - b)) return i;
+        }
+        return r1;
+    };
+    uint32_t cb = 0, ce = 0;
+    uint32_t ci = advance(r0, cb, ce);
+    if (ci >= r1) return;
+    uint32_t cj = cb;   // base of the current trip
+    uint32_t c_cur[4];
+    W w_cur[4];
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+        const uint32_t j = cj + lane + 32 * k;
+        c_cur[k] = j < ce ? ld_stream<NA>(col + j) : 0u;
+        if (w) w_cur[k] = j < ce ? ld_stream<NA>(w + j) : (W)0;
+    }
+    double cx = 0, cd = 0;   // own value and weighted degree of row ci (lane 0)
+    if (lane == 0) {
+        cx = (double)src[ci];
+        cd = w ? deg[ci] : (double)(ce - cb);
+    }
+    ACC acc = 0;
+    while (true) {
+        // position of the next trip
+        uint32_t ni = ci, nb = cb, ne = ce, nj = cj + 128;
+        const bool row_ends = nj >= ce;
+        if (row_ends) {
+            ni = advance(ci + 1, nb, ne);
+            nj = nb;
+        }
+        const bool have_next = ni < r1;
+        uint32_t c_nxt[4];
+        W w_nxt[4];
+#pragma unroll
+        for (int k = 0; k < 4; k++) {
+            const uint32_t j = nj + lane + 32 * k;
+            const bool ok = have_next && j < ne;
+            c_nxt[k] = ok ? ld_stream<NA>(col + j) : 0u;
+            if (w) w_nxt[k] = ok ? ld_stream<NA>(w + j) : (W)0;
+        }
+        double nx = cx, nd = cd;
+        if (row_ends && have_next && lane == 0) {
+            nx = (double)src[ni];
+            nd = w ? deg[ni] : (double)(ne - nb);
+        }
+        // gathers of the current trip
+#pragma unroll
+        for (int k = 0; k < 4; k++) {
+            const bool ok = cj + lane + 32 * k < ce;
+            V x = ok ? src[c_cur[k]] : (V)0;
+            if (w) x *= (V)w_cur[k];
+            acc += (ACC)x;
+        }
+        if (row_ends) {
+            const ACC t = warp_sum(acc);
+            if (lane == 0) fin(ci, t, cd, cx);
+            acc = 0;
+        }
+        if (!have_next) break;
+        ci = ni; cb = nb; ce = ne; cj = nj;
+        cx = nx; cd = nd;
+#pragma unroll
+        for (int k = 0; k < 4; k++) {
+            c_cur[k] = c_nxt[k];
+            if (w) w_cur[k] = w_nxt[k];
+        }
     }
 }
 
@@ -244,7 +347,7 @@ __device__ __forceinline__ void load4(const uint32_t *__restrict__ col, const W 
 // win: this warp's kWin-entry shared-memory window of row offsets.
 template <bool NA, typename W, typename V, typename ACC, typename Fin>
 __device__ __forceinline__ void warp_stream(const uint32_t *__restrict__ rp, const uint32_t *__restrict__ col,
-                                            const W *__restrict__ w, const V *src, uint64_t m, bool vec,
+                                            const W *__restrict__ w, const XView<V> &src, uint64_t m, bool vec,
                                             uint32_t ra, uint32_t rb, const double *deg, uint32_t *win, V *winx,
                                             double *wind, Fin &fin) {
     const unsigned lane = threadIdx.x & 31;
@@ -387,7 +490,8 @@ __device__ __forceinline__ void warp_stream(const uint32_t *__restrict__ rp, con
 }
 
 // MODE 0: normal rows streamed in warp tiles (short-row levels); MODE 4 / 8:
-// one warp per row with 4 / 8 loads in flight per lane (dense levels).
+// one warp per row with 4 / 8 loads in flight per lane (dense levels);
+// MODE 5: one warp per row, trips software-pipelined across rows.
 // NA: matrix loads bypass L1 allocation.
 template <typename W, typename V, int MODE, bool NA>
 __global__ void __launch_bounds__(kPIThreads, 2) k_power_iter(PIArgs a) {
@@ -437,7 +541,8 @@ __global__ void __launch_bounds__(kPIThreads, 2) k_power_iter(PIArgs a) {
             d = (double)warp_sum(s);
         }
         if (lane == 0) {
-            const double x = a.vcmap ? a.x_in[a.vcmap[i]] : a.x_in[i];
+            const uint32_t o = a.inv ? a.inv[i] : i;
+            const double x = a.vcmap ? a.x_in[a.vcmap[o]] : a.x_in[o];
             const V xs = (V)x;
             va[i] = xs;
             p_sum += (double)xs;
@@ -531,8 +636,17 @@ __global__ void __launch_bounds__(kPIThreads, 2) k_power_iter(PIArgs a) {
     uint32_t *win = swin[wk];
     V *winx = swinx[STREAM ? wk : 0];
     double *wind = swind[STREAM ? wk : 0];
+    extern __shared__ __align__(16) unsigned char dyn_smem[];
+    V *xs = reinterpret_cast<V *>(dyn_smem);
+    const uint32_t kc = a.kcache < n ? a.kcache : n;
     while (true) {
         double P[kNP] = {0, 0, 0, 0, 0};
+        // refresh the shared-memory copy of the leading iterate entries
+        if (kc) {
+            for (uint32_t c = threadIdx.x; c < kc; c += blockDim.x) xs[c] = src[c];
+            __syncthreads();
+        }
+        const XView<V> xv{src, xs, kc};
         // finalise row i from its sum of w_ij * src_j, its weighted degree d
         // and its own raw iterate value xi
         auto fin = [&](uint32_t i, ACC acc, double d, double xi) {
@@ -549,10 +663,14 @@ __global__ void __launch_bounds__(kPIThreads, 2) k_power_iter(PIArgs a) {
             uint32_t seg = w_r0;
             for (uint32_t h = wh0; h < wh1; h++) {
                 const uint32_t hr = a.heavy[h];
-                warp_stream<NA, W, V, ACC>(a.rp, a.col, w, src, a.m, a.vec_ok, seg, hr, a.deg, win, winx, wind, fin);
+                warp_stream<NA, W, V, ACC>(a.rp, a.col, w, xv, a.m, a.vec_ok, seg, hr, a.deg, win, winx, wind, fin);
                 seg = hr + 1;
             }
-            warp_stream<NA, W, V, ACC>(a.rp, a.col, w, src, a.m, a.vec_ok, seg, w_r1, a.deg, win, winx, wind, fin);
+            warp_stream<NA, W, V, ACC>(a.rp, a.col, w, xv, a.m, a.vec_ok, seg, w_r1, a.deg, win, winx, wind, fin);
+        } else if (MODE == 5) {
+            const uint32_t T = a.heavy_T;
+            auto skip = [T](uint32_t len) { return len > T || len == 0; };
+            warp_rows_pipelined<NA, W, V, ACC>(a.rp, a.col, w, xv, a.deg, w_r0, w_r1, skip, fin);
         } else {
             uint32_t e = w_r0 < w_r1 ? a.rp[w_r0] : 0;
             for (uint32_t i = w_r0; i < w_r1; i++) {
@@ -566,7 +684,7 @@ __global__ void __launch_bounds__(kPIThreads, 2) k_power_iter(PIArgs a) {
                     if (w) d = a.deg[i];
                 }
                 ACC acc = 0;
-                warp_row_accum<(MODE == 8 ? 8 : 4), NA, W, V, ACC>(a.col, w, src, b + lane, e, acc);
+                warp_row_accum<(MODE == 8 ? 8 : 4), NA, W, V, ACC>(a.col, w, xv, b + lane, e, acc);
                 acc = warp_sum(acc);
                 if (lane == 0) fin(i, acc, d, xi);
             }
@@ -576,7 +694,7 @@ __global__ void __launch_bounds__(kPIThreads, 2) k_power_iter(PIArgs a) {
             const uint32_t i = a.heavy[h];
             const uint32_t b = a.rp[i], e = a.rp[i + 1];
             double acc = 0;
-            row_accum<W, V, double>(a.col, w, src, b + threadIdx.x, e, blockDim.x, acc);
+            row_accum<W, V, double>(a.col, w, xv, b + threadIdx.x, e, blockDim.x, acc);
             double z = 0;
             block_sum2(acc, z, sm);
             if (threadIdx.x == 0) {
@@ -611,7 +729,7 @@ __global__ void __launch_bounds__(kPIThreads, 2) k_power_iter(PIArgs a) {
             // the reference returns u of the last iteration: (src - mu) / nu
             for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
                  i += (uint64_t)gridDim.x * blockDim.x)
-                a.out[i] = ((double)src[i] - mu) * inv_nu;
+                a.out[a.inv ? a.inv[i] : i] = ((double)src[i] - mu) * inv_nu;
             if (blockIdx.x == 0 && threadIdx.x == 0) {
                 a.res[0] = (double)niter;
                 a.res[1] = dot;
@@ -711,6 +829,7 @@ static PIVariant pi_variant(const PIArgs &a) {
         if (!strcmp(s, "stream")) v.mode = 0;
         else if (!strcmp(s, "row4")) v.mode = 4;
         else if (!strcmp(s, "row8")) v.mode = 8;
+        else if (!strcmp(s, "rowp")) v.mode = 5;
     }
     if (const char *s = getenv("SGPB_PI_NA")) v.na = atoi(s) != 0;
     return v;
@@ -721,18 +840,28 @@ static const void *pi_kernel(const PIVariant &v) {
     if (v.na) {
         if (v.mode == 0) return (const void *)k_power_iter<W, V, 0, true>;
         if (v.mode == 8) return (const void *)k_power_iter<W, V, 8, true>;
+        if (v.mode == 5) return (const void *)k_power_iter<W, V, 5, true>;
         return (const void *)k_power_iter<W, V, 4, true>;
     }
     if (v.mode == 0) return (const void *)k_power_iter<W, V, 0, false>;
     if (v.mode == 8) return (const void *)k_power_iter<W, V, 8, false>;
+    if (v.mode == 5) return (const void *)k_power_iter<W, V, 5, false>;
     return (const void *)k_power_iter<W, V, 4, false>;
 }
 
 template <typename W, typename V>
 static int launch_pi(Context &C, PIArgs &a, uint32_t grid) {
-    const void *k = pi_kernel<W, V>(pi_variant(a));
+    const PIVariant var = pi_variant(a);
+    const void *k = pi_kernel<W, V>(var);
+    const size_t cache_bytes = var.mode == 0 ? kCacheBytesStream : kCacheBytesRows;
+    const uint64_t kmax = cache_bytes / sizeof(V);
+    // cache_ok: 1 = relabelled copy (cache its hub prefix), 2 = only when the
+    // whole iterate fits, 0 = off
+    a.kcache = (a.cache_ok == 1 || (a.cache_ok == 2 && a.n <= kmax)) ? (uint32_t)(a.n < kmax ? a.n : kmax) : 0u;
+    const size_t dyn = (size_t)a.kcache * sizeof(V);
+    SGPB_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)cache_bytes));
     int per_sm = 0;
-    SGPB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, kPIThreads, 0));
+    SGPB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, kPIThreads, dyn));
     if (per_sm < 1) {
         set_error("power-iteration kernel does not fit on an SM");
         return SGP_B200_ERR_DEVICE;
@@ -740,7 +869,7 @@ static int launch_pi(Context &C, PIArgs &a, uint32_t grid) {
     if ((uint64_t)grid > (uint64_t)per_sm * C.num_sms) grid = per_sm * C.num_sms;
     SGPB_TRY(dalloc_t(C, &a.partials, (size_t)2 * grid * kNP));
     void *args[] = {&a};
-    SGPB_CUDA(cudaLaunchCooperativeKernel(k, dim3(grid), dim3(kPIThreads), args, 0, C.stream));
+    SGPB_CUDA(cudaLaunchCooperativeKernel(k, dim3(grid), dim3(kPIThreads), args, dyn, C.stream));
     C.kernel_launches++;
     return SGP_B200_OK;
 }
@@ -784,12 +913,50 @@ static int run_pi(Context &C, const Level &L, PIArgs a, int mixed, double *res_d
     return SGP_B200_OK;
 }
 
-int power_iter_level(Context &C, const Level &L, const double *x_in, const uint32_t *vcmap, double *x_out,
+__global__ void k_max_deg(uint32_t n, const uint32_t *rp, uint32_t *out) {
+    uint32_t mx = 0;
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+        uint32_t d = rp[i + 1] - rp[i];
+        mx = d > mx ? d : mx;
+    }
+    mx = warp_max(mx);
+    if ((threadIdx.x & 31) == 0 && mx) atomicMax(out, mx);
+}
+
+int hub_first_copy(Context &C, const Level &L, uint32_t **perm_out, uint32_t **inv_out, Level *out);
+
+int power_iter_level(Context &C, const Level &Lin, const double *x_in, const uint32_t *vcmap, double *x_out,
                      const PowerIterOpts &o, PowerIterResult *res, int want_residual) {
-    const uint32_t n = L.n;
+    const uint32_t n = Lin.n;
     if (n == 0) { *res = PowerIterResult(); return SGP_B200_OK; }
     PIArgs a;
     memset(&a, 0, sizeof(a));
+    // Skewed levels too large to keep whole in shared memory iterate on a
+    // hub-first relabelled copy whose most referenced entries are cached.
+    a.cache_ok = 2;
+    Level L = Lin;
+    {
+        const double avg = (double)Lin.m / n;
+        bool relabel = o.allow_relabel && n > kCacheBytesRows / sizeof(double) && avg >= 8.0;
+        if (const char *s = getenv("SGPB_PI_RELABEL")) relabel = relabel && atoi(s) != 0;
+        if (relabel) {
+            uint32_t *mx, hmx = 0;
+            SGPB_TRY(dalloc_t(C, &mx, 1));
+            SGPB_TRY(dzero(C, mx, 4));
+            uint32_t blocks = cdiv(n, 256);
+            if (blocks > (uint32_t)C.num_sms * 8) blocks = C.num_sms * 8;
+            k_max_deg<<<blocks, 256, 0, C.stream>>>(n, Lin.rp, mx);
+            C.kernel_launches++;
+            SGPB_TRY(read_u32(C, mx, &hmx));
+            relabel = hmx >= 8.0 * avg;
+        }
+        if (relabel) {
+            uint32_t *perm = nullptr, *inv = nullptr;
+            SGPB_TRY(hub_first_copy(C, Lin, &perm, &inv, &L));
+            a.inv = inv;
+            a.cache_ok = 1;
+        }
+    }
     a.n = n; a.m = L.m; a.rp = L.rp; a.col = L.col; a.w = L.w;
     a.vec_ok = (((uintptr_t)L.col | (uintptr_t)L.w) & 15u) == 0;
     // rows longer than one warp's share of the cost are processed block-wide
@@ -863,12 +1030,14 @@ int power_iter_level(Context &C, const Level &L, const double *x_in, const uint3
         double *part, *out2;
         SGPB_TRY(dalloc_t(C, &part, 2 * (size_t)nb));
         SGPB_TRY(dalloc_t(C, &out2, 2));
-        if (L.wbytes == 8)
-            k_residual<unsigned long long><<<nb, 256, 0, C.stream>>>(n, L.rp, L.col, (const unsigned long long *)L.w,
-                                                                     x_out, res->lambda, part);
+        // the result is in the level's own numbering: use the level itself
+        if (Lin.wbytes == 8)
+            k_residual<unsigned long long><<<nb, 256, 0, C.stream>>>(n, Lin.rp, Lin.col,
+                                                                     (const unsigned long long *)Lin.w, x_out,
+                                                                     res->lambda, part);
         else
-            k_residual<uint32_t><<<nb, 256, 0, C.stream>>>(n, L.rp, L.col, (const uint32_t *)L.w, x_out, res->lambda,
-                                                           part);
+            k_residual<uint32_t><<<nb, 256, 0, C.stream>>>(n, Lin.rp, Lin.col, (const uint32_t *)Lin.w, x_out,
+                                                           res->lambda, part);
         k_sum_pairs<<<1, 32, 0, C.stream>>>(part, nb, out2);
         C.kernel_launches += 2;
         SGPB_CUDA(cudaGetLastError());

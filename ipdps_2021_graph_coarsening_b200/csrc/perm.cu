@@ -1,0 +1,123 @@
+// perm.cu -- hub-first relabelled copy of a level for the power iteration.
+//
+// Column references of power-law levels concentrate on few vertices (on the
+// first coarse level of an R-MAT graph the 16k most referenced vertices carry
+// ~3/4 of all entries).  The power iteration of such a level runs on a copy
+// P A P^T whose vertices are ordered by descending floor(log2(degree)),
+// stable in the original order, so the most gathered iterate entries form a
+// prefix that the kernel keeps in shared memory.  The hierarchy itself is not
+// relabelled; only the eigen-solve sees the copy, and it maps its start
+// vector in and its result out through the permutation.
+#include "common.cuh"
+#include "internal.h"
+
+namespace sgpb {
+
+constexpr int kBuckets = 33;       // floor(log2(deg)) + 1 for deg >= 1, 0 for deg == 0
+constexpr int kPermTile = 1024;    // rows per block of the stable scatter
+
+__device__ __forceinline__ uint32_t deg_key(uint32_t deg) {
+    // key 0 = highest degree class; ascending key = descending degree
+    const uint32_t b = deg ? 32u - __clz(deg) : 0u;   // 1..32, 0 for empty
+    return (uint32_t)(kBuckets - 1) - b;
+}
+
+__global__ void k_bucket_count(uint32_t n, const uint32_t *rp, uint32_t nb, uint32_t *cnt) {
+    __shared__ uint32_t c[kBuckets];
+    for (int k = threadIdx.x; k < kBuckets; k += blockDim.x) c[k] = 0;
+    __syncthreads();
+    const uint64_t t0 = (uint64_t)blockIdx.x * kPermTile;
+    for (uint64_t i = t0 + threadIdx.x; i < t0 + kPermTile && i < n; i += blockDim.x)
+        atomicAdd(&c[deg_key(rp[i + 1] - rp[i])], 1u);
+    __syncthreads();
+    for (int k = threadIdx.x; k < kBuckets; k += blockDim.x) cnt[(size_t)k * nb + blockIdx.x] = c[k];
+}
+
+// one thread per tile walks its rows in order: stable, deterministic
+__global__ void k_bucket_scatter(uint32_t n, const uint32_t *rp, uint32_t nb, const uint32_t *off, uint32_t *perm,
+                                 uint32_t *inv) {
+    const uint32_t blk = blockIdx.x * blockDim.x + threadIdx.x;
+    if (blk >= nb) return;
+    uint32_t pos[kBuckets];
+#pragma unroll
+    for (int k = 0; k < kBuckets; k++) pos[k] = off[(size_t)k * nb + blk];
+    const uint64_t t0 = (uint64_t)blk * kPermTile;
+    for (uint64_t i = t0; i < t0 + kPermTile && i < n; i++) {
+        const uint32_t k = deg_key(rp[i + 1] - rp[i]);
+        uint32_t p = 0;
+#pragma unroll
+        for (int q = 0; q < kBuckets; q++)
+            if (q == (int)k) p = pos[q]++;
+        perm[i] = p;
+        inv[p] = (uint32_t)i;
+    }
+}
+
+__global__ void k_perm_degrees(uint32_t n, const uint32_t *rp, const uint32_t *inv, uint32_t *deg) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) {
+        const uint32_t o = inv[i];
+        deg[i] = rp[o + 1] - rp[o];
+    }
+}
+
+template <typename W>
+__global__ void __launch_bounds__(256) k_perm_fill(uint32_t n, const uint32_t *__restrict__ rp,
+                                                  const uint32_t *__restrict__ col, const W *__restrict__ w,
+                                                  const uint32_t *__restrict__ perm, const uint32_t *__restrict__ inv,
+                                                  const uint32_t *__restrict__ nrp, uint32_t *__restrict__ ncol,
+                                                  W *__restrict__ nw) {
+    const unsigned lane = threadIdx.x & 31;
+    const uint64_t wid = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+    for (uint64_t i = wid; i < n; i += nwarps) {
+        const uint32_t o = inv[i];
+        const uint32_t b = rp[o], e = rp[o + 1], d = nrp[i];
+        for (uint32_t j = b + lane; j < e; j += 32) {
+            ncol[d + (j - b)] = perm[col[j]];
+            if (w) nw[d + (j - b)] = w[j];
+        }
+    }
+}
+
+template <typename W>
+static int fill_impl(Context &C, const Level &L, const uint32_t *perm, const uint32_t *inv, Level *out) {
+    W *nw = nullptr;
+    if (L.w) SGPB_TRY(dalloc_t(C, &nw, (size_t)L.m + 4));
+    uint32_t blocks = cdiv((uint64_t)L.n * 32, 256);
+    if (blocks > (uint32_t)C.num_sms * 16) blocks = C.num_sms * 16;
+    k_perm_fill<W><<<blocks ? blocks : 1, 256, 0, C.stream>>>(L.n, L.rp, L.col, (const W *)L.w, perm, inv, out->rp,
+                                                             out->col, nw);
+    C.kernel_launches++;
+    out->w = nw;
+    return SGP_B200_OK;
+}
+
+int hub_first_copy(Context &C, const Level &L, uint32_t **perm_out, uint32_t **inv_out, Level *out) {
+    const uint32_t n = L.n;
+    const uint32_t nb = cdiv(n, kPermTile);
+    uint32_t *cnt, *off, *perm, *inv, *deg;
+    SGPB_TRY(dalloc_t(C, &cnt, (size_t)nb * kBuckets + 1));
+    SGPB_TRY(dalloc_t(C, &off, (size_t)nb * kBuckets + 1));
+    SGPB_TRY(dalloc_t(C, &perm, n));
+    SGPB_TRY(dalloc_t(C, &inv, n));
+    SGPB_TRY(dalloc_t(C, &deg, (size_t)n + 1));
+    k_bucket_count<<<nb, 256, 0, C.stream>>>(n, L.rp, nb, cnt);
+    SGPB_TRY(scan_u32(C, cnt, off, nb * kBuckets, nullptr));
+    k_bucket_scatter<<<cdiv(nb, 64), 64, 0, C.stream>>>(n, L.rp, nb, off, perm, inv);
+    k_perm_degrees<<<cdiv(n, 256), 256, 0, C.stream>>>(n, L.rp, inv, deg);
+    C.kernel_launches += 3;
+    *out = L;
+    out->vcmap = nullptr;
+    SGPB_TRY(dalloc_t(C, &out->rp, (size_t)n + 1));
+    SGPB_TRY(dalloc_t(C, &out->col, (size_t)L.m + 4));
+    SGPB_TRY(scan_u32(C, deg, out->rp, n, nullptr));
+    if (L.wbytes == 8) SGPB_TRY(fill_impl<unsigned long long>(C, L, perm, inv, out));
+    else SGPB_TRY(fill_impl<uint32_t>(C, L, perm, inv, out));
+    SGPB_CUDA(cudaGetLastError());
+    *perm_out = perm;
+    *inv_out = inv;
+    return SGP_B200_OK;
+}
+
+}  // namespace sgpb

@@ -152,7 +152,7 @@ def test_split_bit_exact(partitioner, graph, ties):
 
 
 # ------------------------------------------------------ power iteration --
-@pytest.fixture(params=["auto", "stream", "row4", "row8"])
+@pytest.fixture(params=["auto", "stream", "row4", "row8", "rowp"])
 def spmv_variant(request, monkeypatch):
     """Every SpMV variant of the power-iteration kernel (the default picks one
     per level by mean degree; the others are forced here)."""
