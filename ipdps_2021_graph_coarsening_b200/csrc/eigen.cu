@@ -823,7 +823,7 @@ struct PIVariant {
 };
 static PIVariant pi_variant(const PIArgs &a) {
     PIVariant v;
-    v.mode = (a.n && (double)a.m / a.n <= kStreamMaxAvgDegree) ? 0 : 4;
+    v.mode = (a.n && (double)a.m / a.n <= kStreamMaxAvgDegree) ? 0 : 5;
     v.na = true;
     if (const char *s = getenv("SGPB_PI_MODE")) {
         if (!strcmp(s, "stream")) v.mode = 0;
@@ -937,8 +937,12 @@ int power_iter_level(Context &C, const Level &Lin, const double *x_in, const uin
     Level L = Lin;
     {
         const double avg = (double)Lin.m / n;
+        // Off unless SGPB_PI_RELABEL=1: with rows in degree order the warps at
+        // the tail get long runs of one-entry rows and the barrier waits for
+        // them (measured 3-4x slower on R-MAT levels 0 and 1).
         bool relabel = o.allow_relabel && n > kCacheBytesRows / sizeof(double) && avg >= 8.0;
-        if (const char *s = getenv("SGPB_PI_RELABEL")) relabel = relabel && atoi(s) != 0;
+        const char *rs = getenv("SGPB_PI_RELABEL");
+        relabel = relabel && rs && atoi(rs) != 0;
         if (relabel) {
             uint32_t *mx, hmx = 0;
             SGPB_TRY(dalloc_t(C, &mx, 1));
