@@ -235,6 +235,25 @@ int sgp_b200_power_iter(sgp_b200_ctx_t *ctx, uint32_t n, const uint32_t *row_ptr
 int sgp_b200_split(sgp_b200_ctx_t *ctx, uint32_t n, const uint32_t *row_ptr, const uint32_t *col,
                    const double *evec, int perc_imbalance, uint32_t *part, uint64_t *edgecut);
 
+/* Largest vertex count of sgp_b200_split_noalloc (its fixed scratch). */
+#define SGP_B200_NOALLOC_MAX_N (1u << 20)
+
+/* No counterpart in the reference.  The same median split and edge cut as
+ * sgp_b200_split, for callers that cannot allocate device memory at the time
+ * of the call (a host application that owns every device allocation through
+ * its own pool, code running in an out-of-memory handler, a plug-in whose
+ * host forbids allocation): it allocates nothing and uses a fixed scratch
+ * array inside the library (about 8 MiB per GPU, held until the process
+ * exits).  At most SGP_B200_NOALLOC_MAX_N vertices; larger graphs return
+ * SGP_B200_ERR_TOO_LARGE.  Asynchronous on `stream` (a cudaStream_t, NULL =
+ * default stream): part (n entries) and result (device array: result[0] =
+ * edge cut, result[1] = size of part 0) are valid once the stream has
+ * reached the call.  The first call on a device looks up the scratch address
+ * and should come before any stream capture.  All calls on a device share the
+ * scratch: calls that overlap on the GPU race and must be serialised. */
+int sgp_b200_split_noalloc(void *stream, uint32_t n, const uint32_t *row_ptr, const uint32_t *col,
+                           const double *evec, uint32_t *part, uint64_t *result);
+
 /* Milliseconds of the phases of the last sgp_b200_partition / eigensolve. */
 int sgp_b200_last_timing(sgp_b200_ctx_t *ctx, float *ms_total, float *ms_coarsen,
                          float *ms_eigen, float *ms_split);

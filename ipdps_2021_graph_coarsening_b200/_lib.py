@@ -91,6 +91,7 @@ _SIGS = {
                                     c_int, P(c_u64), P(c_dbl), P(c_dbl)]),
     "sgp_b200_split": (c_int, [c_vp, c_u32, c_vp, c_vp, c_vp, c_int, c_vp, P(c_u64)]),
     "sgp_b200_last_timing": (c_int, [c_vp, P(c_flt), P(c_flt), P(c_flt), P(c_flt)]),
+    "sgp_b200_split_noalloc": (c_int, [c_vp, c_u32, c_vp, c_vp, c_vp, c_vp, c_vp]),
 }
 
 _lib = None

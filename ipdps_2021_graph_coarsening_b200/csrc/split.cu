@@ -13,6 +13,8 @@
 // pass over the CSR counts the cut and the single sweep vertex of an odd n
 // (perc_imbalance_allowed = 0, the value the reference's driver passes,
 // sgpar.cpp:55) is decided on the device.
+#include <mutex>
+
 #include "common.cuh"
 #include "internal.h"
 
@@ -214,6 +216,55 @@ int split_level(Context &C, const Level &L, const double *evec, int perc_imbalan
     return SGP_B200_OK;
 }
 
+// --------------------------------------------------- split, no allocation --
+// Scratch of sgp_b200_split_noalloc: sort keys for SGP_B200_NOALLOC_MAX_N
+// vertices, the three digit histograms, per-block cut partials for up to
+// kNoAllocMaxBlocks blocks and the result words.  It is a file-scope device
+// array, so every GPU that loads this library holds it (about 8 MiB) until the
+// process exits, and every call on a device shares it.
+constexpr uint32_t kNoAllocMaxBlocks = 1024;
+constexpr size_t kNoAllocKeysBytes = (size_t)SGP_B200_NOALLOC_MAX_N * sizeof(unsigned long long);
+constexpr size_t kNoAllocHistOff = kNoAllocKeysBytes;
+constexpr size_t kNoAllocCutOff = kNoAllocHistOff + 768 * sizeof(uint32_t);
+constexpr size_t kNoAllocOutOff = kNoAllocCutOff + 2 * (size_t)kNoAllocMaxBlocks * sizeof(unsigned long long);
+constexpr size_t kNoAllocBytes = kNoAllocOutOff + 4 * sizeof(unsigned long long);
+static __device__ __align__(256) unsigned char g_split_scratch[kNoAllocBytes];
+
+// Per-device set-up, done once by the first call on that device: the host
+// address of g_split_scratch is only a stand-in, so the device address comes
+// from cudaGetSymbolAddress with the device current.
+struct NoAllocDevice {
+    unsigned char *scratch = nullptr;
+    int num_sms = 0;
+    int per_sm = 0;
+    bool ready = false;
+};
+static std::mutex g_noalloc_mu;
+static NoAllocDevice g_noalloc_dev[64];
+
+static int noalloc_setup(int device, NoAllocDevice **out) {
+    if (device < 0 || device >= 64) {
+        set_error("device %d out of range for the no-allocation entry point", device);
+        return SGP_B200_ERR_INVALID;
+    }
+    std::lock_guard<std::mutex> lock(g_noalloc_mu);
+    NoAllocDevice &d = g_noalloc_dev[device];
+    if (!d.ready) {
+        void *p = nullptr;
+        SGPB_CUDA(cudaGetSymbolAddress(&p, g_split_scratch));
+        SGPB_CUDA(cudaDeviceGetAttribute(&d.num_sms, cudaDevAttrMultiProcessorCount, device));
+        SGPB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&d.per_sm, (const void *)k_split, kSplitThreads, 0));
+        if (d.per_sm < 1) {
+            set_error("split kernel does not fit on an SM");
+            return SGP_B200_ERR_DEVICE;
+        }
+        d.scratch = (unsigned char *)p;
+        d.ready = true;
+    }
+    *out = &d;
+    return SGP_B200_OK;
+}
+
 // ------------------------------------------------------------- edge cut --
 __global__ void k_cut(uint32_t n, const uint32_t *rp, const uint32_t *col, const uint32_t *part,
                       unsigned long long *out) {
@@ -333,3 +384,62 @@ int induced_subgraphs(Context &C, const Level &L, const uint32_t *part, Level *g
 }
 
 }  // namespace sgpb
+
+using namespace sgpb;
+
+// Median split + edge cut of a device eigenvector without any allocation: the
+// scratch is g_split_scratch above.  Meant for callers that cannot allocate
+// device memory at that point: a host application that owns every device
+// allocation through its own pool, code running inside an out-of-memory
+// handler, or a plug-in whose allocation calls are forbidden by its host.
+// The first call on a device fetches the scratch address (see
+// noalloc_setup); make that first call before any stream capture.  Calls that
+// overlap on the GPU (different streams, or graphs replayed concurrently)
+// share the scratch and race; serialise them.
+extern "C" int sgp_b200_split_noalloc(void *stream, uint32_t n, const uint32_t *row_ptr, const uint32_t *col,
+                                      const double *evec, uint32_t *part, uint64_t *result) {
+    if (!row_ptr || !col || !evec || !part || !result) {
+        set_error("null argument");
+        return SGP_B200_ERR_INVALID;
+    }
+    if (n == 0 || n > SGP_B200_NOALLOC_MAX_N) {
+        set_error("sgp_b200_split_noalloc handles 1 .. %u vertices (its fixed scratch size); got %u",
+                  (unsigned)SGP_B200_NOALLOC_MAX_N, n);
+        return SGP_B200_ERR_TOO_LARGE;
+    }
+    int device = 0;
+    SGPB_CUDA(cudaGetDevice(&device));
+    NoAllocDevice *d = nullptr;
+    SGPB_TRY(noalloc_setup(device, &d));
+    cudaStream_t s = (cudaStream_t)stream;
+    SplitArgs a;
+    a.n = n;
+    a.rp = row_ptr;
+    a.col = col;
+    a.evec = evec;
+    a.part = part;
+    // sgpar.h:2009-2012 with perc_imbalance_allowed = 0
+    const uint32_t imbr = (uint32_t)ceil(n / 2.0);
+    const uint32_t imbl = n - imbr;
+    a.k = imbl < n ? imbl : n - 1;
+    a.sweep = imbr > imbl ? 1u : 0u;
+    a.keys = reinterpret_cast<unsigned long long *>(d->scratch);
+    a.hist = reinterpret_cast<uint32_t *>(d->scratch + kNoAllocHistOff);
+    a.cut_part = reinterpret_cast<unsigned long long *>(d->scratch + kNoAllocCutOff);
+    a.out = reinterpret_cast<unsigned long long *>(d->scratch + kNoAllocOutOff);
+    // the scratch keeps the previous call's contents: the histograms must
+    // start at zero; keys, partials and results are written before use
+    SGPB_CUDA(cudaMemsetAsync(a.hist, 0, 768 * sizeof(uint32_t), s));
+    const int per_sm = d->per_sm > 2 ? 2 : d->per_sm;
+    uint64_t grid = (uint64_t)per_sm * d->num_sms;
+    const uint64_t want = cdiv(n, kSplitThreads * 8ull);
+    if (want < grid) grid = want;
+    if (grid > kNoAllocMaxBlocks) grid = kNoAllocMaxBlocks;
+    if (grid < 1) grid = 1;
+    void *args[] = {&a};
+    SGPB_CUDA(cudaLaunchCooperativeKernel((const void *)k_split, dim3((unsigned)grid), dim3(kSplitThreads), args, 0, s));
+    // result[0] = edge cut, result[1] = size of part 0 (device array)
+    SGPB_CUDA(cudaMemcpyAsync(result, a.out, 2 * sizeof(uint64_t), cudaMemcpyDeviceToDevice, s));
+    SGPB_CUDA(cudaGetLastError());
+    return SGP_B200_OK;
+}
