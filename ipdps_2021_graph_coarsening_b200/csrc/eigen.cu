@@ -140,9 +140,10 @@ __device__ __forceinline__ uint32_t lower_bound_u32(const uint32_t *pre, uint32_
 }
 
 // acc += sum_j w_j src[col_j] over j = j0, j0 + s, ... < e, four predicated
-// entries in flight per thread (used for block-wide rows).
-template <typename W, typename V, typename ACC>
-__device__ __forceinline__ void row_accum(const uint32_t *__restrict__ col, const W *__restrict__ w, const XView<V> &src,
+// entries in flight per thread (used for block-wide rows).  S is the iterate
+// source: a plain pointer, or an XView when a shared-memory cache is in use.
+template <typename W, typename V, typename ACC, typename S>
+__device__ __forceinline__ void row_accum(const uint32_t *__restrict__ col, const W *__restrict__ w, const S &src,
                                           uint32_t j, uint32_t e, uint32_t s, ACC &acc) {
     for (; j < e; j += 4 * s) {
         const bool p1 = j + s < e, p2 = j + 2 * s < e, p3 = j + 3 * s < e;
@@ -189,12 +190,13 @@ __device__ __forceinline__ unsigned long long ld_stream(const unsigned long long
     return __ldg(p);
 }
 
-// acc += sum_j w_j src[col_j] over the row entries j = j0, j0 + 32, ... < e of
-// one warp (j0 = row start + lane): U predicated entries in flight per lane,
-// destinations and weights first, then the U gathers.
-template <int U, bool NA, typename W, typename V, typename ACC>
+// acc += sum_j w_j src[col_j] (and dsum += sum_j w_j) over the row entries
+// j = j0, j0 + 32, ... < e of one warp (j0 = row start + lane): U predicated
+// entries in flight per lane, destinations and weights first, then the U
+// gathers.
+template <int U, bool NA, typename W, typename V, typename ACC, typename S>
 __device__ __forceinline__ void warp_row_accum(const uint32_t *__restrict__ col, const W *__restrict__ w,
-                                               const XView<V> &src, uint32_t j, uint32_t e, ACC &acc) {
+                                               const S &src, uint32_t j, uint32_t e, ACC &acc, uint64_t &dsum) {
     for (; j < e; j += 32 * U) {
         uint32_t c[U];
         V x[U];
@@ -205,7 +207,10 @@ __device__ __forceinline__ void warp_row_accum(const uint32_t *__restrict__ col,
 #pragma unroll
             for (int k = 0; k < U; k++) wt[k] = (j + 32 * k < e) ? ld_stream<NA>(w + j + 32 * k) : (W)0;
 #pragma unroll
-            for (int k = 0; k < U; k++) x[k] = (j + 32 * k < e) ? (V)wt[k] * src[c[k]] : (V)0;
+            for (int k = 0; k < U; k++) {
+                x[k] = (j + 32 * k < e) ? (V)wt[k] * src[c[k]] : (V)0;
+                dsum += (uint64_t)wt[k];
+            }
         } else {
 #pragma unroll
             for (int k = 0; k < U; k++) x[k] = (j + 32 * k < e) ? src[c[k]] : (V)0;
@@ -221,9 +226,9 @@ __device__ __forceinline__ void warp_row_accum(const uint32_t *__restrict__ col,
 // current trip, so DRAM latency overlaps the L2 gathers; a row's own value
 // and weighted degree are loaded with its first trip.  Rows for which
 // skip(len) holds are left out.  fin(i, sum, d, xi) on lane 0 once per row.
-template <bool NA, typename W, typename V, typename ACC, typename Skip, typename Fin>
+template <bool NA, typename W, typename V, typename ACC, typename S, typename Skip, typename Fin>
 __device__ __forceinline__ void warp_rows_pipelined(const uint32_t *__restrict__ rp, const uint32_t *__restrict__ col,
-                                                    const W *__restrict__ w, const XView<V> &src, const double *deg,
+                                                    const W *__restrict__ w, const S &src, const double *deg,
                                                     uint32_t r0, uint32_t r1, Skip skip, Fin &fin) {
     const unsigned lane = threadIdx.x & 31;
     // find the first processed row at or after i; returns r1 when none
@@ -343,11 +348,11 @@ __device__ __forceinline__ void load4(const uint32_t *__restrict__ col, const W 
 }
 
 // Stream the rows [ra, rb) (all non-empty, none block-wide) through one warp.
-// fin(i, sum, unit_degree) is called exactly once per row, by one lane.
+// fin(i, sum, degree, own value) is called exactly once per row, by one lane.
 // win: this warp's kWin-entry shared-memory window of row offsets.
-template <bool NA, typename W, typename V, typename ACC, typename Fin>
+template <bool NA, typename W, typename V, typename ACC, typename S, typename Fin>
 __device__ __forceinline__ void warp_stream(const uint32_t *__restrict__ rp, const uint32_t *__restrict__ col,
-                                            const W *__restrict__ w, const XView<V> &src, uint64_t m, bool vec,
+                                            const W *__restrict__ w, const S &src, uint64_t m, bool vec,
                                             uint32_t ra, uint32_t rb, const double *deg, uint32_t *win, V *winx,
                                             double *wind, Fin &fin) {
     const unsigned lane = threadIdx.x & 31;
@@ -492,8 +497,15 @@ __device__ __forceinline__ void warp_stream(const uint32_t *__restrict__ rp, con
 // MODE 0: normal rows streamed in warp tiles (short-row levels); MODE 4 / 8:
 // one warp per row with 4 / 8 loads in flight per lane (dense levels);
 // MODE 5: one warp per row, trips software-pipelined across rows.
-// NA: matrix loads bypass L1 allocation.
-template <typename W, typename V, int MODE, bool NA>
+// NA: matrix loads bypass L1 allocation.  CACHE: gathers below kcache read the
+// block's shared-memory copy of the iterate.
+template <bool CACHE, typename V>
+__device__ __forceinline__ auto make_src(const V *g, const V *s, uint32_t k) {
+    if constexpr (CACHE) return XView<V>{g, s, k};
+    else return g;
+}
+
+template <typename W, typename V, int MODE, bool NA, bool CACHE>
 __global__ void __launch_bounds__(kPIThreads, 2) k_power_iter(PIArgs a) {
     constexpr bool STREAM = MODE == 0;
     cg::grid_group grid = cg::this_grid();
@@ -642,11 +654,11 @@ __global__ void __launch_bounds__(kPIThreads, 2) k_power_iter(PIArgs a) {
     while (true) {
         double P[kNP] = {0, 0, 0, 0, 0};
         // refresh the shared-memory copy of the leading iterate entries
-        if (kc) {
+        if (CACHE && kc) {
             for (uint32_t c = threadIdx.x; c < kc; c += blockDim.x) xs[c] = src[c];
             __syncthreads();
         }
-        const XView<V> xv{src, xs, kc};
+        const auto xv = make_src<CACHE, V>(src, xs, kc);
         // finalise row i from its sum of w_ij * src_j, its weighted degree d
         // and its own raw iterate value xi
         auto fin = [&](uint32_t i, ACC acc, double d, double xi) {
@@ -677,16 +689,15 @@ __global__ void __launch_bounds__(kPIThreads, 2) k_power_iter(PIArgs a) {
                 const uint32_t b = e;
                 e = a.rp[i + 1];
                 if (e - b > a.heavy_T || e == b) continue;   // block-wide rows
-                // issue the row's own loads before its entries so their latency overlaps
-                double xi = 0, d = (double)(e - b);
-                if (lane == 0) {
-                    xi = (double)src[i];
-                    if (w) d = a.deg[i];
-                }
+                // the row's own value is loaded before its entries so the
+                // latency overlaps; the weighted degree is summed on the way
+                const double xi = lane == 0 ? (double)src[i] : 0.0;
                 ACC acc = 0;
-                warp_row_accum<(MODE == 8 ? 8 : 4), NA, W, V, ACC>(a.col, w, xv, b + lane, e, acc);
+                uint64_t ds = 0;
+                warp_row_accum<(MODE == 8 ? 8 : 4), NA, W, V, ACC>(a.col, w, xv, b + lane, e, acc, ds);
                 acc = warp_sum(acc);
-                if (lane == 0) fin(i, acc, d, xi);
+                if (w) ds = warp_sum(ds);
+                if (lane == 0) fin(i, acc, w ? (double)ds : (double)(e - b), xi);
             }
         }
         // block-wide rows of this block's range
@@ -828,38 +839,29 @@ static PIVariant pi_variant(const PIArgs &a) {
     if (const char *s = getenv("SGPB_PI_MODE")) {
         if (!strcmp(s, "stream")) v.mode = 0;
         else if (!strcmp(s, "row4")) v.mode = 4;
-        else if (!strcmp(s, "row8")) v.mode = 8;
         else if (!strcmp(s, "rowp")) v.mode = 5;
     }
-    if (const char *s = getenv("SGPB_PI_NA")) v.na = atoi(s) != 0;
     return v;
 }
 
-template <typename W, typename V>
-static const void *pi_kernel(const PIVariant &v) {
-    if (v.na) {
-        if (v.mode == 0) return (const void *)k_power_iter<W, V, 0, true>;
-        if (v.mode == 8) return (const void *)k_power_iter<W, V, 8, true>;
-        if (v.mode == 5) return (const void *)k_power_iter<W, V, 5, true>;
-        return (const void *)k_power_iter<W, V, 4, true>;
-    }
-    if (v.mode == 0) return (const void *)k_power_iter<W, V, 0, false>;
-    if (v.mode == 8) return (const void *)k_power_iter<W, V, 8, false>;
-    if (v.mode == 5) return (const void *)k_power_iter<W, V, 5, false>;
-    return (const void *)k_power_iter<W, V, 4, false>;
+template <typename W, typename V, bool CACHE>
+static const void *pi_kernel_c(int mode) {
+    if (mode == 0) return (const void *)k_power_iter<W, V, 0, true, CACHE>;
+    if (mode == 5) return (const void *)k_power_iter<W, V, 5, true, CACHE>;
+    return (const void *)k_power_iter<W, V, 4, true, CACHE>;
 }
 
 template <typename W, typename V>
 static int launch_pi(Context &C, PIArgs &a, uint32_t grid) {
     const PIVariant var = pi_variant(a);
-    const void *k = pi_kernel<W, V>(var);
     const size_t cache_bytes = var.mode == 0 ? kCacheBytesStream : kCacheBytesRows;
     const uint64_t kmax = cache_bytes / sizeof(V);
     // cache_ok: 1 = relabelled copy (cache its hub prefix), 2 = only when the
     // whole iterate fits, 0 = off
     a.kcache = (a.cache_ok == 1 || (a.cache_ok == 2 && a.n <= kmax)) ? (uint32_t)(a.n < kmax ? a.n : kmax) : 0u;
+    const void *k = a.kcache ? pi_kernel_c<W, V, true>(var.mode) : pi_kernel_c<W, V, false>(var.mode);
     const size_t dyn = (size_t)a.kcache * sizeof(V);
-    SGPB_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)cache_bytes));
+    if (a.kcache) SGPB_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)cache_bytes));
     int per_sm = 0;
     SGPB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, kPIThreads, dyn));
     if (per_sm < 1) {
