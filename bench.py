@@ -262,11 +262,15 @@ def gpu_arm(args, rank: int, ws: int, local: int, distmod):
                for l, (nl, ml, it) in enumerate(zip(r.level_n, r.level_m, r.level_iters)))
     pi_ms = sum(r.level_pi_ms)
     achieved = byts / (pi_ms / 1e3) / 1e9 if pi_ms > 0 else 0.0
+    # DRAM bytes (read + write) of the step's power-iteration launches: the
+    # ratio of measured DRAM bytes to algorithmic bytes from one ncu capture of
+    # the kernel on a smaller level, applied to this step's algorithmic bytes
     traffic = None
     tf = os.path.join(ROOT, "profiles", "power_iter_traffic.json")
     if os.path.exists(tf):
         try:
-            traffic = json.load(open(tf)).get("dram_bytes_per_iteration_per_entry")
+            ratio = json.load(open(tf)).get("dram_to_algorithmic_ratio")
+            traffic = ratio * byts if ratio else None
         except (OSError, ValueError):
             traffic = None
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
