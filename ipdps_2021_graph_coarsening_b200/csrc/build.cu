@@ -412,6 +412,7 @@ int build_coarse_level(Context &C, const Level &F, const uint32_t *vcmap, uint32
     out->n = nc;
     out->rp = crp;
     out->wbytes = out_wbytes;
+    out->sorted = 1;
     if (F.wbytes == 8 && out_wbytes != 8) {
         set_error("coarse weights must be at least as wide as fine weights");
         return SGP_B200_ERR_INVALID;

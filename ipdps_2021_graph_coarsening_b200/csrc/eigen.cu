@@ -57,6 +57,10 @@ struct PIArgs {
     const uint32_t *heavy;        // rows handled block-wide (long or empty), ascending
     const uint32_t *n_heavy_ptr;
     uint32_t heavy_T;
+    const uint32_t *hseg;         // [n+1] prefix of the segment counts of block-wide rows (0 for the others)
+    const uint32_t *seg_row;      // row of each segment
+    double *hpart;                // sum of each segment
+    uint32_t seg_shift;           // segments of 2^seg_shift entries
     const uint32_t *cpre;         // [n+1] prefix of per-row cost, heavy rows 0: warp ranges
     const uint32_t *cpre_all;     // [n+1] prefix of per-row cost of all rows: block ranges
     double *deg;                  // [n] weighted degree (written in phase 0)
@@ -74,11 +78,26 @@ struct PIArgs {
     const uint32_t *inv;          // relabelled copy: new id -> level vertex id (null: identity)
     uint32_t kcache;              // leading iterate entries kept in shared memory
     int cache_ok;                 // host: use the shared-memory cache for this level
+    // column panels (mode 6): the warp rows' entries regrouped panel by panel
+    uint32_t P;                   // panels
+    uint32_t PW;                  // iterate entries per panel (one block's shared-memory copy)
+    const uint32_t *poff;         // [P*n+1] entry offsets, panel-major: panel p row i = [poff[p*n+i], poff[p*n+i+1])
+    const uint16_t *pcol;         // destination minus p*PW
+    const void *pw;               // weights (same width as w), null when unweighted
+    void *yacc;                   // [n] row sums over the panels so far (iterate type)
 };
 
 // dynamic shared memory for the iterate cache, per block (two blocks per SM)
 constexpr size_t kCacheBytesRows = 96 * 1024;
 constexpr size_t kCacheBytesStream = 48 * 1024;
+// dynamic shared memory for one column panel of the iterate, per block
+constexpr size_t kPanelBytes = 96 * 1024;
+constexpr uint32_t kMaxPanels = 31;
+// rows above one warp's share of the cost / kHeavyDiv* are cut into segments
+// of 2^kSegShift entries that the block's warps share
+constexpr uint64_t kHeavyDivRows = 8;
+constexpr uint64_t kHeavyDivStream = 64;
+constexpr uint32_t kSegShift = 10;
 
 // The iterate as the SpMV gathers it: entries below k come from the block's
 // shared-memory copy (the most referenced vertices after hub-first
@@ -499,6 +518,140 @@ __device__ __forceinline__ void warp_stream(const uint32_t *__restrict__ rp, con
 // MODE 5: one warp per row, trips software-pipelined across rows.
 // NA: matrix loads bypass L1 allocation.  CACHE: gathers below kcache read the
 // block's shared-memory copy of the iterate.
+// Destinations of four consecutive panel entries (16-bit, panel-relative).
+template <bool NA>
+__device__ __forceinline__ void ld_pcol4(const uint16_t *p, uint32_t (&c)[4]) {
+    uint32_t lo, hi;
+    if (NA) {
+        asm("ld.global.nc.L1::no_allocate.v2.u32 {%0, %1}, [%2];" : "=r"(lo), "=r"(hi) : "l"(p));
+    } else {
+        const uint2 v = __ldg(reinterpret_cast<const uint2 *>(p));
+        lo = v.x; hi = v.y;
+    }
+    c[0] = lo & 0xFFFFu; c[1] = lo >> 16; c[2] = hi & 0xFFFFu; c[3] = hi >> 16;
+}
+
+// One warp, the up to 32 rows [g, g + gl) restricted to one column panel:
+// each row's sum of w_ij * x_j over its entries in the panel (x_j read from
+// the block's shared-memory copy xs of the panel) is added to yacc[row], or
+// stored there on the first panel.  Entries are taken 128 per trip, four
+// consecutive ones per lane; a trip's per-row sums are formed by runs inside
+// each lane and a segmented scan across lanes, and each row slot receives at
+// most one addition per trip, so the order of additions is fixed by the data.
+// win: 33 words of this warp's shared memory; ysm: 32 accumulators.
+template <bool NA, typename W, typename V, typename ACC>
+__device__ __forceinline__ void panel_rows32(const uint32_t *__restrict__ offp, const uint16_t *__restrict__ pcol,
+                                             const W *__restrict__ pw, const V *xs, uint32_t g, uint32_t gl,
+                                             bool first, uint32_t *win, ACC *ysm, ACC *yacc) {
+    const unsigned lane = threadIdx.x & 31;
+    win[lane] = offp[g + (lane < gl ? lane : gl)];
+    if (lane == 0) win[32] = offp[g + gl];
+    ysm[lane] = (ACC)0;
+    const ACC yprev = (!first && lane < gl) ? yacc[g + lane] : (ACC)0;
+    __syncwarp();
+    const uint32_t E0 = win[0], E1 = win[32];
+    for (uint32_t c = E0 & ~3u; c < E1; c += 128) {
+        const uint32_t q0 = c + 4 * lane;
+        uint32_t cc[4] = {0, 0, 0, 0};
+        W ww[4] = {0, 0, 0, 0};
+        if (q0 < E1) {
+            ld_pcol4<NA>(pcol + q0, cc);
+            if (pw) {
+                if (sizeof(W) == 4) {
+                    const uint4 v = ld_stream4<NA>(reinterpret_cast<const uint32_t *>(pw + q0));
+                    ww[0] = (W)v.x; ww[1] = (W)v.y; ww[2] = (W)v.z; ww[3] = (W)v.w;
+                } else {
+#pragma unroll
+                    for (int k = 0; k < 4; k++) ww[k] = ld_stream<NA>(pw + q0 + k);
+                }
+            }
+        }
+        bool valid[4];
+        V prod[4];
+#pragma unroll
+        for (int k = 0; k < 4; k++) {
+            valid[k] = q0 + k >= E0 && q0 + k < E1;
+            const V x = xs[valid[k] ? cc[k] : 0u];   // entries outside the group may be padding
+            prod[k] = valid[k] ? (pw ? (V)ww[k] * x : x) : (V)0;
+        }
+        // row slot of each valid entry: the last s with win[s] <= q (empty
+        // rows share their start with the next row, so they are passed over)
+        uint32_t sl[4] = {0, 0, 0, 0};
+        {
+            uint32_t s = 0;
+            bool have = false;
+#pragma unroll
+            for (int k = 0; k < 4; k++) {
+                if (!valid[k]) continue;
+                const uint32_t q = q0 + k;
+                if (!have) {
+                    uint32_t lo = 0, hi = gl - 1;
+                    while (lo < hi) {
+                        const uint32_t mid = (lo + hi + 1) >> 1;
+                        if (win[mid] <= q) lo = mid;
+                        else hi = mid - 1;
+                    }
+                    s = lo;
+                    have = true;
+                } else {
+                    while (win[s + 1] <= q) s++;
+                }
+                sl[k] = s;
+            }
+        }
+        // runs of equal slots inside the lane: the first (hs, A) and the last
+        // (ts, B); runs in between belong to rows that start and end here
+        ACC A = 0, B = 0, run = 0;
+        uint32_t hs = 0xFFFFFFFEu, ts = 0xFFFFFFFFu, rs = 0;
+        bool lv = false, multi = false;
+#pragma unroll
+        for (int k = 0; k < 4; k++) {
+            if (!valid[k]) continue;
+            if (!lv) {
+                lv = true;
+                rs = hs = sl[k];
+                run = (ACC)prod[k];
+            } else if (sl[k] != rs) {
+                if (!multi) {
+                    A = run;
+                    multi = true;
+                } else {
+                    ysm[rs] += run;
+                }
+                rs = sl[k];
+                run = (ACC)prod[k];
+            } else {
+                run += (ACC)prod[k];
+            }
+        }
+        if (lv) { ts = rs; B = run; }
+        // segmented inclusive scan of the last runs across lanes: a lane
+        // continues its predecessor when its first slot is the predecessor's
+        // last slot and it holds a single run
+        const uint32_t prev_ts = __shfl_up_sync(0xFFFFFFFFu, ts, 1);
+        const bool cont_prev = lv && lane > 0 && prev_ts == hs;
+        ACC S = lv ? B : (ACC)0;
+        int F = (!lv || multi || !cont_prev) ? 1 : 0;
+#pragma unroll
+        for (int d = 1; d < 32; d <<= 1) {
+            const ACC t = __shfl_up_sync(0xFFFFFFFFu, S, d);
+            const int tf = __shfl_up_sync(0xFFFFFFFFu, F, d);
+            if (lane >= (unsigned)d) {
+                if (!F) S += t;
+                F |= tf;
+            }
+        }
+        const ACC Sprev = __shfl_up_sync(0xFFFFFFFFu, S, 1);
+        const uint32_t next_hs = __shfl_down_sync(0xFFFFFFFFu, hs, 1);
+        const bool cont_next = lane < 31 && next_hs == ts;
+        if (multi) ysm[hs] += A + (cont_prev ? Sprev : (ACC)0);
+        if (lv && !cont_next) ysm[ts] += S;
+        __syncwarp();
+    }
+    if (lane < gl) yacc[g + lane] = yprev + ysm[lane];
+    __syncwarp();
+}
+
 template <bool CACHE, typename V>
 __device__ __forceinline__ auto make_src(const V *g, const V *s, uint32_t k) {
     if constexpr (CACHE) return XView<V>{g, s, k};
@@ -516,6 +669,14 @@ __global__ void __launch_bounds__(kPIThreads, 2) k_power_iter(PIArgs a) {
     __shared__ V swinx[STREAM ? kPIWarps : 1][kTile];
     __shared__ double swind[STREAM ? kPIWarps : 1][kTile];
     typedef typename std::conditional<sizeof(V) == 8, double, float>::type ACC;
+    // panels: per-warp row sums of a 32-row group, group counters (two, used
+    // by alternate panels so one can be reset while the other is in use)
+    constexpr bool PANEL = MODE == 6;
+    __shared__ ACC sysm[PANEL ? kPIWarps : 1][32];
+    __shared__ uint32_t s_grp[2];
+    __shared__ uint32_t s_seg;   // next block-wide-row segment
+    if (threadIdx.x < 2) s_grp[threadIdx.x] = 0;
+    if (threadIdx.x == 0) s_seg = 0;   // first read after the phase-0 barriers
     const uint32_t n = a.n;
     const W *w = (const W *)a.w;
     const unsigned lane = threadIdx.x & 31;
@@ -645,6 +806,7 @@ __global__ void __launch_bounds__(kPIThreads, 2) k_power_iter(PIArgs a) {
     uint64_t best_at = 0;
     uint64_t niter = 0;
     V *src = va, *dst = vb;
+    uint32_t panel_seq = 0;   // panels processed so far: selects the group counter
     uint32_t *win = swin[wk];
     V *winx = swinx[STREAM ? wk : 0];
     double *wind = swind[STREAM ? wk : 0];
@@ -679,6 +841,48 @@ __global__ void __launch_bounds__(kPIThreads, 2) k_power_iter(PIArgs a) {
                 seg = hr + 1;
             }
             warp_stream<NA, W, V, ACC>(a.rp, a.col, w, xv, a.m, a.vec_ok, seg, w_r1, a.deg, win, winx, wind, fin);
+        } else if (PANEL) {
+            // column panels: the block copies panel p of the iterate into
+            // shared memory, then its warps take 32-row groups of the block's
+            // rows from a shared counter and add each row's panel sum to yacc
+            ACC *yacc = (ACC *)a.yacc;
+            const W *pw = (const W *)a.pw;
+            const uint32_t ngroups = (B1 - B0 + 31) / 32;
+            const bool vec = ((uintptr_t)src & 15u) == 0;
+            constexpr uint32_t VPER = 16 / sizeof(V);
+            for (uint32_t p = 0; p < a.P; p++, panel_seq++) {
+                const uint32_t base = p * a.PW;
+                const uint32_t len = n - base < a.PW ? n - base : a.PW;
+                __syncthreads();   // every warp is done with the previous panel
+                if (vec) {
+                    const uint32_t nv = len / VPER;
+                    const uint4 *s4 = reinterpret_cast<const uint4 *>(src + base);
+                    uint4 *d4 = reinterpret_cast<uint4 *>(xs);
+                    for (uint32_t c = threadIdx.x; c < nv; c += blockDim.x) d4[c] = __ldcg(s4 + c);
+                    for (uint32_t c = nv * VPER + threadIdx.x; c < len; c += blockDim.x) xs[c] = __ldcg(src + base + c);
+                } else {
+                    for (uint32_t c = threadIdx.x; c < len; c += blockDim.x) xs[c] = __ldcg(src + base + c);
+                }
+                if (threadIdx.x == 0) s_grp[(panel_seq + 1) & 1] = 0;
+                __syncthreads();
+                const uint32_t *offp = a.poff + (size_t)p * n;
+                uint32_t *ctr = &s_grp[panel_seq & 1];
+                while (true) {
+                    uint32_t k = 0;
+                    if (lane == 0) k = atomicAdd(ctr, 1u);
+                    k = __shfl_sync(0xFFFFFFFFu, k, 0);
+                    if (k >= ngroups) break;
+                    const uint32_t g = B0 + 32 * k;
+                    const uint32_t gl = B1 - g < 32 ? B1 - g : 32;
+                    panel_rows32<NA, W, V, ACC>(offp, a.pcol, pw, xs, g, gl, p == 0, win, sysm[PANEL ? wk : 0], yacc);
+                }
+            }
+            __syncthreads();   // yacc holds every row of the block
+            for (uint32_t i = B0 + threadIdx.x; i < B1; i += blockDim.x) {
+                const uint32_t b = a.rp[i], e = a.rp[i + 1];
+                if (e - b > a.heavy_T || e == b) continue;   // block-wide rows
+                fin(i, yacc[i], w ? a.deg[i] : (double)(e - b), (double)src[i]);
+            }
         } else if (MODE == 5) {
             const uint32_t T = a.heavy_T;
             auto skip = [T](uint32_t len) { return len > T || len == 0; };
@@ -700,23 +904,42 @@ __global__ void __launch_bounds__(kPIThreads, 2) k_power_iter(PIArgs a) {
                 if (lane == 0) fin(i, acc, w ? (double)ds : (double)(e - b), xi);
             }
         }
-        // block-wide rows of this block's range
-        for (uint32_t h = h0; h < h1; h++) {
+        // block-wide rows of this block's range: their segments of 2^seg_shift
+        // entries are taken by the warps from a shared counter as they finish
+        // their own rows; each segment's sum goes to its own slot, and the
+        // slots of a row are added in order once all are written
+        {
+            const uint32_t sg0 = a.hseg[B0], sg1 = a.hseg[B1];
+            while (true) {
+                uint32_t k = 0;
+                if (lane == 0) k = atomicAdd(&s_seg, 1u);
+                const uint32_t sg = sg0 + __shfl_sync(0xFFFFFFFFu, k, 0);
+                if (sg >= sg1) break;
+                const uint32_t i = a.seg_row[sg];
+                const uint32_t e = a.rp[i + 1];
+                const uint32_t b = a.rp[i] + ((sg - a.hseg[i]) << a.seg_shift);
+                const uint32_t e2 = e - b > (1u << a.seg_shift) ? b + (1u << a.seg_shift) : e;
+                ACC acc = 0;
+                uint64_t ds = 0;
+                warp_row_accum<8, NA, W, V, ACC>(a.col, w, xv, b + lane, e2, acc, ds);
+                acc = warp_sum(acc);
+                if (lane == 0) a.hpart[sg] = (double)acc;
+            }
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) s_seg = 0;
+        for (uint32_t h = h0 + threadIdx.x; h < h1; h += blockDim.x) {
             const uint32_t i = a.heavy[h];
             const uint32_t b = a.rp[i], e = a.rp[i + 1];
             double acc = 0;
-            row_accum<W, V, double>(a.col, w, xv, b + threadIdx.x, e, blockDim.x, acc);
-            double z = 0;
-            block_sum2(acc, z, sm);
-            if (threadIdx.x == 0) {
-                const double d = w ? (e > b ? a.deg[i] : 0.0) : (double)(e - b);
-                const double ui = ((double)src[i] - mu) * inv_nu;
-                const double r = (gb - d) * ui + (acc - mu * d) * inv_nu;
-                const V rs = (V)r;
-                dst[i] = rs;
-                const double rd = (double)rs;
-                P[0] += rd; P[1] += rd * rd; P[2] += ui * rd; P[3] += ui; P[4] += ui * ui;
-            }
+            for (uint32_t sg = a.hseg[i]; sg < a.hseg[i + 1]; sg++) acc += a.hpart[sg];
+            const double d = w ? (e > b ? a.deg[i] : 0.0) : (double)(e - b);
+            const double ui = ((double)src[i] - mu) * inv_nu;
+            const double r = (gb - d) * ui + (acc - mu * d) * inv_nu;
+            const V rs = (V)r;
+            dst[i] = rs;
+            const double rd = (double)rs;
+            P[0] += rd; P[1] += rd * rd; P[2] += ui * rd; P[3] += ui; P[4] += ui * ui;
         }
         block_sum_d<kNP>(P, sm);
         double *part = (niter & 1) ? part1 : part0;
@@ -804,16 +1027,159 @@ __global__ void k_heavy_flags(uint32_t n, const uint32_t *rp, uint32_t T, uint8_
     }
 }
 
-// per-row cost used to give every block and warp an equal share: entries
-// plus a fixed row overhead; block-wide rows cost nothing in the warp prefix
-__global__ void k_row_cost(uint32_t n, const uint32_t *rp, uint32_t T, uint32_t shift, uint32_t *cost,
-                           uint32_t *cost_all) {
+// Per-row cost used to give every block and warp an equal share: the row's
+// entries rounded up to whole trips of 2^qs entries (the warp-row variants
+// spend one trip on any row up to 128 entries; streaming has qs = 0) plus a
+// fixed row overhead; block-wide rows cost nothing in the warp prefix.
+__global__ void k_row_cost(uint32_t n, const uint32_t *rp, uint32_t T, uint32_t qs, uint32_t over, uint32_t shift,
+                           uint32_t *cost, uint32_t *cost_all) {
     uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
-    uint32_t len = rp[i + 1] - rp[i];
-    uint32_t c = ((len + 8u) >> shift) + 1u;
+    const uint32_t len = rp[i + 1] - rp[i];
+    const uint64_t trips = ((uint64_t)len + (1u << qs) - 1) >> qs;
+    const uint32_t c = (uint32_t)(((trips << qs) + over) >> shift) + 1u;
     cost[i] = (len > T || len == 0) ? 0u : c;
     cost_all[i] = c;
+}
+
+// Segments of the block-wide rows: cnt[i] = segments of 2^shift entries of
+// row i when it is longer than T, else 0.
+__global__ void k_seg_counts(uint32_t n, const uint32_t *rp, uint32_t T, uint32_t shift, uint32_t *cnt) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const uint32_t len = rp[i + 1] - rp[i];
+    cnt[i] = len > T ? (uint32_t)(((uint64_t)len + (1u << shift) - 1) >> shift) : 0u;
+}
+
+__global__ void k_seg_rows(uint32_t n, const uint32_t *hseg, uint32_t *seg_row) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    for (uint32_t s = hseg[i]; s < hseg[i + 1]; s++) seg_row[s] = i;
+}
+
+// ------------------------------------------------------ column panels --
+// Number of entries of a row below key (the row ascending by destination).
+__device__ __forceinline__ uint32_t row_count_below(const uint32_t *col, uint32_t b, uint32_t e, uint32_t key) {
+    uint32_t lo = b, hi = e;
+    while (lo < hi) {
+        const uint32_t mid = lo + ((hi - lo) >> 1);
+        if (col[mid] < key) lo = mid + 1;
+        else hi = mid;
+    }
+    return lo - b;
+}
+
+// Lane l <= P of the warp holding row i gets the number of the row's entries
+// in panels below l (0 for block-wide rows, which the panels leave out).
+__device__ __forceinline__ uint32_t panel_bounds(const uint32_t *rp, const uint32_t *col, uint32_t i, uint32_t T,
+                                                 uint32_t PW, uint32_t P, uint32_t &b, bool &skip) {
+    const unsigned lane = threadIdx.x & 31;
+    b = rp[i];
+    const uint32_t e = rp[i + 1];
+    skip = e - b > T || e == b;
+    if (skip || lane > P) return 0;
+    if (lane == P) return e - b;
+    return lane == 0 ? 0u : row_count_below(col, b, e, lane * PW);
+}
+
+// cnt[p*n + i] = entries of warp row i in panel p (P <= 31)
+__global__ void k_panel_count(uint32_t n, const uint32_t *rp, const uint32_t *col, uint32_t T, uint32_t PW,
+                              uint32_t P, uint32_t *cnt) {
+    const unsigned lane = threadIdx.x & 31;
+    const uint64_t nw = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+    for (uint64_t r = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; r < n; r += nw) {
+        const uint32_t i = (uint32_t)r;
+        uint32_t b;
+        bool skip;
+        const uint32_t lb = panel_bounds(rp, col, i, T, PW, P, b, skip);
+        const uint32_t nb = __shfl_down_sync(0xFFFFFFFFu, lb, 1);
+        if (lane < P) cnt[(size_t)lane * n + i] = skip ? 0u : nb - lb;
+    }
+}
+
+// copy each warp row's panel segments to their panel-major places
+template <typename W>
+__global__ void k_panel_scatter(uint32_t n, const uint32_t *rp, const uint32_t *col, const W *w, uint32_t T,
+                                uint32_t PW, uint32_t P, const uint32_t *off, uint16_t *pcol, W *pw) {
+    const unsigned lane = threadIdx.x & 31;
+    const uint64_t nw = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+    for (uint64_t r = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; r < n; r += nw) {
+        const uint32_t i = (uint32_t)r;
+        uint32_t b;
+        bool skip;
+        const uint32_t lb = panel_bounds(rp, col, i, T, PW, P, b, skip);
+        if (skip) continue;   // warp-uniform
+        for (uint32_t p = 0; p < P; p++) {
+            const uint32_t s0 = __shfl_sync(0xFFFFFFFFu, lb, p);
+            const uint32_t s1 = __shfl_sync(0xFFFFFFFFu, lb, p + 1);
+            const uint32_t d = off[(size_t)p * n + i];
+            for (uint32_t k = s0 + lane; k < s1; k += 32) {
+                pcol[d + k - s0] = (uint16_t)(col[b + k] - p * PW);
+                if (w) pw[d + k - s0] = w[b + k];
+            }
+        }
+    }
+}
+
+// *bad = 1 when some row is not ascending by destination
+__global__ void k_rows_sorted(uint32_t n, const uint32_t *rp, const uint32_t *col, uint32_t *bad) {
+    const unsigned lane = threadIdx.x & 31;
+    const uint64_t nw = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+    bool ok = true;
+    for (uint64_t r = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; r < n; r += nw) {
+        const uint32_t b = rp[r], e = rp[r + 1];
+        for (uint32_t j = b + lane; j + 1 < e; j += 32) ok = ok && col[j] <= col[j + 1];
+    }
+    if (__any_sync(0xFFFFFFFFu, !ok) && lane == 0) atomicOr(bad, 1u);
+}
+
+struct PanelLayout {
+    uint32_t P = 0, PW = 0;
+    uint32_t *off = nullptr;
+    uint16_t *col = nullptr;
+    void *w = nullptr;
+    void *yacc = nullptr;
+};
+
+// Regroup the warp rows of L (rows of at most T entries) by column panel of
+// kPanelBytes / vbytes iterate entries.  Leaves out->P = 0 when the level
+// needs more than kMaxPanels panels.
+static int build_panels(Context &C, const Level &L, uint32_t T, size_t vbytes, PanelLayout *out) {
+    const uint32_t n = L.n;
+    const uint32_t PW = (uint32_t)(kPanelBytes / vbytes);
+    const uint32_t P = (uint32_t)cdiv(n, PW);
+    *out = PanelLayout();
+    if (P == 0 || P > kMaxPanels || (uint64_t)P * n >= 0xFFFFFFFFull) return SGP_B200_OK;
+    uint32_t *cnt, *off, total = 0;
+    const size_t pn = (size_t)P * n;
+    SGPB_TRY(dalloc_t(C, &cnt, pn + 1));
+    SGPB_TRY(dalloc_t(C, &off, pn + 1));
+    uint32_t g = cdiv(n, 8);
+    if (g > (uint32_t)C.num_sms * 16) g = C.num_sms * 16;
+    k_panel_count<<<g, 256, 0, C.stream>>>(n, L.rp, L.col, T, PW, P, cnt);
+    C.kernel_launches++;
+    SGPB_TRY(scan_u32(C, cnt, off, (uint32_t)pn, nullptr));
+    SGPB_TRY(read_u32(C, off + pn, &total));
+    uint16_t *pcol;
+    SGPB_TRY(dalloc_t(C, &pcol, (size_t)total + 256));
+    void *pw = nullptr;
+    if (L.w) {
+        SGPB_TRY(dalloc(C, &pw, ((size_t)total + 256) * L.wbytes));
+        if (L.wbytes == 8)
+            k_panel_scatter<unsigned long long><<<g, 256, 0, C.stream>>>(n, L.rp, L.col, (const unsigned long long *)L.w,
+                                                                         T, PW, P, off, pcol, (unsigned long long *)pw);
+        else
+            k_panel_scatter<uint32_t><<<g, 256, 0, C.stream>>>(n, L.rp, L.col, (const uint32_t *)L.w, T, PW, P, off,
+                                                               pcol, (uint32_t *)pw);
+    } else {
+        k_panel_scatter<uint32_t><<<g, 256, 0, C.stream>>>(n, L.rp, L.col, nullptr, T, PW, P, off, pcol, nullptr);
+    }
+    C.kernel_launches++;
+    SGPB_CUDA(cudaGetLastError());
+    void *yacc;
+    SGPB_TRY(dalloc(C, &yacc, (size_t)n * vbytes));
+    out->P = P; out->PW = PW; out->off = off; out->col = pcol; out->w = pw; out->yacc = yacc;
+    return SGP_B200_OK;
 }
 
 static uint32_t pi_grid(const Context &C, uint64_t n, uint64_t m) {
@@ -826,10 +1192,11 @@ static uint32_t pi_grid(const Context &C, uint64_t n, uint64_t m) {
 // mean degree above which a level uses one warp per row
 constexpr double kStreamMaxAvgDegree = 64.0;
 
-// SpMV variant of a level: SGPB_PI_MODE = stream | row4 | row8 overrides the
-// degree rule, SGPB_PI_NA = 0 | 1 the L1 policy of the matrix stream.
+// SpMV variant of a level: column panels when a panel layout was built for
+// it, else CSR streaming below kStreamMaxAvgDegree and pipelined warp rows
+// above; SGPB_PI_MODE = stream | row4 | rowp | panel overrides the rule.
 struct PIVariant {
-    int mode;   // 0 stream, 4 / 8 warp rows
+    int mode;   // 0 stream, 4 warp rows, 5 pipelined warp rows, 6 column panels
     bool na;
 };
 static PIVariant pi_variant(const PIArgs &a) {
@@ -841,13 +1208,25 @@ static PIVariant pi_variant(const PIArgs &a) {
         else if (!strcmp(s, "row4")) v.mode = 4;
         else if (!strcmp(s, "rowp")) v.mode = 5;
     }
+    if (a.P) v.mode = 6;
     return v;
+}
+
+// whether a level gets a column-panel layout (SGPB_PI_MODE=panel; rows
+// ascending by destination, in the level's own numbering).  Off by default:
+// on R-MAT levels the per-panel block barriers cost more than the shared-
+// memory gathers save (measured 2x slower than pipelined warp rows).
+static bool panels_wanted(const Level &L, const PIArgs &a) {
+    if (a.inv || L.n == 0) return false;
+    const char *s = getenv("SGPB_PI_MODE");
+    return s && !strcmp(s, "panel");
 }
 
 template <typename W, typename V, bool CACHE>
 static const void *pi_kernel_c(int mode) {
     if (mode == 0) return (const void *)k_power_iter<W, V, 0, true, CACHE>;
     if (mode == 5) return (const void *)k_power_iter<W, V, 5, true, CACHE>;
+    if (mode == 6) return (const void *)k_power_iter<W, V, 6, true, false>;
     return (const void *)k_power_iter<W, V, 4, true, CACHE>;
 }
 
@@ -859,9 +1238,13 @@ static int launch_pi(Context &C, PIArgs &a, uint32_t grid) {
     // cache_ok: 1 = relabelled copy (cache its hub prefix), 2 = only when the
     // whole iterate fits, 0 = off
     a.kcache = (a.cache_ok == 1 || (a.cache_ok == 2 && a.n <= kmax)) ? (uint32_t)(a.n < kmax ? a.n : kmax) : 0u;
+    if (var.mode == 6) a.kcache = 0;
     const void *k = a.kcache ? pi_kernel_c<W, V, true>(var.mode) : pi_kernel_c<W, V, false>(var.mode);
-    const size_t dyn = (size_t)a.kcache * sizeof(V);
-    if (a.kcache) SGPB_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)cache_bytes));
+    const size_t dyn = var.mode == 6 ? (size_t)a.PW * sizeof(V) : (size_t)a.kcache * sizeof(V);
+    if (var.mode == 6)
+        SGPB_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kPanelBytes));
+    else if (a.kcache)
+        SGPB_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)cache_bytes));
     int per_sm = 0;
     SGPB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, kPIThreads, dyn));
     if (per_sm < 1) {
@@ -876,9 +1259,22 @@ static int launch_pi(Context &C, PIArgs &a, uint32_t grid) {
     return SGP_B200_OK;
 }
 
-static int run_pi(Context &C, const Level &L, PIArgs a, int mixed, double *res_d, double res_h[6], float *ms) {
+// panels[0] / panels[1]: layouts for FP32 / FP64 iterates, built on first use
+// when want_panels is set
+static int run_pi(Context &C, const Level &L, PIArgs a, int mixed, double *res_d, double res_h[6], float *ms,
+                  bool want_panels, PanelLayout (&panels)[2], bool (&built)[2]) {
     const uint32_t grid = pi_grid(C, L.n, L.m);
     a.res = res_d;
+    a.P = 0;
+    if (want_panels) {
+        const int k = mixed ? 0 : 1;
+        if (!built[k]) {
+            SGPB_TRY(build_panels(C, L, a.heavy_T, mixed ? sizeof(float) : sizeof(double), &panels[k]));
+            built[k] = true;
+        }
+        const PanelLayout &pl = panels[k];
+        a.P = pl.P; a.PW = pl.PW; a.poff = pl.off; a.pcol = pl.col; a.pw = pl.w; a.yacc = pl.yacc;
+    }
     int rc;
     cudaEvent_t e0, e1;
     SGPB_CUDA(cudaEventCreate(&e0));
@@ -965,9 +1361,25 @@ int power_iter_level(Context &C, const Level &Lin, const double *x_in, const uin
     }
     a.n = n; a.m = L.m; a.rp = L.rp; a.col = L.col; a.w = L.w;
     a.vec_ok = (((uintptr_t)L.col | (uintptr_t)L.w) & 15u) == 0;
-    // rows longer than one warp's share of the cost are processed block-wide
+    // the variant decides the heavy-row threshold and the cost model
+    bool want_panels = panels_wanted(L, a);
+    if (want_panels && !L.sorted) {
+        uint32_t *bad, hbad = 0;
+        SGPB_TRY(dalloc_t(C, &bad, 1));
+        SGPB_TRY(dzero(C, bad, 4));
+        uint32_t g = cdiv(n, 8);
+        if (g > (uint32_t)C.num_sms * 16) g = C.num_sms * 16;
+        k_rows_sorted<<<g, 256, 0, C.stream>>>(n, L.rp, L.col, bad);
+        C.kernel_launches++;
+        SGPB_TRY(read_u32(C, bad, &hbad));
+        want_panels = hbad == 0;
+    }
+    const int mode = want_panels ? 6 : pi_variant(a).mode;
+    // rows longer than a fraction of one warp's share of the cost are cut
+    // into segments shared by the block's warps (streaming profits from a
+    // lower threshold than warp rows: measured on R-MAT levels)
     const uint64_t nwarps = (uint64_t)pi_grid(C, n, L.m) * kPIWarps;
-    uint64_t T = (L.m + 8ull * n) / nwarps;
+    uint64_t T = (L.m + 8ull * n) / nwarps / (mode == 0 ? kHeavyDivStream : kHeavyDivRows);
     if (T < 4ull * kTile) T = 4ull * kTile;
     if (T > 0xFFFFFFFFull) T = 0xFFFFFFFFull;
     a.heavy_T = (uint32_t)T;
@@ -982,10 +1394,29 @@ int power_iter_level(Context &C, const Level &Lin, const double *x_in, const uin
     SGPB_TRY(dalloc_t(C, &cpre_all, (size_t)n + 1));
     SGPB_TRY(dalloc_t(C, &a.deg, (size_t)n + 1));
     k_heavy_flags<<<cdiv(n, 256), 256, 0, C.stream>>>(n, L.rp, a.heavy_T, flags);
-    const uint32_t shift = (L.m + 9ull * n < 0xFFFFFFF0ull) ? 0u : 4u;   // keep the cost total in 32 bits
-    k_row_cost<<<cdiv(n, 256), 256, 0, C.stream>>>(n, L.rp, a.heavy_T, shift, cost, cost_all);
+    // the cost total is kept in 32 bits
+    const uint32_t qs = (mode == 4 || mode == 5) ? 7u : 0u;
+    const uint32_t over = (mode == 4 || mode == 5) ? 32u : 8u;
+    uint32_t shift = 0;
+    while ((L.m + ((1ull << qs) + over + 1) * (uint64_t)n) >> shift >= 0xFFFFFFF0ull) shift++;
+    k_row_cost<<<cdiv(n, 256), 256, 0, C.stream>>>(n, L.rp, a.heavy_T, qs, over, shift, cost, cost_all);
     C.kernel_launches += 2;
     SGPB_TRY(compact_flags(C, flags, n, heavy, nh));
+    {
+        // rows longer than T have more than 512 entries: at most m / 512 of them
+        const uint64_t max_segs = (L.m >> kSegShift) + L.m / (4ull * kTile) + 1;
+        uint32_t *segc, *hseg, *seg_row;
+        double *hpart;
+        SGPB_TRY(dalloc_t(C, &segc, (size_t)n + 1));
+        SGPB_TRY(dalloc_t(C, &hseg, (size_t)n + 1));
+        SGPB_TRY(dalloc_t(C, &seg_row, max_segs));
+        SGPB_TRY(dalloc_t(C, &hpart, max_segs));
+        k_seg_counts<<<cdiv(n, 256), 256, 0, C.stream>>>(n, L.rp, a.heavy_T, kSegShift, segc);
+        SGPB_TRY(scan_u32(C, segc, hseg, n, nullptr));
+        k_seg_rows<<<cdiv(n, 256), 256, 0, C.stream>>>(n, hseg, seg_row);
+        C.kernel_launches += 2;
+        a.hseg = hseg; a.seg_row = seg_row; a.hpart = hpart; a.seg_shift = kSegShift;
+    }
     SGPB_TRY(scan_u32(C, cost, cpre, n, nullptr));
     SGPB_TRY(scan_u32(C, cost_all, cpre_all, n, nullptr));
     a.heavy = heavy; a.n_heavy_ptr = nh; a.cpre = cpre; a.cpre_all = cpre_all;
@@ -1002,6 +1433,8 @@ int power_iter_level(Context &C, const Level &Lin, const double *x_in, const uin
     SGPB_TRY(dalloc_t(C, &res_d, 8));
     double rh[6];
     float kms = 0;
+    PanelLayout panels[2];
+    bool built[2] = {false, false};
     uint64_t total_iters = 0;
     // Mixed precision: FP32 vector storage and gathers under the reference's
     // stopping rule.  When |d dot| stops shrinking before reaching tol (the
@@ -1012,7 +1445,7 @@ int power_iter_level(Context &C, const Level &Lin, const double *x_in, const uin
     if (o.mixed && n >= 4096) {
         a.stall_factor = 0.5;
         a.stall_window = 64;
-        SGPB_TRY(run_pi(C, L, a, 1, res_d, rh, &kms));
+        SGPB_TRY(run_pi(C, L, a, 1, res_d, rh, &kms, want_panels, panels, built));
         total_iters += (uint64_t)rh[0];
         done = rh[5] == 0.0;
         a.x_in = x_out;
@@ -1021,7 +1454,7 @@ int power_iter_level(Context &C, const Level &Lin, const double *x_in, const uin
         a.iter_max = imax > total_iters ? imax - total_iters : 1;
     }
     if (!done) {
-        SGPB_TRY(run_pi(C, L, a, 0, res_d, rh, &kms));
+        SGPB_TRY(run_pi(C, L, a, 0, res_d, rh, &kms, want_panels, panels, built));
         total_iters += (uint64_t)rh[0];
     }
     res->niter = total_iters;

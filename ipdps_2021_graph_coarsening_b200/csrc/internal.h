@@ -85,6 +85,7 @@ struct Level {
     uint32_t *col = nullptr;
     void *w = nullptr;
     int wbytes = 0;
+    int sorted = 0;              // 1: every row ascending by destination (coarse levels)
     uint32_t *vcmap = nullptr;   // this level -> next coarser level
     uint32_t max_deg = 0;
     uint32_t seed_hi = 0, seed_lo = 0;

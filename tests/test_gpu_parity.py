@@ -152,7 +152,7 @@ def test_split_bit_exact(partitioner, graph, ties):
 
 
 # ------------------------------------------------------ power iteration --
-@pytest.fixture(params=["auto", "stream", "row4", "row8", "rowp"])
+@pytest.fixture(params=["auto", "stream", "row4", "rowp", "panel"])
 def spmv_variant(request, monkeypatch):
     """Every SpMV variant of the power-iteration kernel (the default picks one
     per level by mean degree; the others are forced here)."""
@@ -183,6 +183,60 @@ def test_power_iter_matches_oracle(partitioner, graph, weighted, spmv_variant):
     assert abs(np.linalg.norm(u_g) - 1) < 1e-9
     assert abs(u_g.sum()) < 1e-8 * np.sqrt(n)
     assert res_g >= 0
+
+
+@pytest.mark.parametrize("weighted", [False, True])
+def test_power_iter_column_panels(partitioner, weighted, monkeypatch):
+    """Levels wider than one shared-memory panel (several panels per
+    iteration in both precisions), against the oracle at a fixed iteration
+    count."""
+    monkeypatch.setenv("SGPB_PI_MODE", "panel")
+    g = G.grid2d(250, 250)
+    rp, col, w = g.row_ptr, g.col, None
+    if weighted:
+        hn = O.hec_heavy(rp, col, None, True, 8)
+        vc, nc, _ = O.hec_map(hn, 8)
+        rp, col, w = O.build_coarse(rp, col, None, vc, nc)
+    n = rp.shape[0] - 1
+    assert n > 12288   # more than one FP64 panel
+    x0 = np.random.default_rng(n).random(n)
+    cap = 300
+    u_o, it_o, lam_o = O.power_iter(rp, col, w, x0, 1e-10, cap)
+    u_g, it_g, lam_g, _ = partitioner.power_iter(dev_u32(rp), dev_u32(col), None if w is None else dev_u32(w),
+                                                 torch.from_numpy(x0).cuda(), None, 1e-10, cap)
+    assert it_g == it_o == cap
+    assert abs(lam_g - lam_o) <= 1e-9 * abs(lam_o)
+    assert 1 - abs(float(np.dot(u_g.cpu().numpy(), u_o))) <= 1e-9
+
+
+def test_power_iter_panels_unsorted_rows(partitioner, monkeypatch):
+    """Rows that are not ascending by destination cannot be cut into panel
+    segments: the level runs on warp rows and still matches the oracle."""
+    monkeypatch.setenv("SGPB_PI_MODE", "panel")
+    g = G.grid2d(60, 60)
+    rp, col = g.row_ptr, g.col.copy()
+    for i in range(g.n):
+        col[rp[i]:rp[i + 1]] = col[rp[i]:rp[i + 1]][::-1]
+    x0 = np.random.default_rng(4).random(g.n)
+    u_o, it_o, lam_o = O.power_iter(rp, col, None, x0, 1e-10, 200)
+    u_g, it_g, lam_g, _ = partitioner.power_iter(dev_u32(rp), dev_u32(col), None, torch.from_numpy(x0).cuda(), None,
+                                                 1e-10, 200)
+    assert it_g == it_o
+    assert abs(lam_g - lam_o) <= 1e-9 * abs(lam_o)
+
+
+def test_partition_column_panels(partitioner, monkeypatch):
+    """The whole path with every level on column panels, FP64 and mixed."""
+    monkeypatch.setenv("SGPB_PI_MODE", "panel")
+    g = G.rmat(13, seed=3)
+    o = O.partition_graph(g.row_ptr, g.col, None, cutoff=50, tol=1e-10, rng_state=5)
+    r = partitioner.partition(g, cutoff=50, tol=1e-10, rng_state=5)
+    assert r.level_n == o["level_n"]
+    assert r.edgecut == O.edge_cut(g.row_ptr, g.col, r.part)
+    assert abs(r.edgecut - o["edgecut"]) <= 0.02 * o["edgecut"] + 2
+    assert abs(r.lam - o["lambda"]) <= 1e-6 * abs(o["lambda"]) + 1e-12
+    rm = partitioner.partition(g, cutoff=50, tol=1e-10, rng_state=5, mixed=True)
+    assert abs(rm.lam - o["lambda"]) <= 1e-4 * abs(o["lambda"])
 
 
 def test_power_iter_prolongation(partitioner):
