@@ -180,6 +180,29 @@ void sgp_b200_default_options(sgp_b200_options_t *opt);
 int sgp_b200_partition(sgp_b200_ctx_t *ctx, const sgp_b200_graph_t *g,
                        const sgp_b200_options_t *opt, sgp_b200_result_t *res);
 
+/* The reference driver's 4-way mode (sgpar.cpp:62-89, num_partitions = 4):
+ * bisect g, take the two induced subgraphs (sgp_use_partition,
+ * sgpar.h:2666-2752), bisect each with the rng carried on from the previous
+ * call.  All on the device.  part4 (n entries, kind opt->part_mem) gets
+ * 2 * (bisection part) + (part inside its subgraph).  result4[0] = cut of the
+ * bisection, result4[1] = cut4 = result4[0] + both subgraph cuts,
+ * result4[2] = rng state after the three bisections.  Subgraph weights are
+ * dropped, as sgp_use_partition drops them. */
+int sgp_b200_partition_4way(sgp_b200_ctx_t *ctx, const sgp_b200_graph_t *g,
+                            const sgp_b200_options_t *opt, uint32_t *part4, uint64_t *result4);
+
+/* No counterpart in the reference (its experiment runner starts one process
+ * per graph).  Partitions graphs[0..count) independently, each with opt as
+ * given (the same rng seeding for every graph), into results[i] (whose part
+ * the caller sets, kind opt->part_mem).  `workers` graphs are in flight at
+ * once, each on its own stream of the context's device, largest graphs
+ * first; the worker contexts are kept by ctx for later calls.  Results do
+ * not depend on `workers`.  On failure the first error is returned and the
+ * message names the graph. */
+int sgp_b200_partition_batch(sgp_b200_ctx_t *ctx, const sgp_b200_graph_t *graphs, int count,
+                             const sgp_b200_options_t *opt, sgp_b200_result_t *results,
+                             int workers);
+
 /* ---- lower boundary: hierarchy handle (coarsen_kokkos.h:1165,
  *      eigensolve_kokkos.h:1493) ---- */
 typedef struct sgp_b200_hierarchy sgp_b200_hierarchy_t;

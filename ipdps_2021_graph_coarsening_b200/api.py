@@ -208,15 +208,8 @@ class Partitioner:
         torch.cuda.synchronize()
 
     # -- whole path
-    def partition(self, g, cutoff: int = 50, tol: float = 1e-10, mixed: bool = False,
-                  rng_state: int = 0x853C49E6748FEA9B, rng_inc: int = 1, iter_cap: int = 0,
-                  perc_imbalance: int = 0, part_out=None) -> Result:
-        """Partition ``g``: a host :class:`CSR` (numpy) or a dict of CUDA torch
-        tensors ``{"row_ptr", "col", "w"}`` (device-resident input).  The
-        partition is written to ``part_out`` (numpy or CUDA tensor) when
-        given, else returned as numpy."""
+    def _graph(self, g, keep: list) -> L.sgp_b200_graph_t:
         dg = L.sgp_b200_graph_t()
-        keep = []
         if isinstance(g, CSR):
             rp = np.ascontiguousarray(g.row_ptr, dtype=np.uint32)
             col = np.ascontiguousarray(g.col, dtype=np.uint32)
@@ -235,21 +228,29 @@ class Partitioner:
             dg.w = _dptr(g.get("w"))
             dg.mem = L.DEVICE
             self._sync()
+        return dg
+
+    @staticmethod
+    def _options(cutoff, tol, mixed, rng_state, rng_inc, iter_cap, perc_imbalance) -> L.sgp_b200_options_t:
         o = L.sgp_b200_options_t()
         L.lib().sgp_b200_default_options(ctypes.byref(o))
         o.cutoff, o.tol, o.mixed, o.perc_imbalance = cutoff, tol, int(mixed), perc_imbalance
         o.iter_cap, o.rng_state, o.rng_inc = iter_cap, rng_state, rng_inc
-        res = L.sgp_b200_result_t()
+        return o
+
+    @staticmethod
+    def _part_target(n: int, part_out, o: L.sgp_b200_options_t):
+        """(array, pointer) for a partition vector; sets o.part_mem."""
         if part_out is None:
-            part_out = np.zeros(dg.n, dtype=np.uint32)
+            part_out = np.zeros(n, dtype=np.uint32)
         if isinstance(part_out, np.ndarray):
             o.part_mem = L.HOST
-            res.part = part_out.ctypes.data
-        else:
-            o.part_mem = L.DEVICE
-            res.part = _dptr(part_out)
-        L.check(L.lib().sgp_b200_partition(self._ctx, ctypes.byref(dg), ctypes.byref(o), ctypes.byref(res)),
-                "sgp_b200_partition")
+            return part_out, part_out.ctypes.data
+        o.part_mem = L.DEVICE
+        return part_out, _dptr(part_out)
+
+    @staticmethod
+    def _result(res: L.sgp_b200_result_t, part_out) -> Result:
         nl = res.levels
         return Result(part_out, res.edgecut, res.part0_size, res.lambda_, res.residual, nl,
                       list(res.level_n[:nl]), list(res.level_m[:nl]), list(res.level_iters[:nl]),
@@ -257,6 +258,60 @@ class Partitioner:
                       res.rng_state,
                       res.ms_total, res.ms_h2d, res.ms_coarsen, res.ms_eigen, res.ms_split, res.ms_d2h,
                       res.kernel_launches)
+
+    def partition(self, g, cutoff: int = 50, tol: float = 1e-10, mixed: bool = False,
+                  rng_state: int = 0x853C49E6748FEA9B, rng_inc: int = 1, iter_cap: int = 0,
+                  perc_imbalance: int = 0, part_out=None) -> Result:
+        """Partition ``g``: a host :class:`CSR` (numpy) or a dict of CUDA torch
+        tensors ``{"row_ptr", "col", "w"}`` (device-resident input).  The
+        partition is written to ``part_out`` (numpy or CUDA tensor) when
+        given, else returned as numpy."""
+        keep = []
+        dg = self._graph(g, keep)
+        o = self._options(cutoff, tol, mixed, rng_state, rng_inc, iter_cap, perc_imbalance)
+        res = L.sgp_b200_result_t()
+        part_out, res.part = self._part_target(dg.n, part_out, o)
+        L.check(L.lib().sgp_b200_partition(self._ctx, ctypes.byref(dg), ctypes.byref(o), ctypes.byref(res)),
+                "sgp_b200_partition")
+        return self._result(res, part_out)
+
+    def partition_4way(self, g, cutoff: int = 50, tol: float = 1e-10, mixed: bool = False,
+                       rng_state: int = 0x853C49E6748FEA9B, rng_inc: int = 1, iter_cap: int = 0,
+                       part_out=None) -> tuple:
+        """The reference driver's 4-way mode (sgpar.cpp:62-89): returns
+        (part4, cut of the bisection, cut4, rng state after the call) with
+        part4[i] = 2 * bisection part + part inside its induced subgraph."""
+        keep = []
+        dg = self._graph(g, keep)
+        o = self._options(cutoff, tol, mixed, rng_state, rng_inc, iter_cap, 0)
+        part_out, ptr = self._part_target(dg.n, part_out, o)
+        out = (L.c_u64 * 3)()
+        L.check(L.lib().sgp_b200_partition_4way(self._ctx, ctypes.byref(dg), ctypes.byref(o), ptr, out),
+                "sgp_b200_partition_4way")
+        return part_out, int(out[0]), int(out[1]), int(out[2])
+
+    def partition_batch(self, graphs: list, workers: int = 4, cutoff: int = 50, tol: float = 1e-10,
+                        mixed: bool = False, rng_state: int = 0x853C49E6748FEA9B, rng_inc: int = 1,
+                        iter_cap: int = 0) -> list:
+        """Partition independent host graphs, ``workers`` at a time on
+        separate streams (largest first); one :class:`Result` per graph, each
+        as if partitioned alone with the same options."""
+        keep = []
+        cnt = max(1, len(graphs))
+        arr = (L.sgp_b200_graph_t * cnt)()
+        for i, g in enumerate(graphs):
+            arr[i] = self._graph(g, keep)
+        o = self._options(cutoff, tol, mixed, rng_state, rng_inc, iter_cap, 0)
+        o.part_mem = L.HOST
+        res = (L.sgp_b200_result_t * cnt)()
+        parts = []
+        for i in range(len(graphs)):
+            p = np.zeros(arr[i].n, dtype=np.uint32)
+            parts.append(p)
+            res[i].part = p.ctypes.data
+        L.check(L.lib().sgp_b200_partition_batch(self._ctx, arr, len(graphs), ctypes.byref(o), res, workers),
+                "sgp_b200_partition_batch")
+        return [self._result(res[i], parts[i]) for i in range(len(graphs))]
 
     # -- per-kernel entry points (CUDA torch tensors)
     def hec(self, row_ptr, col, w=None, random_level: bool = False, seed: int = 1):

@@ -10,6 +10,11 @@
 #include <stdlib.h>
 #include <string.h>
 
+#include <algorithm>
+#include <atomic>
+#include <mutex>
+#include <string>
+#include <thread>
 #include <vector>
 
 #include "common.cuh"
@@ -204,18 +209,11 @@ static float ev_ms(cudaEvent_t a, cudaEvent_t b) {
     return ms;
 }
 
-static int partition_impl(Context &C, const sgp_b200_graph_t *g, const sgp_b200_options_t *opt,
-                          sgp_b200_result_t *res) {
-    cudaEvent_t ev[6];
-    for (auto &e : ev) SGPB_CUDA(cudaEventCreate(&e));
-    struct EvGuard {
-        cudaEvent_t *e;
-        ~EvGuard() { for (int i = 0; i < 6; i++) cudaEventDestroy(e[i]); }
-    } guard{ev};
-    C.kernel_launches = 0;
-    SGPB_CUDA(cudaEventRecord(ev[0], C.stream));
-    Level L0;
-    SGPB_TRY(stage_input(C, g, &L0));
+// The path on a staged level 0: hierarchy, eigenvector, split.  part_d is a
+// device array of L0.n entries; the caller copies it out.  ev[0] was recorded
+// before staging (the H2D window), ev[1..4] are recorded here.
+static int partition_staged(Context &C, const Level &L0, const sgp_b200_options_t *opt, sgp_b200_result_t *res,
+                            uint32_t *part_d, cudaEvent_t *ev) {
     SGPB_CUDA(cudaEventRecord(ev[1], C.stream));
     uint64_t st = opt->rng_state;
     std::vector<Level> levels;
@@ -229,16 +227,10 @@ static int partition_impl(Context &C, const sgp_b200_graph_t *g, const sgp_b200_
     PowerIterResult fin;
     SGPB_TRY(eigensolve(C, levels, &st, opt->rng_inc, po, &evec, &fin));
     SGPB_CUDA(cudaEventRecord(ev[3], C.stream));
-    uint32_t *part_d = (opt->part_mem == SGP_B200_DEVICE) ? res->part : nullptr;
-    if (!part_d) SGPB_TRY(dalloc_t(C, &part_d, g->n));
     uint64_t cut = 0;
     uint32_t p0 = 0;
     SGPB_TRY(split_level(C, levels[0], evec, opt->perc_imbalance, part_d, &cut, &p0));
     SGPB_CUDA(cudaEventRecord(ev[4], C.stream));
-    if (opt->part_mem != SGP_B200_DEVICE)
-        SGPB_CUDA(cudaMemcpyAsync(res->part, part_d, sizeof(uint32_t) * g->n, cudaMemcpyDeviceToHost, C.stream));
-    SGPB_CUDA(cudaEventRecord(ev[5], C.stream));
-    SGPB_CUDA(cudaStreamSynchronize(C.stream));
     res->edgecut = cut;
     res->part0_size = p0;
     res->lambda = fin.lambda;
@@ -254,14 +246,102 @@ static int partition_impl(Context &C, const sgp_b200_graph_t *g, const sgp_b200_
         res->iter_max_reached |= levels[l].pi_capped;
     }
     res->rng_state = st;
-    res->ms_h2d = ev_ms(ev[0], ev[1]);
-    res->ms_coarsen = ev_ms(ev[1], ev[2]);
-    res->ms_eigen = ev_ms(ev[2], ev[3]);
-    res->ms_split = ev_ms(ev[3], ev[4]);
-    res->ms_d2h = ev_ms(ev[4], ev[5]);
-    res->ms_total = ev_ms(ev[0], ev[5]);
+    return SGP_B200_OK;
+}
+
+struct Events {
+    cudaEvent_t e[6] = {};
+    int create() {
+        for (auto &x : e) SGPB_CUDA(cudaEventCreate(&x));
+        return SGP_B200_OK;
+    }
+    ~Events() {
+        for (auto &x : e)
+            if (x) cudaEventDestroy(x);
+    }
+};
+
+static void fill_times(Context &C, const Events &E, sgp_b200_result_t *res) {
+    res->ms_h2d = ev_ms(E.e[0], E.e[1]);
+    res->ms_coarsen = ev_ms(E.e[1], E.e[2]);
+    res->ms_eigen = ev_ms(E.e[2], E.e[3]);
+    res->ms_split = ev_ms(E.e[3], E.e[4]);
+    res->ms_d2h = ev_ms(E.e[4], E.e[5]);
+    res->ms_total = ev_ms(E.e[0], E.e[5]);
     res->kernel_launches = C.kernel_launches;
     C.t_total = res->ms_total; C.t_coarsen = res->ms_coarsen; C.t_eigen = res->ms_eigen; C.t_split = res->ms_split;
+}
+
+static int partition_impl(Context &C, const sgp_b200_graph_t *g, const sgp_b200_options_t *opt,
+                          sgp_b200_result_t *res) {
+    Events E;
+    SGPB_TRY(E.create());
+    C.kernel_launches = 0;
+    SGPB_CUDA(cudaEventRecord(E.e[0], C.stream));
+    Level L0;
+    SGPB_TRY(stage_input(C, g, &L0));
+    uint32_t *part_d = (opt->part_mem == SGP_B200_DEVICE) ? res->part : nullptr;
+    if (!part_d) SGPB_TRY(dalloc_t(C, &part_d, g->n));
+    SGPB_TRY(partition_staged(C, L0, opt, res, part_d, E.e));
+    if (opt->part_mem != SGP_B200_DEVICE)
+        SGPB_CUDA(cudaMemcpyAsync(res->part, part_d, sizeof(uint32_t) * g->n, cudaMemcpyDeviceToHost, C.stream));
+    SGPB_CUDA(cudaEventRecord(E.e[5], C.stream));
+    SGPB_CUDA(cudaStreamSynchronize(C.stream));
+    fill_times(C, E, res);
+    return SGP_B200_OK;
+}
+
+// part4[i] = 2 part[i] + the sub-bisection's label of i in its induced subgraph
+__global__ void k_combine4(uint32_t n, const uint32_t *part, const uint32_t *map0, const uint32_t *map1,
+                           const uint32_t *pa, const uint32_t *pb, uint32_t *part4) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const uint32_t p = part[i];
+    const uint32_t s = p == 0 ? (pa ? pa[map0[i]] : 0u) : (pb ? pb[map1[i]] : 0u);
+    part4[i] = 2 * p + s;
+}
+
+// sgpar.cpp:62-89: bisection, induced subgraphs (sgpar.h:2666-2752), one
+// bisection of each with the rng carried along, cut4 = cut + ec1 + ec2.
+static int partition4_impl(Context &C, const sgp_b200_graph_t *g, const sgp_b200_options_t *opt, uint32_t *part4,
+                           uint64_t out[3]) {
+    Events E;
+    SGPB_TRY(E.create());
+    C.kernel_launches = 0;
+    SGPB_CUDA(cudaEventRecord(E.e[0], C.stream));
+    Level L0;
+    SGPB_TRY(stage_input(C, g, &L0));
+    const uint32_t n = g->n;
+    sgp_b200_options_t o = *opt;
+    o.part_mem = SGP_B200_DEVICE;
+    std::vector<sgp_b200_result_t> r(3);
+    uint32_t *p;
+    SGPB_TRY(dalloc_t(C, &p, n));
+    SGPB_TRY(partition_staged(C, L0, &o, &r[0], p, E.e));
+    o.rng_state = r[0].rng_state;
+    Level sub[2];
+    uint32_t *maps[2] = {nullptr, nullptr};
+    SGPB_TRY(induced_subgraphs(C, L0, p, &sub[0], &sub[1], &maps[0], &maps[1]));
+    uint32_t *sp[2] = {nullptr, nullptr};
+    uint64_t ec[2] = {0, 0};
+    for (int k = 0; k < 2; k++) {
+        if (sub[k].n < 2) continue;   // nothing to bisect
+        SGPB_TRY(dalloc_t(C, &sp[k], sub[k].n));
+        SGPB_TRY(partition_staged(C, sub[k], &o, &r[k + 1], sp[k], E.e));
+        o.rng_state = r[k + 1].rng_state;
+        ec[k] = r[k + 1].edgecut;
+    }
+    uint32_t *p4 = opt->part_mem == SGP_B200_DEVICE ? part4 : nullptr;
+    if (!p4) SGPB_TRY(dalloc_t(C, &p4, n));
+    k_combine4<<<cdiv(n, 256), 256, 0, C.stream>>>(n, p, maps[0], maps[1], sp[0], sp[1], p4);
+    C.kernel_launches++;
+    SGPB_CUDA(cudaGetLastError());
+    if (opt->part_mem != SGP_B200_DEVICE)
+        SGPB_CUDA(cudaMemcpyAsync(part4, p4, sizeof(uint32_t) * n, cudaMemcpyDeviceToHost, C.stream));
+    SGPB_CUDA(cudaStreamSynchronize(C.stream));
+    out[0] = r[0].edgecut;
+    out[1] = r[0].edgecut + ec[0] + ec[1];
+    out[2] = o.rng_state;
     return SGP_B200_OK;
 }
 
@@ -312,6 +392,75 @@ int sgp_b200_partition(sgp_b200_ctx_t *x, const sgp_b200_graph_t *g, const sgp_b
     int rc = partition_impl(*C, g, opt, res);
     release_all(*C);
     return rc;
+}
+
+int sgp_b200_partition_4way(sgp_b200_ctx_t *x, const sgp_b200_graph_t *g, const sgp_b200_options_t *opt,
+                            uint32_t *part4, uint64_t *result4) {
+    Context *C = ctx_get(x);
+    if (!C || !g || !opt || !part4 || !result4) {
+        set_error("null argument");
+        return SGP_B200_ERR_INVALID;
+    }
+    cudaSetDevice(C->device);
+    int rc = partition4_impl(*C, g, opt, part4, result4);
+    release_all(*C);
+    return rc;
+}
+
+int sgp_b200_partition_batch(sgp_b200_ctx_t *x, const sgp_b200_graph_t *graphs, int count,
+                             const sgp_b200_options_t *opt, sgp_b200_result_t *results, int workers) {
+    Context *C = ctx_get(x);
+    if (!C || (count > 0 && (!graphs || !results)) || !opt || count < 0) {
+        set_error("null argument");
+        return SGP_B200_ERR_INVALID;
+    }
+    for (int i = 0; i < count; i++)
+        if (!results[i].part) {
+            set_error("results[%d].part is null", i);
+            return SGP_B200_ERR_INVALID;
+        }
+    if (count == 0) return SGP_B200_OK;
+    if (workers < 1) workers = 1;
+    if (workers > count) workers = count;
+    cudaSetDevice(C->device);
+    while ((int)C->workers.size() < workers) {
+        sgp_b200_ctx_t *w = sgp_b200_create(C->device);
+        if (!w) return SGP_B200_ERR_DEVICE;
+        C->workers.push_back(w);
+    }
+    // largest graphs first (LPT): the workers take the next index of this order
+    std::vector<int> order(count);
+    for (int i = 0; i < count; i++) order[i] = i;
+    std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return graphs[a].m > graphs[b].m; });
+    std::atomic<int> next(0);
+    std::atomic<int> first_rc(SGP_B200_OK);
+    std::mutex err_mu;
+    std::string err;
+    auto work = [&](sgp_b200_ctx_t *wx) {
+        Context &W = *ctx_get(wx);
+        cudaSetDevice(W.device);
+        while (first_rc.load() == SGP_B200_OK) {
+            const int k = next.fetch_add(1);
+            if (k >= count) break;
+            const int i = order[k];
+            const int rc = partition_impl(W, &graphs[i], opt, &results[i]);
+            release_all(W);
+            if (rc != SGP_B200_OK) {
+                int expect = SGP_B200_OK;
+                if (first_rc.compare_exchange_strong(expect, rc)) {
+                    std::lock_guard<std::mutex> lk(err_mu);
+                    err = std::string("graph ") + std::to_string(i) + ": " + last_error();
+                }
+            }
+        }
+        cudaStreamSynchronize(W.stream);
+    };
+    std::vector<std::thread> th;
+    for (int t = 1; t < workers; t++) th.emplace_back(work, C->workers[t]);
+    work(C->workers[0]);
+    for (auto &t : th) t.join();
+    if (first_rc.load() != SGP_B200_OK) set_error("%s", err.c_str());
+    return first_rc.load();
 }
 
 int sgp_b200_last_timing(sgp_b200_ctx_t *x, float *t, float *c, float *e, float *s) {

@@ -49,6 +49,7 @@ struct Context {
     size_t smem_optin = 0;
     uint64_t *h_pinned = nullptr;   // small pinned staging area for scalar read-backs
     std::vector<void *> owned;      // allocations released at the end of a call
+    std::vector<sgp_b200_ctx_t *> workers;   // contexts of the batch workers (same device), kept across calls
     // timing of the last partition (ms, CUDA events)
     float t_total = 0, t_coarsen = 0, t_eigen = 0, t_split = 0, t_h2d = 0, t_d2h = 0;
     uint32_t kernel_launches = 0;
@@ -120,6 +121,8 @@ int power_iter_level(Context &C, const Level &L, const double *x_in, const uint3
 int split_level(Context &C, const Level &L, const double *evec, int perc_imbalance, uint32_t *part,
                 uint64_t *edgecut, uint32_t *n_part0);
 int edge_cut_device(Context &C, const Level &L, const uint32_t *part, uint64_t *edgecut);
-int induced_subgraphs(Context &C, const Level &L, const uint32_t *part, Level *g1, Level *g2);
+// map0 / map1 (optional): vertex i of L -> its id in g1 (part 0) / g2
+int induced_subgraphs(Context &C, const Level &L, const uint32_t *part, Level *g1, Level *g2,
+                      uint32_t **map0 = nullptr, uint32_t **map1 = nullptr);
 
 }  // namespace sgpb

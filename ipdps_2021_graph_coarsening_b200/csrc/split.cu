@@ -344,7 +344,8 @@ __global__ void k_fill_sub(uint32_t n, const uint32_t *rp, const uint32_t *col, 
     }
 }
 
-int induced_subgraphs(Context &C, const Level &L, const uint32_t *part, Level *g1, Level *g2) {
+int induced_subgraphs(Context &C, const Level &L, const uint32_t *part, Level *g1, Level *g2, uint32_t **map0_out,
+                      uint32_t **map1_out) {
     const uint32_t n = L.n;
     uint32_t *cnt0, *cnt1, *is0, *is1, *off0, *off1, *map0, *map1;
     SGPB_TRY(dalloc_t(C, &cnt0, (size_t)n + 1));
@@ -380,6 +381,8 @@ int induced_subgraphs(Context &C, const Level &L, const uint32_t *part, Level *g
     SGPB_CUDA(cudaMemcpyAsync(g2->rp + nn[1], off1 + n, 4, cudaMemcpyDeviceToDevice, C.stream));
     C.kernel_launches += 2;
     SGPB_CUDA(cudaGetLastError());
+    if (map0_out) *map0_out = map0;
+    if (map1_out) *map1_out = map1;
     return SGP_B200_OK;
 }
 

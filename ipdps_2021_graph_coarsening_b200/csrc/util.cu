@@ -219,6 +219,8 @@ sgp_b200_ctx_t *sgp_b200_create(int device) {
 void sgp_b200_destroy(sgp_b200_ctx_t *x) {
     if (!x) return;
     Context &C = x->c;
+    for (sgp_b200_ctx_t *w : C.workers) sgp_b200_destroy(w);
+    C.workers.clear();
     cudaSetDevice(C.device);
     release_all(C);
     if (C.stream) {

@@ -1,0 +1,144 @@
+"""The parity configurations of the partitioning path beyond R-MAT, at sizes
+the oracle finishes in seconds: the 256x256 grid with coarsening cutoff 32,
+the reference driver's 4-way mode on a 3D random geometric graph, a batch of
+small grids-with-holes and Erdos-Renyi graphs, and weighted Chung-Lu inputs
+(32-bit and 64-bit coarse weights).
+
+Integer results (hierarchy sizes, rng advance, cuts recomputed from the
+partition) are compared exactly; FP64 results within the tolerances stated
+in each test.
+"""
+import numpy as np
+import pytest
+
+from ipdps_2021_graph_coarsening_b200 import graphs as G
+from oracle import bindings as O
+
+pytestmark = pytest.mark.gpu
+
+
+def cut_of(g, labels):
+    """Undirected edges whose endpoints carry different labels."""
+    rows = np.repeat(np.arange(g.n), np.diff(g.row_ptr).astype(np.int64))
+    return int((labels[rows] != labels[g.col]).sum()) // 2
+
+
+def test_grid256_cutoff32(partitioner):
+    g = G.grid2d(256, 256)
+    o = O.partition_graph(g.row_ptr, g.col, None, cutoff=32, tol=1e-10, rng_state=7)
+    r = partitioner.partition(g, cutoff=32, tol=1e-10, rng_state=7)
+    assert r.level_n == o["level_n"] and r.rng_state == o["rng_state"]
+    assert r.edgecut == cut_of(g, r.part)
+    assert int(r.part.sum()) == g.n // 2
+    # FP64 power iteration: same stopping rule, summation order differs
+    assert abs(r.lam - o["lambda"]) <= 1e-6 * o["lambda"]
+    assert abs(r.edgecut - o["edgecut"]) <= 0.05 * o["edgecut"] + 4
+    # the finest iterate approximates the Fiedler pair of the grid:
+    # lambda_2 = 2 - 2 cos(pi / 256)
+    lam2 = 2 - 2 * np.cos(np.pi / 256)
+    assert abs(r.lam - lam2) / lam2 < 0.1
+
+
+def oracle_4way(g, rng_state, cutoff=50):
+    """sgpar.cpp:62-89 on the oracle: bisection, induced subgraphs, one
+    bisection of each with the rng carried on."""
+    o = O.partition_graph(g.row_ptr, g.col, None, cutoff=cutoff, tol=1e-10, rng_state=rng_state)
+    (rp1, c1), (rp2, c2) = O.use_partition(g.row_ptr, g.col, o["part"])
+    st = o["rng_state"]
+    cuts = [o["edgecut"]]
+    for rp, c in ((rp1, c1), (rp2, c2)):
+        s = O.partition_graph(rp, c, None, cutoff=cutoff, tol=1e-10, rng_state=st)
+        st = s["rng_state"]
+        cuts.append(s["edgecut"])
+    return cuts, st
+
+
+def test_rgg_4way_matches_driver(partitioner):
+    g = G.rgg3d(20000, seed=3)
+    part4, cut2, cut4, st = partitioner.partition_4way(g, rng_state=11)
+    # the bisection is the plain partition with the same seed
+    r = partitioner.partition(g, rng_state=11)
+    assert np.array_equal(part4 >> 1, r.part) and cut2 == r.edgecut
+    # labels 0..3, each half split in halves, cut4 counts every cut edge once
+    sizes = np.bincount(part4, minlength=4)
+    assert part4.max() <= 3 and sizes.sum() == g.n
+    n0 = int((r.part == 0).sum())
+    assert sorted([sizes[0], sizes[1]]) == sorted([n0 // 2, n0 - n0 // 2])
+    assert cut4 == cut_of(g, part4)
+    # against the oracle driver: FP64 differences may move a few vertices
+    ocuts, _ = oracle_4way(g, 11)
+    assert abs(cut2 - ocuts[0]) <= 0.05 * ocuts[0] + 4
+    assert abs(cut4 - sum(ocuts)) <= 0.05 * sum(ocuts) + 8
+
+
+def test_4way_device_resident(partitioner):
+    torch = pytest.importorskip("torch")
+    g = G.grid2d_holes(120, 90, seed=2)
+    dev = {"row_ptr": torch.from_numpy(g.row_ptr.view(np.int32)).cuda(),
+           "col": torch.from_numpy(g.col.view(np.int32)).cuda()}
+    out = torch.zeros(g.n, dtype=torch.int32, device="cuda")
+    _, cut2, cut4, _ = partitioner.partition_4way(dev, rng_state=5, part_out=out)
+    host, h2, h4, _ = partitioner.partition_4way(g, rng_state=5)
+    assert np.array_equal(out.cpu().numpy().view(np.uint32), host) and (cut2, cut4) == (h2, h4)
+
+
+def batch_graphs(count, seed=17, lo=1000, hi=12000):
+    """Vertex counts log-uniform in [lo, hi]; even indices grids with 10% of
+    the vertices removed, odd ones Erdos-Renyi of mean degree 8 (LCC)."""
+    rng = np.random.default_rng(seed)
+    sizes = np.exp(rng.uniform(np.log(lo), np.log(hi), count)).astype(int)
+    out = []
+    for i, s in enumerate(sizes):
+        if i % 2 == 0:
+            nx = int(np.sqrt(s))
+            out.append(G.grid2d_holes(nx, max(2, int(s) // nx), seed=i + 1))
+        else:
+            out.append(G.erdos_renyi(int(s), 8.0, seed=i + 1))
+    return out
+
+
+def test_batch_equals_single_calls(partitioner):
+    gs = batch_graphs(12)
+    many = partitioner.partition_batch(gs, workers=4, rng_state=9)
+    one = partitioner.partition_batch(gs, workers=1, rng_state=9)
+    for g, a, b in zip(gs, many, one):
+        s = partitioner.partition(g, rng_state=9)
+        for r in (a, b):
+            assert np.array_equal(r.part, s.part)
+            assert r.edgecut == s.edgecut == cut_of(g, r.part)
+            assert r.level_iters == s.level_iters and r.rng_state == s.rng_state
+
+
+def test_batch_matches_oracle(partitioner):
+    gs = batch_graphs(6, seed=23)
+    rs = partitioner.partition_batch(gs, workers=3, rng_state=4)
+    for g, r in zip(gs, rs):
+        o = O.partition_graph(g.row_ptr, g.col, None, cutoff=50, tol=1e-10, rng_state=4)
+        assert r.level_n == o["level_n"] and r.rng_state == o["rng_state"]
+        assert abs(r.edgecut - o["edgecut"]) <= 0.05 * o["edgecut"] + 4
+
+
+def test_batch_reports_the_failing_graph(partitioner):
+    from ipdps_2021_graph_coarsening_b200 import _lib as L
+    gs = batch_graphs(3)
+    bad = G.CSR(gs[1].row_ptr.copy(), gs[1].col.copy())
+    bad.col[0] = bad.n + 5   # destination out of range
+    with pytest.raises(L.SgparError) as e:
+        partitioner.partition_batch([gs[0], bad, gs[2]], workers=2)
+    assert "graph 1" in str(e.value)
+
+
+@pytest.mark.parametrize("wmax", [100, 1 << 22])
+def test_chunglu_weighted(partitioner, wmax):
+    """Weighted input; wmax 2^22 makes the total weight exceed 2^32, so the
+    coarse weights are 64-bit."""
+    g = G.chung_lu(20000, wmax=wmax, seed=5)
+    assert g.w is not None
+    total = int(g.w.astype(np.uint64).sum())
+    assert (total > 0xFFFFFFFF) == (wmax > 1000)
+    o = O.partition_graph(g.row_ptr, g.col, g.w, cutoff=50, tol=1e-10, rng_state=3)
+    r = partitioner.partition(g, cutoff=50, tol=1e-10, rng_state=3)
+    assert r.level_n == o["level_n"] and r.rng_state == o["rng_state"]
+    assert r.edgecut == cut_of(g, r.part)
+    assert abs(r.lam - o["lambda"]) <= 1e-6 * abs(o["lambda"])
+    assert abs(r.edgecut - o["edgecut"]) <= 0.05 * o["edgecut"] + 4
