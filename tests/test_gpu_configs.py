@@ -142,3 +142,14 @@ def test_chunglu_weighted(partitioner, wmax):
     assert r.edgecut == cut_of(g, r.part)
     assert abs(r.lam - o["lambda"]) <= 1e-6 * abs(o["lambda"])
     assert abs(r.edgecut - o["edgecut"]) <= 0.05 * o["edgecut"] + 4
+
+
+def test_sharded_batch_on_one_rank(partitioner):
+    """The multi-rank batch driver on a single rank runs the whole batch
+    through the batched entry point, in the graphs' order."""
+    from ipdps_2021_graph_coarsening_b200 import shard
+    gs = batch_graphs(5, seed=31)
+    out = shard.partition_sharded(gs, lambda l: partitioner.partition_batch(l, workers=2, rng_state=6), 0, 1)
+    for g, r in zip(gs, out):
+        s = partitioner.partition(g, rng_state=6)
+        assert np.array_equal(r.part, s.part) and r.edgecut == s.edgecut
