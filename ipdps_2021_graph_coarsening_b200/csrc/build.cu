@@ -21,66 +21,88 @@ namespace sgpb {
 constexpr int kT2 = 4096;
 constexpr uint32_t kSentinel = 0xFFFFFFFFu;
 
-template <int G>
-__device__ __forceinline__ unsigned group_mask() {
-    if (G == 32) return 0xFFFFFFFFu;
-    const unsigned lane = threadIdx.x & 31;
-    return ((1u << G) - 1u) << (lane & ~(unsigned)(G - 1));
-}
-
 // ---------------------------------------------------------------- count --
+// Per fine row u: krow[u] = entries whose coarse destination differs from
+// vcmap[u]; cnt[vcmap[u]] += krow[u].  A group of G lanes per row, 4 entries
+// per lane in flight (destinations, then the vcmap gathers).
 template <int G>
 __global__ void __launch_bounds__(256) k_build_count(uint32_t n, const uint32_t *__restrict__ rp,
                                                      const uint32_t *__restrict__ col,
                                                      const uint32_t *__restrict__ vcmap,
-                                                     uint32_t *__restrict__ cnt) {
+                                                     uint32_t *__restrict__ cnt, uint32_t *__restrict__ krow) {
     const unsigned gm = group_mask<G>();
     const uint32_t lane = threadIdx.x & (G - 1);
     const uint64_t gid = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) / G;
     const uint64_t ngroups = ((uint64_t)gridDim.x * blockDim.x) / G;
     for (uint64_t u = gid; u < n; u += ngroups) {
-        uint32_t cu = vcmap[u];
+        const uint32_t cu = vcmap[u];
+        const uint32_t b = rp[u], e = rp[u + 1];
         uint32_t c = 0;
-        for (uint32_t j = rp[u] + lane; j < rp[u + 1]; j += G) c += (__ldg(vcmap + __ldg(col + j)) != cu);
+        for (uint32_t j0 = b + lane; j0 < e; j0 += 4 * G) {
+            uint32_t d[4];
+#pragma unroll
+            for (int q = 0; q < 4; q++) d[q] = j0 + q * G < e ? __ldg(col + j0 + q * G) : 0u;
+#pragma unroll
+            for (int q = 0; q < 4; q++)
+                if (j0 + q * G < e) c += (__ldg(vcmap + d[q]) != cu);
+        }
 #pragma unroll
         for (int o = G / 2; o > 0; o >>= 1) c += __shfl_xor_sync(gm, c, o);
-        if (lane == 0 && c) atomicAdd(cnt + cu, c);
+        if (lane == 0) {
+            krow[u] = c;
+            if (c) atomicAdd(cnt + cu, c);
+        }
     }
 }
 
 // -------------------------------------------------------------- scatter --
+// Row u reserves krow[u] consecutive slots of bucket vcmap[u] with one atomic
+// and writes its kept (coarse destination, weight) pairs there in entry
+// order.  The order of the rows inside a bucket depends on the atomics; the
+// dedupe sorts each bucket, so the coarse graph does not.
 template <int G, typename WI>
 __global__ void __launch_bounds__(256) k_build_scatter(uint32_t n, const uint32_t *__restrict__ rp,
                                                        const uint32_t *__restrict__ col, const WI *__restrict__ w,
                                                        const uint32_t *__restrict__ vcmap,
+                                                       const uint32_t *__restrict__ krow,
                                                        const uint32_t *__restrict__ boff, uint32_t *__restrict__ fill,
                                                        uint32_t *__restrict__ bdst, WI *__restrict__ bw) {
     const unsigned gm = group_mask<G>();
     const uint32_t lane = threadIdx.x & (G - 1);
     const unsigned lane32 = threadIdx.x & 31;
     const unsigned gshift = lane32 & ~(unsigned)(G - 1);
+    const unsigned gbits = 0xFFFFFFFFu >> (32 - G);
     const uint64_t gid = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) / G;
     const uint64_t ngroups = ((uint64_t)gridDim.x * blockDim.x) / G;
     for (uint64_t u = gid; u < n; u += ngroups) {
+        const uint32_t k = krow[u];
+        if (k == 0) continue;   // group-uniform
         const uint32_t cu = vcmap[u];
         const uint32_t b = rp[u], e = rp[u + 1];
-        const uint32_t base_off = boff[cu];
-        for (uint32_t j0 = b; j0 < e; j0 += G) {
-            const uint32_t j = j0 + lane;
-            uint32_t cv = 0;
-            bool keep = false;
-            if (j < e) {
-                cv = __ldg(vcmap + __ldg(col + j));
-                keep = cv != cu;
+        uint32_t base = 0;
+        if (lane == 0) base = boff[cu] + atomicAdd(fill + cu, k);
+        base = __shfl_sync(gm, base, 0, G);
+        for (uint32_t j0 = b; j0 < e; j0 += 4 * G) {
+            uint32_t cv[4];
+            WI wv[4];
+#pragma unroll
+            for (int q = 0; q < 4; q++) {
+                const uint32_t j = j0 + q * G + lane;
+                cv[q] = j < e ? __ldg(col + j) : 0u;
+                if (w) wv[q] = j < e ? __ldg(w + j) : (WI)0;
             }
-            unsigned bal = (__ballot_sync(gm, keep) >> gshift) & (G == 32 ? 0xFFFFFFFFu : ((1u << G) - 1u));
-            uint32_t slot = 0;
-            if (lane == 0 && bal) slot = atomicAdd(fill + cu, (uint32_t)__popc(bal));
-            slot = __shfl_sync(gm, slot, 0, G);
-            if (keep) {
-                uint32_t p = base_off + slot + __popc(bal & ((1u << lane) - 1u));
-                bdst[p] = cv;
-                if (w) bw[p] = __ldg(w + j);
+#pragma unroll
+            for (int q = 0; q < 4; q++) cv[q] = j0 + q * G + lane < e ? __ldg(vcmap + cv[q]) : cu;
+#pragma unroll
+            for (int q = 0; q < 4; q++) {
+                const bool keep = cv[q] != cu;
+                const unsigned bal = (__ballot_sync(gm, keep) >> gshift) & gbits;
+                if (keep) {
+                    const uint32_t p = base + __popc(bal & ((1u << lane) - 1u));
+                    bdst[p] = cv[q];
+                    if (w) bw[p] = wv[q];
+                }
+                base += __popc(bal);
             }
         }
     }
@@ -223,6 +245,71 @@ __global__ void __launch_bounds__(kT2Threads) k_dedupe_block(const uint32_t *__r
     }
 }
 
+// Tier 2 for 32-bit (or unit) input weights: (destination, weight) packed in
+// one 64-bit word, destination high, so one bitonic sort of words orders the
+// bucket by destination with half the shared-memory traffic of separate
+// key and weight arrays.
+template <typename WI, typename WO>
+__global__ void __launch_bounds__(kT2Threads) k_dedupe_block_packed(const uint32_t *__restrict__ list,
+                                                                    const uint32_t *__restrict__ count,
+                                                                    const uint32_t *__restrict__ boff,
+                                                                    uint32_t *__restrict__ bdst,
+                                                                    const WI *__restrict__ bw, WO *__restrict__ tw,
+                                                                    uint32_t *__restrict__ dcnt) {
+    static_assert(sizeof(WI) == 4, "packed dedupe takes 32-bit input weights");
+    extern __shared__ __align__(16) unsigned char smraw[];
+    unsigned long long *sk = (unsigned long long *)smraw;   // kT2
+    __shared__ uint64_t scan_sm[33];
+    constexpr unsigned long long kNone = ~0ull;
+    const uint32_t cntv = *count;
+    for (uint32_t k = blockIdx.x; k < cntv; k += gridDim.x) {
+        const uint32_t c = list[k];
+        const uint32_t b = boff[c], sz = boff[c + 1] - b;
+        uint32_t P = 64;
+        while (P < sz) P <<= 1;
+        for (uint32_t i = threadIdx.x; i < P; i += blockDim.x)
+            sk[i] = i < sz ? ((unsigned long long)bdst[b + i] << 32) | (bw ? (uint32_t)bw[b + i] : 1u) : kNone;
+        __syncthreads();
+        for (uint32_t kk = 2; kk <= P; kk <<= 1) {
+            for (uint32_t j = kk >> 1; j > 0; j >>= 1) {
+                for (uint32_t t = threadIdx.x; t < P / 2; t += blockDim.x) {
+                    const uint32_t i = ((t & ~(j - 1)) << 1) | (t & (j - 1));
+                    const uint32_t q = i | j;
+                    const bool up = (i & kk) == 0;
+                    const unsigned long long x = sk[i], y = sk[q];
+                    if (up ? x > y : x < y) { sk[i] = y; sk[q] = x; }
+                }
+                __syncthreads();
+            }
+        }
+        // heads of destination runs; each thread owns a contiguous segment
+        const uint32_t per = P / blockDim.x > 0 ? P / blockDim.x : 1;
+        const uint32_t s0 = threadIdx.x * per;
+        uint64_t h = 0;
+        for (uint32_t i = s0; i < s0 + per && i < P; i++) {
+            const unsigned long long x = sk[i];
+            if (x != kNone && (i == 0 || (sk[i - 1] >> 32) != (x >> 32))) h++;
+        }
+        uint64_t tot;
+        const uint64_t inc = block_scan_u64(h, scan_sm, &tot);
+        uint64_t pos = inc - h;
+        for (uint32_t i = s0; i < s0 + per && i < P; i++) {
+            const unsigned long long x = sk[i];
+            const uint32_t key = (uint32_t)(x >> 32);
+            if (x != kNone && (i == 0 || (uint32_t)(sk[i - 1] >> 32) != key)) {
+                uint64_t sum = (uint32_t)x;
+                for (uint32_t q = i + 1; q < P && (uint32_t)(sk[q] >> 32) == key && sk[q] != kNone; q++)
+                    sum += (uint32_t)sk[q];
+                bdst[b + pos] = key;
+                tw[b + pos] = (WO)sum;
+                pos++;
+            }
+        }
+        if (threadIdx.x == 0) dcnt[c] = (uint32_t)tot;
+        __syncthreads();
+    }
+}
+
 // --------------------------------------------------------------- tier 3 --
 // scatter-add of the rows [r0, r0 + nrows) of the tier-3 list into dense
 // slots; blockIdx.y = row within the batch.
@@ -329,8 +416,10 @@ static int build_impl(Context &C, const Level &F, const WI *w, const uint32_t *v
     else if (avg <= 16) SGPB_ROWS_LAUNCH(KERNEL_T(16), 16, __VA_ARGS__)                    \
     else SGPB_ROWS_LAUNCH(KERNEL_T(32), 32, __VA_ARGS__)
 
+    uint32_t *krow;
+    SGPB_TRY(dalloc_t(C, &krow, (size_t)n + 1));
 #define K_COUNT(G) k_build_count<G>
-    SGPB_BY_G(K_COUNT, n, F.rp, F.col, vcmap, cnt)
+    SGPB_BY_G(K_COUNT, n, F.rp, F.col, vcmap, cnt, krow)
     SGPB_TRY(scan_u32(C, cnt, boff, nc, nullptr));
     uint32_t kept = 0;
     SGPB_TRY(read_u32(C, boff + nc, &kept));
@@ -341,7 +430,7 @@ static int build_impl(Context &C, const Level &F, const WI *w, const uint32_t *v
     if (w) SGPB_TRY(dalloc_t(C, &bw, (size_t)kept + 1));
     SGPB_TRY(dalloc_t(C, &tw, (size_t)kept + 1));
 #define K_SCATTER(G) k_build_scatter<G, WI>
-    SGPB_BY_G(K_SCATTER, n, F.rp, F.col, w, vcmap, boff, fill, bdst, bw)
+    SGPB_BY_G(K_SCATTER, n, F.rp, F.col, w, vcmap, krow, boff, fill, bdst, bw)
 #undef K_COUNT
 #undef K_SCATTER
 #undef SGPB_BY_G
@@ -352,10 +441,21 @@ static int build_impl(Context &C, const Level &F, const WI *w, const uint32_t *v
         uint32_t g1 = cdiv(nc, 8);
         if (g1 > (uint32_t)C.num_sms * 16) g1 = C.num_sms * 16;
         k_dedupe_warp<WI, WO><<<g1 ? g1 : 1, 256, 0, C.stream>>>(lists, tcount, boff, bdst, bw, tw, dcnt);
-        size_t sm2 = (size_t)kT2 * (sizeof(uint32_t) + sizeof(uint64_t));
-        SGPB_CUDA(cudaFuncSetAttribute(k_dedupe_block<WI, WO>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm2));
-        uint32_t g2 = (uint32_t)C.num_sms * 4;
-        k_dedupe_block<WI, WO><<<g2, kT2Threads, sm2, C.stream>>>(lists + nc, tcount + 1, boff, bdst, bw, tw, dcnt);
+        if constexpr (sizeof(WI) == 4) {
+            const size_t sm2 = (size_t)kT2 * sizeof(unsigned long long);
+            SGPB_CUDA(cudaFuncSetAttribute(k_dedupe_block_packed<WI, WO>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                           (int)sm2));
+            const uint32_t g2 = (uint32_t)C.num_sms * 6;
+            k_dedupe_block_packed<WI, WO><<<g2, kT2Threads, sm2, C.stream>>>(lists + nc, tcount + 1, boff, bdst, bw,
+                                                                            tw, dcnt);
+        } else {
+            const size_t sm2 = (size_t)kT2 * (sizeof(uint32_t) + sizeof(uint64_t));
+            SGPB_CUDA(cudaFuncSetAttribute(k_dedupe_block<WI, WO>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                           (int)sm2));
+            const uint32_t g2 = (uint32_t)C.num_sms * 4;
+            k_dedupe_block<WI, WO><<<g2, kT2Threads, sm2, C.stream>>>(lists + nc, tcount + 1, boff, bdst, bw, tw,
+                                                                     dcnt);
+        }
         C.kernel_launches += 3;
         SGPB_CUDA(cudaGetLastError());
         uint32_t n3 = 0;

@@ -45,11 +45,24 @@ __device__ __forceinline__ T warp_max(T v) {
     for (int o = 16; o > 0; o >>= 1) { T x = __shfl_xor_sync(0xFFFFFFFFu, v, o); v = x > v ? x : v; }
     return v;
 }
-// sum over aligned groups of G lanes (G power of two <= 32); result in all lanes of the group
+// mask of this lane's aligned group of G lanes (G power of two <= 32): the
+// lanes that a group-level shuffle may name, so groups of one warp can leave
+// a row loop after different numbers of rows
+template <int G>
+__device__ __forceinline__ unsigned group_mask() {
+    if constexpr (G == 32) {
+        return 0xFFFFFFFFu;
+    } else {
+        const unsigned lane = threadIdx.x & 31;
+        return ((1u << G) - 1u) << (lane & ~(unsigned)(G - 1));
+    }
+}
+// sum over aligned groups of G lanes; result in all lanes of the group
 template <int G, typename T>
 __device__ __forceinline__ T group_sum(T v) {
+    const unsigned gm = group_mask<G>();
 #pragma unroll
-    for (int o = G / 2; o > 0; o >>= 1) v += __shfl_xor_sync(0xFFFFFFFFu, v, o);
+    for (int o = G / 2; o > 0; o >>= 1) v += __shfl_xor_sync(gm, v, o);
     return v;
 }
 

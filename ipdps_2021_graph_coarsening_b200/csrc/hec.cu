@@ -34,6 +34,7 @@ template <int G, typename W>
 __global__ void __launch_bounds__(256) k_hn_heavy(uint32_t n, const uint32_t *__restrict__ rp,
                                                   const uint32_t *__restrict__ col, const W *__restrict__ w,
                                                   uint64_t seed, uint32_t *__restrict__ hn) {
+    const unsigned gm = group_mask<G>();
     const uint32_t lane = threadIdx.x & (G - 1);
     const uint64_t gid = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) / G;
     const uint64_t ngroups = ((uint64_t)gridDim.x * blockDim.x) / G;
@@ -50,9 +51,9 @@ __global__ void __launch_bounds__(256) k_hn_heavy(uint32_t n, const uint32_t *__
         }
 #pragma unroll
         for (int o = G / 2; o > 0; o >>= 1) {
-            uint64_t ow = __shfl_xor_sync(0xFFFFFFFFu, bw, o);
-            uint64_t ok = __shfl_xor_sync(0xFFFFFFFFu, bk, o);
-            int oh = __shfl_xor_sync(0xFFFFFFFFu, (int)have, o);
+            uint64_t ow = __shfl_xor_sync(gm, bw, o);
+            uint64_t ok = __shfl_xor_sync(gm, bk, o);
+            int oh = __shfl_xor_sync(gm, (int)have, o);
             if (oh && (!have || ow > bw || (ow == bw && ok > bk))) { bw = ow; bk = ok; have = true; }
         }
         if (lane == 0) hn[u] = (e == b) ? (uint32_t)(rand_draw(seed, u) % n) : (uint32_t)(bk & 0xFFFFFFFFu);
