@@ -190,7 +190,11 @@ static int eigensolve(Context &C, std::vector<Level> &levels, uint64_t *rng_stat
         SGPB_TRY(dalloc_t(C, &xo, lv.n));
         PowerIterResult r;
         const uint32_t *vc = (l == L - 1) ? nullptr : lv.vcmap;
-        SGPB_TRY(power_iter_level(C, lv, xin, vc, xo, o, &r, l == 0));
+        // the finest level runs few iterations from the prolonged vector: a
+        // relabelled copy of it would not pay for itself
+        PowerIterOpts ol = o;
+        ol.allow_relabel = o.allow_relabel && l > 0;
+        SGPB_TRY(power_iter_level(C, lv, xin, vc, xo, ol, &r, l == 0));
         lv.pi_iters = r.niter;
         lv.pi_ms = r.kernel_ms;
         lv.pi_capped = r.capped;

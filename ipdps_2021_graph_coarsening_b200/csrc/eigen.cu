@@ -76,8 +76,8 @@ struct PIArgs {
     uint32_t stall_window;
     double *res;                  // [0] niter [1] dot [2] gb [3] lambda [4] capped [5] stalled
     const uint32_t *inv;          // relabelled copy: new id -> level vertex id (null: identity)
-    uint32_t kcache;              // leading iterate entries kept in shared memory
-    int cache_ok;                 // host: use the shared-memory cache for this level
+    uint32_t kcache;              // leading iterate entries: shared-memory copy, or the L1 hub prefix
+    int cache_ok;                 // host: 2 shared-memory copy when it fits, 3 L1 hub prefix, 0 none
     // column panels (mode 6): the warp rows' entries regrouped panel by panel
     uint32_t P;                   // panels
     uint32_t PW;                  // iterate entries per panel (one block's shared-memory copy)
@@ -90,6 +90,8 @@ struct PIArgs {
 // dynamic shared memory for the iterate cache, per block (two blocks per SM)
 constexpr size_t kCacheBytesRows = 96 * 1024;
 constexpr size_t kCacheBytesStream = 48 * 1024;
+// iterate bytes of a relabelled level gathered with L1 evict-last priority
+constexpr size_t kSplitBytes = 128 * 1024;
 // dynamic shared memory for one column panel of the iterate, per block
 constexpr size_t kPanelBytes = 96 * 1024;
 constexpr uint32_t kMaxPanels = 31;
@@ -99,9 +101,8 @@ constexpr uint64_t kHeavyDivRows = 8;
 constexpr uint64_t kHeavyDivStream = 64;
 constexpr uint32_t kSegShift = 10;
 
-// The iterate as the SpMV gathers it: entries below k come from the block's
-// shared-memory copy (the most referenced vertices after hub-first
-// relabelling, or the whole vector of a small level), the rest from global.
+// The iterate of a small level as the SpMV gathers it: entries below k (all
+// of them) come from the block's shared-memory copy.
 template <typename V>
 struct XView {
     const V *g;
@@ -109,6 +110,40 @@ struct XView {
     uint32_t k;
     __device__ __forceinline__ V operator[](uint32_t c) const { return c < k ? s[c] : g[c]; }
 };
+
+// Gathers of a hub-first relabelled level through L1 only for its leading k
+// entries (the most referenced vertices, densely packed): those are loaded
+// with L1 evict-last priority, all others bypass L1 allocation, so the other
+// gathers cannot push the hub lines out of L1.
+__device__ __forceinline__ double ld_hub(const double *p) {
+    double v;
+    asm volatile("ld.global.L1::evict_last.f64 %0, [%1];" : "=d"(v) : "l"(p));
+    return v;
+}
+__device__ __forceinline__ float ld_hub(const float *p) {
+    float v;
+    asm volatile("ld.global.L1::evict_last.f32 %0, [%1];" : "=f"(v) : "l"(p));
+    return v;
+}
+__device__ __forceinline__ double ld_tail(const double *p) {
+    double v;
+    asm volatile("ld.global.L1::no_allocate.f64 %0, [%1];" : "=d"(v) : "l"(p));
+    return v;
+}
+__device__ __forceinline__ float ld_tail(const float *p) {
+    float v;
+    asm volatile("ld.global.L1::no_allocate.f32 %0, [%1];" : "=f"(v) : "l"(p));
+    return v;
+}
+template <typename V>
+struct SplitView {
+    const V *g;
+    uint32_t k;
+    __device__ __forceinline__ V operator[](uint32_t c) const { return c < k ? ld_hub(g + c) : ld_tail(g + c); }
+};
+
+// iterate sources of the SpMV gathers
+constexpr int kCacheNone = 0, kCachePrefix = 1, kCacheSplit = 2;
 
 __device__ __forceinline__ void grid_barrier(cg::grid_group &g) {
     if (gridDim.x == 1) __syncthreads();
@@ -513,11 +548,6 @@ __device__ __forceinline__ void warp_stream(const uint32_t *__restrict__ rp, con
     }
 }
 
-// MODE 0: normal rows streamed in warp tiles (short-row levels); MODE 4 / 8:
-// one warp per row with 4 / 8 loads in flight per lane (dense levels);
-// MODE 5: one warp per row, trips software-pipelined across rows.
-// NA: matrix loads bypass L1 allocation.  CACHE: gathers below kcache read the
-// block's shared-memory copy of the iterate.
 // Destinations of four consecutive panel entries (16-bit, panel-relative).
 template <bool NA>
 __device__ __forceinline__ void ld_pcol4(const uint16_t *p, uint32_t (&c)[4]) {
@@ -652,13 +682,21 @@ __device__ __forceinline__ void panel_rows32(const uint32_t *__restrict__ offp, 
     __syncwarp();
 }
 
-template <bool CACHE, typename V>
+template <int CACHE, typename V>
 __device__ __forceinline__ auto make_src(const V *g, const V *s, uint32_t k) {
-    if constexpr (CACHE) return XView<V>{g, s, k};
+    if constexpr (CACHE == kCachePrefix) return XView<V>{g, s, k};
+    else if constexpr (CACHE == kCacheSplit) return SplitView<V>{g, k};
     else return g;
 }
 
-template <typename W, typename V, int MODE, bool NA, bool CACHE>
+// MODE 0: normal rows streamed in warp tiles (short-row levels); MODE 4: one
+// warp per row with 4 loads in flight per lane; MODE 5: one warp per row,
+// trips software-pipelined across rows (dense levels); MODE 6: column panels.
+// NA: matrix loads bypass L1 allocation.  CACHE: kCachePrefix -- gathers read
+// the block's shared-memory copy of a small level's iterate; kCacheSplit --
+// gathers below kcache (the hub prefix of a relabelled level) use L1
+// evict-last priority, the others bypass L1 allocation.
+template <typename W, typename V, int MODE, bool NA, int CACHE>
 __global__ void __launch_bounds__(kPIThreads, 2) k_power_iter(PIArgs a) {
     constexpr bool STREAM = MODE == 0;
     cg::grid_group grid = cg::this_grid();
@@ -816,7 +854,7 @@ __global__ void __launch_bounds__(kPIThreads, 2) k_power_iter(PIArgs a) {
     while (true) {
         double P[kNP] = {0, 0, 0, 0, 0};
         // refresh the shared-memory copy of the leading iterate entries
-        if (CACHE && kc) {
+        if (CACHE == kCachePrefix && kc) {
             for (uint32_t c = threadIdx.x; c < kc; c += blockDim.x) xs[c] = src[c];
             __syncthreads();
         }
@@ -1222,11 +1260,11 @@ static bool panels_wanted(const Level &L, const PIArgs &a) {
     return s && !strcmp(s, "panel");
 }
 
-template <typename W, typename V, bool CACHE>
+template <typename W, typename V, int CACHE>
 static const void *pi_kernel_c(int mode) {
     if (mode == 0) return (const void *)k_power_iter<W, V, 0, true, CACHE>;
     if (mode == 5) return (const void *)k_power_iter<W, V, 5, true, CACHE>;
-    if (mode == 6) return (const void *)k_power_iter<W, V, 6, true, false>;
+    if (mode == 6) return (const void *)k_power_iter<W, V, 6, true, kCacheNone>;
     return (const void *)k_power_iter<W, V, 4, true, CACHE>;
 }
 
@@ -1235,17 +1273,24 @@ static int launch_pi(Context &C, PIArgs &a, uint32_t grid) {
     const PIVariant var = pi_variant(a);
     const size_t cache_bytes = var.mode == 0 ? kCacheBytesStream : kCacheBytesRows;
     const uint64_t kmax = cache_bytes / sizeof(V);
-    // cache_ok: 1 = relabelled copy (cache its hub prefix), 2 = only when the
-    // whole iterate fits, 0 = off
-    a.kcache = (a.cache_ok == 1 || (a.cache_ok == 2 && a.n <= kmax)) ? (uint32_t)(a.n < kmax ? a.n : kmax) : 0u;
+    // cache_ok: 2 = the whole iterate in shared memory when it fits, 3 =
+    // relabelled copy (L1 policy by hub prefix), 0 = off
+    a.kcache = (a.cache_ok == 2 && a.n <= kmax) ? (uint32_t)a.n : 0u;
+    const bool split = a.cache_ok == 3 && var.mode != 6;
+    if (split) a.kcache = (uint32_t)(a.n < kSplitBytes / sizeof(V) ? a.n : kSplitBytes / sizeof(V));
     if (var.mode == 6) a.kcache = 0;
-    const void *k = a.kcache ? pi_kernel_c<W, V, true>(var.mode) : pi_kernel_c<W, V, false>(var.mode);
-    const size_t dyn = var.mode == 6 ? (size_t)a.PW * sizeof(V) : (size_t)a.kcache * sizeof(V);
+    const void *k = split ? pi_kernel_c<W, V, kCacheSplit>(var.mode)
+                  : a.kcache ? pi_kernel_c<W, V, kCachePrefix>(var.mode) : pi_kernel_c<W, V, kCacheNone>(var.mode);
+    const size_t dyn = var.mode == 6 ? (size_t)a.PW * sizeof(V) : split ? 0 : (size_t)a.kcache * sizeof(V);
     if (var.mode == 6)
         SGPB_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kPanelBytes));
-    else if (a.kcache)
+    else if (a.kcache && !split)
         SGPB_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)cache_bytes));
     int per_sm = 0;
+    // shared-memory carveout preference in percent (SGPB_PI_CARVEOUT; -1 =
+    // the driver's choice)
+    if (const char *cv = getenv("SGPB_PI_CARVEOUT"))
+        SGPB_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributePreferredSharedMemoryCarveout, atoi(cv)));
     SGPB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, kPIThreads, dyn));
     if (per_sm < 1) {
         set_error("power-iteration kernel does not fit on an SM");
@@ -1329,18 +1374,19 @@ int power_iter_level(Context &C, const Level &Lin, const double *x_in, const uin
     if (n == 0) { *res = PowerIterResult(); return SGP_B200_OK; }
     PIArgs a;
     memset(&a, 0, sizeof(a));
-    // Skewed levels too large to keep whole in shared memory iterate on a
-    // hub-first relabelled copy whose most referenced entries are cached.
+    // A level whose whole iterate fits in 96 KB keeps it in shared memory.
+    // Skewed levels larger than the L1 hub prefix iterate on a hub-first
+    // relabelled copy: the most referenced entries then sit densely at the
+    // front of the iterate and are gathered with L1 evict-last priority while
+    // all other gathers bypass L1 allocation (measured on R-MAT scale 22
+    // level 1: 206 -> 187 ms).  SGPB_PI_RELABEL=0 turns the copy off.
     a.cache_ok = 2;
     Level L = Lin;
     {
         const double avg = (double)Lin.m / n;
-        // Off unless SGPB_PI_RELABEL=1: with rows in degree order the warps at
-        // the tail get long runs of one-entry rows and the barrier waits for
-        // them (measured 3-4x slower on R-MAT levels 0 and 1).
-        bool relabel = o.allow_relabel && n > kCacheBytesRows / sizeof(double) && avg >= 8.0;
+        bool relabel = o.allow_relabel && n > kSplitBytes / sizeof(double) && avg >= 8.0;
         const char *rs = getenv("SGPB_PI_RELABEL");
-        relabel = relabel && rs && atoi(rs) != 0;
+        if (rs && atoi(rs) == 0) relabel = false;
         if (relabel) {
             uint32_t *mx, hmx = 0;
             SGPB_TRY(dalloc_t(C, &mx, 1));
@@ -1356,7 +1402,7 @@ int power_iter_level(Context &C, const Level &Lin, const double *x_in, const uin
             uint32_t *perm = nullptr, *inv = nullptr;
             SGPB_TRY(hub_first_copy(C, Lin, &perm, &inv, &L));
             a.inv = inv;
-            a.cache_ok = 1;
+            a.cache_ok = 3;
         }
     }
     a.n = n; a.m = L.m; a.rp = L.rp; a.col = L.col; a.w = L.w;

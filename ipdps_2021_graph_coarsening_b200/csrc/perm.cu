@@ -1,11 +1,14 @@
 // perm.cu -- hub-first relabelled copy of a level for the power iteration.
 //
 // Column references of power-law levels concentrate on few vertices (on the
-// first coarse level of an R-MAT graph the 16k most referenced vertices carry
-// ~3/4 of all entries).  The power iteration of such a level runs on a copy
-// P A P^T whose vertices are ordered by descending floor(log2(degree)),
-// stable in the original order, so the most gathered iterate entries form a
-// prefix that the kernel keeps in shared memory.  The hierarchy itself is not
+// first coarse level of an R-MAT scale-20 graph the 16k most referenced
+// vertices carry ~3/4 of all entries, ~1/2 at scale 22).  The power iteration
+// of such a level runs on a copy P A P^T whose vertices are ordered by
+// descending floor(log2(degree)), stable in the original order, so the most
+// gathered iterate entries form a dense prefix: the kernel gathers it with L1
+// evict-last priority and every other entry without L1 allocation, and L1
+// keeps the hub lines.  Each row keeps its entries in their original order.
+// The hierarchy itself is not
 // relabelled; only the eigen-solve sees the copy, and it maps its start
 // vector in and its result out through the permutation.
 #include "common.cuh"

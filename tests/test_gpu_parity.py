@@ -239,6 +239,50 @@ def test_partition_column_panels(partitioner, monkeypatch):
     assert abs(rm.lam - o["lambda"]) <= 1e-4 * abs(o["lambda"])
 
 
+def rmat18_level1():
+    g = G.rmat(18, seed=2)
+    hn = O.hec_heavy(g.row_ptr, g.col, None, True, 5)
+    vc, nc, _ = O.hec_map(hn, 5)
+    return O.build_coarse(g.row_ptr, g.col, None, vc, nc)
+
+
+@pytest.mark.parametrize("variant", ["auto", "row4", "stream"])
+def test_power_iter_hub_first_copy(partitioner, monkeypatch, variant):
+    """A skewed level above 16384 vertices iterates on a hub-first
+    relabelled copy whose leading entries are gathered through L1; the
+    result (mapped back to the level's numbering) matches the run without
+    the copy and the oracle."""
+    rp, col, w = rmat18_level1()
+    n = rp.shape[0] - 1
+    assert n > 16384
+    if variant != "auto":
+        monkeypatch.setenv("SGPB_PI_MODE", variant)
+    x0 = torch.from_numpy(np.random.default_rng(n).random(n)).cuda()
+    args = (dev_u32(rp), dev_u32(col), dev_u32(w), x0, None, 1e-10, 400)
+    u_r, it_r, lam_r, res_r = partitioner.power_iter(*args)
+    monkeypatch.setenv("SGPB_PI_RELABEL", "0")
+    u_p, it_p, lam_p, _ = partitioner.power_iter(*args)
+    assert abs(it_r - it_p) <= 2
+    assert abs(lam_r - lam_p) <= 1e-9 * abs(lam_p)
+    if it_r == it_p:
+        assert 1 - abs(float(torch.dot(u_r, u_p))) <= 1e-9
+    u_o, it_o, lam_o = O.power_iter(rp, col, w, x0.cpu().numpy(), 1e-10, 400)
+    assert abs(it_r - it_o) <= max(2, it_o // 50)
+    assert abs(lam_r - lam_o) <= 1e-6 * abs(lam_o)
+    assert res_r >= 0
+
+
+def test_partition_with_and_without_hub_first_copy(partitioner, monkeypatch):
+    g = G.rmat(18, seed=2)
+    a = partitioner.partition(g, rng_state=21)
+    monkeypatch.setenv("SGPB_PI_RELABEL", "0")
+    b = partitioner.partition(g, rng_state=21)
+    assert a.level_n == b.level_n and a.rng_state == b.rng_state
+    assert a.level_n[1] > 16384
+    assert abs(a.edgecut - b.edgecut) <= 0.01 * b.edgecut
+    assert abs(a.lam - b.lam) <= 1e-6 * abs(b.lam)
+
+
 def test_power_iter_prolongation(partitioner):
     g = G.grid2d(40, 40)
     hn = O.hec_heavy(g.row_ptr, g.col, None, True, 3)
