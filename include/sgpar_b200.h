@@ -172,6 +172,7 @@ typedef struct {
     uint64_t rng_state;         /* rng after the call */
     float ms_total, ms_h2d, ms_coarsen, ms_eigen, ms_split, ms_d2h;
     uint32_t kernel_launches;
+    float ms_map, ms_build;     /* coarsening split into HEC mapping and coarse builds */
 } sgp_b200_result_t;
 
 void sgp_b200_default_options(sgp_b200_options_t *opt);
@@ -276,6 +277,20 @@ int sgp_b200_split(sgp_b200_ctx_t *ctx, uint32_t n, const uint32_t *row_ptr, con
  * scratch: calls that overlap on the GPU race and must be serialised. */
 int sgp_b200_split_noalloc(void *stream, uint32_t n, const uint32_t *row_ptr, const uint32_t *col,
                            const double *evec, uint32_t *part, uint64_t *result);
+
+/* Appends the record of one partition to the JSON metrics file `path` in the
+ * layout of the reference's ExperimentLoggerUtil::log
+ * (ExperimentLoggerUtil.cpp:145-192): "[" before the first record (first
+ * != 0), "," after every record but the last, "]" after the last (last != 0),
+ * so the reference's experiment runner aggregates it unchanged.  Times follow
+ * the reference's window (sgpar.h:2379-2407): total = upload + coarsening +
+ * eigensolve (not the split), coarsen = upload + coarsening, refine =
+ * eigensolve; coarsen-map / coarsen-build are the HEC and coarse-build shares;
+ * the per-kernel timers this path does not have are 0.  coarse-levels lists
+ * the levels coarsest first with their power iterations; the finest carries
+ * the cut. */
+int sgp_b200_write_metrics(const char *path, const sgp_b200_result_t *res, uint64_t edge_cut_4way,
+                           uint64_t partition_diff, int first, int last);
 
 /* Milliseconds of the phases of the last sgp_b200_partition / eigensolve. */
 int sgp_b200_last_timing(sgp_b200_ctx_t *ctx, float *ms_total, float *ms_coarsen,

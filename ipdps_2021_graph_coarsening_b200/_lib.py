@@ -52,7 +52,8 @@ class sgp_b200_result_t(ctypes.Structure):
                 ("level_hec_rounds", c_int * MAX_LEVELS), ("level_pi_ms", c_flt * MAX_LEVELS),
                 ("iter_max_reached", c_int),
                 ("rng_state", c_u64), ("ms_total", c_flt), ("ms_h2d", c_flt), ("ms_coarsen", c_flt),
-                ("ms_eigen", c_flt), ("ms_split", c_flt), ("ms_d2h", c_flt), ("kernel_launches", c_u32)]
+                ("ms_eigen", c_flt), ("ms_split", c_flt), ("ms_d2h", c_flt), ("kernel_launches", c_u32),
+                ("ms_map", c_flt), ("ms_build", c_flt)]
 
 
 _SIGS = {
@@ -94,6 +95,7 @@ _SIGS = {
                                     c_int, P(c_u64), P(c_dbl), P(c_dbl)]),
     "sgp_b200_split": (c_int, [c_vp, c_u32, c_vp, c_vp, c_vp, c_int, c_vp, P(c_u64)]),
     "sgp_b200_last_timing": (c_int, [c_vp, P(c_flt), P(c_flt), P(c_flt), P(c_flt)]),
+    "sgp_b200_write_metrics": (c_int, [ctypes.c_char_p, P(sgp_b200_result_t), c_u64, c_u64, c_int, c_int]),
     "sgp_b200_split_noalloc": (c_int, [c_vp, c_u32, c_vp, c_vp, c_vp, c_vp, c_vp]),
 }
 

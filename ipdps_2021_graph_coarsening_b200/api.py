@@ -137,6 +137,16 @@ def use_partition(part: np.ndarray, g: CSR) -> tuple[CSR, CSR]:
     return out[0], out[1]
 
 
+def write_metrics(path: str, result: "Result", edge_cut_4way: int = 0, partition_diff: int = 0,
+                  first: bool = True, last: bool = True) -> None:
+    """Append ``result`` to the JSON metrics file ``path`` in the layout of
+    the reference's ExperimentLoggerUtil::log (ExperimentLoggerUtil.cpp:145-192)."""
+    if result.raw is None:
+        raise ValueError("result has no C record (it was not produced by Partitioner)")
+    L.check(L.lib().sgp_b200_write_metrics(path.encode(), ctypes.byref(result.raw), edge_cut_4way, partition_diff,
+                                            int(first), int(last)), "sgp_b200_write_metrics")
+
+
 def compute_partition_edit_distance(p1: np.ndarray, p2: np.ndarray) -> int:
     a = np.ascontiguousarray(p1, dtype=np.uint32)
     b = np.ascontiguousarray(p2, dtype=np.uint32)
@@ -169,6 +179,9 @@ class Result:
     ms_split: float = 0.0
     ms_d2h: float = 0.0
     kernel_launches: int = 0
+    ms_map: float = 0.0
+    ms_build: float = 0.0
+    raw: object = None          # the C result struct (for write_metrics)
 
 
 class _DevArray:
@@ -257,7 +270,7 @@ class Partitioner:
                       list(res.level_hec_rounds[:nl]), list(res.level_pi_ms[:nl]), bool(res.iter_max_reached),
                       res.rng_state,
                       res.ms_total, res.ms_h2d, res.ms_coarsen, res.ms_eigen, res.ms_split, res.ms_d2h,
-                      res.kernel_launches)
+                      res.kernel_launches, res.ms_map, res.ms_build, res)
 
     def partition(self, g, cutoff: int = 50, tol: float = 1e-10, mixed: bool = False,
                   rng_state: int = 0x853C49E6748FEA9B, rng_inc: int = 1, iter_cap: int = 0,

@@ -130,6 +130,13 @@ static int generate(Context &C, const Level &L0, uint32_t cutoff, uint64_t *rng_
     levels.push_back(L0);
     int out_wbytes = 4;
     SGPB_TRY(weight_width(C, L0, &out_wbytes));
+    cudaEvent_t ev[3];
+    for (auto &e : ev) SGPB_CUDA(cudaEventCreate(&e));
+    struct EvFree {
+        cudaEvent_t *e;
+        ~EvFree() { for (int i = 0; i < 3; i++) cudaEventDestroy(e[i]); }
+    } evfree{ev};
+    C.t_map = C.t_build = 0;
     while (levels.back().n > cutoff) {
         Level &F = levels.back();
         uint32_t hi = pcg32(rng_state, rng_inc);
@@ -142,11 +149,20 @@ static int generate(Context &C, const Level &L0, uint32_t cutoff, uint64_t *rng_
         uint32_t nc = 0;
         int rounds = 0;
         const int random_level = (levels.size() == 1) && (L0.w == nullptr);
+        SGPB_CUDA(cudaEventRecord(ev[0], C.stream));
         SGPB_TRY(hec_map_level(C, F, random_level, seed, vcmap, nullptr, &nc, &rounds));
         F.vcmap = vcmap;
         F.hec_rounds = rounds;
+        SGPB_CUDA(cudaEventRecord(ev[1], C.stream));
         Level Cl;
         SGPB_TRY(build_coarse_level(C, F, vcmap, nc, out_wbytes, &Cl));
+        SGPB_CUDA(cudaEventRecord(ev[2], C.stream));
+        SGPB_CUDA(cudaEventSynchronize(ev[2]));
+        float a = 0, b = 0;
+        cudaEventElapsedTime(&a, ev[0], ev[1]);
+        cudaEventElapsedTime(&b, ev[1], ev[2]);
+        C.t_map += a;
+        C.t_build += b;
         levels.push_back(Cl);
         if (levels.size() > 200) break;
     }
@@ -273,6 +289,8 @@ static void fill_times(Context &C, const Events &E, sgp_b200_result_t *res) {
     res->ms_d2h = ev_ms(E.e[4], E.e[5]);
     res->ms_total = ev_ms(E.e[0], E.e[5]);
     res->kernel_launches = C.kernel_launches;
+    res->ms_map = C.t_map;
+    res->ms_build = C.t_build;
     C.t_total = res->ms_total; C.t_coarsen = res->ms_coarsen; C.t_eigen = res->ms_eigen; C.t_split = res->ms_split;
 }
 

@@ -52,6 +52,7 @@ struct Context {
     std::vector<sgp_b200_ctx_t *> workers;   // contexts of the batch workers (same device), kept across calls
     // timing of the last partition (ms, CUDA events)
     float t_total = 0, t_coarsen = 0, t_eigen = 0, t_split = 0, t_h2d = 0, t_d2h = 0;
+    float t_map = 0, t_build = 0;   // coarsening of the last partition: HEC mapping / coarse builds
     uint32_t kernel_launches = 0;
 };
 

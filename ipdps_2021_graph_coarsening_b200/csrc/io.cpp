@@ -122,4 +122,55 @@ int sgp_load_config(const char *config_f, config_t *c) {
     return EXIT_SUCCESS;
 }
 
+// ExperimentLoggerUtil.cpp:145-192 (record layout), :57-63 (coarse level),
+// sgpar.h:2405-2409 (timing window, finest cut), eigensolve_kokkos.h:190-198
+// (one coarse-level entry per power iteration, coarsest first).
+int sgp_b200_write_metrics(const char *path, const sgp_b200_result_t *r, uint64_t edge_cut_4way,
+                           uint64_t partition_diff, int first, int last) {
+    if (!path || !r) {
+        sgpb::set_error("null argument");
+        return SGP_B200_ERR_INVALID;
+    }
+    if (r->levels < 1 || r->levels > SGP_B200_MAX_LEVELS) {
+        sgpb::set_error("result holds %d levels", r->levels);
+        return SGP_B200_ERR_INVALID;
+    }
+    FILE *f = fopen(path, "a");
+    if (!f) {
+        sgpb::set_error("could not open %s", path);
+        return EXIT_FAILURE;
+    }
+    static const char *names[] = {"coarsen-map", "coarsen-build", "coarsen-count", "coarsen-prefix-sum",
+                                  "coarsen-bucket", "coarsen-dedupe", "coarsen-radix-sort", "coarsen-radix-dedupe",
+                                  "coarsen-write-graph", "coarsen-permute", "coarsen-map-construct", "fm-refine",
+                                  "fm-recoarsen", "heavy"};
+    const double s_h2d = r->ms_h2d / 1e3, s_coarsen = r->ms_coarsen / 1e3, s_eigen = r->ms_eigen / 1e3;
+    const double meas[14] = {r->ms_map / 1e3, r->ms_build / 1e3, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
+    if (first) fputc('[', f);
+    fprintf(f, "{\"edge-cut\":%llu,\"edge-cut-four-way\":%llu,\"partition-diff\":%llu,",
+            (unsigned long long)r->edgecut, (unsigned long long)edge_cut_4way, (unsigned long long)partition_diff);
+    fprintf(f, "\"total-duration-seconds\":%.9g,\"coarsen-duration-seconds\":%.9g,\"refine-duration-seconds\":%.9g,",
+            s_h2d + s_coarsen + s_eigen, s_h2d + s_coarsen, s_eigen);
+    fprintf(f, "\"number-coarse-levels\":%d,", r->levels);
+    fprintf(f, "\"level-1-first-two-passes-assign-rate\":0,\"level-1-total-passes\":%d,",
+            r->levels > 1 ? r->level_hec_rounds[0] : 0);
+    fprintf(f, "\"level-2-first-two-passes-assign-rate\":0,\"level-2-total-passes\":%d,",
+            r->levels > 2 ? r->level_hec_rounds[1] : 0);
+    for (int i = 0; i < 14; i++) fprintf(f, "\"%s-duration-seconds\":%.9g,", names[i], meas[i]);
+    fputs("\"coarse-levels\":[", f);
+    for (int l = r->levels - 1; l >= 0; l--) {
+        // the per-level cap without an iteration budget: 1e14 / n (eigensolve_kokkos.h:153), at most 5e6
+        uint64_t cap = r->level_n[l] ? 100000000000000ULL / r->level_n[l] : 0;
+        if (cap > 5000000ULL) cap = 5000000ULL;
+        fprintf(f, "%s{\"refine-iterations\":%llu,\"iteration-max-reached\":%d,\"number-vertices\":%u,"
+                   "\"unrefined-edge-cut\":%llu}",
+                l == r->levels - 1 ? "" : ",", (unsigned long long)r->level_iters[l],
+                r->level_iters[l] >= cap ? 1 : 0, r->level_n[l], (unsigned long long)(l == 0 ? r->edgecut : 0));
+    }
+    fputs("]}", f);
+    fputc(last ? ']' : ',', f);
+    fclose(f);
+    return SGP_B200_OK;
+}
+
 }  // extern "C"

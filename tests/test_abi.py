@@ -81,3 +81,48 @@ def test_no_silent_cpu_path_without_a_device():
         pytest.skip("a device is present")
     assert not L.lib().sgp_b200_create(0)
     assert L.last_error()
+
+
+# keys of one record of the reference's metrics file (ExperimentLoggerUtil.cpp:145-192)
+METRIC_KEYS = ["edge-cut", "edge-cut-four-way", "partition-diff", "total-duration-seconds",
+               "coarsen-duration-seconds", "refine-duration-seconds", "number-coarse-levels",
+               "level-1-first-two-passes-assign-rate", "level-1-total-passes",
+               "level-2-first-two-passes-assign-rate", "level-2-total-passes"] + \
+    [f"{k}-duration-seconds" for k in ["coarsen-map", "coarsen-build", "coarsen-count", "coarsen-prefix-sum",
+                                       "coarsen-bucket", "coarsen-dedupe", "coarsen-radix-sort",
+                                       "coarsen-radix-dedupe", "coarsen-write-graph", "coarsen-permute",
+                                       "coarsen-map-construct", "fm-refine", "fm-recoarsen", "heavy"]] + \
+    ["coarse-levels"]
+LEVEL_KEYS = ["refine-iterations", "iteration-max-reached", "number-vertices", "unrefined-edge-cut"]
+
+
+def test_metrics_file_has_the_reference_layout(tmp_path):
+    """Two records appended like the reference driver's loop (first / last
+    flags) form one JSON list with the reference's keys, in its order."""
+    import json
+    from ipdps_2021_graph_coarsening_b200.api import Result, write_metrics
+    recs = []
+    for k in range(2):
+        r = L.sgp_b200_result_t()
+        r.edgecut, r.levels = 100 + k, 3
+        for i, (n, it) in enumerate([(1000, 12), (300, 40), (40, 700)]):
+            r.level_n[i], r.level_iters[i], r.level_hec_rounds[i] = n, it, 5 + i
+        r.ms_h2d, r.ms_coarsen, r.ms_eigen, r.ms_split, r.ms_map, r.ms_build = 1.0, 4.0, 20.0, 2.0, 1.5, 2.5
+        recs.append(Result(None, r.edgecut, 0, 0.0, 0.0, 3, raw=r))
+    path = str(tmp_path / "metrics.json")
+    write_metrics(path, recs[0], edge_cut_4way=250, first=True, last=False)
+    write_metrics(path, recs[1], edge_cut_4way=260, first=False, last=True)
+    data = json.load(open(path))
+    assert len(data) == 2
+    for k, d in enumerate(data):
+        assert list(d) == METRIC_KEYS
+        assert d["edge-cut"] == 100 + k and d["edge-cut-four-way"] == 250 + 10 * k
+        assert abs(d["total-duration-seconds"] - 0.025) < 1e-12       # upload + coarsen + eigensolve
+        assert abs(d["coarsen-duration-seconds"] - 0.005) < 1e-12
+        assert abs(d["coarsen-map-duration-seconds"] - 0.0015) < 1e-12
+        assert d["number-coarse-levels"] == 3 and d["level-1-total-passes"] == 5 and d["level-2-total-passes"] == 6
+        lv = d["coarse-levels"]
+        assert [list(x) for x in lv] == [LEVEL_KEYS] * 3
+        assert [x["number-vertices"] for x in lv] == [40, 300, 1000]      # coarsest first
+        assert [x["unrefined-edge-cut"] for x in lv] == [0, 0, 100 + k]  # the finest carries the cut
+        assert [x["refine-iterations"] for x in lv] == [700, 40, 12]

@@ -153,3 +153,22 @@ def test_sharded_batch_on_one_rank(partitioner):
     for g, r in zip(gs, out):
         s = partitioner.partition(g, rng_state=6)
         assert np.array_equal(r.part, s.part) and r.edgecut == s.edgecut
+
+
+def test_metrics_record_of_a_partition(partitioner, tmp_path):
+    """A real partition written in the reference's metrics layout: phase
+    times add up and the levels match the result."""
+    import json
+    from ipdps_2021_graph_coarsening_b200.api import write_metrics
+    g = G.rmat(13, seed=3)
+    r = partitioner.partition(g, rng_state=2)
+    part4, _, cut4, _ = partitioner.partition_4way(g, rng_state=2)
+    path = str(tmp_path / "m.json")
+    write_metrics(path, r, edge_cut_4way=cut4)
+    (d,) = json.load(open(path))
+    assert d["edge-cut"] == r.edgecut and d["edge-cut-four-way"] == cut4
+    assert d["number-coarse-levels"] == r.levels == len(d["coarse-levels"])
+    assert [x["number-vertices"] for x in d["coarse-levels"]] == r.level_n[::-1]
+    assert [x["refine-iterations"] for x in d["coarse-levels"]] == r.level_iters[::-1]
+    assert 0 < d["coarsen-map-duration-seconds"] + d["coarsen-build-duration-seconds"] <= d["coarsen-duration-seconds"]
+    assert d["total-duration-seconds"] > d["refine-duration-seconds"] > 0
