@@ -234,6 +234,25 @@ __device__ __forceinline__ uint32_t ld_stream(const uint32_t *p) {
     }
     return __ldg(p);
 }
+// narrow weights of a relabelled copy (levels whose weights fit 8 / 16 bits)
+template <bool NA>
+__device__ __forceinline__ uint16_t ld_stream(const uint16_t *p) {
+    if (NA) {
+        unsigned short v;
+        asm("ld.global.nc.L1::no_allocate.u16 %0, [%1];" : "=h"(v) : "l"(p));
+        return v;
+    }
+    return __ldg(p);
+}
+template <bool NA>
+__device__ __forceinline__ uint8_t ld_stream(const uint8_t *p) {
+    if (NA) {
+        unsigned short v;
+        asm("ld.global.nc.L1::no_allocate.u8 %0, [%1];" : "=h"(v) : "l"(p));
+        return (uint8_t)v;
+    }
+    return __ldg(p);
+}
 template <bool NA>
 __device__ __forceinline__ unsigned long long ld_stream(const unsigned long long *p) {
     if (NA) {
@@ -379,7 +398,15 @@ __device__ __forceinline__ void load4(const uint32_t *__restrict__ col, const W 
         const uint4 v = ld_stream4<NA>(col + p);
         c[0] = v.x; c[1] = v.y; c[2] = v.z; c[3] = v.w;
         if (w) {
-            if (sizeof(W) == 4) {
+            if (sizeof(W) == 1) {   // four bytes at a 4-byte boundary (p is a multiple of 4)
+                const uint32_t q = ld_stream<NA>(reinterpret_cast<const uint32_t *>(w + p));
+                wt[0] = (W)(q & 0xFFu); wt[1] = (W)((q >> 8) & 0xFFu);
+                wt[2] = (W)((q >> 16) & 0xFFu); wt[3] = (W)(q >> 24);
+            } else if (sizeof(W) == 2) {   // four halves at an 8-byte boundary
+                const unsigned long long q = ld_stream<NA>(reinterpret_cast<const unsigned long long *>(w + p));
+                wt[0] = (W)(q & 0xFFFFu); wt[1] = (W)((q >> 16) & 0xFFFFu);
+                wt[2] = (W)((q >> 32) & 0xFFFFu); wt[3] = (W)(q >> 48);
+            } else if (sizeof(W) == 4) {
                 const uint4 q = ld_stream4<NA>(reinterpret_cast<const uint32_t *>(w + p));
                 wt[0] = (W)q.x; wt[1] = (W)q.y; wt[2] = (W)q.z; wt[3] = (W)q.w;
             } else {
@@ -1264,7 +1291,8 @@ template <typename W, typename V, int CACHE>
 static const void *pi_kernel_c(int mode) {
     if (mode == 0) return (const void *)k_power_iter<W, V, 0, true, CACHE>;
     if (mode == 5) return (const void *)k_power_iter<W, V, 5, true, CACHE>;
-    if (mode == 6) return (const void *)k_power_iter<W, V, 6, true, kCacheNone>;
+    if constexpr (sizeof(W) >= 4)
+        if (mode == 6) return (const void *)k_power_iter<W, V, 6, true, kCacheNone>;
     return (const void *)k_power_iter<W, V, 4, true, CACHE>;
 }
 
@@ -1279,8 +1307,18 @@ static int launch_pi(Context &C, PIArgs &a, uint32_t grid) {
     const bool split = a.cache_ok == 3 && var.mode != 6;
     if (split) a.kcache = (uint32_t)(a.n < kSplitBytes / sizeof(V) ? a.n : kSplitBytes / sizeof(V));
     if (var.mode == 6) a.kcache = 0;
-    const void *k = split ? pi_kernel_c<W, V, kCacheSplit>(var.mode)
+    const void *k = nullptr;
+    if constexpr (sizeof(W) < 4) {
+        // narrow weights exist only in relabelled copies, which use the split
+        if (!split) {
+            set_error("narrow weights outside a relabelled copy");
+            return SGP_B200_ERR_INVALID;
+        }
+        k = pi_kernel_c<W, V, kCacheSplit>(var.mode);
+    } else {
+        k = split ? pi_kernel_c<W, V, kCacheSplit>(var.mode)
                   : a.kcache ? pi_kernel_c<W, V, kCachePrefix>(var.mode) : pi_kernel_c<W, V, kCacheNone>(var.mode);
+    }
     const size_t dyn = var.mode == 6 ? (size_t)a.PW * sizeof(V) : split ? 0 : (size_t)a.kcache * sizeof(V);
     if (var.mode == 6)
         SGPB_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kPanelBytes));
@@ -1332,6 +1370,8 @@ static int run_pi(Context &C, const Level &L, PIArgs a, int mixed, double *res_d
         // partials are allocated inside launch_pi; the events bracket the launch
         SGPB_CUDA(cudaEventRecord(e0, C.stream));
         if (L.wbytes == 8) rc = launch_pi<unsigned long long, float>(C, a, grid);
+        else if (L.wbytes == 2) rc = launch_pi<uint16_t, float>(C, a, grid);
+        else if (L.wbytes == 1) rc = launch_pi<uint8_t, float>(C, a, grid);
         else rc = launch_pi<uint32_t, float>(C, a, grid);
     } else {
         double *va, *vb;
@@ -1340,6 +1380,8 @@ static int run_pi(Context &C, const Level &L, PIArgs a, int mixed, double *res_d
         a.va = va; a.vb = vb;
         SGPB_CUDA(cudaEventRecord(e0, C.stream));
         if (L.wbytes == 8) rc = launch_pi<unsigned long long, double>(C, a, grid);
+        else if (L.wbytes == 2) rc = launch_pi<uint16_t, double>(C, a, grid);
+        else if (L.wbytes == 1) rc = launch_pi<uint8_t, double>(C, a, grid);
         else rc = launch_pi<uint32_t, double>(C, a, grid);
     }
     cudaEventRecord(e1, C.stream);

@@ -79,7 +79,8 @@ inline uint32_t cdiv(uint64_t a, uint64_t b) { return (uint32_t)((a + b - 1) / b
 
 // --------------------------------------------------------------- levels --
 // One level of the hierarchy on the device.  wbytes: 0 = unit weights,
-// 4 = uint32, 8 = uint64.
+// 4 = uint32, 8 = uint64; 1 = uint8 and 2 = uint16 only in the relabelled
+// copy a power iteration makes of a level.
 struct Level {
     uint32_t n = 0;
     uint64_t m = 0;              // directed entries

@@ -64,12 +64,12 @@ __global__ void k_perm_degrees(uint32_t n, const uint32_t *rp, const uint32_t *i
     }
 }
 
-template <typename W>
+template <typename WI, typename WO>
 __global__ void __launch_bounds__(256) k_perm_fill(uint32_t n, const uint32_t *__restrict__ rp,
-                                                  const uint32_t *__restrict__ col, const W *__restrict__ w,
+                                                  const uint32_t *__restrict__ col, const WI *__restrict__ w,
                                                   const uint32_t *__restrict__ perm, const uint32_t *__restrict__ inv,
                                                   const uint32_t *__restrict__ nrp, uint32_t *__restrict__ ncol,
-                                                  W *__restrict__ nw) {
+                                                  WO *__restrict__ nw) {
     const unsigned lane = threadIdx.x & 31;
     const uint64_t wid = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
@@ -78,22 +78,33 @@ __global__ void __launch_bounds__(256) k_perm_fill(uint32_t n, const uint32_t *_
         const uint32_t b = rp[o], e = rp[o + 1], d = nrp[i];
         for (uint32_t j = b + lane; j < e; j += 32) {
             ncol[d + (j - b)] = perm[col[j]];
-            if (w) nw[d + (j - b)] = w[j];
+            if (w) nw[d + (j - b)] = (WO)w[j];
         }
     }
 }
 
-template <typename W>
+// the copy's weights are WO (as wide as the input, or narrower when every
+// weight fits); the padding lets vector loads run past the last entry
+template <typename WI, typename WO>
 static int fill_impl(Context &C, const Level &L, const uint32_t *perm, const uint32_t *inv, Level *out) {
-    W *nw = nullptr;
-    if (L.w) SGPB_TRY(dalloc_t(C, &nw, (size_t)L.m + 4));
+    WO *nw = nullptr;
+    if (L.w) SGPB_TRY(dalloc_t(C, &nw, (size_t)L.m + 16));
     uint32_t blocks = cdiv((uint64_t)L.n * 32, 256);
     if (blocks > (uint32_t)C.num_sms * 16) blocks = C.num_sms * 16;
-    k_perm_fill<W><<<blocks ? blocks : 1, 256, 0, C.stream>>>(L.n, L.rp, L.col, (const W *)L.w, perm, inv, out->rp,
-                                                             out->col, nw);
+    k_perm_fill<WI, WO><<<blocks ? blocks : 1, 256, 0, C.stream>>>(L.n, L.rp, L.col, (const WI *)L.w, perm, inv,
+                                                                  out->rp, out->col, nw);
     C.kernel_launches++;
     out->w = nw;
+    out->wbytes = L.w ? (int)sizeof(WO) : 0;
     return SGP_B200_OK;
+}
+
+__global__ void k_max_u32(uint64_t m, const uint32_t *w, uint32_t *out) {
+    uint32_t mx = 0;
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < m; i += (uint64_t)gridDim.x * blockDim.x)
+        mx = w[i] > mx ? w[i] : mx;
+    mx = warp_max(mx);
+    if ((threadIdx.x & 31) == 0 && mx) atomicMax(out, mx);
 }
 
 int hub_first_copy(Context &C, const Level &L, uint32_t **perm_out, uint32_t **inv_out, Level *out) {
@@ -115,8 +126,25 @@ int hub_first_copy(Context &C, const Level &L, uint32_t **perm_out, uint32_t **i
     SGPB_TRY(dalloc_t(C, &out->rp, (size_t)n + 1));
     SGPB_TRY(dalloc_t(C, &out->col, (size_t)L.m + 4));
     SGPB_TRY(scan_u32(C, deg, out->rp, n, nullptr));
-    if (L.wbytes == 8) SGPB_TRY(fill_impl<unsigned long long>(C, L, perm, inv, out));
-    else SGPB_TRY(fill_impl<uint32_t>(C, L, perm, inv, out));
+    if (L.wbytes == 8) {
+        SGPB_TRY((fill_impl<unsigned long long, unsigned long long>(C, L, perm, inv, out)));
+    } else if (L.w) {
+        // 32-bit weights that all fit 8 or 16 bits are stored narrow: the
+        // power iteration streams them every iteration
+        uint32_t *mx, hmx = 0;
+        SGPB_TRY(dalloc_t(C, &mx, 1));
+        SGPB_TRY(dzero(C, mx, 4));
+        uint32_t g = (uint32_t)cdiv(L.m, 256);
+        if (g > (uint32_t)C.num_sms * 8) g = C.num_sms * 8;
+        k_max_u32<<<g ? g : 1, 256, 0, C.stream>>>(L.m, (const uint32_t *)L.w, mx);
+        C.kernel_launches++;
+        SGPB_TRY(read_u32(C, mx, &hmx));
+        if (hmx <= 0xFFu) SGPB_TRY((fill_impl<uint32_t, uint8_t>(C, L, perm, inv, out)));
+        else if (hmx <= 0xFFFFu) SGPB_TRY((fill_impl<uint32_t, uint16_t>(C, L, perm, inv, out)));
+        else SGPB_TRY((fill_impl<uint32_t, uint32_t>(C, L, perm, inv, out)));
+    } else {
+        SGPB_TRY((fill_impl<uint32_t, uint32_t>(C, L, perm, inv, out)));
+    }
     SGPB_CUDA(cudaGetLastError());
     *perm_out = perm;
     *inv_out = inv;

@@ -246,13 +246,17 @@ def rmat18_level1():
     return O.build_coarse(g.row_ptr, g.col, None, vc, nc)
 
 
-@pytest.mark.parametrize("variant", ["auto", "row4", "stream"])
-def test_power_iter_hub_first_copy(partitioner, monkeypatch, variant):
+@pytest.mark.parametrize("variant,wscale", [("auto", 1), ("row4", 1), ("stream", 1), ("auto", 300),
+                                            ("stream", 300), ("auto", 100000)])
+def test_power_iter_hub_first_copy(partitioner, monkeypatch, variant, wscale):
     """A skewed level above 16384 vertices iterates on a hub-first
-    relabelled copy whose leading entries are gathered through L1; the
-    result (mapped back to the level's numbering) matches the run without
-    the copy and the oracle."""
+    relabelled copy whose leading entries are gathered through L1 and whose
+    weights are stored in 8 bits (wscale 1: all weights <= 255), 16 bits
+    (wscale 300) or 32 bits (wscale 100000); the result (mapped back to the
+    level's numbering) matches the run without the copy and the oracle."""
     rp, col, w = rmat18_level1()
+    w = w * wscale
+    assert int(w.max()) <= 0xFFFFFFFF and ((int(w.max()) <= 255) == (wscale == 1))
     n = rp.shape[0] - 1
     assert n > 16384
     if variant != "auto":
