@@ -121,8 +121,11 @@ def test_build_bit_exact(partitioner, graph, out_wbytes):
     assert np.array_equal(gw.astype(np.uint64), w2)
 
 
-def test_build_large_rows_dense_tier(partitioner):
-    g = star_plus_ring(12000, 4000)
+@pytest.mark.parametrize("n_leaves,ring", [(12000, 4000), (90000, 30000)])
+def test_build_large_rows_dense_tier(partitioner, n_leaves, ring):
+    """Buckets above 4096 entries: with few coarse vertices the dense slots
+    live in shared memory, with more (60001 here) in global memory."""
+    g = star_plus_ring(n_leaves, ring)
     # map everything in the first half to one aggregate: one huge bucket
     n = g.n
     vc = np.zeros(n, np.uint32)
