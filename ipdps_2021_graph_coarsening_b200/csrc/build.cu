@@ -367,61 +367,6 @@ __global__ void __launch_bounds__(256) k_dense_collect(const uint32_t *__restric
     if (threadIdx.x == 0) dcnt[c] = (uint32_t)base;
 }
 
-// Tier 3 when [0, nc) fits in shared memory: one block per bucket adds the
-// bucket's weights into a shared-memory slot per coarse destination, marks
-// them in a bitmap, and writes the distinct destinations in ascending order
-// with their sums back into the bucket (clearing the slots it used).
-constexpr uint32_t kDenseSmemThreads = 1024;
-constexpr size_t kDenseSmemBytes = 200 * 1024;
-
-template <typename WI, typename WO>
-__global__ void __launch_bounds__(kDenseSmemThreads) k_dense_smem(const uint32_t *__restrict__ list,
-                                                                 const uint32_t *__restrict__ count,
-                                                                 const uint32_t *__restrict__ boff, uint32_t nc,
-                                                                 uint32_t *__restrict__ bdst, const WI *__restrict__ bw,
-                                                                 WO *__restrict__ tw, uint32_t *__restrict__ dcnt) {
-    extern __shared__ __align__(16) unsigned char smraw[];
-    WO *acc = (WO *)smraw;
-    const uint32_t nwords = (nc + 31) / 32;
-    uint32_t *bits = (uint32_t *)(smraw + (((size_t)nc * sizeof(WO) + 15) & ~(size_t)15));
-    __shared__ uint64_t scan_sm[33];
-    for (uint32_t v = threadIdx.x; v < nc; v += blockDim.x) acc[v] = 0;
-    for (uint32_t q = threadIdx.x; q < nwords; q += blockDim.x) bits[q] = 0;
-    __syncthreads();
-    const uint32_t cntv = *count;
-    for (uint32_t k = blockIdx.x; k < cntv; k += gridDim.x) {
-        const uint32_t c = list[k];
-        const uint32_t b = boff[c], e = boff[c + 1];
-        for (uint32_t j = b + threadIdx.x; j < e; j += blockDim.x) {
-            const uint32_t v = bdst[j];
-            atomicAdd(acc + v, bw ? (WO)bw[j] : (WO)1);
-            atomicOr(bits + (v >> 5), 1u << (v & 31));
-        }
-        __syncthreads();
-        uint64_t base = 0;
-        for (uint32_t w0 = 0; w0 < nwords; w0 += blockDim.x) {
-            const uint32_t wi = w0 + threadIdx.x;
-            uint32_t word = wi < nwords ? bits[wi] : 0u;
-            const uint64_t pc = __popc(word);
-            uint64_t tot;
-            const uint64_t inc = block_scan_u64(pc, scan_sm, &tot);
-            uint64_t pos = base + inc - pc;
-            while (word) {
-                const uint32_t v = wi * 32 + (__ffs(word) - 1);
-                word &= word - 1;
-                bdst[b + pos] = v;
-                tw[b + pos] = acc[v];
-                acc[v] = 0;
-                pos++;
-            }
-            if (wi < nwords) bits[wi] = 0;
-            base += tot;
-        }
-        if (threadIdx.x == 0) dcnt[c] = (uint32_t)base;
-        __syncthreads();
-    }
-}
-
 // ---------------------------------------------------------- compaction --
 template <typename WO>
 __global__ void __launch_bounds__(256) k_compact_rows(uint32_t nc, const uint32_t *__restrict__ boff,
@@ -530,15 +475,7 @@ static int build_impl(Context &C, const Level &F, const WI *w, const uint32_t *v
         SGPB_CUDA(cudaGetLastError());
         uint32_t n3 = 0;
         SGPB_TRY(read_u32(C, tcount + 2, &n3));
-        const size_t dense_smem = (((size_t)nc * sizeof(WO) + 15) & ~(size_t)15) + (((size_t)nc + 31) / 32) * 4;
-        if (n3 && dense_smem <= kDenseSmemBytes) {
-            SGPB_CUDA(cudaFuncSetAttribute(k_dense_smem<WI, WO>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                           (int)dense_smem));
-            uint32_t g3 = n3 < (uint32_t)C.num_sms ? n3 : (uint32_t)C.num_sms;
-            k_dense_smem<WI, WO><<<g3, kDenseSmemThreads, dense_smem, C.stream>>>(lists + 2 * (size_t)nc, tcount + 2,
-                                                                               boff, nc, bdst, bw, tw, dcnt);
-            C.kernel_launches++;
-        } else if (n3) {
+        if (n3) {
             const size_t words = ((size_t)nc + 31) / 32;
             const size_t slot_bytes = (size_t)nc * sizeof(WO) + words * 4;
             size_t slots = ((size_t)1 << 30) / (slot_bytes ? slot_bytes : 1);

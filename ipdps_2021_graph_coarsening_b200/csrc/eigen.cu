@@ -1045,6 +1045,179 @@ __global__ void __launch_bounds__(kPIThreads, 2) k_power_iter(PIArgs a) {
     }
 }
 
+// ------------------------------------------------------- small levels --
+// A level that the main kernel would run on a single block (the coarsest
+// levels, which often need the most iterations) runs here: one block stages
+// the whole level (offsets, destinations, weights), its weighted degrees and
+// both iterate buffers in shared memory, one thread per row, and each
+// iteration costs three block barriers.  Same recurrence, stopping rule and
+// result as k_power_iter.
+constexpr int kSmallThreads = 1024;
+constexpr size_t kSmallSmemBytes = 200 * 1024;
+
+template <typename W, typename V>
+static size_t small_level_bytes(uint32_t n, uint64_t m, bool weighted) {
+    size_t b = ((size_t)n + 1) * 4 + (size_t)m * 4;
+    b = (b + 15) & ~(size_t)15;
+    if (weighted) b = (b + (size_t)m * sizeof(W) + 15) & ~(size_t)15;
+    b += (size_t)n * 8;                              // degrees
+    b += 2 * (((size_t)n * sizeof(V) + 15) & ~(size_t)15);
+    return b;
+}
+
+template <typename W, typename V>
+__global__ void __launch_bounds__(kSmallThreads, 1) k_power_iter_small(PIArgs a) {
+    typedef typename std::conditional<sizeof(V) == 8, double, float>::type ACC;
+    __shared__ double sm[256];
+    extern __shared__ __align__(16) unsigned char dyn_smem[];
+    const uint32_t n = a.n;
+    const uint64_t m = a.m;
+    const W *wg = (const W *)a.w;
+    unsigned char *p = dyn_smem;
+    uint32_t *rp = (uint32_t *)p;
+    p += ((size_t)n + 1) * 4;
+    uint32_t *col = (uint32_t *)p;
+    p += (size_t)m * 4;
+    p = (unsigned char *)(((uintptr_t)p + 15) & ~(uintptr_t)15);
+    W *w = nullptr;
+    if (wg) {
+        w = (W *)p;
+        p += (size_t)m * sizeof(W);
+        p = (unsigned char *)(((uintptr_t)p + 15) & ~(uintptr_t)15);
+    }
+    double *deg = (double *)p;
+    p += (size_t)n * 8;
+    V *xa = (V *)p;
+    p += ((size_t)n * sizeof(V) + 15) & ~(size_t)15;
+    V *xb = (V *)p;
+    for (uint32_t i = threadIdx.x; i <= n; i += blockDim.x) rp[i] = a.rp[i];
+    for (uint64_t j = threadIdx.x; j < m; j += blockDim.x) {
+        col[j] = a.col[j];
+        if (wg) w[j] = wg[j];
+    }
+    __syncthreads();
+    // phase 0: prolongation, weighted degrees, shift
+    double p_sum = 0, p_maxd = 0;
+    for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) {
+        const uint32_t b = rp[i], e = rp[i + 1];
+        double d = (double)(e - b);
+        if (wg) {
+            uint64_t s = 0;
+            for (uint32_t j = b; j < e; j++) s += (uint64_t)w[j];
+            d = (double)s;
+        }
+        deg[i] = d;
+        p_maxd = d > p_maxd ? d : p_maxd;
+        const V xs = (V)(a.vcmap ? a.x_in[a.vcmap[i]] : a.x_in[i]);
+        xa[i] = xs;
+        p_sum += (double)xs;
+    }
+    double v2[2] = {p_sum, 0};
+    block_sum_d<2>(v2, sm);
+    {
+        const double mx = warp_max(p_maxd);
+        if ((threadIdx.x & 31) == 0) sm[210 + (threadIdx.x >> 5)] = mx;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double mxd = 0;
+        for (int k = 0; k < (int)(blockDim.x >> 5); k++) mxd = sm[210 + k] > mxd ? sm[210 + k] : mxd;
+        sm[200] = v2[0];
+        sm[201] = mxd;
+    }
+    __syncthreads();
+    const double S1 = sm[200];
+    double gb = 2.0 * sm[201];
+    if (gb < 2.0) gb = 2.0;
+    double mu = S1 / (double)n;
+    __syncthreads();
+    double p_sq = 0;
+    for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) {
+        const double x = (double)xa[i] - mu;
+        p_sq += x * x;
+    }
+    double q2[2] = {p_sq, 0};
+    block_sum_d<2>(q2, sm);
+    if (threadIdx.x == 0) sm[200] = q2[0];
+    __syncthreads();
+    double inv_nu = 1.0 / sqrt(sm[200]);
+    __syncthreads();
+    double dot = 0, last = 1, best_delta = 1e300;
+    uint64_t best_at = 0, niter = 0;
+    V *src = xa, *dst = xb;
+    // rows of at least 8 entries on average: one warp per row, else one thread
+    const bool warp_rows = m >= 8ull * n;
+    const unsigned lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+    while (true) {
+        double P[kNP] = {0, 0, 0, 0, 0};
+        auto fin = [&](uint32_t i, ACC acc) {
+            const double d = deg[i];
+            const double ui = ((double)src[i] - mu) * inv_nu;
+            const double r = (gb - d) * ui + ((double)acc - mu * d) * inv_nu;
+            const V rs = (V)r;
+            dst[i] = rs;
+            const double rd = (double)rs;
+            P[0] += rd; P[1] += rd * rd; P[2] += ui * rd; P[3] += ui; P[4] += ui * ui;
+        };
+        if (warp_rows) {
+            for (uint32_t i = wid; i < n; i += nwarps) {
+                const uint32_t b = rp[i], e = rp[i + 1];
+                ACC acc = 0;
+                for (uint32_t j = b + lane; j < e; j += 32) {
+                    const V x = src[col[j]];
+                    acc += (ACC)(wg ? (V)w[j] * x : x);
+                }
+                acc = warp_sum(acc);
+                if (lane == 0) fin(i, acc);
+            }
+        } else {
+            for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) {
+                const uint32_t b = rp[i], e = rp[i + 1];
+                ACC acc = 0;
+                for (uint32_t j = b; j < e; j++) {
+                    const V x = src[col[j]];
+                    acc += (ACC)(wg ? (V)w[j] * x : x);
+                }
+                fin(i, acc);
+            }
+        }
+        block_sum_d<kNP>(P, sm);
+        if (threadIdx.x == 0)
+#pragma unroll
+            for (int k = 0; k < kNP; k++) sm[200 + k] = P[k];
+        __syncthreads();
+        double S[kNP];
+#pragma unroll
+        for (int k = 0; k < kNP; k++) S[k] = sm[200 + k];
+        __syncthreads();
+        const double mu_n = S[0] / (double)n;
+        const double nsq = S[1] - mu_n * S[0];
+        const double inv_nu_n = 1.0 / sqrt(nsq);
+        last = dot;
+        dot = (S[2] - mu_n * S[3]) * inv_nu_n;
+        niter++;
+        const double delta = fabs(dot - last);
+        if (niter > 2 && delta < best_delta * a.stall_factor) { best_delta = delta; best_at = niter; }
+        const bool converged = !(delta > a.tol && niter < a.iter_max);
+        const bool stalled = a.stall_factor > 0 && niter > 2 && niter - best_at > a.stall_window;
+        if (converged || stalled) {
+            for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) a.out[i] = ((double)src[i] - mu) * inv_nu;
+            if (threadIdx.x == 0) {
+                a.res[0] = (double)niter;
+                a.res[1] = dot;
+                a.res[2] = gb;
+                a.res[3] = (gb * S[4] - S[2]) / S[4];
+                a.res[4] = niter >= a.iter_max ? 1.0 : 0.0;
+                a.res[5] = converged ? 0.0 : 1.0;
+            }
+            return;
+        }
+        mu = mu_n;
+        inv_nu = inv_nu_n;
+        V *t = src; src = dst; dst = t;
+    }
+}
+
 // ----------------------------------------------------------- residual --
 // |L x - lambda x|^2 partial sums per block (x unit-norm FP64 vector).
 template <typename W>
@@ -1058,10 +1231,21 @@ __global__ void __launch_bounds__(256) k_residual(uint32_t n, const uint32_t *__
     const uint64_t nw = ((uint64_t)gridDim.x * blockDim.x) >> 5;
     for (uint64_t i = wid; i < n; i += nw) {
         double acc = 0, d = 0;
-        for (uint32_t j = rp[i] + lane; j < rp[i + 1]; j += 32) {
-            double wt = w ? (double)w[j] : 1.0;
-            acc += wt * x[col[j]];
-            d += wt;
+        const uint32_t e = rp[i + 1];
+        for (uint32_t j0 = rp[i] + lane; j0 < e; j0 += 128) {
+            uint32_t c[4];
+            double wt[4];
+#pragma unroll
+            for (int k = 0; k < 4; k++) {
+                const uint32_t j = j0 + 32 * k;
+                c[k] = j < e ? col[j] : 0u;
+                wt[k] = j < e ? (w ? (double)w[j] : 1.0) : 0.0;
+            }
+#pragma unroll
+            for (int k = 0; k < 4; k++) {
+                acc += wt[k] * (j0 + 32 * k < e ? x[c[k]] : 0.0);
+                d += wt[k];
+            }
         }
         acc = warp_sum(acc);
         d = warp_sum(d);
@@ -1362,7 +1546,29 @@ static int run_pi(Context &C, const Level &L, PIArgs a, int mixed, double *res_d
     cudaEvent_t e0, e1;
     SGPB_CUDA(cudaEventCreate(&e0));
     SGPB_CUDA(cudaEventCreate(&e1));
-    if (mixed) {
+    // levels the main kernel would run on one block, when they fit in shared
+    // memory (not when SGPB_PI_MODE forces a variant of the main kernel)
+    const char *forced = getenv("SGPB_PI_MODE");
+    const bool small = !(forced && *forced) && !a.P && !a.inv && grid == 1 &&
+                       (L.wbytes == 0 || L.wbytes == 4 || L.wbytes == 8) &&
+                       (mixed ? small_level_bytes<unsigned long long, float>(L.n, L.m, L.w != nullptr)
+                              : small_level_bytes<unsigned long long, double>(L.n, L.m, L.w != nullptr)) <=
+                           kSmallSmemBytes;
+    if (small) {
+        auto launch_small = [&](auto wtag, auto vtag) -> int {
+            using Wt = decltype(wtag);
+            using Vt = decltype(vtag);
+            const size_t bytes = small_level_bytes<Wt, Vt>(L.n, L.m, L.w != nullptr);
+            const void *k = (const void *)k_power_iter_small<Wt, Vt>;
+            SGPB_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
+            SGPB_CUDA(cudaEventRecord(e0, C.stream));
+            k_power_iter_small<Wt, Vt><<<1, kSmallThreads, bytes, C.stream>>>(a);
+            C.kernel_launches++;
+            return SGP_B200_OK;
+        };
+        if (mixed) rc = L.wbytes == 8 ? launch_small((unsigned long long)0, 0.0f) : launch_small((uint32_t)0, 0.0f);
+        else rc = L.wbytes == 8 ? launch_small((unsigned long long)0, 0.0) : launch_small((uint32_t)0, 0.0);
+    } else if (mixed) {
         float *va, *vb;
         SGPB_TRY(dalloc_t(C, &va, L.n));
         SGPB_TRY(dalloc_t(C, &vb, L.n));

@@ -43,11 +43,22 @@ __global__ void __launch_bounds__(256) k_hn_heavy(uint32_t n, const uint32_t *__
         uint32_t b = rp[u], e = rp[u + 1];
         uint64_t bw = 0, bk = 0;   // (weight, tiebreak<<32 | dest); 0 = none
         bool have = false;
-        for (uint32_t j = b + lane; j < e; j += G) {
-            uint32_t v = __ldg(col + j);
-            uint64_t wt = wload(w, j);
-            uint64_t k = ((uint64_t)tiebreak(seed, u, v) << 32) | v;
-            if (!have || wt > bw || (wt == bw && k > bk)) { bw = wt; bk = k; have = true; }
+        for (uint32_t j0 = b + lane; j0 < e; j0 += 4 * G) {
+            // four entries per lane in flight, then the lexicographic max
+            uint32_t v[4];
+            uint64_t wt[4];
+#pragma unroll
+            for (int q = 0; q < 4; q++) {
+                const uint32_t j = j0 + q * G;
+                v[q] = j < e ? __ldg(col + j) : 0u;
+                wt[q] = j < e ? wload(w, j) : 0ull;
+            }
+#pragma unroll
+            for (int q = 0; q < 4; q++) {
+                if (j0 + q * G >= e) continue;
+                const uint64_t k = ((uint64_t)tiebreak(seed, u, v[q]) << 32) | v[q];
+                if (!have || wt[q] > bw || (wt[q] == bw && k > bk)) { bw = wt[q]; bk = k; have = true; }
+            }
         }
 #pragma unroll
         for (int o = G / 2; o > 0; o >>= 1) {

@@ -76,9 +76,26 @@ __global__ void __launch_bounds__(256) k_perm_fill(uint32_t n, const uint32_t *_
     for (uint64_t i = wid; i < n; i += nwarps) {
         const uint32_t o = inv[i];
         const uint32_t b = rp[o], e = rp[o + 1], d = nrp[i];
-        for (uint32_t j = b + lane; j < e; j += 32) {
-            ncol[d + (j - b)] = perm[col[j]];
-            if (w) nw[d + (j - b)] = (WO)w[j];
+        // four entries per lane in flight: destinations, their new ids, stores
+        for (uint32_t j0 = b + lane; j0 < e; j0 += 128) {
+            uint32_t c[4];
+            WI x[4];
+#pragma unroll
+            for (int k = 0; k < 4; k++) {
+                const uint32_t j = j0 + 32 * k;
+                c[k] = j < e ? col[j] : 0u;
+                if (w) x[k] = j < e ? w[j] : (WI)0;
+            }
+#pragma unroll
+            for (int k = 0; k < 4; k++) c[k] = j0 + 32 * k < e ? perm[c[k]] : 0u;
+#pragma unroll
+            for (int k = 0; k < 4; k++) {
+                const uint32_t j = j0 + 32 * k;
+                if (j < e) {
+                    ncol[d + (j - b)] = c[k];
+                    if (w) nw[d + (j - b)] = (WO)x[k];
+                }
+            }
         }
     }
 }

@@ -123,8 +123,8 @@ def test_build_bit_exact(partitioner, graph, out_wbytes):
 
 @pytest.mark.parametrize("n_leaves,ring", [(12000, 4000), (90000, 30000)])
 def test_build_large_rows_dense_tier(partitioner, n_leaves, ring):
-    """Buckets above 4096 entries: with few coarse vertices the dense slots
-    live in shared memory, with more (60001 here) in global memory."""
+    """Buckets above 4096 entries (the dense tier), with 6001 and 60001
+    coarse vertices."""
     g = star_plus_ring(n_leaves, ring)
     # map everything in the first half to one aggregate: one huge bucket
     n = g.n
@@ -288,6 +288,33 @@ def test_partition_with_and_without_hub_first_copy(partitioner, monkeypatch):
     assert a.level_n[1] > 16384
     assert abs(a.edgecut - b.edgecut) <= 0.01 * b.edgecut
     assert abs(a.lam - b.lam) <= 1e-6 * abs(b.lam)
+
+
+@pytest.mark.parametrize("weighted", [False, True])
+@pytest.mark.parametrize("name", ["grid", "rmat10"])
+def test_power_iter_small_level_kernel(partitioner, monkeypatch, weighted, name):
+    """Levels that fit one block run on the shared-memory small-level kernel
+    (one thread per row for the grid, one warp per row for the denser R-MAT);
+    it follows the main kernel's recurrence (forced here with a variant)."""
+    g = G.grid2d(33, 47) if name == "grid" else G.rmat(10, seed=4)
+    assert g.m_directed + 8 * g.n <= 32768
+    rp, col, w = g.row_ptr, g.col, None
+    if weighted:
+        hn = O.hec_heavy(rp, col, None, True, 5)
+        vc, nc, _ = O.hec_map(hn, 5)
+        rp, col, w = O.build_coarse(rp, col, None, vc, nc)
+    n = rp.shape[0] - 1
+    x0 = torch.from_numpy(np.random.default_rng(n).random(n)).cuda()
+    args = (dev_u32(rp), dev_u32(col), None if w is None else dev_u32(w), x0, None, 1e-10, 3000)
+    u_s, it_s, lam_s, _ = partitioner.power_iter(*args)
+    monkeypatch.setenv("SGPB_PI_MODE", "rowp")
+    u_m, it_m, lam_m, _ = partitioner.power_iter(*args)
+    assert abs(it_s - it_m) <= 2
+    assert abs(lam_s - lam_m) <= 1e-9 * abs(lam_m)
+    u_o, it_o, lam_o = O.power_iter(rp, col, w, x0.cpu().numpy(), 1e-10, 3000)
+    assert abs(it_s - it_o) <= max(2, it_o // 50) and abs(lam_s - lam_o) <= 1e-6 * abs(lam_o)
+    if it_s == it_o:
+        assert 1 - abs(float(np.dot(u_s.cpu().numpy(), u_o))) <= 1e-8
 
 
 def test_power_iter_prolongation(partitioner):
