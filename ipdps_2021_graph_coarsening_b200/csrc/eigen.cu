@@ -1046,13 +1046,14 @@ __global__ void __launch_bounds__(kPIThreads, 2) k_power_iter(PIArgs a) {
 }
 
 // ------------------------------------------------------- small levels --
-// A level that the main kernel would run on a single block (the coarsest
-// levels, which often need the most iterations) runs here: one block stages
+// A small level (the coarsest levels, which often need the most
+// iterations) runs here: one block stages
 // the whole level (offsets, destinations, weights), its weighted degrees and
 // both iterate buffers in shared memory, one thread per row, and each
 // iteration costs three block barriers.  Same recurrence, stopping rule and
 // result as k_power_iter.
 constexpr int kSmallThreads = 1024;
+constexpr uint64_t kSmallCost = 32768;   // m + 8n of the largest level run here
 constexpr size_t kSmallSmemBytes = 200 * 1024;
 
 template <typename W, typename V>
@@ -1433,7 +1434,11 @@ static int build_panels(Context &C, const Level &L, uint32_t T, size_t vbytes, P
 
 static uint32_t pi_grid(const Context &C, uint64_t n, uint64_t m) {
     const uint64_t maxg = (uint64_t)2 * C.num_sms;   // two resident blocks per SM (launch bounds)
-    const uint64_t want = cdiv(m + 8 * n, (uint64_t)kPIThreads * 64);
+    // 16 cost units per thread: mid-size levels are latency-bound, and more
+    // warps shorten each warp's serial chain of rows (a 50k-vertex
+    // Erdos-Renyi graph: 63 -> 31 ms); levels large enough to fill the GPU
+    // are unaffected
+    const uint64_t want = cdiv(m + 8 * n, (uint64_t)kPIThreads * 16);
     uint64_t grid = want < maxg ? want : maxg;
     return (uint32_t)(grid < 1 ? 1 : grid);
 }
@@ -1546,10 +1551,10 @@ static int run_pi(Context &C, const Level &L, PIArgs a, int mixed, double *res_d
     cudaEvent_t e0, e1;
     SGPB_CUDA(cudaEventCreate(&e0));
     SGPB_CUDA(cudaEventCreate(&e1));
-    // levels the main kernel would run on one block, when they fit in shared
-    // memory (not when SGPB_PI_MODE forces a variant of the main kernel)
+    // levels of at most kSmallCost cost units that fit in shared memory (not
+    // when SGPB_PI_MODE forces a variant of the main kernel)
     const char *forced = getenv("SGPB_PI_MODE");
-    const bool small = !(forced && *forced) && !a.P && !a.inv && grid == 1 &&
+    const bool small = !(forced && *forced) && !a.P && !a.inv && L.m + 8ull * L.n <= kSmallCost &&
                        (L.wbytes == 0 || L.wbytes == 4 || L.wbytes == 8) &&
                        (mixed ? small_level_bytes<unsigned long long, float>(L.n, L.m, L.w != nullptr)
                               : small_level_bytes<unsigned long long, double>(L.n, L.m, L.w != nullptr)) <=
