@@ -270,8 +270,10 @@ __global__ void __launch_bounds__(kT2Threads) k_dedupe_block_packed(const uint32
         for (uint32_t i = threadIdx.x; i < P; i += blockDim.x)
             sk[i] = i < sz ? ((unsigned long long)bdst[b + i] << 32) | (bw ? (uint32_t)bw[b + i] : 1u) : kNone;
         __syncthreads();
+        const unsigned lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
         for (uint32_t kk = 2; kk <= P; kk <<= 1) {
-            for (uint32_t j = kk >> 1; j > 0; j >>= 1) {
+            // partners 64 or more apart: pairs through shared memory
+            for (uint32_t j = kk >> 1; j >= 64; j >>= 1) {
                 for (uint32_t t = threadIdx.x; t < P / 2; t += blockDim.x) {
                     const uint32_t i = ((t & ~(j - 1)) << 1) | (t & (j - 1));
                     const uint32_t q = i | j;
@@ -281,6 +283,31 @@ __global__ void __launch_bounds__(kT2Threads) k_dedupe_block_packed(const uint32
                 }
                 __syncthreads();
             }
+            // partners closer than 64: each warp sorts 64-word chunks in
+            // registers, two consecutive words per lane (the partner of word
+            // q at distance j >= 2 is the same word of lane ^ j/2)
+            for (uint32_t ch = wid; ch < P / 64; ch += nwarps) {
+                const uint32_t q0 = ch * 64 + 2 * lane;
+                const ulonglong2 v = reinterpret_cast<const ulonglong2 *>(sk)[q0 >> 1];
+                unsigned long long x0 = v.x, x1 = v.y;
+                const bool up = (q0 & kk) == 0;   // same for both words: kk > 1
+                for (uint32_t j = (kk >> 1) < 32 ? (kk >> 1) : 32; j >= 2; j >>= 1) {
+                    const unsigned long long y0 = __shfl_xor_sync(0xFFFFFFFFu, x0, j >> 1);
+                    const unsigned long long y1 = __shfl_xor_sync(0xFFFFFFFFu, x1, j >> 1);
+                    const bool lower = (q0 & j) == 0;
+                    // the lower word of a pair keeps the minimum when ascending
+                    const bool keep_min = lower == up;
+                    x0 = keep_min ? (y0 < x0 ? y0 : x0) : (y0 > x0 ? y0 : x0);
+                    x1 = keep_min ? (y1 < x1 ? y1 : x1) : (y1 > x1 ? y1 : x1);
+                }
+                if (up ? x0 > x1 : x0 < x1) {   // j = 1: the lane's own pair
+                    const unsigned long long t = x0;
+                    x0 = x1;
+                    x1 = t;
+                }
+                reinterpret_cast<ulonglong2 *>(sk)[q0 >> 1] = make_ulonglong2(x0, x1);
+            }
+            __syncthreads();
         }
         // heads of destination runs; each thread owns a contiguous segment
         const uint32_t per = P / blockDim.x > 0 ? P / blockDim.x : 1;
