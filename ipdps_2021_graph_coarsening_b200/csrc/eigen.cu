@@ -97,7 +97,7 @@ constexpr size_t kPanelBytes = 96 * 1024;
 constexpr uint32_t kMaxPanels = 31;
 // rows above one warp's share of the cost / kHeavyDiv* are cut into segments
 // of 2^kSegShift entries that the block's warps share
-constexpr uint64_t kHeavyDivRows = 8;
+constexpr uint64_t kHeavyDivRows = 16;
 constexpr uint64_t kHeavyDivStream = 64;
 constexpr uint32_t kSegShift = 10;
 
