@@ -1232,21 +1232,10 @@ __global__ void __launch_bounds__(256) k_residual(uint32_t n, const uint32_t *__
     const uint64_t nw = ((uint64_t)gridDim.x * blockDim.x) >> 5;
     for (uint64_t i = wid; i < n; i += nw) {
         double acc = 0, d = 0;
-        const uint32_t e = rp[i + 1];
-        for (uint32_t j0 = rp[i] + lane; j0 < e; j0 += 128) {
-            uint32_t c[4];
-            double wt[4];
-#pragma unroll
-            for (int k = 0; k < 4; k++) {
-                const uint32_t j = j0 + 32 * k;
-                c[k] = j < e ? col[j] : 0u;
-                wt[k] = j < e ? (w ? (double)w[j] : 1.0) : 0.0;
-            }
-#pragma unroll
-            for (int k = 0; k < 4; k++) {
-                acc += wt[k] * (j0 + 32 * k < e ? x[c[k]] : 0.0);
-                d += wt[k];
-            }
+        for (uint32_t j = rp[i] + lane; j < rp[i + 1]; j += 32) {
+            double wt = w ? (double)w[j] : 1.0;
+            acc += wt * x[col[j]];
+            d += wt;
         }
         acc = warp_sum(acc);
         d = warp_sum(d);
