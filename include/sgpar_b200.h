@@ -90,8 +90,9 @@ int compute_partition_edit_distance(const sgp_vid_t *part1, const sgp_vid_t *par
  * iteration (tolerance config->tol, FP64) up the hierarchy, median split.
  * part[n] is caller-allocated host memory; *edge_cut receives the cut of the
  * bisection.  rng seeds the mapping hashes and the coarsest guess and is
- * advanced.  config->refine_alg must be 0 (shifted combinatorial Laplacian)
- * and config->local_search_alg 0; other values return EXIT_FAILURE.  With
+ * advanced.  config->refine_alg 0 (shifted combinatorial Laplacian) or 1
+ * (normalized Laplacian) and config->local_search_alg 0; other values return
+ * EXIT_FAILURE.  With
  * config->num_partitions == 4 the call still bisects (the 4-way recursion is
  * the caller's, sgpar.cpp:62-89, via sgp_use_partition). */
 int sgp_partition_graph(sgp_vid_t *part, sgp_eid_t *edge_cut, config_t *config,
@@ -152,6 +153,9 @@ typedef struct {
     uint64_t iter_cap;          /* extra cap on power iterations per level, 0 = none */
     uint64_t rng_state, rng_inc;/* PCG32 seeding (advanced copy returned in result) */
     int part_mem;               /* memory kind of result->part */
+    int refine_alg;             /* 0: shifted combinatorial Laplacian (reference default);
+                                   1: normalized Laplacian, lazy random walk (I + D^-1 A) / 2
+                                   without deflation in the loop, as eigensolve_kokkos.h:103-206 */
 } sgp_b200_options_t;
 
 #define SGP_B200_MAX_LEVELS 202

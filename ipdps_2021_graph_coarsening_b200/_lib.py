@@ -42,7 +42,8 @@ class sgp_b200_graph_t(ctypes.Structure):
 
 class sgp_b200_options_t(ctypes.Structure):
     _fields_ = [("cutoff", c_u32), ("tol", c_dbl), ("mixed", c_int), ("perc_imbalance", c_int),
-                ("iter_cap", c_u64), ("rng_state", c_u64), ("rng_inc", c_u64), ("part_mem", c_int)]
+                ("iter_cap", c_u64), ("rng_state", c_u64), ("rng_inc", c_u64), ("part_mem", c_int),
+                ("refine_alg", c_int)]
 
 
 class sgp_b200_result_t(ctypes.Structure):

@@ -244,11 +244,13 @@ class Partitioner:
         return dg
 
     @staticmethod
-    def _options(cutoff, tol, mixed, rng_state, rng_inc, iter_cap, perc_imbalance) -> L.sgp_b200_options_t:
+    def _options(cutoff, tol, mixed, rng_state, rng_inc, iter_cap, perc_imbalance,
+                 refine_alg: int = 0) -> L.sgp_b200_options_t:
         o = L.sgp_b200_options_t()
         L.lib().sgp_b200_default_options(ctypes.byref(o))
         o.cutoff, o.tol, o.mixed, o.perc_imbalance = cutoff, tol, int(mixed), perc_imbalance
         o.iter_cap, o.rng_state, o.rng_inc = iter_cap, rng_state, rng_inc
+        o.refine_alg = refine_alg
         return o
 
     @staticmethod
@@ -274,14 +276,14 @@ class Partitioner:
 
     def partition(self, g, cutoff: int = 50, tol: float = 1e-10, mixed: bool = False,
                   rng_state: int = 0x853C49E6748FEA9B, rng_inc: int = 1, iter_cap: int = 0,
-                  perc_imbalance: int = 0, part_out=None) -> Result:
+                  perc_imbalance: int = 0, part_out=None, refine_alg: int = 0) -> Result:
         """Partition ``g``: a host :class:`CSR` (numpy) or a dict of CUDA torch
         tensors ``{"row_ptr", "col", "w"}`` (device-resident input).  The
         partition is written to ``part_out`` (numpy or CUDA tensor) when
         given, else returned as numpy."""
         keep = []
         dg = self._graph(g, keep)
-        o = self._options(cutoff, tol, mixed, rng_state, rng_inc, iter_cap, perc_imbalance)
+        o = self._options(cutoff, tol, mixed, rng_state, rng_inc, iter_cap, perc_imbalance, refine_alg)
         res = L.sgp_b200_result_t()
         part_out, res.part = self._part_target(dg.n, part_out, o)
         L.check(L.lib().sgp_b200_partition(self._ctx, ctypes.byref(dg), ctypes.byref(o), ctypes.byref(res)),

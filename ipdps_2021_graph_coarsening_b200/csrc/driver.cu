@@ -234,6 +234,10 @@ static float ev_ms(cudaEvent_t a, cudaEvent_t b) {
 // before staging (the H2D window), ev[1..4] are recorded here.
 static int partition_staged(Context &C, const Level &L0, const sgp_b200_options_t *opt, sgp_b200_result_t *res,
                             uint32_t *part_d, cudaEvent_t *ev) {
+    if (opt->refine_alg != 0 && opt->refine_alg != 1) {
+        set_error("refine_alg %d: 0 (shifted combinatorial Laplacian) or 1 (normalized Laplacian)", opt->refine_alg);
+        return SGP_B200_ERR_INVALID;
+    }
     SGPB_CUDA(cudaEventRecord(ev[1], C.stream));
     uint64_t st = opt->rng_state;
     std::vector<Level> levels;
@@ -243,6 +247,7 @@ static int partition_staged(Context &C, const Level &L0, const sgp_b200_options_
     po.tol = opt->tol;
     po.iter_cap = opt->iter_cap;
     po.mixed = opt->mixed;
+    po.normlap = opt->refine_alg == 1;
     double *evec = nullptr;
     PowerIterResult fin;
     SGPB_TRY(eigensolve(C, levels, &st, opt->rng_inc, po, &evec, &fin));
@@ -401,6 +406,7 @@ void sgp_b200_default_options(sgp_b200_options_t *o) {
     o->rng_state = 0x853c49e6748fea9bULL;
     o->rng_inc = 1;
     o->part_mem = SGP_B200_HOST;
+    o->refine_alg = 0;
 }
 
 int sgp_b200_partition(sgp_b200_ctx_t *x, const sgp_b200_graph_t *g, const sgp_b200_options_t *opt,
@@ -678,8 +684,9 @@ int sgp_partition_graph(sgp_vid_t *part, sgp_eid_t *edge_cut, config_t *config, 
         set_error("null argument");
         return 1;
     }
-    if (config->refine_alg != 0 || config->local_search_alg != 0) {
-        set_error("only refine_alg 0 (shifted combinatorial Laplacian) and local_search_alg 0 are on this path");
+    if ((config->refine_alg != 0 && config->refine_alg != 1) || config->local_search_alg != 0) {
+        set_error("refine_alg must be 0 (shifted combinatorial Laplacian) or 1 (normalized Laplacian), "
+                  "local_search_alg 0");
         return 1;
     }
     Context *C = default_ctx();
@@ -694,6 +701,7 @@ int sgp_partition_graph(sgp_vid_t *part, sgp_eid_t *edge_cut, config_t *config, 
     sgp_b200_options_t o;
     sgp_b200_default_options(&o);
     o.tol = config->tol > 0 ? config->tol : g_tol;
+    o.refine_alg = config->refine_alg;
     o.perc_imbalance = perc_imbalance_allowed;
     o.rng_state = rng->state;
     o.rng_inc = rng->inc;

@@ -78,6 +78,7 @@ struct PIArgs {
     const uint32_t *inv;          // relabelled copy: new id -> level vertex id (null: identity)
     uint32_t kcache;              // leading iterate entries: shared-memory copy, or the L1 hub prefix
     int cache_ok;                 // host: 2 shared-memory copy when it fits, 3 L1 hub prefix, 0 none
+    int normlap;                  // refine_alg 1: lazy random walk (I + D^-1 A) / 2, no deflation in the loop
     // column panels (mode 6): the warp rows' entries regrouped panel by panel
     uint32_t P;                   // panels
     uint32_t PW;                  // iterate entries per panel (one block's shared-memory copy)
@@ -768,7 +769,7 @@ __global__ void __launch_bounds__(kPIThreads, 2) k_power_iter(PIArgs a) {
     const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
 
     // ---- phase 0a: prolongate / load the start vector, weighted degrees
-    double p_sum = 0, p_maxd = 0;
+    double p_sum = 0, p_maxd = 0, p_xd = 0, p_d = 0;   // p_xd, p_d: D-weighted mean (normlap)
     for (uint64_t i64 = gwarp; i64 < n; i64 += nwarps) {
         const uint32_t i = (uint32_t)i64;
         const uint32_t b = a.rp[i], e = a.rp[i + 1];
@@ -787,6 +788,8 @@ __global__ void __launch_bounds__(kPIThreads, 2) k_power_iter(PIArgs a) {
             if (!w || e - b <= a.heavy_T) {
                 a.deg[i] = d;
                 if (d > p_maxd) p_maxd = d;
+                p_xd += (double)xs * d;
+                p_d += d;
             }
         }
     }
@@ -802,44 +805,58 @@ __global__ void __launch_bounds__(kPIThreads, 2) k_power_iter(PIArgs a) {
             if (threadIdx.x == 0) {
                 a.deg[i] = sd;
                 if (sd > p_maxd) p_maxd = sd;
+                const uint32_t o = a.inv ? a.inv[i] : i;
+                const V xs = (V)(a.vcmap ? a.x_in[a.vcmap[o]] : a.x_in[o]);
+                p_xd += (double)xs * sd;
+                p_d += sd;
             }
         }
     }
     {
-        double v2[2] = {p_sum, 0};
-        block_sum_d<2>(v2, sm);
+        double v3[3] = {p_sum, p_xd, p_d};
+        block_sum_d<3>(v3, sm);
         double mx = warp_max(p_maxd);
         if ((threadIdx.x & 31) == 0) sm[210 + (threadIdx.x >> 5)] = mx;
         __syncthreads();
         if (threadIdx.x == 0) {
             double m = 0;
             for (int k = 0; k < (int)(blockDim.x >> 5); k++) m = sm[210 + k] > m ? sm[210 + k] : m;
-            part0[(size_t)blockIdx.x * kNP + 0] = v2[0];
+            part0[(size_t)blockIdx.x * kNP + 0] = v3[0];
             part0[(size_t)blockIdx.x * kNP + 1] = m;
+            part0[(size_t)blockIdx.x * kNP + 2] = v3[1];
+            part0[(size_t)blockIdx.x * kNP + 3] = v3[2];
         }
     }
     grid_barrier(grid);
-    double S1 = 0, maxd = 0;
+    double S1 = 0, maxd = 0, Sxd = 0, Sd = 0;
     {
         if (threadIdx.x < 32) {
-            double s = 0, m = 0;
+            double s = 0, m = 0, xd = 0, dd = 0;
             for (uint32_t b = lane; b < gridDim.x; b += 32) {
                 s += part0[(size_t)b * kNP + 0];
                 double x = part0[(size_t)b * kNP + 1];
                 m = x > m ? x : m;
+                xd += part0[(size_t)b * kNP + 2];
+                dd += part0[(size_t)b * kNP + 3];
             }
             s = warp_sum(s);
             m = warp_max(m);
-            if (lane == 0) { sm[0] = s; sm[1] = m; }
+            xd = warp_sum(xd);
+            dd = warp_sum(dd);
+            if (lane == 0) { sm[0] = s; sm[1] = m; sm[2] = xd; sm[3] = dd; }
         }
         __syncthreads();
         S1 = sm[0];
         maxd = sm[1];
+        Sxd = sm[2];
+        Sd = sm[3];
         __syncthreads();
     }
     double gb = 2.0 * maxd;
     if (gb < 2.0) gb = 2.0;
-    double mu = S1 / (double)n;
+    // the start vector is orthogonalised against the constant vector (mean)
+    // or, for the normalized Laplacian, D-orthogonalised (degree-weighted mean)
+    double mu = a.normlap ? (Sd > 0 ? Sxd / Sd : 0.0) : S1 / (double)n;
     // ---- phase 0b: norm of the deflated start vector
     double p_sq = 0;
     for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
@@ -890,7 +907,8 @@ __global__ void __launch_bounds__(kPIThreads, 2) k_power_iter(PIArgs a) {
         // and its own raw iterate value xi
         auto fin = [&](uint32_t i, ACC acc, double d, double xi) {
             const double ui = (xi - mu) * inv_nu;
-            const double r = (gb - d) * ui + ((double)acc - mu * d) * inv_nu;
+            const double au = ((double)acc - mu * d) * inv_nu;   // (A u)_i
+            const double r = a.normlap ? 0.5 * ui + (d > 0 ? 0.5 * au / d : 0.0) : (gb - d) * ui + au;
             const V rs = (V)r;
             dst[i] = rs;
             const double rd = (double)rs;
@@ -1000,7 +1018,8 @@ __global__ void __launch_bounds__(kPIThreads, 2) k_power_iter(PIArgs a) {
             for (uint32_t sg = a.hseg[i]; sg < a.hseg[i + 1]; sg++) acc += a.hpart[sg];
             const double d = w ? (e > b ? a.deg[i] : 0.0) : (double)(e - b);
             const double ui = ((double)src[i] - mu) * inv_nu;
-            const double r = (gb - d) * ui + (acc - mu * d) * inv_nu;
+            const double au = (acc - mu * d) * inv_nu;
+            const double r = a.normlap ? 0.5 * ui + (d > 0 ? 0.5 * au / d : 0.0) : (gb - d) * ui + au;
             const V rs = (V)r;
             dst[i] = rs;
             const double rd = (double)rs;
@@ -1014,7 +1033,7 @@ __global__ void __launch_bounds__(kPIThreads, 2) k_power_iter(PIArgs a) {
         grid_barrier(grid);
         double S[kNP];
         reduce_partials(part, S, sm);
-        const double mu_n = S[0] / (double)n;
+        const double mu_n = a.normlap ? 0.0 : S[0] / (double)n;   // no deflation in the normalized loop
         const double nsq = S[1] - mu_n * S[0];
         const double inv_nu_n = 1.0 / sqrt(nsq);
         last = dot;
@@ -1033,7 +1052,9 @@ __global__ void __launch_bounds__(kPIThreads, 2) k_power_iter(PIArgs a) {
                 a.res[0] = (double)niter;
                 a.res[1] = dot;
                 a.res[2] = gb;
-                a.res[3] = (gb * S[4] - S[2]) / S[4];
+                // eigenvalue: of L from the shifted operator, or of the
+                // random-walk Laplacian from the lazy walk's quotient
+                a.res[3] = a.normlap ? 2.0 * (1.0 - S[2] / S[4]) : (gb * S[4] - S[2]) / S[4];
                 a.res[4] = niter >= a.iter_max ? 1.0 : 0.0;
                 a.res[5] = converged ? 0.0 : 1.0;
             }
@@ -1098,7 +1119,7 @@ __global__ void __launch_bounds__(kSmallThreads, 1) k_power_iter_small(PIArgs a)
     }
     __syncthreads();
     // phase 0: prolongation, weighted degrees, shift
-    double p_sum = 0, p_maxd = 0;
+    double p_sum = 0, p_maxd = 0, p_xd = 0, p_d = 0;
     for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) {
         const uint32_t b = rp[i], e = rp[i + 1];
         double d = (double)(e - b);
@@ -1112,9 +1133,11 @@ __global__ void __launch_bounds__(kSmallThreads, 1) k_power_iter_small(PIArgs a)
         const V xs = (V)(a.vcmap ? a.x_in[a.vcmap[i]] : a.x_in[i]);
         xa[i] = xs;
         p_sum += (double)xs;
+        p_xd += (double)xs * d;
+        p_d += d;
     }
-    double v2[2] = {p_sum, 0};
-    block_sum_d<2>(v2, sm);
+    double v2[3] = {p_sum, p_xd, p_d};
+    block_sum_d<3>(v2, sm);
     {
         const double mx = warp_max(p_maxd);
         if ((threadIdx.x & 31) == 0) sm[210 + (threadIdx.x >> 5)] = mx;
@@ -1125,12 +1148,14 @@ __global__ void __launch_bounds__(kSmallThreads, 1) k_power_iter_small(PIArgs a)
         for (int k = 0; k < (int)(blockDim.x >> 5); k++) mxd = sm[210 + k] > mxd ? sm[210 + k] : mxd;
         sm[200] = v2[0];
         sm[201] = mxd;
+        sm[202] = v2[1];
+        sm[203] = v2[2];
     }
     __syncthreads();
     const double S1 = sm[200];
     double gb = 2.0 * sm[201];
     if (gb < 2.0) gb = 2.0;
-    double mu = S1 / (double)n;
+    double mu = a.normlap ? (sm[203] > 0 ? sm[202] / sm[203] : 0.0) : S1 / (double)n;
     __syncthreads();
     double p_sq = 0;
     for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) {
@@ -1154,7 +1179,8 @@ __global__ void __launch_bounds__(kSmallThreads, 1) k_power_iter_small(PIArgs a)
         auto fin = [&](uint32_t i, ACC acc) {
             const double d = deg[i];
             const double ui = ((double)src[i] - mu) * inv_nu;
-            const double r = (gb - d) * ui + ((double)acc - mu * d) * inv_nu;
+            const double au = ((double)acc - mu * d) * inv_nu;
+            const double r = a.normlap ? 0.5 * ui + (d > 0 ? 0.5 * au / d : 0.0) : (gb - d) * ui + au;
             const V rs = (V)r;
             dst[i] = rs;
             const double rd = (double)rs;
@@ -1191,7 +1217,7 @@ __global__ void __launch_bounds__(kSmallThreads, 1) k_power_iter_small(PIArgs a)
 #pragma unroll
         for (int k = 0; k < kNP; k++) S[k] = sm[200 + k];
         __syncthreads();
-        const double mu_n = S[0] / (double)n;
+        const double mu_n = a.normlap ? 0.0 : S[0] / (double)n;   // no deflation in the normalized loop
         const double nsq = S[1] - mu_n * S[0];
         const double inv_nu_n = 1.0 / sqrt(nsq);
         last = dot;
@@ -1207,7 +1233,9 @@ __global__ void __launch_bounds__(kSmallThreads, 1) k_power_iter_small(PIArgs a)
                 a.res[0] = (double)niter;
                 a.res[1] = dot;
                 a.res[2] = gb;
-                a.res[3] = (gb * S[4] - S[2]) / S[4];
+                // eigenvalue: of L from the shifted operator, or of the
+                // random-walk Laplacian from the lazy walk's quotient
+                a.res[3] = a.normlap ? 2.0 * (1.0 - S[2] / S[4]) : (gb * S[4] - S[2]) / S[4];
                 a.res[4] = niter >= a.iter_max ? 1.0 : 0.0;
                 a.res[5] = converged ? 0.0 : 1.0;
             }
@@ -1221,10 +1249,12 @@ __global__ void __launch_bounds__(kSmallThreads, 1) k_power_iter_small(PIArgs a)
 
 // ----------------------------------------------------------- residual --
 // |L x - lambda x|^2 partial sums per block (x unit-norm FP64 vector).
+// normlap: the random-walk Laplacian I - D^-1 A instead of L = D - A.
 template <typename W>
 __global__ void __launch_bounds__(256) k_residual(uint32_t n, const uint32_t *__restrict__ rp,
                                                  const uint32_t *__restrict__ col, const W *__restrict__ w,
-                                                 const double *__restrict__ x, double lambda, double *part) {
+                                                 const double *__restrict__ x, double lambda, int normlap,
+                                                 double *part) {
     __shared__ double sm[96];
     double s[2] = {0, 0};
     const unsigned lane = threadIdx.x & 31;
@@ -1240,7 +1270,7 @@ __global__ void __launch_bounds__(256) k_residual(uint32_t n, const uint32_t *__
         acc = warp_sum(acc);
         d = warp_sum(d);
         if (lane == 0) {
-            double r = d * x[i] - acc - lambda * x[i];
+            double r = normlap ? x[i] - (d > 0 ? acc / d : 0.0) - lambda * x[i] : d * x[i] - acc - lambda * x[i];
             s[0] += r * r;
             s[1] += x[i] * x[i];
         }
@@ -1648,6 +1678,7 @@ int power_iter_level(Context &C, const Level &Lin, const double *x_in, const uin
         }
     }
     a.n = n; a.m = L.m; a.rp = L.rp; a.col = L.col; a.w = L.w;
+    a.normlap = o.normlap;
     a.vec_ok = (((uintptr_t)L.col | (uintptr_t)L.w) & 15u) == 0;
     // the variant decides the heavy-row threshold and the cost model
     bool want_panels = panels_wanted(L, a);
@@ -1761,17 +1792,18 @@ int power_iter_level(Context &C, const Level &Lin, const double *x_in, const uin
         if (Lin.wbytes == 8)
             k_residual<unsigned long long><<<nb, 256, 0, C.stream>>>(n, Lin.rp, Lin.col,
                                                                      (const unsigned long long *)Lin.w, x_out,
-                                                                     res->lambda, part);
+                                                                     res->lambda, o.normlap, part);
         else
             k_residual<uint32_t><<<nb, 256, 0, C.stream>>>(n, Lin.rp, Lin.col, (const uint32_t *)Lin.w, x_out,
-                                                           res->lambda, part);
+                                                           res->lambda, o.normlap, part);
         k_sum_pairs<<<1, 32, 0, C.stream>>>(part, nb, out2);
         C.kernel_launches += 2;
         SGPB_CUDA(cudaGetLastError());
         SGPB_CUDA(cudaMemcpyAsync(C.h_pinned, out2, 2 * sizeof(double), cudaMemcpyDeviceToHost, C.stream));
         SGPB_CUDA(cudaStreamSynchronize(C.stream));
         double r2 = ((double *)C.h_pinned)[0], x2 = ((double *)C.h_pinned)[1];
-        res->resid = sqrt(r2 / (x2 > 0 ? x2 : 1)) / (res->gb > 0 ? res->gb : 1);
+        const double scale = o.normlap ? 2.0 : (res->gb > 0 ? res->gb : 1);   // bound on the spectrum
+        res->resid = sqrt(r2 / (x2 > 0 ? x2 : 1)) / scale;
     }
     return SGP_B200_OK;
 }

@@ -109,6 +109,7 @@ struct PowerIterOpts {
     uint64_t iter_cap = 0;   // 0: the reference's 1e14 / n only
     int mixed = 0;           // 1: float vector storage / gathers, fp64 reductions
     int allow_relabel = 1;   // skewed levels may iterate on a hub-first relabelled copy
+    int normlap = 0;         // refine_alg 1: normalized-Laplacian (lazy random walk) iteration
 };
 struct PowerIterResult {
     uint64_t niter = 0;

@@ -67,6 +67,8 @@ def lib():
         L.orc_power_iter.argtypes = [c_u32, u32p, u32p, ctypes.c_void_p, f64p, c_dbl, c_u64,
                                      ctypes.POINTER(c_dbl)]
         L.orc_power_iter.restype = c_u64
+        L.orc_power_iter_nl.argtypes = L.orc_power_iter.argtypes
+        L.orc_power_iter_nl.restype = c_u64
         L.orc_compute_partition.argtypes = [c_u32, u32p, u32p, f64p, c_int, u32p, u64ref]
         L.orc_compute_partition.restype = c_int
         L.orc_edge_cut.argtypes = [c_u32, u32p, u32p, u32p]
@@ -74,7 +76,7 @@ def lib():
         L.orc_use_partition.argtypes = [c_u32, u32p, u32p, u32p, u32ref, u32p, u32p, u32ref, u32p, u32p]
         L.orc_use_partition.restype = c_int
         L.orc_partition_graph.argtypes = [c_u32, u32p, u32p, ctypes.c_void_p, c_u32, c_dbl,
-                                          u64ref, c_u64, c_int, u32p, u64ref, f64p, f64p]
+                                          u64ref, c_u64, c_int, c_int, u32p, u64ref, f64p, f64p]
         L.orc_partition_graph.restype = c_int
         _orc = L
     return _orc
@@ -152,6 +154,18 @@ def power_iter(row_ptr, col, w, u0, tol: float = 1e-10, iter_cap: int = 0):
     return u, int(it), lam.value
 
 
+def power_iter_normalized(row_ptr, col, w, u0, tol: float = 1e-10, iter_cap: int = 0):
+    """refine_alg 1 (normalized Laplacian).  Returns (u, niter, eigenvalue of
+    the random-walk Laplacian)."""
+    rp, cl = _u32(row_ptr), _u32(col)
+    n = rp.shape[0] - 1
+    u = np.ascontiguousarray(u0, dtype=np.float64).copy()
+    keep, wp = _w64(w)
+    lam = ctypes.c_double(0)
+    it = lib().orc_power_iter_nl(n, rp, cl, wp, u, tol, iter_cap, ctypes.byref(lam))
+    return u, int(it), lam.value
+
+
 def compute_partition(row_ptr, col, evec, perc_imbalance: int = 0):
     rp, cl = _u32(row_ptr), _u32(col)
     n = rp.shape[0] - 1
@@ -180,7 +194,7 @@ def use_partition(row_ptr, col, part):
 
 
 def partition_graph(row_ptr, col, w=None, cutoff: int = 50, tol: float = 1e-10,
-                    rng_state: int = 42, rng_inc: int = 1, perc_imbalance: int = 0):
+                    rng_state: int = 42, rng_inc: int = 1, perc_imbalance: int = 0, refine_alg: int = 0):
     """Whole multilevel path.  Returns dict(part, edgecut, evec, levels,
     lambda, niter (finest), level_n, level_iters, rng_state)."""
     rp, cl = _u32(row_ptr), _u32(col)
@@ -191,7 +205,7 @@ def partition_graph(row_ptr, col, w=None, cutoff: int = 50, tol: float = 1e-10,
     s = ctypes.c_uint64(rng_state)
     ec = ctypes.c_uint64(0)
     keep, wp = _w64(w)
-    lib().orc_partition_graph(n, rp, cl, wp, cutoff, tol, ctypes.byref(s), rng_inc, perc_imbalance,
+    lib().orc_partition_graph(n, rp, cl, wp, cutoff, tol, ctypes.byref(s), rng_inc, perc_imbalance, int(refine_alg),
                               part, ctypes.byref(ec), ev, stats)
     nl = int(stats[0])
     return dict(part=part, edgecut=ec.value, evec=ev, levels=nl, **{"lambda": stats[1]},
@@ -222,6 +236,7 @@ def ref(kind: str = "serial", cutoff: int = 50):
         L = ctypes.CDLL(path)
         vp = ctypes.c_void_p
         L.ref_power_iter.argtypes = [c_u32, u32p, u32p, vp, c_int, f64p, c_dbl, c_int]
+        L.ref_power_iter_nl.argtypes = [c_u32, u32p, u32p, vp, f64p, c_dbl, c_int]
         L.ref_compute_partition.argtypes = [c_u32, u32p, u32p, f64p, c_int, u32p, u64ref, c_int]
         L.ref_build_coarse_msd.argtypes = [c_u32, u32p, u32p, vp, c_int, c_int, u32p, c_u32,
                                            u32p, u32p, u32p, u32p, u64ref]
@@ -241,6 +256,16 @@ def ref_power_iter(row_ptr, col, w, u0, final_level: bool, tol: float = 1e-10, k
     wk = None if w is None else _u32(w)
     ref(kind).ref_power_iter(n, rp, cl, None if wk is None else wk.ctypes.data, int(final_level),
                              u, tol, 1)
+    return u
+
+
+def ref_power_iter_normalized(row_ptr, col, w, u0, tol: float = 1e-10, kind: str = "serial"):
+    """The reference's refine_alg 1 power iteration on a coarse level."""
+    rp, cl = _u32(row_ptr), _u32(col)
+    n = rp.shape[0] - 1
+    u = np.ascontiguousarray(u0, dtype=np.float64).copy()
+    wk = None if w is None else _u32(w)
+    ref(kind).ref_power_iter_nl(n, rp, cl, None if wk is None else wk.ctypes.data, u, tol, 1)
     return u
 
 

@@ -92,6 +92,36 @@ int ref_power_iter(uint32_t n, const uint32_t *row_ptr, const uint32_t *col,
     return rc;
 }
 
+/* sgp_power_iter with normLap = 1 (refine_alg 1) on a coarse level
+ * (final = 0: weighted degrees and weights set, as the serial driver has
+ * them for every level but the finest). */
+int ref_power_iter_nl(uint32_t n, const uint32_t *row_ptr, const uint32_t *col,
+                      const uint32_t *w, double *u, double tol, int quiet) {
+    Quiet q(quiet);
+    change_tol(tol);
+    sgp_graph_t g = make_graph(n, row_ptr, col);
+    uint32_t *eps = (uint32_t *)malloc((size_t)n * sizeof(uint32_t));
+    uint32_t *wd = (uint32_t *)malloc((size_t)n * sizeof(uint32_t));
+    uint32_t *ones = NULL;
+    if (!w) {
+        ones = (uint32_t *)malloc((size_t)row_ptr[n] * sizeof(uint32_t) + 4);
+        for (uint32_t j = 0; j < row_ptr[n]; j++) ones[j] = 1;
+    }
+    const uint32_t *ww = w ? w : ones;
+    for (uint32_t i = 0; i < n; i++) {
+        eps[i] = row_ptr[i + 1] - row_ptr[i];
+        uint32_t s = 0;
+        for (uint32_t j = row_ptr[i]; j < row_ptr[i + 1]; j++) s += ww[j];
+        wd[i] = s;
+    }
+    g.edges_per_source = eps;
+    g.weighted_degree = wd;
+    g.eweights = (sgp_wgt_t *)ww;
+    int rc = sgp_power_iter(u, g, 1, 0);
+    free(eps); free(wd); free(ones);
+    return rc;
+}
+
 /* sgpar.h:1969 sgp_compute_partition with 2 parts, local search off. */
 int ref_compute_partition(uint32_t n, const uint32_t *row_ptr, const uint32_t *col,
                           double *evec, int perc_imbalance_allowed,

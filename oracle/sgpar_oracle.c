@@ -367,6 +367,83 @@ uint64_t orc_power_iter(uint32_t n, const uint32_t *row_ptr, const uint32_t *col
     return niter;
 }
 
+/* sgpar.h:1790-1948 with normLap = 1 (refine_alg 1; eigensolve_kokkos.h
+ * :103-206 is the same recurrence), non-final form: d = weighted degrees.
+ * The start vector is D-orthogonalised against the normalised constant
+ * vector (sgpar.h:1732-1757: u -= (u.D1 / 1.D1) 1 with 1 normalised) and
+ * normalised; each iteration v_i = 0.5 u_i + 0.5 (A u)_i / d_i, v normalised
+ * (no deflation inside the loop), dot = u.v.  Same operation order as the
+ * reference serial build.  *lambda_out: eigenvalue of the random-walk
+ * Laplacian from the Rayleigh quotient of the lazy walk, 2 (1 - u.Mu / u.u).
+ * A vertex of degree 0 contributes 0.5 u_i (the reference divides by 0). */
+uint64_t orc_power_iter_nl(uint32_t n, const uint32_t *row_ptr, const uint32_t *col,
+                           const uint64_t *w64, double *u, double tol, uint64_t iter_cap,
+                           double *lambda_out) {
+    double *vec1 = (double *)malloc((size_t)n * sizeof(double));
+    double *v = (double *)malloc((size_t)n * sizeof(double));
+    uint64_t *d = (uint64_t *)malloc((size_t)n * sizeof(uint64_t));
+    for (uint32_t i = 0; i < n; i++) {
+        uint64_t s = 0;
+        for (uint32_t j = row_ptr[i]; j < row_ptr[i + 1]; j++) s += w64 ? w64[j] : 1;
+        d[i] = s;
+    }
+    uint64_t iter_max = 100000000000000ULL / (uint64_t)n;
+    if (iter_cap && iter_max > iter_cap) iter_max = iter_cap;
+    double ss = 0;
+    for (uint32_t i = 0; i < n; i++) vec1[i] = 1.0;
+    for (uint32_t i = 0; i < n; i++) ss += vec1[i] * vec1[i];
+    double inv = 1 / sqrt(ss);
+    for (uint32_t i = 0; i < n; i++) vec1[i] = vec1[i] * inv;
+    /* D-orthogonalise u against vec1 (sgpar.h:1732-1757) */
+    double numer = 0, denom = 0;
+    for (uint32_t i = 0; i < n; i++) {
+        numer += u[i] * (double)d[i] * vec1[i];
+        denom += vec1[i] * (double)d[i] * vec1[i];
+    }
+    for (uint32_t i = 0; i < n; i++) u[i] -= numer * vec1[i] / denom;
+    ss = 0;
+    for (uint32_t i = 0; i < n; i++) ss += u[i] * u[i];
+    inv = 1 / sqrt(ss);
+    for (uint32_t i = 0; i < n; i++) u[i] = u[i] * inv;
+    for (uint32_t i = 0; i < n; i++) v[i] = u[i];
+    double dot = 0, last = 1;
+    uint64_t niter = 0;
+    while (fabs(dot - last) > tol && niter < iter_max) {
+        for (uint32_t i = 0; i < n; i++) u[i] = v[i];
+        for (uint32_t i = 0; i < n; i++) {
+            const double dinv = 1.0 / (double)d[i];
+            double vi = 0.5 * u[i];
+            double mv = 0;
+            for (uint32_t j = row_ptr[i]; j < row_ptr[i + 1]; j++) {
+                if (w64) mv += u[col[j]] * (double)w64[j];
+                else mv += u[col[j]];
+            }
+            if (d[i]) vi += 0.5 * mv * dinv;
+            v[i] = vi;
+        }
+        ss = 0;
+        for (uint32_t i = 0; i < n; i++) ss += v[i] * v[i];
+        inv = 1 / sqrt(ss);
+        for (uint32_t i = 0; i < n; i++) v[i] = v[i] * inv;
+        last = dot;
+        dot = 0;
+        for (uint32_t i = 0; i < n; i++) dot += u[i] * v[i];
+        niter++;
+    }
+    if (lambda_out) {
+        double num = 0, den = 0;
+        for (uint32_t i = 0; i < n; i++) {
+            double mv = 0;
+            for (uint32_t j = row_ptr[i]; j < row_ptr[i + 1]; j++) mv += (w64 ? (double)w64[j] : 1.0) * u[col[j]];
+            const double mu = 0.5 * u[i] + (d[i] ? 0.5 * mv / (double)d[i] : 0.0);
+            num += u[i] * mu; den += u[i] * u[i];
+        }
+        *lambda_out = 2.0 * (1.0 - num / den);
+    }
+    free(vec1); free(v); free(d);
+    return niter;
+}
+
 /* ------------------------------------------------------------ the split -- */
 typedef struct { double ev; uint32_t u; } orc_vu_t;
 static int cmp_vu(const void *a, const void *b) {
@@ -459,7 +536,7 @@ typedef struct { uint32_t n; uint32_t *rp; uint32_t *col; uint64_t *w; uint32_t 
 int orc_partition_graph(uint32_t n, const uint32_t *row_ptr, const uint32_t *col,
                         const uint64_t *w64, uint32_t cutoff, double tol,
                         uint64_t *rng_state, uint64_t rng_inc,
-                        int perc_imbalance_allowed,
+                        int perc_imbalance_allowed, int normlap,
                         uint32_t *part, uint64_t *edgecut, double *evec_out, double *stats) {
     orc_level_t L[202];
     int nl = 1;
@@ -503,7 +580,8 @@ int orc_partition_graph(uint32_t n, const uint32_t *row_ptr, const uint32_t *col
     double lambda = 0;
     for (int l = nl - 1; l >= 0; l--) {
         orc_level_t *lv = &L[l];
-        uint64_t it = orc_power_iter(lv->n, lv->rp, lv->col, lv->w, vec, tol, 0, l == 0 ? &lambda : NULL);
+        uint64_t it = normlap ? orc_power_iter_nl(lv->n, lv->rp, lv->col, lv->w, vec, tol, 0, l == 0 ? &lambda : NULL)
+                              : orc_power_iter(lv->n, lv->rp, lv->col, lv->w, vec, tol, 0, l == 0 ? &lambda : NULL);
         if (stats) { stats[3 + 2 * l] = lv->n; stats[4 + 2 * l] = (double)it; }
         if (l == 0) { if (stats) stats[2] = (double)it; break; }
         /* prolongation fine[i] = coarse[vcmap[i]] (eigensolve_kokkos.h:1556-1559) */

@@ -172,3 +172,33 @@ def test_metrics_record_of_a_partition(partitioner, tmp_path):
     assert [x["refine-iterations"] for x in d["coarse-levels"]] == r.level_iters[::-1]
     assert 0 < d["coarsen-map-duration-seconds"] + d["coarsen-build-duration-seconds"] <= d["coarsen-duration-seconds"]
     assert d["total-duration-seconds"] > d["refine-duration-seconds"] > 0
+
+
+@pytest.mark.parametrize("name", ["grid64", "holes", "rmat12"])
+def test_normalized_laplacian_variant(partitioner, name):
+    """refine_alg 1 (eigensolve_kokkos.h:103-206): the lazy random walk with
+    a D-orthogonalised start and no deflation in the loop.  On grids it finds
+    the normalized Fiedler pair like the oracle; on R-MAT levels the constant
+    vector grows back from rounding and both collapse onto it (lambda ~ 0),
+    as the reference does."""
+    g = {"grid64": lambda: G.grid2d(64, 64), "holes": lambda: G.grid2d_holes(60, 60, 0.1, 4),
+         "rmat12": lambda: G.rmat(12, seed=3)}[name]()
+    o = O.partition_graph(g.row_ptr, g.col, None, rng_state=77, refine_alg=1)
+    r = partitioner.partition(g, rng_state=77, refine_alg=1)
+    assert r.level_n == o["level_n"] and r.rng_state == o["rng_state"]
+    assert r.edgecut == cut_of(g, r.part)
+    assert int((r.part == 0).sum()) in (g.n // 2, (g.n + 1) // 2)
+    if name == "rmat12":
+        assert abs(r.lam) < 1e-4 and abs(o["lambda"]) < 1e-4
+    else:
+        assert abs(r.lam - o["lambda"]) <= 1e-3 * o["lambda"]
+        assert abs(r.edgecut - o["edgecut"]) <= 0.05 * o["edgecut"] + 4
+        # and it differs from the combinatorial variant's eigenvalue
+        c = partitioner.partition(g, rng_state=77)
+        assert abs(c.lam - r.lam) > 0.5 * r.lam
+
+
+def test_refine_alg_out_of_range_is_rejected(partitioner):
+    from ipdps_2021_graph_coarsening_b200 import _lib as L
+    with pytest.raises(L.SgparError):
+        partitioner.partition(G.grid2d(20, 20), refine_alg=2)

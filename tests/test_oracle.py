@@ -133,6 +133,26 @@ def test_power_iter_matches_reference_directly(seed):
 
 
 @needs_ref
+@pytest.mark.parametrize("seed", [6, 7])
+def test_normalized_power_iter_matches_reference_directly(seed):
+    """refine_alg 1 on a weighted coarse level: the oracle's normalized-
+    Laplacian iteration is bit-identical to the reference's serial build.
+    Without deflation inside the loop, rounding lets the constant vector
+    (eigenvalue 1 of the lazy walk) grow back, and both converge to it:
+    lambda of the random-walk Laplacian ~ 0, a near-constant vector."""
+    g = G.rmat(9, seed=seed)
+    hn = O.hec_heavy(g.row_ptr, g.col, None, True, seed)
+    vc, nc, _ = O.hec_map(hn, seed)
+    rp, col, w = O.build_coarse(g.row_ptr, g.col, None, vc, nc)
+    u0 = np.random.default_rng(seed).random(nc)
+    ours, it, lam = O.power_iter_normalized(rp, col, w, u0)
+    ref = O.ref_power_iter_normalized(rp, col, w, u0)
+    assert it > 2 and abs(lam) < 1e-3
+    assert np.array_equal(ours, ref)
+    assert abs(abs(float(ours.sum())) / np.sqrt(nc) - 1) < 1e-3   # near the normalised constant vector
+
+
+@needs_ref
 @pytest.mark.parametrize("seed", [4, 5])
 def test_build_matches_reference_directly(seed):
     g = G.erdos_renyi(2000, 10.0, seed=seed)
