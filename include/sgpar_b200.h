@@ -296,6 +296,56 @@ int sgp_b200_split_noalloc(void *stream, uint32_t n, const uint32_t *row_ptr, co
 int sgp_b200_write_metrics(const char *path, const sgp_b200_result_t *res, uint64_t edge_cut_4way,
                            uint64_t partition_diff, int first, int last);
 
+/* ------------------------------------------------------------------------ *
+ * Part 3: MatrixMarket input (replaces the cmg/mtx2csr.cpp command)          *
+ * ------------------------------------------------------------------------ */
+
+typedef struct {
+    uint64_t rows, cols, entries_declared;  /* the size line */
+    uint64_t lines;             /* lines after the size line (entries, comments, blank) */
+    int bipartite;              /* 1: "general" rectangular matrix read as a bipartite graph */
+    uint32_t n_all;             /* vertices before the component filter */
+    uint64_t m_all;             /* directed entries after dedupe and self-loop removal */
+    uint32_t components;        /* connected components, isolated vertices included */
+    uint32_t n;                 /* vertices of the largest component (the output) */
+    uint64_t m;                 /* its directed entries */
+    float ms_total;             /* whole call (host clock) */
+    float ms_read;              /* file read + copy of the text to the device (host clock) */
+    float ms_parse, ms_rows, ms_components, ms_extract;   /* device phases (CUDA events) */
+    float ms_out;               /* result copy-out (host clock) */
+} sgp_b200_mtx_info_t;
+
+/* MatrixMarket coordinate text -> symmetric CSR of its largest connected
+ * component, computed on the device.  Same rules and output as
+ * cmg/mtx2csr.cpp:13-264: banner lines must say "coordinate"; "general"
+ * reads a square matrix as A + A^T and a rectangular one as a bipartite graph
+ * (columns are vertices 0..cols-1, rows cols..cols+rows-1); every entry adds
+ * both directions, self loops dropped unless bipartite, values ignored; rows
+ * sorted with duplicates removed; the largest component kept (the first in
+ * vertex order among equally large ones), renumbered in ascending order.
+ * Where the reference's behaviour is undefined (an id of 0 or beyond the size
+ * line, an entry line that is not "i j ...", a "symmetric" banner on a
+ * non-square size line, a later banner that switches to "general") the call
+ * fails with SGP_B200_ERR_INVALID naming the line; blank lines are skipped.
+ *
+ * `out` receives library-allocated arrays (out->w NULL) of kind out_mem
+ * (SGP_B200_HOST: malloc; SGP_B200_DEVICE: cudaMalloc on the context's device);
+ * release them with sgp_b200_graph_free.  `info` may be NULL. */
+int sgp_b200_mtx_read(sgp_b200_ctx_t *ctx, const char *mtx_path, int out_mem, sgp_b200_graph_t *out,
+                      sgp_b200_mtx_info_t *info);
+/* The same from `len` bytes of file text at `text` (kind text_mem). */
+int sgp_b200_mtx_parse(sgp_b200_ctx_t *ctx, const char *text, uint64_t len, int text_mem, int out_mem,
+                       sgp_b200_graph_t *out, sgp_b200_mtx_info_t *info);
+void sgp_b200_graph_free(sgp_b200_graph_t *g);
+/* Writes a host graph as the reference's binary CSR file (mtx2csr.cpp:266-289):
+ * six 64-bit words n, m (directed entries), 1, 0, 1, 0, then row offsets[n+1]
+ * and destinations[m] as 32-bit words (id_bytes 4) or 64-bit words (id_bytes
+ * 8, the layout of cmg/mtx2csr_large.cpp). */
+int sgp_b200_csr_write(const char *csr_path, const sgp_b200_graph_t *g, int id_bytes);
+/* The command `mtx2csr <MM file> <binary CSR file>`: read + write. */
+int sgp_b200_mtx2csr(sgp_b200_ctx_t *ctx, const char *mtx_path, const char *csr_path, int id_bytes,
+                     sgp_b200_mtx_info_t *info);
+
 /* Milliseconds of the phases of the last sgp_b200_partition / eigensolve. */
 int sgp_b200_last_timing(sgp_b200_ctx_t *ctx, float *ms_total, float *ms_coarsen,
                          float *ms_eigen, float *ms_split);

@@ -57,6 +57,13 @@ class sgp_b200_result_t(ctypes.Structure):
                 ("ms_map", c_flt), ("ms_build", c_flt)]
 
 
+class sgp_b200_mtx_info_t(ctypes.Structure):
+    _fields_ = [("rows", c_u64), ("cols", c_u64), ("entries_declared", c_u64), ("lines", c_u64),
+                ("bipartite", c_int), ("n_all", c_u32), ("m_all", c_u64), ("components", c_u32), ("n", c_u32),
+                ("m", c_u64), ("ms_total", c_flt), ("ms_read", c_flt), ("ms_parse", c_flt), ("ms_rows", c_flt),
+                ("ms_components", c_flt), ("ms_extract", c_flt), ("ms_out", c_flt)]
+
+
 _SIGS = {
     # part 1: sgpar.h API
     "sgp_pcg32_random_r": (c_u32, [P(sgp_pcg32_random_t)]),
@@ -98,6 +105,13 @@ _SIGS = {
     "sgp_b200_last_timing": (c_int, [c_vp, P(c_flt), P(c_flt), P(c_flt), P(c_flt)]),
     "sgp_b200_write_metrics": (c_int, [ctypes.c_char_p, P(sgp_b200_result_t), c_u64, c_u64, c_int, c_int]),
     "sgp_b200_split_noalloc": (c_int, [c_vp, c_u32, c_vp, c_vp, c_vp, c_vp, c_vp]),
+    # part 3: MatrixMarket input
+    "sgp_b200_mtx_read": (c_int, [c_vp, ctypes.c_char_p, c_int, P(sgp_b200_graph_t), P(sgp_b200_mtx_info_t)]),
+    "sgp_b200_mtx_parse": (c_int, [c_vp, c_vp, c_u64, c_int, c_int, P(sgp_b200_graph_t),
+                                   P(sgp_b200_mtx_info_t)]),
+    "sgp_b200_graph_free": (None, [P(sgp_b200_graph_t)]),
+    "sgp_b200_csr_write": (c_int, [ctypes.c_char_p, P(sgp_b200_graph_t), c_int]),
+    "sgp_b200_mtx2csr": (c_int, [c_vp, ctypes.c_char_p, ctypes.c_char_p, c_int, P(sgp_b200_mtx_info_t)]),
 }
 
 _lib = None

@@ -195,6 +195,20 @@ def _dptr(t) -> Optional[int]:
     return None if t is None else int(t.data_ptr())
 
 
+def csr_write(path: str, g: CSR, id_bytes: int = 4) -> None:
+    """The reference's binary CSR file (mtx2csr.cpp:266-289; id_bytes 8:
+    mtx2csr_large.cpp) of a host graph."""
+    rp = np.ascontiguousarray(g.row_ptr, dtype=np.uint32)
+    col = np.ascontiguousarray(g.col, dtype=np.uint32)
+    dg = L.sgp_b200_graph_t()
+    dg.n, dg.m, dg.row_ptr, dg.col, dg.mem = g.n, len(col), rp.ctypes.data, col.ctypes.data, L.HOST
+    L.check(L.lib().sgp_b200_csr_write(str(path).encode(), ctypes.byref(dg), id_bytes), "sgp_b200_csr_write")
+
+
+def _mtx_info(i: L.sgp_b200_mtx_info_t) -> dict:
+    return {name: getattr(i, name) for name, _ in L.sgp_b200_mtx_info_t._fields_}
+
+
 class Partitioner:
     """One context (device, stream, memory pool) of libsgpar_b200."""
 
@@ -389,6 +403,57 @@ class Partitioner:
         L.check(L.lib().sgp_b200_split(self._ctx, n, _dptr(row_ptr), _dptr(col), _dptr(evec), perc_imbalance,
                                        _dptr(part), ctypes.byref(cut)), "sgp_b200_split")
         return part, cut.value
+
+    # -- MatrixMarket input (cmg/mtx2csr.cpp)
+    def mtx_read(self, source, device_out: bool = False):
+        """MatrixMarket coordinate text -> (graph of its largest connected
+        component, info dict), computed on the device.  ``source``: a file
+        path, ``bytes``, or a CUDA uint8 tensor holding the text.  Returns a
+        host ``CSR``, or with ``device_out`` a pair of CUDA int32 tensors
+        (row_ptr, col)."""
+        out = L.sgp_b200_graph_t()
+        info = L.sgp_b200_mtx_info_t()
+        mem = L.DEVICE if device_out else L.HOST
+        if isinstance(source, (bytes, bytearray, memoryview)):
+            buf = np.frombuffer(bytes(source), dtype=np.uint8)
+            rc = L.lib().sgp_b200_mtx_parse(self._ctx, buf.ctypes.data if len(buf) else None, len(buf), L.HOST,
+                                           mem, ctypes.byref(out), ctypes.byref(info))
+            where = "sgp_b200_mtx_parse"
+        elif hasattr(source, "data_ptr"):
+            self._sync()
+            rc = L.lib().sgp_b200_mtx_parse(self._ctx, _dptr(source), source.numel(), L.DEVICE, mem,
+                                           ctypes.byref(out), ctypes.byref(info))
+            where = "sgp_b200_mtx_parse"
+        else:
+            rc = L.lib().sgp_b200_mtx_read(self._ctx, str(source).encode(), mem, ctypes.byref(out),
+                                          ctypes.byref(info))
+            where = "sgp_b200_mtx_read"
+        L.check(rc, where)
+        try:
+            n, m = out.n, out.m
+            if device_out:
+                import torch
+                rp = torch.as_tensor(_DevArray(out.row_ptr, n + 1, "<i4"), device="cuda").clone()
+                col = torch.as_tensor(_DevArray(out.col, m, "<i4"), device="cuda").clone() if m else \
+                    torch.zeros(0, dtype=torch.int32, device="cuda")
+                torch.cuda.synchronize()
+                g = (rp, col)
+            else:
+                rp = np.ctypeslib.as_array(ctypes.cast(out.row_ptr, _u32p), shape=(n + 1,)).copy()
+                col = np.ctypeslib.as_array(ctypes.cast(out.col, _u32p), shape=(m,)).copy() if m else \
+                    np.zeros(0, dtype=np.uint32)
+                g = CSR(rp, col)
+        finally:
+            L.lib().sgp_b200_graph_free(ctypes.byref(out))
+        return g, _mtx_info(info)
+
+    def mtx2csr(self, mtx_path: str, csr_path: str, id_bytes: int = 4) -> dict:
+        """The reference command ``mtx2csr <MM file> <binary CSR file>``
+        (``id_bytes`` 8: ``mtx2csr_hg``).  Returns the info dict."""
+        info = L.sgp_b200_mtx_info_t()
+        L.check(L.lib().sgp_b200_mtx2csr(self._ctx, str(mtx_path).encode(), str(csr_path).encode(), id_bytes,
+                                        ctypes.byref(info)), "sgp_b200_mtx2csr")
+        return _mtx_info(info)
 
     # -- hierarchy (lower boundary)
     def generate_coarse_graphs(self, g: CSR, cutoff: int = 50, rng: Optional[PCG32] = None) -> "Hierarchy":

@@ -427,57 +427,18 @@ __global__ void __launch_bounds__(256) k_compact_rows(uint32_t nc, const uint32_
     }
 }
 
-// ---------------------------------------------------------------- driver --
+// ---------------------------------------------------------------- dedupe --
+// Sort + merge of every bucket [boff[r], boff[r+1]) of bdst (weights bw, or
+// unit weights when bw is null): dcnt[r] = distinct destinations of bucket
+// r, written ascending to the bucket's head with summed weights in tw.
+// Empty buckets get dcnt 0.
 template <typename WI, typename WO>
-static int build_impl(Context &C, const Level &F, const WI *w, const uint32_t *vcmap, uint32_t nc,
-                      uint32_t *crp, uint32_t **ccol_io, WO **cw_io, uint64_t *m_c, bool alloc_out) {
-    const uint32_t n = F.n;
-    uint32_t *cnt, *boff, *fill, *dcnt, *lists, *tcount;
-    SGPB_TRY(dalloc_t(C, &cnt, (size_t)nc + 1));
-    SGPB_TRY(dalloc_t(C, &boff, (size_t)nc + 1));
-    SGPB_TRY(dalloc_t(C, &fill, (size_t)nc + 1));
-    SGPB_TRY(dalloc_t(C, &dcnt, (size_t)nc + 1));
+static int dedupe_buckets(Context &C, uint32_t nc, const uint32_t *boff, uint32_t *bdst, const WI *bw, WO *tw,
+                          uint32_t *dcnt) {
+    uint32_t *lists, *tcount;
     SGPB_TRY(dalloc_t(C, &lists, (size_t)3 * nc + 3));
     SGPB_TRY(dalloc_t(C, &tcount, 4));
-    SGPB_TRY(dzero(C, cnt, sizeof(uint32_t) * ((size_t)nc + 1)));
-    SGPB_TRY(dzero(C, fill, sizeof(uint32_t) * ((size_t)nc + 1)));
     SGPB_TRY(dzero(C, tcount, sizeof(uint32_t) * 4));
-
-    const double avg = n ? (double)F.m / n : 0;
-    uint32_t cap = (uint32_t)C.num_sms * 16;
-#define SGPB_ROWS_LAUNCH(KERNEL, G, ...)                                                   \
-    {                                                                                      \
-        uint32_t blocks = cdiv((uint64_t)n * G, 256);                                      \
-        if (blocks > cap) blocks = cap;                                                    \
-        if (blocks < 1) blocks = 1;                                                        \
-        KERNEL<<<blocks, 256, 0, C.stream>>>(__VA_ARGS__);                                 \
-    }
-#define SGPB_BY_G(KERNEL_T, ...)                                                           \
-    if (avg <= 4) SGPB_ROWS_LAUNCH(KERNEL_T(4), 4, __VA_ARGS__)                            \
-    else if (avg <= 8) SGPB_ROWS_LAUNCH(KERNEL_T(8), 8, __VA_ARGS__)                       \
-    else if (avg <= 16) SGPB_ROWS_LAUNCH(KERNEL_T(16), 16, __VA_ARGS__)                    \
-    else SGPB_ROWS_LAUNCH(KERNEL_T(32), 32, __VA_ARGS__)
-
-    uint32_t *krow;
-    SGPB_TRY(dalloc_t(C, &krow, (size_t)n + 1));
-#define K_COUNT(G) k_build_count<G>
-    SGPB_BY_G(K_COUNT, n, F.rp, F.col, vcmap, cnt, krow)
-    SGPB_TRY(scan_u32(C, cnt, boff, nc, nullptr));
-    uint32_t kept = 0;
-    SGPB_TRY(read_u32(C, boff + nc, &kept));
-    uint32_t *bdst;
-    WI *bw = nullptr;
-    WO *tw;
-    SGPB_TRY(dalloc_t(C, &bdst, (size_t)kept + 1));
-    if (w) SGPB_TRY(dalloc_t(C, &bw, (size_t)kept + 1));
-    SGPB_TRY(dalloc_t(C, &tw, (size_t)kept + 1));
-#define K_SCATTER(G) k_build_scatter<G, WI>
-    SGPB_BY_G(K_SCATTER, n, F.rp, F.col, w, vcmap, krow, boff, fill, bdst, bw)
-#undef K_COUNT
-#undef K_SCATTER
-#undef SGPB_BY_G
-#undef SGPB_ROWS_LAUNCH
-    C.kernel_launches += 2;
     if (nc) {
         k_classify<<<cdiv(nc, 256), 256, 0, C.stream>>>(nc, boff, dcnt, lists, tcount);
         uint32_t g1 = cdiv(nc, 8);
@@ -526,6 +487,58 @@ static int build_impl(Context &C, const Level &F, const WI *w, const uint32_t *v
             SGPB_CUDA(cudaGetLastError());
         }
     }
+    return SGP_B200_OK;
+}
+
+// ---------------------------------------------------------------- driver --
+template <typename WI, typename WO>
+static int build_impl(Context &C, const Level &F, const WI *w, const uint32_t *vcmap, uint32_t nc,
+                      uint32_t *crp, uint32_t **ccol_io, WO **cw_io, uint64_t *m_c, bool alloc_out) {
+    const uint32_t n = F.n;
+    uint32_t *cnt, *boff, *fill, *dcnt;
+    SGPB_TRY(dalloc_t(C, &cnt, (size_t)nc + 1));
+    SGPB_TRY(dalloc_t(C, &boff, (size_t)nc + 1));
+    SGPB_TRY(dalloc_t(C, &fill, (size_t)nc + 1));
+    SGPB_TRY(dalloc_t(C, &dcnt, (size_t)nc + 1));
+    SGPB_TRY(dzero(C, cnt, sizeof(uint32_t) * ((size_t)nc + 1)));
+    SGPB_TRY(dzero(C, fill, sizeof(uint32_t) * ((size_t)nc + 1)));
+
+    const double avg = n ? (double)F.m / n : 0;
+    uint32_t cap = (uint32_t)C.num_sms * 16;
+#define SGPB_ROWS_LAUNCH(KERNEL, G, ...)                                                   \
+    {                                                                                      \
+        uint32_t blocks = cdiv((uint64_t)n * G, 256);                                      \
+        if (blocks > cap) blocks = cap;                                                    \
+        if (blocks < 1) blocks = 1;                                                        \
+        KERNEL<<<blocks, 256, 0, C.stream>>>(__VA_ARGS__);                                 \
+    }
+#define SGPB_BY_G(KERNEL_T, ...)                                                           \
+    if (avg <= 4) SGPB_ROWS_LAUNCH(KERNEL_T(4), 4, __VA_ARGS__)                            \
+    else if (avg <= 8) SGPB_ROWS_LAUNCH(KERNEL_T(8), 8, __VA_ARGS__)                       \
+    else if (avg <= 16) SGPB_ROWS_LAUNCH(KERNEL_T(16), 16, __VA_ARGS__)                    \
+    else SGPB_ROWS_LAUNCH(KERNEL_T(32), 32, __VA_ARGS__)
+
+    uint32_t *krow;
+    SGPB_TRY(dalloc_t(C, &krow, (size_t)n + 1));
+#define K_COUNT(G) k_build_count<G>
+    SGPB_BY_G(K_COUNT, n, F.rp, F.col, vcmap, cnt, krow)
+    SGPB_TRY(scan_u32(C, cnt, boff, nc, nullptr));
+    uint32_t kept = 0;
+    SGPB_TRY(read_u32(C, boff + nc, &kept));
+    uint32_t *bdst;
+    WI *bw = nullptr;
+    WO *tw;
+    SGPB_TRY(dalloc_t(C, &bdst, (size_t)kept + 1));
+    if (w) SGPB_TRY(dalloc_t(C, &bw, (size_t)kept + 1));
+    SGPB_TRY(dalloc_t(C, &tw, (size_t)kept + 1));
+#define K_SCATTER(G) k_build_scatter<G, WI>
+    SGPB_BY_G(K_SCATTER, n, F.rp, F.col, w, vcmap, krow, boff, fill, bdst, bw)
+#undef K_COUNT
+#undef K_SCATTER
+#undef SGPB_BY_G
+#undef SGPB_ROWS_LAUNCH
+    C.kernel_launches += 2;
+    SGPB_TRY((dedupe_buckets<WI, WO>(C, nc, boff, bdst, bw, tw, dcnt)));
     SGPB_TRY(scan_u32(C, dcnt, crp, nc, nullptr));
     uint32_t mc = 0;
     SGPB_TRY(read_u32(C, crp + nc, &mc));
@@ -595,6 +608,11 @@ int build_coarse_into(Context &C, const Level &F, const uint32_t *vcmap, uint32_
     }
     uint32_t *w4 = (uint32_t *)cw;
     return build_impl<uint32_t, uint32_t>(C, F, (const uint32_t *)F.w, vcmap, nc, crp, &ccol, &w4, m_c, false);
+}
+
+int dedupe_buckets_unit(Context &C, uint32_t nc, const uint32_t *boff, uint32_t *bdst, uint32_t *tw,
+                        uint32_t *dcnt) {
+    return dedupe_buckets<uint32_t, uint32_t>(C, nc, boff, bdst, nullptr, tw, dcnt);
 }
 
 }  // namespace sgpb

@@ -23,6 +23,7 @@
 #include <numeric>
 #include <atomic>
 #include <omp.h>
+#include <string>
 
 extern "C" {
 typedef struct {
@@ -392,5 +393,47 @@ int sgpgen_write_csr(const char *path, const sgpgen_csr_t *g) {
 }
 
 int sgpgen_num_threads(void) { return omp_get_max_threads(); }
+
+// MatrixMarket entry lines "u+1 v+1[ value]\n" (or "\r\n") for m pairs,
+// formatted in parallel chunks: the input text of the MatrixMarket converter
+// at benchmark sizes.  value_kind 0: none, 1: real values, 2: integer values
+// (cycling through a few spellings, so parsers must skip them).  Returns the
+// bytes written to out, or 0 when cap is too small.
+uint64_t sgpgen_mtx_lines(const uint32_t *u, const uint32_t *v, uint64_t m, int value_kind, int crlf, char *out,
+                          uint64_t cap) {
+    static const char *reals[4] = {" 1", " -2.5", " 3.75e-1", " 0.125"};
+    static const char *ints[3] = {" 1", " 7", " -3"};
+    const int T = omp_get_max_threads();
+    const uint64_t per = (m + T - 1) / (T ? T : 1);
+    std::vector<std::string> part(T);
+#pragma omp parallel num_threads(T)
+    {
+        const int t = omp_get_thread_num();
+        const uint64_t b = (uint64_t)t * per, e = std::min<uint64_t>(m, b + per);
+        std::string &s = part[t];
+        if (b < e) s.reserve((e - b) * 24);
+        char buf[64];
+        for (uint64_t i = b; i < e; i++) {
+            int k = snprintf(buf, sizeof(buf), "%u %u", u[i] + 1u, v[i] + 1u);
+            s.append(buf, k);
+            if (value_kind == 1) s.append(reals[i & 3]);
+            else if (value_kind == 2) s.append(ints[i % 3]);
+            if (crlf) s.push_back('\r');
+            s.push_back('\n');
+        }
+    }
+    uint64_t total = 0;
+    for (auto &p : part) total += p.size();
+    if (total > cap) return 0;
+    uint64_t off = 0;
+    std::vector<uint64_t> offs(T);
+    for (int t = 0; t < T; t++) {
+        offs[t] = off;
+        off += part[t].size();
+    }
+#pragma omp parallel for num_threads(T)
+    for (int t = 0; t < T; t++) memcpy(out + offs[t], part[t].data(), part[t].size());
+    return total;
+}
 
 }  // extern "C"

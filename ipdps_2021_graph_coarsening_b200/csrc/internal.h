@@ -48,6 +48,9 @@ struct Context {
     int num_sms = 0;
     size_t smem_optin = 0;
     uint64_t *h_pinned = nullptr;   // small pinned staging area for scalar read-backs
+    uint8_t *h_stage = nullptr;     // pinned ring for streaming host bytes to the device (mtx.cu)
+    size_t h_stage_slot = 0;        // bytes per ring slot
+    cudaEvent_t stage_ev[4] = {};   // copy of each slot done
     std::vector<void *> owned;      // allocations released at the end of a call
     std::vector<sgp_b200_ctx_t *> workers;   // contexts of the batch workers (same device), kept across calls
     // timing of the last partition (ms, CUDA events)
@@ -127,5 +130,10 @@ int edge_cut_device(Context &C, const Level &L, const uint32_t *part, uint64_t *
 // map0 / map1 (optional): vertex i of L -> its id in g1 (part 0) / g2
 int induced_subgraphs(Context &C, const Level &L, const uint32_t *part, Level *g1, Level *g2,
                       uint32_t **map0 = nullptr, uint32_t **map1 = nullptr);
+// sort + merge of unweighted buckets [boff[r], boff[r+1]) of bdst, r < nc:
+// the dcnt[r] distinct destinations of bucket r land ascending at its head,
+// their multiplicities in tw (build.cu)
+int dedupe_buckets_unit(Context &C, uint32_t nc, const uint32_t *boff, uint32_t *bdst, uint32_t *tw,
+                        uint32_t *dcnt);
 
 }  // namespace sgpb

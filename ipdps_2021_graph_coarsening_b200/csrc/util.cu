@@ -228,6 +228,9 @@ void sgp_b200_destroy(sgp_b200_ctx_t *x) {
         cudaStreamDestroy(C.stream);
     }
     if (C.h_pinned) cudaFreeHost(C.h_pinned);
+    if (C.h_stage) cudaFreeHost(C.h_stage);
+    for (cudaEvent_t e : C.stage_ev)
+        if (e) cudaEventDestroy(e);
     delete x;
 }
 

@@ -69,6 +69,8 @@ def _gen():
         lib.sgpgen_write_csr.argtypes = [ctypes.c_char_p, P]
         lib.sgpgen_free.argtypes = [P]
         lib.sgpgen_free.restype = None
+        lib.sgpgen_mtx_lines.argtypes = [ctypes.c_void_p, ctypes.c_void_p, u64, i32, i32, ctypes.c_void_p, u64]
+        lib.sgpgen_mtx_lines.restype = u64
         _lib = lib
     return _lib
 
@@ -139,3 +141,48 @@ def write_csr(path: str, g: CSR) -> None:
     raw.col = col.ctypes.data_as(ctypes.POINTER(ctypes.c_uint32))
     if _gen().sgpgen_write_csr(path.encode(), ctypes.byref(raw)) != 0:
         raise OSError(f"could not write {path}")
+
+
+# ------------------------------------------------------------ MatrixMarket --
+def mtx_text(u, v, rows: int, cols: int, field: str = "pattern", symmetry: str = "symmetric",
+             comments=(), crlf: bool = False, nnz: Optional[int] = None) -> bytes:
+    """MatrixMarket coordinate text of the 0-based entries ``(u[i], v[i])``
+    in the given order: banner, ``%`` comment lines, size line, one line per
+    entry (``real`` / ``integer`` fields get values the reader must skip)."""
+    u = np.ascontiguousarray(u, dtype=np.uint32)
+    v = np.ascontiguousarray(v, dtype=np.uint32)
+    m = int(u.shape[0])
+    vk = {"pattern": 0, "real": 1, "integer": 2}[field]
+    nl = b"\r\n" if crlf else b"\n"
+    head = f"%%MatrixMarket matrix coordinate {field} {symmetry}".encode() + nl
+    for c in comments:
+        head += b"%" + c.encode() + nl
+    head += f"{rows} {cols} {m if nnz is None else nnz}".encode() + nl
+    cap = m * 48 + 16
+    buf = np.empty(cap, dtype=np.uint8)
+    k = _gen().sgpgen_mtx_lines(u.ctypes.data, v.ctypes.data, m, vk, int(crlf), buf.ctypes.data, cap)
+    if m and k == 0:
+        raise RuntimeError("MatrixMarket formatting buffer too small")
+    return head + buf[:k].tobytes()
+
+
+def mtx_of(g: CSR, symmetry: str = "symmetric", field: str = "pattern", seed: Optional[int] = 0,
+           dup_frac: float = 0.0, extra_vertices: int = 0, **kw) -> bytes:
+    """A symmetric graph as MatrixMarket text.  ``symmetric`` stores the
+    lower triangle (row > col), ``general`` every directed entry.  Lines are
+    shuffled with ``seed`` (None: row order); ``dup_frac`` of them repeated;
+    ``extra_vertices`` isolated vertices appended to the size line."""
+    rows = np.repeat(np.arange(g.n, dtype=np.uint32), np.diff(g.row_ptr).astype(np.int64))
+    cols = np.asarray(g.col, dtype=np.uint32)
+    if symmetry == "symmetric":
+        keep = rows > cols
+        rows, cols = rows[keep], cols[keep]
+    rng = np.random.default_rng(seed if seed is not None else 0)
+    if dup_frac > 0:
+        extra = rng.choice(rows.shape[0], int(dup_frac * rows.shape[0]), replace=True)
+        rows, cols = np.concatenate([rows, rows[extra]]), np.concatenate([cols, cols[extra]])
+    if seed is not None:
+        p = rng.permutation(rows.shape[0])
+        rows, cols = rows[p], cols[p]
+    n = g.n + extra_vertices
+    return mtx_text(rows, cols, n, n, field=field, symmetry=symmetry, **kw)
