@@ -9,7 +9,8 @@
 //
 // Per-row dedupe is tiered by bucket size:
 //   tier 1 (<= 32 entries)   one warp, bitonic sort in registers
-//   tier 2 (<= kT2 entries)  one block, bitonic sort in shared memory
+//   tier 2 (<= kT1 entries)  a 64-thread block, bitonic sort in shared memory
+//   tier 2 (<= kT2 entries)  a kT2Threads block, bitonic sort in shared memory
 //   tier 3 (larger)          dense accumulation over [0, nc) in global memory
 //                            (bitmap + weight array, L2-resident), compacted in
 //                            ascending destination order
@@ -109,15 +110,32 @@ __global__ void __launch_bounds__(256) k_build_scatter(uint32_t n, const uint32_
 }
 
 // ------------------------------------------------------------- classify --
+// Bucket sizes 1..32 -> list 0 (one warp), 33..kT1 -> list 1 (small block),
+// ..kT2 -> list 2 (block), larger -> list 3 (dense); one atomic per warp and
+// list.
+constexpr uint32_t kT1 = 256;
+constexpr int kT1Threads = 64;
+
 __global__ void k_classify(uint32_t nc, const uint32_t *__restrict__ boff, uint32_t *__restrict__ dcnt,
-                           uint32_t *__restrict__ lists /* 3 x nc */, uint32_t *__restrict__ tcount /* 3 */) {
-    uint32_t c = blockIdx.x * blockDim.x + threadIdx.x;
-    if (c >= nc) return;
-    uint32_t sz = boff[c + 1] - boff[c];
-    if (sz == 0) { dcnt[c] = 0; return; }
-    int t = sz <= 32 ? 0 : (sz <= (uint32_t)kT2 ? 1 : 2);
-    uint32_t p = atomicAdd(tcount + t, 1u);
-    lists[(size_t)t * nc + p] = c;
+                           uint32_t *__restrict__ lists /* 4 x nc */, uint32_t *__restrict__ tcount /* 4 */) {
+    const uint32_t c = blockIdx.x * blockDim.x + threadIdx.x;
+    const unsigned lane = threadIdx.x & 31;
+    int t = -1;
+    if (c < nc) {
+        const uint32_t sz = boff[c + 1] - boff[c];
+        if (sz == 0) dcnt[c] = 0;
+        else t = sz <= 32 ? 0 : sz <= kT1 ? 1 : sz <= (uint32_t)kT2 ? 2 : 3;
+    }
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+        const unsigned m = __ballot_sync(0xFFFFFFFFu, t == q);
+        if (!m) continue;   // warp-uniform
+        const int leader = __ffs(m) - 1;
+        uint32_t base = 0;
+        if ((int)lane == leader) base = atomicAdd(tcount + q, (uint32_t)__popc(m));
+        base = __shfl_sync(0xFFFFFFFFu, base, leader);
+        if (t == q) lists[(size_t)q * nc + base + __popc(m & ((1u << lane) - 1u))] = c;
+    }
 }
 
 // --------------------------------------------------------------- tier 1 --
@@ -182,10 +200,11 @@ __global__ void __launch_bounds__(kT2Threads) k_dedupe_block(const uint32_t *__r
                                                              const uint32_t *__restrict__ count,
                                                              const uint32_t *__restrict__ boff,
                                                              uint32_t *__restrict__ bdst, const WI *__restrict__ bw,
-                                                             WO *__restrict__ tw, uint32_t *__restrict__ dcnt) {
+                                                             WO *__restrict__ tw, uint32_t *__restrict__ dcnt,
+                                                             uint32_t cap /* largest bucket, even */) {
     extern __shared__ __align__(16) unsigned char smraw[];
-    uint32_t *skey = (uint32_t *)smraw;                       // kT2
-    uint64_t *sw = (uint64_t *)(smraw + kT2 * sizeof(uint32_t));   // kT2
+    uint32_t *skey = (uint32_t *)smraw;                        // cap
+    uint64_t *sw = (uint64_t *)(smraw + cap * sizeof(uint32_t));   // cap
     __shared__ uint64_t scan_sm[33];
     const uint32_t cntv = *count;
     for (uint32_t k = blockIdx.x; k < cntv; k += gridDim.x) {
@@ -359,7 +378,11 @@ __global__ void __launch_bounds__(256) k_dense_add(const uint32_t *__restrict__ 
 }
 
 // compaction of one dense slot per block, in ascending destination order;
-// clears the slot for reuse.
+// clears the slot for reuse.  Each thread takes kCollectWords consecutive
+// bitmap words per pass, so a pass covers 4096 words (131072 destinations)
+// with one block scan.
+constexpr int kCollectWords = 16;
+
 template <typename WO>
 __global__ void __launch_bounds__(256) k_dense_collect(const uint32_t *__restrict__ list, uint32_t r0,
                                                       const uint32_t *__restrict__ boff, uint32_t nc,
@@ -373,22 +396,33 @@ __global__ void __launch_bounds__(256) k_dense_collect(const uint32_t *__restric
     const uint32_t nwords = (nc + 31) / 32;
     uint32_t *bm = bits + (size_t)blockIdx.x * nwords;
     uint64_t base = 0;
-    for (uint32_t w0 = 0; w0 < nwords; w0 += blockDim.x) {
-        uint32_t wi = w0 + threadIdx.x;
-        uint32_t word = wi < nwords ? bm[wi] : 0u;
-        uint64_t pc = __popc(word), tot;
-        uint64_t inc = block_scan_u64(pc, scan_sm, &tot);
-        uint64_t pos = base + inc - pc;
-        while (word) {
-            int bit = __ffs(word) - 1;
-            word &= word - 1;
-            uint32_t v = wi * 32 + bit;
-            bdst[b + pos] = v;
-            tw[b + pos] = a[v];
-            a[v] = 0;
-            pos++;
+    for (uint32_t w0 = 0; w0 < nwords; w0 += blockDim.x * kCollectWords) {
+        const uint32_t wb = w0 + threadIdx.x * kCollectWords;
+        uint32_t word[kCollectWords];
+        uint32_t pc = 0;
+#pragma unroll
+        for (int q = 0; q < kCollectWords; q++) {
+            word[q] = wb + q < nwords ? __ldcg(bm + wb + q) : 0u;
+            pc += __popc(word[q]);
         }
-        if (wi < nwords) bm[wi] = 0;
+        uint64_t tot;
+        const uint64_t inc = block_scan_u64(pc, scan_sm, &tot);
+        uint64_t pos = base + inc - pc;
+#pragma unroll
+        for (int q = 0; q < kCollectWords; q++) {
+            uint32_t wq = word[q];
+            if (!wq) continue;
+            bm[wb + q] = 0;
+            while (wq) {
+                const int bit = __ffs(wq) - 1;
+                wq &= wq - 1;
+                const uint32_t v = (wb + q) * 32 + bit;
+                bdst[b + pos] = v;
+                tw[b + pos] = a[v];
+                a[v] = 0;
+                pos++;
+            }
+        }
         base += tot;
     }
     if (threadIdx.x == 0) dcnt[c] = (uint32_t)base;
@@ -436,7 +470,7 @@ template <typename WI, typename WO>
 static int dedupe_buckets(Context &C, uint32_t nc, const uint32_t *boff, uint32_t *bdst, const WI *bw, WO *tw,
                           uint32_t *dcnt) {
     uint32_t *lists, *tcount;
-    SGPB_TRY(dalloc_t(C, &lists, (size_t)3 * nc + 3));
+    SGPB_TRY(dalloc_t(C, &lists, (size_t)4 * nc + 4));
     SGPB_TRY(dalloc_t(C, &tcount, 4));
     SGPB_TRY(dzero(C, tcount, sizeof(uint32_t) * 4));
     if (nc) {
@@ -444,25 +478,32 @@ static int dedupe_buckets(Context &C, uint32_t nc, const uint32_t *boff, uint32_
         uint32_t g1 = cdiv(nc, 8);
         if (g1 > (uint32_t)C.num_sms * 16) g1 = C.num_sms * 16;
         k_dedupe_warp<WI, WO><<<g1 ? g1 : 1, 256, 0, C.stream>>>(lists, tcount, boff, bdst, bw, tw, dcnt);
+        // the block kernels size their sort by the bucket: small buckets run
+        // in small blocks, many per SM, large ones in kT2Threads
         if constexpr (sizeof(WI) == 4) {
             const size_t sm2 = (size_t)kT2 * sizeof(unsigned long long);
             SGPB_CUDA(cudaFuncSetAttribute(k_dedupe_block_packed<WI, WO>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                            (int)sm2));
+            k_dedupe_block_packed<WI, WO><<<(uint32_t)C.num_sms * 32, kT1Threads, kT1 * sizeof(unsigned long long),
+                                            C.stream>>>(lists + nc, tcount + 1, boff, bdst, bw, tw, dcnt);
             const uint32_t g2 = (uint32_t)C.num_sms * 6;
-            k_dedupe_block_packed<WI, WO><<<g2, kT2Threads, sm2, C.stream>>>(lists + nc, tcount + 1, boff, bdst, bw,
-                                                                            tw, dcnt);
+            k_dedupe_block_packed<WI, WO><<<g2, kT2Threads, sm2, C.stream>>>(lists + 2 * (size_t)nc, tcount + 2,
+                                                                            boff, bdst, bw, tw, dcnt);
         } else {
             const size_t sm2 = (size_t)kT2 * (sizeof(uint32_t) + sizeof(uint64_t));
             SGPB_CUDA(cudaFuncSetAttribute(k_dedupe_block<WI, WO>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                            (int)sm2));
+            k_dedupe_block<WI, WO><<<(uint32_t)C.num_sms * 32, kT1Threads,
+                                     kT1 * (sizeof(uint32_t) + sizeof(uint64_t)), C.stream>>>(
+                lists + nc, tcount + 1, boff, bdst, bw, tw, dcnt, kT1);
             const uint32_t g2 = (uint32_t)C.num_sms * 4;
-            k_dedupe_block<WI, WO><<<g2, kT2Threads, sm2, C.stream>>>(lists + nc, tcount + 1, boff, bdst, bw, tw,
-                                                                     dcnt);
+            k_dedupe_block<WI, WO><<<g2, kT2Threads, sm2, C.stream>>>(lists + 2 * (size_t)nc, tcount + 2, boff, bdst,
+                                                                     bw, tw, dcnt, (uint32_t)kT2);
         }
-        C.kernel_launches += 3;
+        C.kernel_launches += 4;
         SGPB_CUDA(cudaGetLastError());
         uint32_t n3 = 0;
-        SGPB_TRY(read_u32(C, tcount + 2, &n3));
+        SGPB_TRY(read_u32(C, tcount + 3, &n3));
         if (n3) {
             const size_t words = ((size_t)nc + 31) / 32;
             const size_t slot_bytes = (size_t)nc * sizeof(WO) + words * 4;
@@ -479,8 +520,8 @@ static int dedupe_buckets(Context &C, uint32_t nc, const uint32_t *boff, uint32_
             for (uint32_t r0 = 0; r0 < n3; r0 += (uint32_t)slots) {
                 uint32_t nr = n3 - r0 < slots ? n3 - r0 : (uint32_t)slots;
                 dim3 ga(8, nr);
-                k_dense_add<WI, WO><<<ga, 256, 0, C.stream>>>(lists + 2 * (size_t)nc, r0, boff, bdst, bw, nc, acc, bits);
-                k_dense_collect<WO><<<nr, 256, 0, C.stream>>>(lists + 2 * (size_t)nc, r0, boff, nc, acc, bits, bdst, tw,
+                k_dense_add<WI, WO><<<ga, 256, 0, C.stream>>>(lists + 3 * (size_t)nc, r0, boff, bdst, bw, nc, acc, bits);
+                k_dense_collect<WO><<<nr, 256, 0, C.stream>>>(lists + 3 * (size_t)nc, r0, boff, nc, acc, bits, bdst, tw,
                                                              dcnt);
                 C.kernel_launches += 2;
             }

@@ -1584,7 +1584,10 @@ static int run_pi(Context &C, const Level &L, PIArgs a, int mixed, double *res_d
             using Vt = decltype(vtag);
             const size_t bytes = small_level_bytes<Wt, Vt>(L.n, L.m, L.w != nullptr);
             const void *k = (const void *)k_power_iter_small<Wt, Vt>;
-            SGPB_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
+            // the limit is a property of the function, shared by every host
+            // thread (batch workers): always the same bound, never this
+            // launch's size, so no thread lowers it under another's launch
+            SGPB_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmallSmemBytes));
             SGPB_CUDA(cudaEventRecord(e0, C.stream));
             k_power_iter_small<Wt, Vt><<<1, kSmallThreads, bytes, C.stream>>>(a);
             C.kernel_launches++;

@@ -35,10 +35,14 @@
 //      (files sorted by row or column repeat ids within a warp);
 //   4. a bucket scatter places both directions of every entry, the coarse
 //      build's sort + merge tiers sort each row and drop duplicates;
-//   5. a lock-free union-find labels components by their smallest vertex:
-//      every vertex starts under its smallest neighbour, each edge (u < v)
-//      hooks the larger of the two roots under the smaller with a CAS, finds
-//      halve paths; parent[x] <= x always holds, so every walk terminates;
+//   5. a lock-free union-find labels components by their smallest vertex: a
+//      union hooks the larger of two roots under the smaller with a CAS,
+//      finds halve paths, and parent[x] <= x always holds, so every walk
+//      terminates.  Edges are joined in the sampling order of Afforest
+//      (Sutton, Ben-Nun, Barak, IPDPS 2018): every vertex with its first two
+//      neighbours, then the root holding most of 1024 probed vertices is the
+//      giant component and only vertices outside it join their remaining
+//      neighbours;
 //   6. component sizes by warp-aggregated atomics, the largest (ties: the
 //      smallest label, i.e. the first the reference's BFS finds) by a 64-bit
 //      max over (size << 32 | ~label);
@@ -49,8 +53,10 @@
 #include <string.h>
 #include <sys/stat.h>
 
+#include <algorithm>
 #include <chrono>
 #include <string>
+#include <vector>
 
 #include "common.cuh"
 #include "internal.h"
@@ -286,33 +292,50 @@ __device__ __forceinline__ void cc_union(uint32_t *parent, uint32_t a, uint32_t 
     }
 }
 
-__global__ void __launch_bounds__(256) k_cc_init(uint32_t n, const uint32_t *__restrict__ rp,
-                                                 const uint32_t *__restrict__ col, uint32_t *__restrict__ parent) {
+__global__ void __launch_bounds__(256) k_cc_init(uint32_t n, uint32_t *__restrict__ parent) {
     const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
-    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
-        uint32_t p = (uint32_t)i;
-        const uint32_t b = rp[i];
-        if (b < rp[i + 1]) {
-            const uint32_t c = __ldg(col + b);   // rows are sorted: the smallest neighbour
-            if (c < p) p = c;
-        }
-        parent[i] = p;
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) parent[i] = (uint32_t)i;
+}
+
+// sampling round r: every vertex joins its r-th neighbour
+__global__ void __launch_bounds__(256) k_cc_sample(uint32_t n, const uint32_t *__restrict__ rp,
+                                                   const uint32_t *__restrict__ col, uint32_t *parent, uint32_t r,
+                                                   uint32_t *err) {
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    for (uint64_t u = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; u < n; u += stride) {
+        const uint32_t j = rp[u] + r;
+        if (j < rp[u + 1]) cc_union(parent, (uint32_t)u, __ldg(col + j), n + 1, err);
     }
 }
 
-// G lanes per row; each edge once, from its smaller endpoint
+// parent[x] = root of x
+__global__ void __launch_bounds__(256) k_cc_compress(uint32_t n, uint32_t *parent) {
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride)
+        __stcg(parent + i, cc_find(parent, (uint32_t)i));
+}
+
+__global__ void k_cc_probe(uint32_t n, uint32_t count, const uint32_t *__restrict__ parent, uint32_t *out) {
+    const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k < count) out[k] = parent[(uint64_t)k * n / count];
+}
+
+// The entries from r0 on of every vertex not hanging directly under `skip`
+// (the root of the component that the sampling made largest), G lanes per
+// row.  An edge (u, v) skipped from u's side is joined from v's unless v
+// hangs under `skip` too, in which case both ends are already connected.
 template <int G>
-__global__ void __launch_bounds__(256) k_cc_hook(uint32_t n, const uint32_t *__restrict__ rp,
-                                                 const uint32_t *__restrict__ col, uint32_t *parent,
-                                                 uint32_t *err) {
+__global__ void __launch_bounds__(256) k_cc_rest(uint32_t n, const uint32_t *__restrict__ rp,
+                                                 const uint32_t *__restrict__ col, uint32_t *parent, uint32_t skip,
+                                                 uint32_t r0, uint32_t *err) {
     const uint32_t lane = threadIdx.x & (G - 1);
     const uint64_t ng = ((uint64_t)gridDim.x * blockDim.x) / G;
     for (uint64_t u = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) / G; u < n; u += ng) {
+        // each lane reads this on its own, so lanes of a row may differ when
+        // u is hooked meanwhile; skipping any subset of u's entries is safe
+        if (__ldcg(parent + u) == skip) continue;
         const uint32_t e = rp[u + 1];
-        for (uint32_t j = rp[u] + lane; j < e; j += G) {
-            const uint32_t c = __ldg(col + j);
-            if (c > u) cc_union(parent, (uint32_t)u, c, n + 1, err);
-        }
+        for (uint32_t j = rp[u] + r0 + lane; j < e; j += G) cc_union(parent, (uint32_t)u, __ldg(col + j), n + 1, err);
     }
 }
 
@@ -790,18 +813,42 @@ static int mtx_impl(Context &C, MtxSource &src, int out_mem, sgp_b200_graph_t *o
         SGPB_TRY(dzero(C, size, sizeof(uint32_t) * ((size_t)n + 1)));
         SGPB_TRY(dzero(C, cc, 8));
         SGPB_TRY(dzero(C, best, 8));
-        k_cc_init<<<grid_for(C, n, 256), 256, 0, C.stream>>>(n, rp, col, parent);
+        // sampling (two neighbour rounds), the largest sampled component,
+        // then the remaining entries of the vertices outside it
+        constexpr uint32_t kRounds = 2, kProbe = 1024;
+        k_cc_init<<<grid_for(C, n, 256), 256, 0, C.stream>>>(n, parent);
+        for (uint32_t r = 0; r < kRounds; r++)
+            k_cc_sample<<<grid_for(C, n, 256), 256, 0, C.stream>>>(n, rp, col, parent, r, cc);
+        k_cc_compress<<<grid_for(C, n, 256), 256, 0, C.stream>>>(n, parent);
+        const uint32_t probes = n < kProbe ? n : kProbe;
+        k_cc_probe<<<cdiv(probes, 256), 256, 0, C.stream>>>(n, probes, parent, size);
+        SGPB_CUDA(cudaGetLastError());
+        std::vector<uint32_t> lab(probes);
+        SGPB_TRY(read_u32(C, size, lab.data(), (int)probes));
+        std::sort(lab.begin(), lab.end());
+        uint32_t skip = lab[0], run = 0, best_run = 0;
+        for (uint32_t i = 0; i < probes; i++) {
+            run = (i > 0 && lab[i] == lab[i - 1]) ? run + 1 : 1;
+            if (run > best_run) {
+                best_run = run;
+                skip = lab[i];
+            }
+        }
+        SGPB_TRY(dzero(C, size, sizeof(uint32_t) * ((size_t)n + 1)));
         const double avg = (double)m_all / n;
         if (avg <= 4)
-            k_cc_hook<4><<<grid_for(C, (uint64_t)n * 4, 256), 256, 0, C.stream>>>(n, rp, col, parent, cc);
+            k_cc_rest<4><<<grid_for(C, (uint64_t)n * 4, 256), 256, 0, C.stream>>>(n, rp, col, parent, skip, kRounds, cc);
         else if (avg <= 16)
-            k_cc_hook<16><<<grid_for(C, (uint64_t)n * 16, 256), 256, 0, C.stream>>>(n, rp, col, parent, cc);
+            k_cc_rest<16><<<grid_for(C, (uint64_t)n * 16, 256), 256, 0, C.stream>>>(n, rp, col, parent, skip, kRounds,
+                                                                                   cc);
         else
-            k_cc_hook<32><<<grid_for(C, (uint64_t)n * 32, 256), 256, 0, C.stream>>>(n, rp, col, parent, cc);
+            k_cc_rest<32><<<grid_for(C, (uint64_t)n * 32, 256), 256, 0, C.stream>>>(n, rp, col, parent, skip, kRounds,
+                                                                                   cc);
+        C.kernel_launches += 3 + kRounds;
         k_cc_flatten<<<grid_for(C, n, 256), 256, 0, C.stream>>>(n, parent, size);
         k_cc_best<<<grid_for(C, n, 256), 256, 0, C.stream>>>(n, parent, size, best, cc + 1);
         SGPB_CUDA(cudaGetLastError());
-        C.kernel_launches += 4;
+        C.kernel_launches += 2;
         uint32_t ccv[2];
         uint64_t bk = 0;
         SGPB_TRY(read_u32(C, cc, ccv, 2));
