@@ -17,6 +17,14 @@ value = total edges of all replicas / max over ranks of the step time.
 
 `--impl reference` times the reference's own OpenMP path (cmg/sgpar.h built
 by oracle/Makefile) on the host cores on a bounded R-MAT sample.
+
+`--workload mtx2csr` measures the MatrixMarket converter instead (the
+reference's cmg/mtx2csr.cpp): one step = one conversion of the R-MAT scale-22
+graph written as a shuffled symmetric pattern file with 10% repeated entry
+lines and 1% extra isolated vertices (symmetrise, dedupe and largest-component
+extraction all do work); value = entry lines per second with the text resident
+in HBM and the CSR left there, e2e = pinned host text to a host CSR, and the
+reference arm times the reference converter binary on the same file.
 """
 from __future__ import annotations
 
@@ -299,6 +307,155 @@ def gpu_arm(args, rank: int, ws: int, local: int, distmod):
         dist.destroy_process_group()
 
 
+MTX_METRIC = "MatrixMarket entry lines/s converted to CSR (R-MAT scale 22 file, LCC kept)"
+MTX_SAMPLE_SCALE = 20
+
+
+def mtx_text(scale: int):
+    """The converter's input: R-MAT `scale` as a shuffled symmetric pattern
+    file with 10% repeated lines and 1% extra isolated vertices."""
+    from ipdps_2021_graph_coarsening_b200 import graphs as G
+    g = rmat_graph(scale)
+    return g, G.mtx_of(g, seed=7, dup_frac=0.1, extra_vertices=g.n // 100)
+
+
+def mtx_config(g, text, lines, scale):
+    return {"workload": f"rmat{scale} as MatrixMarket (symmetric pattern, lower triangle shuffled, "
+                        f"10% repeated lines, 1% isolated vertices)",
+            "text_bytes": len(text), "entry_lines": lines, "n_out": g.n, "m_out_directed": g.m_directed,
+            "l2": "inputs larger than L2 (text 1.2 GB)"}
+
+
+def mtx_reference_arm(args, rank: int):
+    """The reference converter (cmg/mtx2csr.cpp, built by oracle/Makefile) on
+    the host: one step converts a file of the same construction at a bounded
+    scale, file to file, as its command does."""
+    if rank != 0:
+        return
+    ref = os.path.join(ROOT, "oracle", "_ref", "mtx2csr")
+    if not os.path.exists(ref):
+        print(json.dumps({"impl": "reference", "unavailable": "reference converter (oracle/_ref/mtx2csr) not built"}))
+        return
+    import tempfile
+    g, text = mtx_text(MTX_SAMPLE_SCALE)
+    lines = text.count(b"\n") - 2
+    with tempfile.TemporaryDirectory() as d:
+        src, dst = os.path.join(d, "g.mtx"), os.path.join(d, "g.csr")
+        with open(src, "wb") as f:
+            f.write(text)
+        times = []
+        for i in range(args.warmup + args.steps):
+            t = time.perf_counter()
+            subprocess.run([ref, src, dst], check=True, capture_output=True)
+            if i >= args.warmup:
+                times.append(time.perf_counter() - t)
+    sec = float(np.mean(times))
+    value = lines / sec
+    line = {"impl": "reference", "metric": MTX_METRIC, "value": value, "unit": "lines/s", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": sec * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "u32", "data": "synthetic",
+            "config": mtx_config(g, text, lines, MTX_SAMPLE_SCALE),
+            "cpu_baseline": {"value": value, "unit": "lines/s", "cores": 1, "kind": "reference",
+                             "sample": f"R-MAT scale {MTX_SAMPLE_SCALE} file of the same construction, "
+                                       f"cmg/mtx2csr.cpp binary (serial), file to file"},
+            "e2e": {"value": value, "unit": "lines/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+
+
+def mtx_arm(args, rank: int, ws: int, local: int, distmod):
+    import torch
+    from ipdps_2021_graph_coarsening_b200.api import Partitioner
+    from ipdps_2021_graph_coarsening_b200 import _lib as L
+
+    torch.cuda.set_device(local)
+    dist = None
+    if distmod:
+        dist, td = distmod
+        dist.init_process_group("nccl", timeout=td(seconds=600), device_id=torch.device("cuda", local))
+    g, text = mtx_text(args.scale)
+    lines = text.count(b"\n") - 2
+    p = Partitioner(local)
+    stream = torch.cuda.ExternalStream(L.lib().sgp_b200_stream(p._ctx))
+    dtext = torch.frombuffer(bytearray(text), dtype=torch.uint8).cuda()
+    htext = torch.frombuffer(bytearray(text), dtype=torch.uint8).pin_memory()
+
+    def barrier():
+        if dist:
+            dist.barrier()
+
+    def timed(fn, steps):
+        torch.cuda.synchronize()
+        barrier()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        out = [fn() for _ in range(steps)]
+        e1.record(stream)
+        torch.cuda.synchronize()
+        barrier()
+        ms = e0.elapsed_time(e1) / steps
+        if dist:
+            t = torch.tensor([ms], device="cuda")
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            ms = float(t.item())
+        return ms, out
+
+    def dev_step():
+        return p.mtx_read(dtext, device_out=True)[1]
+
+    def host_step():
+        return p.mtx_read(htext)[1]
+
+    for _ in range(args.warmup):
+        dev_step()
+    with Clocks(local) as clk:
+        ms, infos = timed(dev_step, args.steps)
+    info = infos[-1]
+    assert info["n"] == g.n and info["m"] == g.m_directed, "converter output differs from the generated graph"
+    clocks = clk.summary()
+    value = ws * lines / (ms / 1e3)
+    host_step()
+    ms_e2e, _ = timed(host_step, args.steps)
+    e2e = {"value": ws * lines / (ms_e2e / 1e3), "unit": "lines/s", "h2d_bytes_per_step": len(text),
+           "d2h_bytes_per_step": 4 * (g.n + 1) + 4 * g.m_directed, "ms_per_step": ms_e2e}
+    # roofline: the parse pass (line starts, ids, degrees) is the byte-bound
+    # kernel; the phase split says where the rest of the step goes
+    peak, peak_kind = load_peaks()
+    parse_bytes = 2 * len(text) + 8 * lines
+    roofline = {"bound": "hbm", "kernel": "k_mtx_count + k_mtx_parse (text pass)",
+                "algorithmic_bytes": parse_bytes, "kernel_ms": info["ms_parse"],
+                "achieved": parse_bytes / (info["ms_parse"] / 1e3) / 1e9, "peak": peak, "unit": "GB/s",
+                "peak_kind": peak_kind, "traffic": None}
+    roofline["frac"] = roofline["achieved"] / peak
+    line = {"metric": MTX_METRIC, "value": value, "unit": "lines/s", "n_gpus": ws, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "u32", "data": "synthetic",
+            "config": mtx_config(g, text, lines, args.scale),
+            "phase_ms": {k: info[k] for k in ("ms_parse", "ms_rows", "ms_components", "ms_extract")},
+            "components": info["components"], "clocks": clocks, "e2e": e2e, "roofline": roofline,
+            "gpu_launches": info["kernel_launches"] * args.steps}
+    if rank == 0 and ws == 1 and not args.no_cpu_baseline:
+        ref = os.path.join(ROOT, "oracle", "_ref", "mtx2csr")
+        if os.path.exists(ref):
+            import tempfile
+            gs, ts = mtx_text(MTX_SAMPLE_SCALE)
+            with tempfile.TemporaryDirectory() as d:
+                src, dst = os.path.join(d, "g.mtx"), os.path.join(d, "g.csr")
+                with open(src, "wb") as f:
+                    f.write(ts)
+                t = time.perf_counter()
+                subprocess.run([ref, src, dst], check=True, capture_output=True)
+                sec = time.perf_counter() - t
+            nl = ts.count(b"\n") - 2
+            line["cpu_baseline"] = {"value": nl / sec, "unit": "lines/s", "cores": 1, "kind": "reference",
+                                    "sample": f"R-MAT scale {MTX_SAMPLE_SCALE} file of the same construction "
+                                              f"({nl} lines), cmg/mtx2csr.cpp binary, file to file"}
+    if rank == 0:
+        print(json.dumps(line))
+    p.close()
+    if dist:
+        dist.destroy_process_group()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -309,16 +466,24 @@ def main():
     ap.add_argument("--scale", type=int, default=SCALE, help="R-MAT scale (the benchmark is 22)")
     ap.add_argument("--single", action="store_true", help="one partition of --scale and exit (profiling)")
     ap.add_argument("--mixed", action="store_true", help="with --single: mixed-precision power iteration")
+    ap.add_argument("--workload", default="partition", choices=["partition", "mtx2csr"],
+                    help="partition (the headline) or the MatrixMarket converter")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
     rank, ws, local, distmod = dist_setup()
     if args.impl == "reference":
         os.environ.setdefault("OMP_NUM_THREADS", str(os.cpu_count() or 1))
-        reference_arm(args, rank, ws)
+        if args.workload == "mtx2csr":
+            mtx_reference_arm(args, rank)
+        else:
+            reference_arm(args, rank, ws)
         return
     os.environ.setdefault("OMP_NUM_THREADS", str(os.cpu_count() or 1))
-    gpu_arm(args, rank, ws, local, distmod)
+    if args.workload == "mtx2csr":
+        mtx_arm(args, rank, ws, local, distmod)
+    else:
+        gpu_arm(args, rank, ws, local, distmod)
 
 
 if __name__ == "__main__":

@@ -86,7 +86,10 @@ int compute_partition_edit_distance(const sgp_vid_t *part1, const sgp_vid_t *par
                                     sgp_vid_t size, sgp_vid_t *diff);
 
 /* sgpar.h:2363 -- multilevel spectral bisection of g on the current CUDA
- * device: HEC coarsening until at most 50 vertices remain, Fiedler power
+ * device: coarsening until at most 50 vertices remain (HEC; heavy-edge
+ * matching when config->coarsening_alg & 1, stopping after a level that keeps
+ * more than 0.9 of the vertices; none when config->coarsening_alg & 16, as
+ * sgpar.h:2457-2475 reads those bits), Fiedler power
  * iteration (tolerance config->tol, FP64) up the hierarchy, median split.
  * part[n] is caller-allocated host memory; *edge_cut receives the cut of the
  * bisection.  rng seeds the mapping hashes and the coarsest guess and is
@@ -156,7 +159,18 @@ typedef struct {
     int refine_alg;             /* 0: shifted combinatorial Laplacian (reference default);
                                    1: normalized Laplacian, lazy random walk (I + D^-1 A) / 2
                                    without deflation in the loop, as eigensolve_kokkos.h:103-206 */
+    int coarsener;              /* SGP_B200_COARSEN_*: the reference's compile-time coarsener
+                                   choice (coarsen_kokkos.h:1138-1150); | SGP_B200_COARSEN_NONE
+                                   skips coarsening, | SGP_B200_COARSEN_RATIO_STOP stops after a
+                                   level keeping more than 0.9 of the vertices (sgpar.h:2466-2475) */
 } sgp_b200_options_t;
+
+#define SGP_B200_COARSEN_HEC 0      /* heavy-edge coarsening, heuristics.h:930-1031 (default) */
+#define SGP_B200_COARSEN_MATCH 1    /* heavy-edge matching, heuristics.h:1584-1740 (PUREMATCH) */
+#define SGP_B200_COARSEN_MIS2 2     /* distance-2 independent-set aggregation, heuristics.h:8-80, :218-310 */
+#define SGP_B200_COARSEN_GOSH 3     /* degree-keyed cluster aggregation, heuristics.h:81-216, :312-365 */
+#define SGP_B200_COARSEN_NONE 16
+#define SGP_B200_COARSEN_RATIO_STOP 32
 
 #define SGP_B200_MAX_LEVELS 202
 
@@ -260,6 +274,13 @@ int sgp_b200_power_iter(sgp_b200_ctx_t *ctx, uint32_t n, const uint32_t *row_ptr
 
 /* Median split + edge cut (sgpar.h:1969-2071) of a device eigenvector;
  * part is a device array of n entries. */
+/* One level's mapping by an alternative coarsener (coarsener MATCH, MIS2 or
+ * GOSH; the HEC mapping is sgp_b200_hec) on device arrays: vcmap[n] receives
+ * the coarse vertex of each vertex, *nc the coarse count, *rounds the
+ * matching rounds or independent-set iterations. */
+int sgp_b200_coarsen_map(sgp_b200_ctx_t *ctx, uint32_t n, const uint32_t *row_ptr, const uint32_t *col,
+                         const void *w, int wbytes, int coarsener, int random_level, uint64_t seed,
+                         uint32_t *vcmap, uint32_t *nc, int *rounds);
 int sgp_b200_split(sgp_b200_ctx_t *ctx, uint32_t n, const uint32_t *row_ptr, const uint32_t *col,
                    const double *evec, int perc_imbalance, uint32_t *part, uint64_t *edgecut);
 
@@ -313,6 +334,7 @@ typedef struct {
     float ms_read;              /* file read + copy of the text to the device (host clock) */
     float ms_parse, ms_rows, ms_components, ms_extract;   /* device phases (CUDA events) */
     float ms_out;               /* result copy-out (host clock) */
+    uint32_t kernel_launches;   /* kernels this call launched */
 } sgp_b200_mtx_info_t;
 
 /* MatrixMarket coordinate text -> symmetric CSR of its largest connected

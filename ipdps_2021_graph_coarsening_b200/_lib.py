@@ -19,6 +19,8 @@ P = ctypes.POINTER
 MAX_LEVELS = 202
 OK, FAIL, ERR_INVALID, ERR_DEVICE, ERR_TOO_LARGE, ERR_BUDGET = 0, 1, 2, 3, 4, 5
 HOST, DEVICE = 0, 1
+COARSEN_HEC, COARSEN_MATCH, COARSEN_MIS2, COARSEN_GOSH = 0, 1, 2, 3
+COARSEN_NONE, COARSEN_RATIO_STOP = 16, 32
 
 
 class sgp_pcg32_random_t(ctypes.Structure):
@@ -43,7 +45,7 @@ class sgp_b200_graph_t(ctypes.Structure):
 class sgp_b200_options_t(ctypes.Structure):
     _fields_ = [("cutoff", c_u32), ("tol", c_dbl), ("mixed", c_int), ("perc_imbalance", c_int),
                 ("iter_cap", c_u64), ("rng_state", c_u64), ("rng_inc", c_u64), ("part_mem", c_int),
-                ("refine_alg", c_int)]
+                ("refine_alg", c_int), ("coarsener", c_int)]
 
 
 class sgp_b200_result_t(ctypes.Structure):
@@ -61,7 +63,8 @@ class sgp_b200_mtx_info_t(ctypes.Structure):
     _fields_ = [("rows", c_u64), ("cols", c_u64), ("entries_declared", c_u64), ("lines", c_u64),
                 ("bipartite", c_int), ("n_all", c_u32), ("m_all", c_u64), ("components", c_u32), ("n", c_u32),
                 ("m", c_u64), ("ms_total", c_flt), ("ms_read", c_flt), ("ms_parse", c_flt), ("ms_rows", c_flt),
-                ("ms_components", c_flt), ("ms_extract", c_flt), ("ms_out", c_flt)]
+                ("ms_components", c_flt), ("ms_extract", c_flt), ("ms_out", c_flt),
+                ("kernel_launches", c_u32)]
 
 
 _SIGS = {
@@ -102,6 +105,8 @@ _SIGS = {
     "sgp_b200_power_iter": (c_int, [c_vp, c_u32, c_vp, c_vp, c_vp, c_int, c_vp, c_vp, c_vp, c_dbl, c_u64,
                                     c_int, P(c_u64), P(c_dbl), P(c_dbl)]),
     "sgp_b200_split": (c_int, [c_vp, c_u32, c_vp, c_vp, c_vp, c_int, c_vp, P(c_u64)]),
+    "sgp_b200_coarsen_map": (c_int, [c_vp, c_u32, c_vp, c_vp, c_vp, c_int, c_int, c_int, c_u64, c_vp, P(c_u32),
+                                     P(c_int)]),
     "sgp_b200_last_timing": (c_int, [c_vp, P(c_flt), P(c_flt), P(c_flt), P(c_flt)]),
     "sgp_b200_write_metrics": (c_int, [ctypes.c_char_p, P(sgp_b200_result_t), c_u64, c_u64, c_int, c_int]),
     "sgp_b200_split_noalloc": (c_int, [c_vp, c_u32, c_vp, c_vp, c_vp, c_vp, c_vp]),

@@ -259,12 +259,13 @@ class Partitioner:
 
     @staticmethod
     def _options(cutoff, tol, mixed, rng_state, rng_inc, iter_cap, perc_imbalance,
-                 refine_alg: int = 0) -> L.sgp_b200_options_t:
+                 refine_alg: int = 0, coarsener: int = 0) -> L.sgp_b200_options_t:
         o = L.sgp_b200_options_t()
         L.lib().sgp_b200_default_options(ctypes.byref(o))
         o.cutoff, o.tol, o.mixed, o.perc_imbalance = cutoff, tol, int(mixed), perc_imbalance
         o.iter_cap, o.rng_state, o.rng_inc = iter_cap, rng_state, rng_inc
         o.refine_alg = refine_alg
+        o.coarsener = coarsener
         return o
 
     @staticmethod
@@ -290,14 +291,14 @@ class Partitioner:
 
     def partition(self, g, cutoff: int = 50, tol: float = 1e-10, mixed: bool = False,
                   rng_state: int = 0x853C49E6748FEA9B, rng_inc: int = 1, iter_cap: int = 0,
-                  perc_imbalance: int = 0, part_out=None, refine_alg: int = 0) -> Result:
+                  perc_imbalance: int = 0, part_out=None, refine_alg: int = 0, coarsener: int = 0) -> Result:
         """Partition ``g``: a host :class:`CSR` (numpy) or a dict of CUDA torch
         tensors ``{"row_ptr", "col", "w"}`` (device-resident input).  The
         partition is written to ``part_out`` (numpy or CUDA tensor) when
-        given, else returned as numpy."""
+        given, else returned as numpy.  ``coarsener``: ``_lib.COARSEN_*``."""
         keep = []
         dg = self._graph(g, keep)
-        o = self._options(cutoff, tol, mixed, rng_state, rng_inc, iter_cap, perc_imbalance, refine_alg)
+        o = self._options(cutoff, tol, mixed, rng_state, rng_inc, iter_cap, perc_imbalance, refine_alg, coarsener)
         res = L.sgp_b200_result_t()
         part_out, res.part = self._part_target(dg.n, part_out, o)
         L.check(L.lib().sgp_b200_partition(self._ctx, ctypes.byref(dg), ctypes.byref(o), ctypes.byref(res)),
@@ -306,13 +307,13 @@ class Partitioner:
 
     def partition_4way(self, g, cutoff: int = 50, tol: float = 1e-10, mixed: bool = False,
                        rng_state: int = 0x853C49E6748FEA9B, rng_inc: int = 1, iter_cap: int = 0,
-                       part_out=None) -> tuple:
+                       part_out=None, coarsener: int = 0) -> tuple:
         """The reference driver's 4-way mode (sgpar.cpp:62-89): returns
         (part4, cut of the bisection, cut4, rng state after the call) with
         part4[i] = 2 * bisection part + part inside its induced subgraph."""
         keep = []
         dg = self._graph(g, keep)
-        o = self._options(cutoff, tol, mixed, rng_state, rng_inc, iter_cap, 0)
+        o = self._options(cutoff, tol, mixed, rng_state, rng_inc, iter_cap, 0, 0, coarsener)
         part_out, ptr = self._part_target(dg.n, part_out, o)
         out = (L.c_u64 * 3)()
         L.check(L.lib().sgp_b200_partition_4way(self._ctx, ctypes.byref(dg), ctypes.byref(o), ptr, out),
@@ -321,7 +322,7 @@ class Partitioner:
 
     def partition_batch(self, graphs: list, workers: int = 4, cutoff: int = 50, tol: float = 1e-10,
                         mixed: bool = False, rng_state: int = 0x853C49E6748FEA9B, rng_inc: int = 1,
-                        iter_cap: int = 0) -> list:
+                        iter_cap: int = 0, coarsener: int = 0) -> list:
         """Partition independent host graphs, ``workers`` at a time on
         separate streams (largest first); one :class:`Result` per graph, each
         as if partitioned alone with the same options."""
@@ -330,7 +331,7 @@ class Partitioner:
         arr = (L.sgp_b200_graph_t * cnt)()
         for i, g in enumerate(graphs):
             arr[i] = self._graph(g, keep)
-        o = self._options(cutoff, tol, mixed, rng_state, rng_inc, iter_cap, 0)
+        o = self._options(cutoff, tol, mixed, rng_state, rng_inc, iter_cap, 0, 0, coarsener)
         o.part_mem = L.HOST
         res = (L.sgp_b200_result_t * cnt)()
         parts = []
@@ -343,6 +344,21 @@ class Partitioner:
         return [self._result(res[i], parts[i]) for i in range(len(graphs))]
 
     # -- per-kernel entry points (CUDA torch tensors)
+    def coarsen_map(self, row_ptr, col, w=None, coarsener: int = 1, random_level: bool = False, seed: int = 1):
+        """One level's mapping by an alternative coarsener (MATCH / MIS2 /
+        GOSH): returns (vcmap CUDA tensor, nc, rounds)."""
+        import torch
+        n = row_ptr.numel() - 1
+        vc = torch.empty(n, dtype=torch.int32, device=row_ptr.device)
+        nc = ctypes.c_uint32(0)
+        rounds = ctypes.c_int(0)
+        wb = 0 if w is None else w.element_size()
+        self._sync()
+        L.check(L.lib().sgp_b200_coarsen_map(self._ctx, n, _dptr(row_ptr), _dptr(col), _dptr(w), wb, coarsener,
+                                             int(random_level), seed, _dptr(vc), ctypes.byref(nc),
+                                             ctypes.byref(rounds)), "sgp_b200_coarsen_map")
+        return vc, nc.value, rounds.value
+
     def hec(self, row_ptr, col, w=None, random_level: bool = False, seed: int = 1):
         """Returns (hn, vcmap, nc, rounds) as CUDA tensors / ints."""
         import torch
@@ -408,22 +424,25 @@ class Partitioner:
     def mtx_read(self, source, device_out: bool = False):
         """MatrixMarket coordinate text -> (graph of its largest connected
         component, info dict), computed on the device.  ``source``: a file
-        path, ``bytes``, or a CUDA uint8 tensor holding the text.  Returns a
-        host ``CSR``, or with ``device_out`` a pair of CUDA int32 tensors
-        (row_ptr, col)."""
+        path, ``bytes``, a uint8 numpy array, or a uint8 torch tensor (host
+        memory, pinned or not, or CUDA) holding the text.  Returns a host
+        ``CSR``, or with ``device_out`` a pair of CUDA int32 tensors (row_ptr,
+        col)."""
         out = L.sgp_b200_graph_t()
         info = L.sgp_b200_mtx_info_t()
         mem = L.DEVICE if device_out else L.HOST
-        if isinstance(source, (bytes, bytearray, memoryview)):
-            buf = np.frombuffer(bytes(source), dtype=np.uint8)
-            rc = L.lib().sgp_b200_mtx_parse(self._ctx, buf.ctypes.data if len(buf) else None, len(buf), L.HOST,
+        where = "sgp_b200_mtx_parse"
+        if isinstance(source, (bytes, bytearray, memoryview, np.ndarray)):
+            buf = source if isinstance(source, np.ndarray) else np.frombuffer(source, dtype=np.uint8)
+            buf = np.ascontiguousarray(buf).view(np.uint8).reshape(-1)
+            rc = L.lib().sgp_b200_mtx_parse(self._ctx, buf.ctypes.data if buf.size else None, buf.size, L.HOST,
                                            mem, ctypes.byref(out), ctypes.byref(info))
-            where = "sgp_b200_mtx_parse"
         elif hasattr(source, "data_ptr"):
-            self._sync()
-            rc = L.lib().sgp_b200_mtx_parse(self._ctx, _dptr(source), source.numel(), L.DEVICE, mem,
-                                           ctypes.byref(out), ctypes.byref(info))
-            where = "sgp_b200_mtx_parse"
+            if source.is_cuda:
+                self._sync()
+            rc = L.lib().sgp_b200_mtx_parse(self._ctx, _dptr(source) if source.numel() else None, source.numel(),
+                                           L.DEVICE if source.is_cuda else L.HOST, mem, ctypes.byref(out),
+                                           ctypes.byref(info))
         else:
             rc = L.lib().sgp_b200_mtx_read(self._ctx, str(source).encode(), mem, ctypes.byref(out),
                                           ctypes.byref(info))

@@ -377,55 +377,93 @@ __global__ void __launch_bounds__(256) k_dense_add(const uint32_t *__restrict__ 
     }
 }
 
-// compaction of one dense slot per block, in ascending destination order;
-// clears the slot for reuse.  Each thread takes kCollectWords consecutive
-// bitmap words per pass, so a pass covers 4096 words (131072 destinations)
-// with one block scan.
-constexpr int kCollectWords = 16;
+// Compaction of the dense slots in ascending destination order, clearing
+// them for reuse.  A slot's bitmap is cut into chunks of kChunkWords words,
+// one block per (chunk, slot): k_dense_count counts the bits of each chunk,
+// k_dense_collect finds its chunk's output offset from the counts before it
+// and writes the chunk -- every warp 32 consecutive words at a time, a lane
+// per word -- so the weight loads of many chunks are in flight at once.
+constexpr uint32_t kChunkWords = 8192;
+constexpr int kCollectWarps = 8;                         // 256 threads
+constexpr uint32_t kWarpWords = kChunkWords / kCollectWarps;   // contiguous words per warp
+
+__global__ void __launch_bounds__(256) k_dense_count(uint32_t nc, const uint32_t *__restrict__ bits,
+                                                    uint32_t *__restrict__ chunk_cnt) {
+    const uint32_t nwords = (nc + 31) / 32;
+    const uint32_t nchunks = gridDim.x;
+    const uint32_t *bm = bits + (size_t)blockIdx.y * nwords;
+    const uint32_t w0 = blockIdx.x * kChunkWords;
+    uint32_t c = 0;
+    for (uint32_t w = w0 + threadIdx.x; w < w0 + kChunkWords && w < nwords; w += blockDim.x) c += __popc(__ldcg(bm + w));
+    c = warp_sum(c);
+    __shared__ uint32_t ws[8];
+    if ((threadIdx.x & 31) == 0) ws[threadIdx.x >> 5] = c;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        uint32_t t = 0;
+        for (int i = 0; i < (int)(blockDim.x >> 5); i++) t += ws[i];
+        chunk_cnt[(size_t)blockIdx.y * nchunks + blockIdx.x] = t;
+    }
+}
 
 template <typename WO>
 __global__ void __launch_bounds__(256) k_dense_collect(const uint32_t *__restrict__ list, uint32_t r0,
                                                       const uint32_t *__restrict__ boff, uint32_t nc,
                                                       WO *__restrict__ acc, uint32_t *__restrict__ bits,
+                                                      const uint32_t *__restrict__ chunk_cnt,
                                                       uint32_t *__restrict__ bdst, WO *__restrict__ tw,
                                                       uint32_t *__restrict__ dcnt) {
-    __shared__ uint64_t scan_sm[33];
-    const uint32_t c = list[r0 + blockIdx.x];
+    __shared__ uint32_t warp_tot[kCollectWarps];
+    __shared__ uint32_t chunk_base;
+    const uint32_t c = list[r0 + blockIdx.y];
     const uint32_t b = boff[c];
-    WO *a = acc + (size_t)blockIdx.x * nc;
     const uint32_t nwords = (nc + 31) / 32;
-    uint32_t *bm = bits + (size_t)blockIdx.x * nwords;
-    uint64_t base = 0;
-    for (uint32_t w0 = 0; w0 < nwords; w0 += blockDim.x * kCollectWords) {
-        const uint32_t wb = w0 + threadIdx.x * kCollectWords;
-        uint32_t word[kCollectWords];
-        uint32_t pc = 0;
-#pragma unroll
-        for (int q = 0; q < kCollectWords; q++) {
-            word[q] = wb + q < nwords ? __ldcg(bm + wb + q) : 0u;
-            pc += __popc(word[q]);
+    const uint32_t nchunks = gridDim.x;
+    WO *a = acc + (size_t)blockIdx.y * nc;
+    uint32_t *bm = bits + (size_t)blockIdx.y * nwords;
+    const uint32_t *cc = chunk_cnt + (size_t)blockIdx.y * nchunks;
+    const unsigned lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    if (threadIdx.x == 0) {
+        uint32_t before = 0, all = 0;
+        for (uint32_t k = 0; k < nchunks; k++) {
+            if (k == blockIdx.x) before = all;
+            all += cc[k];
         }
-        uint64_t tot;
-        const uint64_t inc = block_scan_u64(pc, scan_sm, &tot);
-        uint64_t pos = base + inc - pc;
-#pragma unroll
-        for (int q = 0; q < kCollectWords; q++) {
-            uint32_t wq = word[q];
-            if (!wq) continue;
-            bm[wb + q] = 0;
-            while (wq) {
-                const int bit = __ffs(wq) - 1;
-                wq &= wq - 1;
-                const uint32_t v = (wb + q) * 32 + bit;
-                bdst[b + pos] = v;
-                tw[b + pos] = a[v];
-                a[v] = 0;
-                pos++;
-            }
-        }
-        base += tot;
+        chunk_base = before;
+        if (blockIdx.x == 0) dcnt[c] = all;
     }
-    if (threadIdx.x == 0) dcnt[c] = (uint32_t)base;
+    // this warp's words and their bit count
+    const uint32_t ws0 = blockIdx.x * kChunkWords + wid * kWarpWords;
+    uint32_t cnt = 0;
+    for (uint32_t w = ws0 + lane; w < ws0 + kWarpWords && w < nwords; w += 32) cnt += __popc(__ldcg(bm + w));
+    cnt = warp_sum(cnt);
+    if (lane == 0) warp_tot[wid] = cnt;
+    __syncthreads();
+    uint32_t pos = b + chunk_base;
+    for (uint32_t k = 0; k < wid; k++) pos += warp_tot[k];
+    for (uint32_t w0 = ws0; w0 < ws0 + kWarpWords && w0 < nwords; w0 += 32) {
+        const uint32_t w = w0 + lane;
+        uint32_t word = w < nwords ? __ldcg(bm + w) : 0u;
+        const uint32_t pc = __popc(word);
+        uint32_t incl = pc;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t y = __shfl_up_sync(0xFFFFFFFFu, incl, o);
+            if (lane >= (unsigned)o) incl += y;
+        }
+        uint32_t p = pos + incl - pc;
+        if (word) bm[w] = 0;
+        while (word) {
+            const int bit = __ffs(word) - 1;
+            word &= word - 1;
+            const uint32_t v = w * 32 + bit;
+            bdst[p] = v;
+            tw[p] = a[v];
+            a[v] = 0;
+            p++;
+        }
+        pos += __shfl_sync(0xFFFFFFFFu, incl, 31);
+    }
 }
 
 // ---------------------------------------------------------- compaction --
@@ -512,18 +550,21 @@ static int dedupe_buckets(Context &C, uint32_t nc, const uint32_t *boff, uint32_
             if (slots > n3) slots = n3;
             if (slots > 65535) slots = 65535;
             WO *acc;
-            uint32_t *bits;
+            uint32_t *bits, *chunk_cnt;
+            const uint32_t nchunks = cdiv(words, kChunkWords);
             SGPB_TRY(dalloc_t(C, &acc, slots * nc));
             SGPB_TRY(dalloc_t(C, &bits, slots * words));
+            SGPB_TRY(dalloc_t(C, &chunk_cnt, slots * nchunks));
             SGPB_TRY(dzero(C, acc, slots * nc * sizeof(WO)));
             SGPB_TRY(dzero(C, bits, slots * words * 4));
             for (uint32_t r0 = 0; r0 < n3; r0 += (uint32_t)slots) {
                 uint32_t nr = n3 - r0 < slots ? n3 - r0 : (uint32_t)slots;
-                dim3 ga(8, nr);
+                dim3 ga(8, nr), gc(nchunks, nr);
                 k_dense_add<WI, WO><<<ga, 256, 0, C.stream>>>(lists + 3 * (size_t)nc, r0, boff, bdst, bw, nc, acc, bits);
-                k_dense_collect<WO><<<nr, 256, 0, C.stream>>>(lists + 3 * (size_t)nc, r0, boff, nc, acc, bits, bdst, tw,
-                                                             dcnt);
-                C.kernel_launches += 2;
+                k_dense_count<<<gc, 256, 0, C.stream>>>(nc, bits, chunk_cnt);
+                k_dense_collect<WO><<<gc, 256, 0, C.stream>>>(lists + 3 * (size_t)nc, r0, boff, nc, acc, bits,
+                                                             chunk_cnt, bdst, tw, dcnt);
+                C.kernel_launches += 3;
             }
             SGPB_CUDA(cudaGetLastError());
         }

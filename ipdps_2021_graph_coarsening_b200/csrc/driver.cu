@@ -125,7 +125,13 @@ static int weight_width(Context &C, const Level &L0, int *wbytes) {
 // coarsen_kokkos.h:1196-1232: levels while n > cutoff, at most 200; a
 // coarsest level below 10 vertices is dropped.
 static int generate(Context &C, const Level &L0, uint32_t cutoff, uint64_t *rng_state, uint64_t rng_inc,
-                    std::vector<Level> &levels) {
+                    std::vector<Level> &levels, int coarsener = SGP_B200_COARSEN_HEC) {
+    const int kind = coarsener & 15;
+    if (kind > SGP_B200_COARSEN_GOSH || (coarsener & ~(15 | SGP_B200_COARSEN_NONE | SGP_B200_COARSEN_RATIO_STOP))) {
+        set_error("coarsener %d: HEC 0, MATCH 1, MIS2 2 or GOSH 3, optionally | NONE (16) | RATIO_STOP (32)",
+                  coarsener);
+        return SGP_B200_ERR_INVALID;
+    }
     levels.clear();
     levels.push_back(L0);
     int out_wbytes = 4;
@@ -137,7 +143,7 @@ static int generate(Context &C, const Level &L0, uint32_t cutoff, uint64_t *rng_
         ~EvFree() { for (int i = 0; i < 3; i++) cudaEventDestroy(e[i]); }
     } evfree{ev};
     C.t_map = C.t_build = 0;
-    while (levels.back().n > cutoff) {
+    while (!(coarsener & SGP_B200_COARSEN_NONE) && levels.back().n > cutoff) {
         Level &F = levels.back();
         uint32_t hi = pcg32(rng_state, rng_inc);
         uint32_t lo = pcg32(rng_state, rng_inc);
@@ -150,7 +156,12 @@ static int generate(Context &C, const Level &L0, uint32_t cutoff, uint64_t *rng_
         int rounds = 0;
         const int random_level = (levels.size() == 1) && (L0.w == nullptr);
         SGPB_CUDA(cudaEventRecord(ev[0], C.stream));
-        SGPB_TRY(hec_map_level(C, F, random_level, seed, vcmap, nullptr, &nc, &rounds));
+        if (kind == SGP_B200_COARSEN_HEC)
+            SGPB_TRY(hec_map_level(C, F, random_level, seed, vcmap, nullptr, &nc, &rounds));
+        else if (kind == SGP_B200_COARSEN_MATCH)
+            SGPB_TRY(match_map_level(C, F, random_level, seed, vcmap, &nc, &rounds));
+        else
+            SGPB_TRY(set_map_level(C, F, kind == SGP_B200_COARSEN_GOSH, seed, vcmap, &nc, &rounds));
         F.vcmap = vcmap;
         F.hec_rounds = rounds;
         SGPB_CUDA(cudaEventRecord(ev[1], C.stream));
@@ -163,8 +174,10 @@ static int generate(Context &C, const Level &L0, uint32_t cutoff, uint64_t *rng_
         cudaEventElapsedTime(&b, ev[1], ev[2]);
         C.t_map += a;
         C.t_build += b;
+        const uint32_t fine_n = F.n;   // F is invalidated by the push
         levels.push_back(Cl);
         if (levels.size() > 200) break;
+        if ((coarsener & SGP_B200_COARSEN_RATIO_STOP) && (double)nc / (double)fine_n > 0.9) break;
     }
     if (levels.size() > 1 && levels.back().n < 10) {
         levels.pop_back();
@@ -241,7 +254,7 @@ static int partition_staged(Context &C, const Level &L0, const sgp_b200_options_
     SGPB_CUDA(cudaEventRecord(ev[1], C.stream));
     uint64_t st = opt->rng_state;
     std::vector<Level> levels;
-    SGPB_TRY(generate(C, L0, opt->cutoff, &st, opt->rng_inc, levels));
+    SGPB_TRY(generate(C, L0, opt->cutoff, &st, opt->rng_inc, levels, opt->coarsener));
     SGPB_CUDA(cudaEventRecord(ev[2], C.stream));
     PowerIterOpts po;
     po.tol = opt->tol;
@@ -407,6 +420,7 @@ void sgp_b200_default_options(sgp_b200_options_t *o) {
     o->rng_inc = 1;
     o->part_mem = SGP_B200_HOST;
     o->refine_alg = 0;
+    o->coarsener = SGP_B200_COARSEN_HEC;
 }
 
 int sgp_b200_partition(sgp_b200_ctx_t *x, const sgp_b200_graph_t *g, const sgp_b200_options_t *opt,
@@ -615,6 +629,34 @@ int sgp_b200_hec(sgp_b200_ctx_t *x, uint32_t n, const uint32_t *rp, const uint32
     return rc;
 }
 
+int sgp_b200_coarsen_map(sgp_b200_ctx_t *x, uint32_t n, const uint32_t *rp, const uint32_t *col, const void *w,
+                         int wbytes, int coarsener, int random_level, uint64_t seed, uint32_t *vcmap, uint32_t *nc,
+                         int *rounds) {
+    Context *C = ctx_get(x);
+    if (!C || !rp || !vcmap || !nc) { set_error("null argument"); return SGP_B200_ERR_INVALID; }
+    if (wbytes != 0 && wbytes != 4 && wbytes != 8) { set_error("wbytes must be 0, 4 or 8"); return SGP_B200_ERR_INVALID; }
+    if (coarsener < SGP_B200_COARSEN_MATCH || coarsener > SGP_B200_COARSEN_GOSH) {
+        set_error("sgp_b200_coarsen_map takes MATCH (1), MIS2 (2) or GOSH (3); HEC is sgp_b200_hec");
+        return SGP_B200_ERR_INVALID;
+    }
+    cudaSetDevice(C->device);
+    Level L;
+    L.n = n; L.rp = (uint32_t *)rp; L.col = (uint32_t *)col; L.w = (void *)(wbytes ? w : nullptr);
+    L.wbytes = wbytes ? wbytes : 0;
+    uint32_t mm = 0;
+    int rc = n ? read_u32(*C, rp + n, &mm) : 0;
+    L.m = mm;
+    int r = 0;
+    if (rc == SGP_B200_OK) {
+        if (coarsener == SGP_B200_COARSEN_MATCH) rc = match_map_level(*C, L, random_level, seed, vcmap, nc, &r);
+        else rc = set_map_level(*C, L, coarsener == SGP_B200_COARSEN_GOSH, seed, vcmap, nc, &r);
+    }
+    if (rounds) *rounds = r;
+    cudaStreamSynchronize(C->stream);
+    release_all(*C);
+    return rc;
+}
+
 int sgp_b200_build_coarse(sgp_b200_ctx_t *x, uint32_t n, const uint32_t *rp, const uint32_t *col, const void *w,
                           int wbytes, const uint32_t *vcmap, uint32_t nc, int out_wbytes, uint32_t *crp,
                           uint32_t *ccol, void *cw, uint64_t *m_c) {
@@ -702,6 +744,12 @@ int sgp_partition_graph(sgp_vid_t *part, sgp_eid_t *edge_cut, config_t *config, 
     sgp_b200_default_options(&o);
     o.tol = config->tol > 0 ? config->tol : g_tol;
     o.refine_alg = config->refine_alg;
+    // sgpar.h:2457-2475: bit 4 skips coarsening, bit 0 picks heavy-edge
+    // matching with the 0.9 coarsening-ratio stop (bits 1-2 choose a dedupe
+    // method, which does not change the coarse graph)
+    o.coarsener = (config->coarsening_alg & 16) ? SGP_B200_COARSEN_NONE
+                  : (config->coarsening_alg & 1) ? (SGP_B200_COARSEN_MATCH | SGP_B200_COARSEN_RATIO_STOP)
+                                                 : SGP_B200_COARSEN_HEC;
     o.perc_imbalance = perc_imbalance_allowed;
     o.rng_state = rng->state;
     o.rng_inc = rng->inc;

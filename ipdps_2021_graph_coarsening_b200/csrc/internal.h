@@ -107,6 +107,12 @@ int hec_map_level(Context &C, const Level &L, int random_level, uint64_t seed, u
                   uint32_t *hn_out, uint32_t *nc_out, int *rounds_out);
 int build_coarse_level(Context &C, const Level &F, const uint32_t *vcmap, uint32_t nc, int out_wbytes,
                        Level *out);
+// the alternative coarseners (coarsen_alt.cu): heavy-edge matching, and the
+// MIS-2 (gosh false) / GOSH (gosh true) aggregations
+int match_map_level(Context &C, const Level &L, int random_level, uint64_t seed, uint32_t *vcmap, uint32_t *nc_out,
+                    int *rounds_out);
+int set_map_level(Context &C, const Level &L, bool gosh, uint64_t seed, uint32_t *vcmap, uint32_t *nc_out,
+                  int *rounds_out);
 struct PowerIterOpts {
     double tol = 1e-10;
     uint64_t iter_cap = 0;   // 0: the reference's 1e14 / n only

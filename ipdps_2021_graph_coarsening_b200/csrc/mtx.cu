@@ -53,9 +53,16 @@
 #include <string.h>
 #include <sys/stat.h>
 
+#include <unistd.h>
+
 #include <algorithm>
+#include <atomic>
 #include <chrono>
+#include <condition_variable>
+#include <functional>
+#include <mutex>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "common.cuh"
@@ -69,7 +76,7 @@ constexpr uint64_t kMtxTile = (uint64_t)kMtxThreads * kMtxBytes;  // bytes per b
 constexpr uint32_t kNoEdge = 0xFFFFFFFFu;
 constexpr int kMaxBanners = 16;
 constexpr int kStageSlots = 4;
-constexpr size_t kStageSlotBytes = (size_t)16 << 20;
+constexpr size_t kStageSlotBytes = (size_t)32 << 20;
 
 enum : uint32_t { kLineSyntax = 1, kLineZero = 2, kLineRange = 3 };
 
@@ -506,6 +513,110 @@ static int read_head(Context &C, MtxSource &src, MtxHead *h) {
     }
 }
 
+// A process-wide pool of host threads for the staging copies: one core's
+// memcpy or pread (5-10 GB/s) is far below the host<->device copy rate, so
+// the pinned ring is filled and drained by several.  Jobs run one at a time.
+class HostPool {
+  public:
+    static HostPool &get() {
+        static HostPool *p = new HostPool();   // never destroyed: idle workers end with the process
+        return *p;
+    }
+    int width() const { return (int)th_.size() + 1; }
+    // fn(k) for every k in [0, parts), on the workers and the calling thread
+    void run(int parts, const std::function<void(int)> &fn) {
+        std::lock_guard<std::mutex> one(run_mu_);
+        {
+            std::lock_guard<std::mutex> lk(mu_);
+            job_ = &fn;
+            parts_ = parts;
+            next_.store(0);
+            busy_ = (int)th_.size();
+            gen_++;
+        }
+        cv_.notify_all();
+        work();
+        std::unique_lock<std::mutex> lk(mu_);
+        done_.wait(lk, [&] { return busy_ == 0; });
+        job_ = nullptr;
+    }
+
+  private:
+    HostPool() {
+        const unsigned hw = std::thread::hardware_concurrency();
+        const int w = hw > 8 ? 8 : (hw ? (int)hw : 1);
+        for (int i = 1; i < w; i++) th_.emplace_back([this] { loop(); });
+    }
+    void work() {
+        for (;;) {
+            const int k = next_.fetch_add(1);
+            if (k >= parts_) return;
+            (*job_)(k);
+        }
+    }
+    void loop() {
+        uint64_t seen = 0;
+        for (;;) {
+            {
+                std::unique_lock<std::mutex> lk(mu_);
+                cv_.wait(lk, [&] { return gen_ != seen; });
+                seen = gen_;
+            }
+            work();
+            std::lock_guard<std::mutex> lk(mu_);
+            if (--busy_ == 0) done_.notify_one();
+        }
+    }
+    std::vector<std::thread> th_;
+    std::mutex run_mu_, mu_;
+    std::condition_variable cv_, done_;
+    const std::function<void(int)> *job_ = nullptr;
+    int parts_ = 0, busy_ = 0;
+    std::atomic<int> next_{0};
+    uint64_t gen_ = 0;
+};
+
+// dst[0, n) = src[0, n) in pool-sized pieces of at least 1 MiB
+static void par_copy(void *dst, const void *src, size_t n) {
+    HostPool &P = HostPool::get();
+    const size_t min_piece = (size_t)1 << 20;
+    int parts = (int)((n + min_piece - 1) / min_piece);
+    if (parts > P.width()) parts = P.width();
+    if (parts <= 1) {
+        memcpy(dst, src, n);
+        return;
+    }
+    const size_t piece = (n + parts - 1) / parts;
+    P.run(parts, [&](int k) {
+        const size_t o = (size_t)k * piece;
+        if (o < n) memcpy((char *)dst + o, (const char *)src + o, n - o < piece ? n - o : piece);
+    });
+}
+
+// buf[0, n) = bytes [off, off + n) of file descriptor fd, in parallel pieces
+static bool par_pread(int fd, uint8_t *buf, size_t n, uint64_t off) {
+    HostPool &P = HostPool::get();
+    const size_t min_piece = (size_t)1 << 20;
+    int parts = (int)((n + min_piece - 1) / min_piece);
+    if (parts > P.width()) parts = P.width();
+    if (parts < 1) parts = 1;
+    const size_t piece = (n + parts - 1) / parts;
+    std::atomic<bool> ok{true};
+    P.run(parts, [&](int k) {
+        size_t o = (size_t)k * piece;
+        const size_t e = o + piece < n ? o + piece : n;
+        while (o < e) {
+            const ssize_t r = pread(fd, buf + o, e - o, (off_t)(off + o));
+            if (r <= 0) {
+                ok.store(false);
+                return;
+            }
+            o += (size_t)r;
+        }
+    });
+    return ok.load();
+}
+
 static int ensure_stage(Context &C) {
     if (C.h_stage) return SGP_B200_OK;
     SGPB_CUDA(cudaMallocHost((void **)&C.h_stage, kStageSlots * kStageSlotBytes));
@@ -514,42 +625,78 @@ static int ensure_stage(Context &C) {
     return SGP_B200_OK;
 }
 
+static bool is_pinned(const void *p) {
+    cudaPointerAttributes at;
+    const bool pinned = cudaPointerGetAttributes(&at, p) == cudaSuccess && at.type == cudaMemoryTypeHost;
+    cudaGetLastError();
+    return pinned;
+}
+
 // The whole text into `dtext` (capacity >= len): pinned host memory and device
 // memory in one copy; pageable memory and files through the pinned ring, the
-// fill of one slot overlapping the copies of the others.
+// fill of one slot (by the host pool) overlapping the copies of the others.
 static int upload_text(Context &C, MtxSource &src, uint8_t *dtext) {
     if (src.dev) {
         SGPB_CUDA(cudaMemcpyAsync(dtext, src.dev, src.len, cudaMemcpyDeviceToDevice, C.stream));
         return SGP_B200_OK;
     }
-    if (src.host) {
-        cudaPointerAttributes at;
-        if (cudaPointerGetAttributes(&at, src.host) == cudaSuccess && at.type == cudaMemoryTypeHost) {
-            SGPB_CUDA(cudaMemcpyAsync(dtext, src.host, src.len, cudaMemcpyHostToDevice, C.stream));
-            return SGP_B200_OK;
-        }
-        cudaGetLastError();
+    if (src.host && is_pinned(src.host)) {
+        SGPB_CUDA(cudaMemcpyAsync(dtext, src.host, src.len, cudaMemcpyHostToDevice, C.stream));
+        return SGP_B200_OK;
     }
     SGPB_TRY(ensure_stage(C));
-    if (src.f && fseek(src.f, 0, SEEK_SET) != 0) {
-        set_error("seek failed");
-        return SGP_B200_ERR_INVALID;
-    }
     int slot = 0;
     for (uint64_t off = 0; off < src.len; off += C.h_stage_slot, slot = (slot + 1) % kStageSlots) {
         const size_t n = (size_t)(src.len - off < C.h_stage_slot ? src.len - off : C.h_stage_slot);
         uint8_t *buf = C.h_stage + (size_t)slot * C.h_stage_slot;
         SGPB_CUDA(cudaEventSynchronize(C.stage_ev[slot]));
         if (src.f) {
-            if (fread(buf, 1, n, src.f) != n) {
+            if (!par_pread(fileno(src.f), buf, n, off)) {
                 set_error("short read at byte %llu", (unsigned long long)off);
                 return SGP_B200_ERR_INVALID;
             }
         } else {
-            memcpy(buf, src.host + off, n);
+            par_copy(buf, src.host + off, n);
         }
         SGPB_CUDA(cudaMemcpyAsync(dtext + off, buf, n, cudaMemcpyHostToDevice, C.stream));
         SGPB_CUDA(cudaEventRecord(C.stage_ev[slot], C.stream));
+    }
+    return SGP_B200_OK;
+}
+
+// Device -> pageable host through the pinned ring: the copy of one slot out
+// (by the host pool) overlaps the transfers into the others.
+struct CopySeg {
+    void *dst;
+    const void *src;
+    size_t bytes;
+};
+static int download_staged(Context &C, const CopySeg *segs, int nseg) {
+    SGPB_TRY(ensure_stage(C));
+    struct Chunk {
+        char *dst;
+        const char *src;
+        size_t n;
+    };
+    std::vector<Chunk> ch;
+    for (int i = 0; i < nseg; i++)
+        for (size_t o = 0; o < segs[i].bytes; o += C.h_stage_slot)
+            ch.push_back({(char *)segs[i].dst + o, (const char *)segs[i].src + o,
+                          segs[i].bytes - o < C.h_stage_slot ? segs[i].bytes - o : C.h_stage_slot});
+    const int K = (int)ch.size();
+    auto issue = [&](int k) -> int {
+        const int slot = k % kStageSlots;
+        SGPB_CUDA(cudaMemcpyAsync(C.h_stage + (size_t)slot * C.h_stage_slot, ch[k].src, ch[k].n,
+                                  cudaMemcpyDeviceToHost, C.stream));
+        SGPB_CUDA(cudaEventRecord(C.stage_ev[slot], C.stream));
+        return SGP_B200_OK;
+    };
+    for (int k = 0; k < K && k < kStageSlots; k++) SGPB_TRY(issue(k));
+    for (int k = 0; k < K; k++) {
+        const int slot = k % kStageSlots;
+        SGPB_CUDA(cudaEventSynchronize(C.stage_ev[slot]));
+        par_copy(ch[k].dst, C.h_stage + (size_t)slot * C.h_stage_slot, ch[k].n);
+        if (k + kStageSlots < K) SGPB_TRY(issue(k + kStageSlots));
     }
     return SGP_B200_OK;
 }
@@ -603,11 +750,20 @@ static int copy_out(Context &C, uint32_t n, uint64_t m, const uint32_t *rp, cons
             return SGP_B200_ERR_INVALID;
         }
     }
-    const cudaMemcpyKind kind = out_mem == SGP_B200_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;
-    cudaError_t e = cudaMemcpyAsync(orp, rp, brp, kind, C.stream);
-    if (e == cudaSuccess && m) e = cudaMemcpyAsync(ocol, col, sizeof(uint32_t) * m, kind, C.stream);
-    if (e == cudaSuccess) e = cudaStreamSynchronize(C.stream);
-    if (e != cudaSuccess) {
+    int rc = SGP_B200_OK;
+    if (out_mem == SGP_B200_DEVICE) {
+        cudaError_t e = cudaMemcpyAsync(orp, rp, brp, cudaMemcpyDeviceToDevice, C.stream);
+        if (e == cudaSuccess && m) e = cudaMemcpyAsync(ocol, col, sizeof(uint32_t) * m, cudaMemcpyDeviceToDevice, C.stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(C.stream);
+        if (e != cudaSuccess) {
+            set_error("CUDA error copying the output graph: %s", cudaGetErrorString(e));
+            rc = SGP_B200_ERR_DEVICE;
+        }
+    } else {
+        const CopySeg segs[2] = {{orp, rp, brp}, {ocol, col, sizeof(uint32_t) * m}};
+        rc = download_staged(C, segs, m ? 2 : 1);
+    }
+    if (rc != SGP_B200_OK) {
         if (out_mem == SGP_B200_DEVICE) {
             cudaFree(orp);
             cudaFree(ocol);
@@ -615,8 +771,7 @@ static int copy_out(Context &C, uint32_t n, uint64_t m, const uint32_t *rp, cons
             free(orp);
             free(ocol);
         }
-        set_error("CUDA error copying the output graph: %s", cudaGetErrorString(e));
-        return SGP_B200_ERR_DEVICE;
+        return rc;
     }
     out->n = n;
     out->m = m;
@@ -629,6 +784,7 @@ static int copy_out(Context &C, uint32_t n, uint64_t m, const uint32_t *rp, cons
 
 static int mtx_impl(Context &C, MtxSource &src, int out_mem, sgp_b200_graph_t *out, sgp_b200_mtx_info_t *info) {
     const double t_start = now_ms();
+    const uint32_t launches0 = C.kernel_launches;
     sgp_b200_mtx_info_t I;
     memset(&I, 0, sizeof(I));
     MtxHead h;
@@ -904,6 +1060,7 @@ static int mtx_impl(Context &C, MtxSource &src, int out_mem, sgp_b200_graph_t *o
     const double t_end = now_ms();
     I.ms_out = (float)(t_end - t_out);
     I.ms_total = (float)(t_end - t_start);
+    I.kernel_launches = C.kernel_launches - launches0;
     if (info) *info = I;
     return SGP_B200_OK;
 }

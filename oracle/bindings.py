@@ -76,7 +76,11 @@ def lib():
         L.orc_use_partition.argtypes = [c_u32, u32p, u32p, u32p, u32ref, u32p, u32p, u32ref, u32p, u32p]
         L.orc_use_partition.restype = c_int
         L.orc_partition_graph.argtypes = [c_u32, u32p, u32p, ctypes.c_void_p, c_u32, c_dbl,
-                                          u64ref, c_u64, c_int, c_int, u32p, u64ref, f64p, f64p]
+                                          u64ref, c_u64, c_int, c_int, c_int, u32p, u64ref, f64p, f64p]
+        L.orc_match_map.argtypes = [c_u32, u32p, u32p, ctypes.c_void_p, c_int, c_u64, u32p, u32ref, u32ref]
+        L.orc_match_map.restype = c_int
+        L.orc_set_map.argtypes = [c_u32, u32p, u32p, c_int, c_u64, u32p, u32ref, u32ref]
+        L.orc_set_map.restype = c_int
         L.orc_partition_graph.restype = c_int
         _orc = L
     return _orc
@@ -193,8 +197,31 @@ def use_partition(row_ptr, col, part):
     return (rp1[:a + 1].copy(), c1[:rp1[a]].copy()), (rp2[:b + 1].copy(), c2[:rp2[b]].copy())
 
 
+def match_map(row_ptr, col, w, random_level: bool, seed: int):
+    """MATCH coarsener mapping -> (vcmap, nc, rounds)."""
+    rp, cl = _u32(row_ptr), _u32(col)
+    n = rp.shape[0] - 1
+    keep, wp = _w64(w)
+    vc = np.zeros(max(n, 1), np.uint32)
+    nc, rounds = ctypes.c_uint32(0), ctypes.c_uint32(0)
+    lib().orc_match_map(n, rp, cl, wp, int(random_level), seed, vc, ctypes.byref(nc), ctypes.byref(rounds))
+    return vc[:n], nc.value, rounds.value
+
+
+def set_map(row_ptr, col, gosh: bool, seed: int):
+    """MIS-2 (gosh False) or GOSH coarsener mapping -> (vcmap, nc, iterations)."""
+    rp, cl = _u32(row_ptr), _u32(col)
+    n = rp.shape[0] - 1
+    vc = np.zeros(max(n, 1), np.uint32)
+    nc, its = ctypes.c_uint32(0), ctypes.c_uint32(0)
+    if lib().orc_set_map(n, rp, cl, int(gosh), seed, vc, ctypes.byref(nc), ctypes.byref(its)):
+        raise RuntimeError("oracle coarsener left a vertex outside every aggregate")
+    return vc[:n], nc.value, its.value
+
+
 def partition_graph(row_ptr, col, w=None, cutoff: int = 50, tol: float = 1e-10,
-                    rng_state: int = 42, rng_inc: int = 1, perc_imbalance: int = 0, refine_alg: int = 0):
+                    rng_state: int = 42, rng_inc: int = 1, perc_imbalance: int = 0, refine_alg: int = 0,
+                    coarsener: int = 0):
     """Whole multilevel path.  Returns dict(part, edgecut, evec, levels,
     lambda, niter (finest), level_n, level_iters, rng_state)."""
     rp, cl = _u32(row_ptr), _u32(col)
@@ -205,8 +232,9 @@ def partition_graph(row_ptr, col, w=None, cutoff: int = 50, tol: float = 1e-10,
     s = ctypes.c_uint64(rng_state)
     ec = ctypes.c_uint64(0)
     keep, wp = _w64(w)
-    lib().orc_partition_graph(n, rp, cl, wp, cutoff, tol, ctypes.byref(s), rng_inc, perc_imbalance, int(refine_alg),
-                              part, ctypes.byref(ec), ev, stats)
+    if lib().orc_partition_graph(n, rp, cl, wp, cutoff, tol, ctypes.byref(s), rng_inc, perc_imbalance,
+                                 int(refine_alg), int(coarsener), part, ctypes.byref(ec), ev, stats):
+        raise RuntimeError("oracle coarsener left a vertex outside every aggregate")
     nl = int(stats[0])
     return dict(part=part, edgecut=ec.value, evec=ev, levels=nl, **{"lambda": stats[1]},
                 niter=int(stats[2]), level_n=[int(stats[3 + 2 * l]) for l in range(nl)],

@@ -21,6 +21,8 @@
  *   - induced sub-graphs for 4-way recursion (sgpar.h:2666-2752)
  *   - the level loop of sgp_generate_coarse_graphs (coarsen_kokkos.h:1165-1234)
  *     and sgp_eigensolve (eigensolve_kokkos.h:1493-1595)
+ *   - the alternative coarseners MATCH, MIS-2 and GOSH (heuristics.h:8-365,
+ *     :1584-1740) with this project's deterministic rules
  *
  * Parity pins: the power iteration, the split and the coarse build are checked
  * against the reference's own serial build compiled from its sources
@@ -521,6 +523,188 @@ int orc_use_partition(uint32_t n, const uint32_t *row_ptr, const uint32_t *col,
     return 0;
 }
 
+/* ---------------------------------------------- alternative coarseners -- */
+/* The reference's other coarseners with this project's deterministic rules
+ * (the CUDA path, coarsen_alt.cu, follows the same rules):
+ *   MATCH  heuristics.h:1584-1740 (PUREMATCH): proposal rounds along the
+ *          heavy edge, retries along the heaviest unmatched edge, singletons
+ *   MIS2   heuristics.h:8-80 + :218-310: distance-2 maximal independent set,
+ *          roots take their neighbours, the rest join the first aggregated
+ *          neighbour in row order
+ *   GOSH   heuristics.h:81-216 + :312-365: degree-keyed independent set
+ *          ignoring edges between two vertices above the mean degree, the
+ *          rest join their set neighbour of largest degree (first on a tie)
+ * Random keys are orc_prio_key(seed, u); aggregates are numbered by
+ * ascending root vertex. */
+static uint64_t orc_wt(const uint64_t *w, uint32_t j) { return w ? w[j] : 1; }
+
+/* number aggregates by ascending root (vcmap[u] == u marks a root) */
+static uint32_t orc_number_roots(uint32_t n, uint32_t *vcmap) {
+    uint32_t *rank = (uint32_t *)malloc(((size_t)n + 1) * sizeof(uint32_t));
+    uint32_t nc = 0;
+    for (uint32_t u = 0; u < n; u++) rank[u] = vcmap[u] == u ? nc++ : 0;
+    for (uint32_t u = 0; u < n; u++) vcmap[u] = rank[vcmap[u]];
+    free(rank);
+    return nc;
+}
+
+int orc_match_map(uint32_t n, const uint32_t *rp, const uint32_t *col, const uint64_t *w, int random_level,
+                  uint64_t seed, uint32_t *vcmap, uint32_t *nc_out, uint32_t *rounds_out) {
+    uint32_t *hn = (uint32_t *)malloc(((size_t)n + 1) * sizeof(uint32_t));
+    uint32_t *list = (uint32_t *)malloc(((size_t)n + 1) * sizeof(uint32_t));
+    uint32_t *next = (uint32_t *)malloc(((size_t)n + 1) * sizeof(uint32_t));
+    uint64_t *claim = (uint64_t *)calloc((size_t)n + 1, sizeof(uint64_t));
+    uint8_t *act = (uint8_t *)calloc((size_t)n + 1, 1);
+    /* initial heavy neighbour (heuristics.h:1616-1640) */
+    for (uint32_t u = 0; u < n; u++) {
+        uint32_t b = rp[u], e = rp[u + 1];
+        vcmap[u] = ORC_UNASSIGNED;
+        list[u] = u;
+        if (b == e) { hn[u] = u; continue; }
+        if (random_level) { hn[u] = col[b + (uint32_t)(orc_rand_draw(seed, u) % (e - b))]; continue; }
+        uint64_t bw = orc_wt(w, b);
+        uint32_t bj = b;
+        for (uint32_t j = b + 1; j < e; j++)
+            if (orc_wt(w, j) > bw) { bw = orc_wt(w, j); bj = j; }
+        hn[u] = col[bj];
+    }
+    uint32_t len = n, swap = 1, rounds = 0;
+    for (;;) {
+        for (uint32_t i = 0; i < len; i++) {
+            uint32_t u = list[i], v = hn[u];
+            act[u] = 0;
+            if (v == u) continue;
+            uint64_t ku = orc_prio_key(seed, u), kv = orc_prio_key(seed, v);
+            if ((uint32_t)(ku < kv) ^ swap) {
+                act[u] = 1;
+                if (claim[u] < ku + 1) claim[u] = ku + 1;
+                if (claim[v] < ku + 1) claim[v] = ku + 1;
+            }
+        }
+        for (uint32_t i = 0; i < len; i++) {
+            uint32_t u = list[i];
+            if (!act[u]) continue;
+            uint32_t v = hn[u];
+            uint64_t k = orc_prio_key(seed, u) + 1;
+            if (claim[u] == k && claim[v] == k) { vcmap[u] = u; vcmap[v] = u; }
+        }
+        uint32_t nn = 0;
+        for (uint32_t i = 0; i < len; i++) {
+            uint32_t u = list[i];
+            claim[u] = 0;
+            if (vcmap[u] != ORC_UNASSIGNED) continue;
+            /* heaviest unmatched neighbour, the last maximum in row order
+             * (heuristics.h:1686-1716, "<="); level 1 orders by key */
+            uint64_t bk = 0;
+            uint32_t bj = ORC_UNASSIGNED;
+            for (uint32_t j = rp[u]; j < rp[u + 1]; j++) {
+                uint32_t v = col[j];
+                if (vcmap[v] != ORC_UNASSIGNED) continue;
+                uint64_t k = random_level ? orc_prio_key(seed, v) + 1 : orc_wt(w, j);
+                if (bj == ORC_UNASSIGNED || k >= bk) { bk = k; bj = j; }
+            }
+            if (bj != ORC_UNASSIGNED) { hn[u] = col[bj]; next[nn++] = u; }
+        }
+        rounds++;
+        if (nn == 0) break;
+        uint32_t *t = list; list = next; next = t;
+        len = nn;
+        swap ^= 1u;
+    }
+    for (uint32_t u = 0; u < n; u++)
+        if (vcmap[u] == ORC_UNASSIGNED) vcmap[u] = u;
+    *nc_out = orc_number_roots(n, vcmap);
+    *rounds_out = rounds;
+    free(hn); free(list); free(next); free(claim); free(act);
+    return 0;
+}
+
+typedef struct { int s; uint64_t k; uint32_t i; } orc_tup_t;
+static int orc_tup_gt(orc_tup_t x, orc_tup_t y) {
+    return x.s > y.s || (x.s == y.s && (x.k > y.k || (x.k == y.k && x.i > y.i)));
+}
+
+/* gosh = 0: MIS-2 (two hops of the maximum per iteration, random keys);
+ * gosh = 1: GOSH_clusters (one hop, degree keys, decided vertices keep their
+ * own tuple, edges between two vertices of degree > nnz / n ignored). */
+int orc_set_map(uint32_t n, const uint32_t *rp, const uint32_t *col, int gosh, uint64_t seed, uint32_t *vcmap,
+                uint32_t *nc_out, uint32_t *iters_out) {
+    int *state = (int *)calloc((size_t)n + 1, sizeof(int));
+    orc_tup_t *a = (orc_tup_t *)malloc(((size_t)n + 1) * sizeof(orc_tup_t));
+    orc_tup_t *b = (orc_tup_t *)malloc(((size_t)n + 1) * sizeof(orc_tup_t));
+    const uint64_t thr = n ? (uint64_t)rp[n] / n : 0;
+    int it = 0;
+    for (;; it++) {
+        for (uint32_t u = 0; u < n; u++) {
+            a[u].s = state[u];
+            a[u].k = gosh ? (uint64_t)(rp[u + 1] - rp[u]) : orc_prio_key(seed, u);
+            a[u].i = u;
+        }
+        for (int h = 0; h < (gosh ? 1 : 2); h++) {
+            for (uint32_t u = 0; u < n; u++) {
+                if (gosh && state[u] != 0) {
+                    b[u].s = state[u]; b[u].k = rp[u + 1] - rp[u]; b[u].i = u;
+                    continue;
+                }
+                orc_tup_t best = a[u];
+                int u_big = gosh && (uint64_t)(rp[u + 1] - rp[u]) > thr;
+                for (uint32_t j = rp[u]; j < rp[u + 1]; j++) {
+                    uint32_t v = col[j];
+                    if (u_big && (uint64_t)(rp[v + 1] - rp[v]) > thr) continue;
+                    if (orc_tup_gt(a[v], best)) best = a[v];
+                }
+                b[u] = best;
+            }
+            orc_tup_t *t = a; a = b; b = t;
+        }
+        uint32_t left = 0;
+        for (uint32_t u = 0; u < n; u++) {
+            if (state[u] != 0) continue;
+            uint32_t m = a[u].i;
+            if (m == u) state[u] = 1;
+            else if (a[u].s == 1 || a[m].i == m) state[u] = -1;
+            else left++;
+        }
+        if (left == 0) break;
+    }
+    *iters_out = (uint32_t)(it + 1);
+    uint32_t *rank = (uint32_t *)malloc(((size_t)n + 1) * sizeof(uint32_t));
+    uint32_t nc = 0;
+    for (uint32_t u = 0; u < n; u++) rank[u] = state[u] == 1 ? nc++ : ORC_UNASSIGNED;
+    int rc = 0;
+    if (!gosh) {
+        uint32_t *vc1 = (uint32_t *)malloc(((size_t)n + 1) * sizeof(uint32_t));
+        for (uint32_t u = 0; u < n; u++) vc1[u] = ORC_UNASSIGNED;
+        for (uint32_t u = 0; u < n; u++) {
+            if (state[u] != 1) continue;
+            vc1[u] = rank[u];
+            for (uint32_t j = rp[u]; j < rp[u + 1]; j++) vc1[col[j]] = rank[u];
+        }
+        for (uint32_t u = 0; u < n; u++) {
+            vcmap[u] = vc1[u];
+            if (vc1[u] != ORC_UNASSIGNED) continue;
+            for (uint32_t j = rp[u]; j < rp[u + 1]; j++)
+                if (vc1[col[j]] != ORC_UNASSIGNED) { vcmap[u] = vc1[col[j]]; break; }
+            if (vcmap[u] == ORC_UNASSIGNED) rc = 1;
+        }
+        free(vc1);
+    } else {
+        for (uint32_t u = 0; u < n; u++) {
+            if (state[u] == 1) { vcmap[u] = rank[u]; continue; }
+            uint32_t bd = 0, bv = ORC_UNASSIGNED;
+            for (uint32_t j = rp[u]; j < rp[u + 1]; j++) {
+                uint32_t v = col[j], d = rp[v + 1] - rp[v];
+                if (state[v] == 1 && d > bd) { bd = d; bv = v; }
+            }
+            vcmap[u] = bv == ORC_UNASSIGNED ? ORC_UNASSIGNED : rank[bv];
+            if (bv == ORC_UNASSIGNED) rc = 1;
+        }
+    }
+    *nc_out = nc;
+    free(state); free(a); free(b); free(rank);
+    return rc;
+}
+
 /* ------------------------------------------------------ multilevel path -- */
 /* The whole path with this project's seeding convention: every coarsening
  * level draws two PCG32 outputs (high word first) for its hash seed; the
@@ -536,23 +720,32 @@ typedef struct { uint32_t n; uint32_t *rp; uint32_t *col; uint64_t *w; uint32_t 
 int orc_partition_graph(uint32_t n, const uint32_t *row_ptr, const uint32_t *col,
                         const uint64_t *w64, uint32_t cutoff, double tol,
                         uint64_t *rng_state, uint64_t rng_inc,
-                        int perc_imbalance_allowed, int normlap,
+                        int perc_imbalance_allowed, int normlap, int coarsener,
                         uint32_t *part, uint64_t *edgecut, double *evec_out, double *stats) {
     orc_level_t L[202];
     int nl = 1;
+    const int kind = coarsener & 15;
     L[0].n = n; L[0].rp = (uint32_t *)row_ptr; L[0].col = (uint32_t *)col;
     L[0].w = (uint64_t *)w64; L[0].vcmap = NULL;
-    while (L[nl - 1].n > cutoff) {
+    /* coarsener: 0 HEC, 1 MATCH, 2 MIS2, 3 GOSH; | 16 no coarsening, | 32 stop
+     * after a level keeping more than 0.9 of the vertices (sgpar.h:2466-2475) */
+    while (!(coarsener & 16) && L[nl - 1].n > cutoff) {
         orc_level_t *f = &L[nl - 1];
         uint64_t seed = ((uint64_t)orc_pcg32(rng_state, rng_inc) << 32);
         seed |= orc_pcg32(rng_state, rng_inc);
-        uint32_t *hn = (uint32_t *)malloc((size_t)f->n * sizeof(uint32_t));
         f->vcmap = (uint32_t *)malloc((size_t)f->n * sizeof(uint32_t));
         int random_level = (nl == 1) && (w64 == NULL);
-        orc_hec_heavy(f->n, f->rp, f->col, f->w, random_level, seed, hn);
-        uint32_t nc = 0;
-        orc_hec_map(f->n, hn, seed, f->vcmap, &nc);
-        free(hn);
+        uint32_t nc = 0, rounds = 0;
+        if (kind == 0) {
+            uint32_t *hn = (uint32_t *)malloc((size_t)f->n * sizeof(uint32_t));
+            orc_hec_heavy(f->n, f->rp, f->col, f->w, random_level, seed, hn);
+            orc_hec_map(f->n, hn, seed, f->vcmap, &nc);
+            free(hn);
+        } else if (kind == 1) {
+            orc_match_map(f->n, f->rp, f->col, f->w, random_level, seed, f->vcmap, &nc, &rounds);
+        } else {
+            if (orc_set_map(f->n, f->rp, f->col, kind == 3, seed, f->vcmap, &nc, &rounds)) return 1;
+        }
         orc_level_t *c = &L[nl];
         uint32_t mf = f->rp[f->n];
         c->n = nc;
@@ -563,6 +756,7 @@ int orc_partition_graph(uint32_t n, const uint32_t *row_ptr, const uint32_t *col
         orc_build_coarse(f->n, f->rp, f->col, f->w, f->vcmap, nc, NULL, NULL, c->rp, c->col, c->w);
         nl++;
         if (nl > 200) break;
+        if ((coarsener & 32) && (double)nc / (double)f->n > 0.9) break;
     }
     if (nl > 1 && L[nl - 1].n < 10) {
         nl--;
