@@ -133,3 +133,17 @@ def test_converter_feeds_the_partitioner(partitioner):
     host, _ = partitioner.mtx_read(text)
     r_host = partitioner.partition(host, rng_state=5)
     assert np.array_equal(r_dev.part, r_host.part) and r_dev.edgecut == r_host.edgecut
+
+
+def test_command_line_module(tmp_path):
+    """python -m ipdps_2021_graph_coarsening_b200.mtx2csr writes the same file."""
+    import subprocess
+    import sys
+    src, dst = tmp_path / "g.mtx", tmp_path / "g.csr"
+    text = VALID["holes_dups_isolated"]
+    src.write_bytes(text)
+    want, _ = expected(text, tmp_path)
+    r = subprocess.run([sys.executable, "-m", "ipdps_2021_graph_coarsening_b200.mtx2csr", str(src), str(dst)],
+                       capture_output=True, text=True, cwd=MC.ROOT)
+    assert r.returncode == 0, r.stderr
+    assert dst.read_bytes() == want and "components" in r.stdout
