@@ -94,8 +94,9 @@ int compute_partition_edit_distance(const sgp_vid_t *part1, const sgp_vid_t *par
  * part[n] is caller-allocated host memory; *edge_cut receives the cut of the
  * bisection.  rng seeds the mapping hashes and the coarsest guess and is
  * advanced.  config->refine_alg 0 (shifted combinatorial Laplacian) or 1
- * (normalized Laplacian) and config->local_search_alg 0; other values return
- * EXIT_FAILURE.  With
+ * (normalized Laplacian); config->local_search_alg != 0 runs the reference's
+ * local search after the split (sgpar.h:2080-2170); other refine_alg values
+ * return EXIT_FAILURE.  With
  * config->num_partitions == 4 the call still bisects (the 4-way recursion is
  * the caller's, sgpar.cpp:62-89, via sgp_use_partition). */
 int sgp_partition_graph(sgp_vid_t *part, sgp_eid_t *edge_cut, config_t *config,
@@ -159,6 +160,8 @@ typedef struct {
     int refine_alg;             /* 0: shifted combinatorial Laplacian (reference default);
                                    1: normalized Laplacian, lazy random walk (I + D^-1 A) / 2
                                    without deflation in the loop, as eigensolve_kokkos.h:103-206 */
+    int local_search_alg;       /* != 0: the reference's local search after the split
+                                   (sgpar.h:2080-2170), as config_t.local_search_alg */
     int coarsener;              /* SGP_B200_COARSEN_*: the reference's compile-time coarsener
                                    choice (coarsen_kokkos.h:1138-1150); | SGP_B200_COARSEN_NONE
                                    skips coarsening, | SGP_B200_COARSEN_RATIO_STOP stops after a
@@ -191,6 +194,7 @@ typedef struct {
     float ms_total, ms_h2d, ms_coarsen, ms_eigen, ms_split, ms_d2h;
     uint32_t kernel_launches;
     float ms_map, ms_build;     /* coarsening split into HEC mapping and coarse builds */
+    uint32_t ls_swaps;          /* local-search move pairs (local_search_alg != 0) */
 } sgp_b200_result_t;
 
 void sgp_b200_default_options(sgp_b200_options_t *opt);

@@ -45,7 +45,7 @@ class sgp_b200_graph_t(ctypes.Structure):
 class sgp_b200_options_t(ctypes.Structure):
     _fields_ = [("cutoff", c_u32), ("tol", c_dbl), ("mixed", c_int), ("perc_imbalance", c_int),
                 ("iter_cap", c_u64), ("rng_state", c_u64), ("rng_inc", c_u64), ("part_mem", c_int),
-                ("refine_alg", c_int), ("coarsener", c_int)]
+                ("refine_alg", c_int), ("local_search_alg", c_int), ("coarsener", c_int)]
 
 
 class sgp_b200_result_t(ctypes.Structure):
@@ -56,7 +56,7 @@ class sgp_b200_result_t(ctypes.Structure):
                 ("iter_max_reached", c_int),
                 ("rng_state", c_u64), ("ms_total", c_flt), ("ms_h2d", c_flt), ("ms_coarsen", c_flt),
                 ("ms_eigen", c_flt), ("ms_split", c_flt), ("ms_d2h", c_flt), ("kernel_launches", c_u32),
-                ("ms_map", c_flt), ("ms_build", c_flt)]
+                ("ms_map", c_flt), ("ms_build", c_flt), ("ls_swaps", c_u32)]
 
 
 class sgp_b200_mtx_info_t(ctypes.Structure):

@@ -181,6 +181,7 @@ class Result:
     kernel_launches: int = 0
     ms_map: float = 0.0
     ms_build: float = 0.0
+    ls_swaps: int = 0           # local-search move pairs
     raw: object = None          # the C result struct (for write_metrics)
 
 
@@ -259,13 +260,14 @@ class Partitioner:
 
     @staticmethod
     def _options(cutoff, tol, mixed, rng_state, rng_inc, iter_cap, perc_imbalance,
-                 refine_alg: int = 0, coarsener: int = 0) -> L.sgp_b200_options_t:
+                 refine_alg: int = 0, coarsener: int = 0, local_search_alg: int = 0) -> L.sgp_b200_options_t:
         o = L.sgp_b200_options_t()
         L.lib().sgp_b200_default_options(ctypes.byref(o))
         o.cutoff, o.tol, o.mixed, o.perc_imbalance = cutoff, tol, int(mixed), perc_imbalance
         o.iter_cap, o.rng_state, o.rng_inc = iter_cap, rng_state, rng_inc
         o.refine_alg = refine_alg
         o.coarsener = coarsener
+        o.local_search_alg = local_search_alg
         return o
 
     @staticmethod
@@ -287,18 +289,20 @@ class Partitioner:
                       list(res.level_hec_rounds[:nl]), list(res.level_pi_ms[:nl]), bool(res.iter_max_reached),
                       res.rng_state,
                       res.ms_total, res.ms_h2d, res.ms_coarsen, res.ms_eigen, res.ms_split, res.ms_d2h,
-                      res.kernel_launches, res.ms_map, res.ms_build, res)
+                      res.kernel_launches, res.ms_map, res.ms_build, res.ls_swaps, res)
 
     def partition(self, g, cutoff: int = 50, tol: float = 1e-10, mixed: bool = False,
                   rng_state: int = 0x853C49E6748FEA9B, rng_inc: int = 1, iter_cap: int = 0,
-                  perc_imbalance: int = 0, part_out=None, refine_alg: int = 0, coarsener: int = 0) -> Result:
+                  perc_imbalance: int = 0, part_out=None, refine_alg: int = 0, coarsener: int = 0,
+                  local_search_alg: int = 0) -> Result:
         """Partition ``g``: a host :class:`CSR` (numpy) or a dict of CUDA torch
         tensors ``{"row_ptr", "col", "w"}`` (device-resident input).  The
         partition is written to ``part_out`` (numpy or CUDA tensor) when
         given, else returned as numpy.  ``coarsener``: ``_lib.COARSEN_*``."""
         keep = []
         dg = self._graph(g, keep)
-        o = self._options(cutoff, tol, mixed, rng_state, rng_inc, iter_cap, perc_imbalance, refine_alg, coarsener)
+        o = self._options(cutoff, tol, mixed, rng_state, rng_inc, iter_cap, perc_imbalance, refine_alg, coarsener,
+                          local_search_alg)
         res = L.sgp_b200_result_t()
         part_out, res.part = self._part_target(dg.n, part_out, o)
         L.check(L.lib().sgp_b200_partition(self._ctx, ctypes.byref(dg), ctypes.byref(o), ctypes.byref(res)),

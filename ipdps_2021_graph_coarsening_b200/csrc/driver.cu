@@ -268,6 +268,17 @@ static int partition_staged(Context &C, const Level &L0, const sgp_b200_options_
     uint64_t cut = 0;
     uint32_t p0 = 0;
     SGPB_TRY(split_level(C, levels[0], evec, opt->perc_imbalance, part_d, &cut, &p0));
+    res->ls_swaps = 0;
+    if (opt->local_search_alg) {
+        // the part-0 size is the reference's curr_split when the split's
+        // sweep range holds at most one vertex (perc_imbalance_allowed 0)
+        if (opt->perc_imbalance != 0) {
+            set_error("the local search takes perc_imbalance_allowed 0");
+            return SGP_B200_ERR_INVALID;
+        }
+        SGPB_TRY(local_search_level(C, levels[0], part_d, p0, &res->ls_swaps, &p0));
+        SGPB_TRY(edge_cut_device(C, levels[0], part_d, &cut));
+    }
     SGPB_CUDA(cudaEventRecord(ev[4], C.stream));
     res->edgecut = cut;
     res->part0_size = p0;
@@ -421,6 +432,7 @@ void sgp_b200_default_options(sgp_b200_options_t *o) {
     o->part_mem = SGP_B200_HOST;
     o->refine_alg = 0;
     o->coarsener = SGP_B200_COARSEN_HEC;
+    o->local_search_alg = 0;
 }
 
 int sgp_b200_partition(sgp_b200_ctx_t *x, const sgp_b200_graph_t *g, const sgp_b200_options_t *opt,
@@ -726,9 +738,8 @@ int sgp_partition_graph(sgp_vid_t *part, sgp_eid_t *edge_cut, config_t *config, 
         set_error("null argument");
         return 1;
     }
-    if ((config->refine_alg != 0 && config->refine_alg != 1) || config->local_search_alg != 0) {
-        set_error("refine_alg must be 0 (shifted combinatorial Laplacian) or 1 (normalized Laplacian), "
-                  "local_search_alg 0");
+    if (config->refine_alg != 0 && config->refine_alg != 1) {
+        set_error("refine_alg must be 0 (shifted combinatorial Laplacian) or 1 (normalized Laplacian)");
         return 1;
     }
     Context *C = default_ctx();
@@ -751,6 +762,7 @@ int sgp_partition_graph(sgp_vid_t *part, sgp_eid_t *edge_cut, config_t *config, 
                   : (config->coarsening_alg & 1) ? (SGP_B200_COARSEN_MATCH | SGP_B200_COARSEN_RATIO_STOP)
                                                  : SGP_B200_COARSEN_HEC;
     o.perc_imbalance = perc_imbalance_allowed;
+    o.local_search_alg = config->local_search_alg;
     o.rng_state = rng->state;
     o.rng_inc = rng->inc;
     sgp_b200_result_t *r = (sgp_b200_result_t *)calloc(1, sizeof(sgp_b200_result_t));
@@ -768,7 +780,10 @@ int sgp_partition_graph(sgp_vid_t *part, sgp_eid_t *edge_cut, config_t *config, 
 int sgp_compute_partition(sgp_vid_t *part, sgp_vid_t num_partitions, sgp_eid_t *edgecut, int perc_imbalance_allowed,
                           int local_search_alg, sgp_real_t *evec, sgp_graph_t g) {
     if (num_partitions != 2 && num_partitions != 4) { set_error("num_partitions must be 2 or 4"); return 1; }
-    if (local_search_alg != 0) { set_error("local_search_alg must be 0"); return 1; }
+    if (local_search_alg != 0 && perc_imbalance_allowed != 0) {
+        set_error("the local search takes perc_imbalance_allowed 0");
+        return 1;
+    }
     Context *C = default_ctx();
     if (!C || !part || !edgecut || !evec) return 1;
     cudaSetDevice(C->device);
@@ -789,7 +804,12 @@ int sgp_compute_partition(sgp_vid_t *part, sgp_vid_t num_partitions, sgp_eid_t *
         cudaMemcpyAsync(ev, evec, sizeof(double) * g.nvertices, cudaMemcpyHostToDevice, C->stream) != cudaSuccess)
         rc = SGP_B200_ERR_DEVICE;
     uint64_t cut = 0;
-    if (rc == SGP_B200_OK) rc = split_level(*C, L0, ev, perc_imbalance_allowed, pd, &cut, nullptr);
+    uint32_t p0 = 0;
+    if (rc == SGP_B200_OK) rc = split_level(*C, L0, ev, perc_imbalance_allowed, pd, &cut, &p0);
+    if (rc == SGP_B200_OK && local_search_alg) {   // sgpar.h:2080-2170
+        rc = local_search_level(*C, L0, pd, p0, nullptr, nullptr);
+        if (rc == SGP_B200_OK) rc = edge_cut_device(*C, L0, pd, &cut);
+    }
     if (rc == SGP_B200_OK &&
         cudaMemcpyAsync(part, pd, sizeof(uint32_t) * g.nvertices, cudaMemcpyDeviceToHost, C->stream) != cudaSuccess)
         rc = SGP_B200_ERR_DEVICE;

@@ -133,6 +133,10 @@ int power_iter_level(Context &C, const Level &L, const double *x_in, const uint3
 int split_level(Context &C, const Level &L, const double *evec, int perc_imbalance, uint32_t *part,
                 uint64_t *edgecut, uint32_t *n_part0);
 int edge_cut_device(Context &C, const Level &L, const uint32_t *part, uint64_t *edgecut);
+// the reference's local search after the split (sgpar.h:2080-2170); mid =
+// the part-0 size the split left
+int local_search_level(Context &C, const Level &L, uint32_t *part, uint32_t mid, uint32_t *swaps_out,
+                       uint32_t *part0_out);
 // map0 / map1 (optional): vertex i of L -> its id in g1 (part 0) / g2
 int induced_subgraphs(Context &C, const Level &L, const uint32_t *part, Level *g1, Level *g2,
                       uint32_t **map0 = nullptr, uint32_t **map1 = nullptr);

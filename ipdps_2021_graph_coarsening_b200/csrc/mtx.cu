@@ -1000,7 +1000,7 @@ static int mtx_impl(Context &C, MtxSource &src, int out_mem, sgp_b200_graph_t *o
         else
             k_cc_rest<32><<<grid_for(C, (uint64_t)n * 32, 256), 256, 0, C.stream>>>(n, rp, col, parent, skip, kRounds,
                                                                                    cc);
-        C.kernel_launches += 3 + kRounds;
+        C.kernel_launches += 4 + kRounds;   // init, samples, compress, probe, rest
         k_cc_flatten<<<grid_for(C, n, 256), 256, 0, C.stream>>>(n, parent, size);
         k_cc_best<<<grid_for(C, n, 256), 256, 0, C.stream>>>(n, parent, size, best, cc + 1);
         SGPB_CUDA(cudaGetLastError());

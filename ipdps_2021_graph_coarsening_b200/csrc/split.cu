@@ -15,6 +15,8 @@
 // sgpar.cpp:55) is decided on the device.
 #include <mutex>
 
+#include <cooperative_groups.h>
+
 #include "common.cuh"
 #include "internal.h"
 
@@ -293,6 +295,158 @@ int edge_cut_device(Context &C, const Level &L, const uint32_t *part, uint64_t *
     uint64_t h;
     SGPB_TRY(read_u64(C, (const uint64_t *)o, &h));
     *edgecut = h / 2;
+    return SGP_B200_OK;
+}
+
+// --------------------------------------------------------- local search --
+// sgpar.h:2080-2170: after the split, alternately flip the vertex of largest
+// positive gain (cross minus same-side neighbours; first id on a tie) among
+// ids [mid - n/3, mid) and then among [mid, mid + n/3), mid being the part-0
+// size the split left; a missing second move undoes the first and ends the
+// search, as does a missing first move or n/3 completed pairs.  The
+// reference recomputes every candidate's gain per move (O(n m) in all); here
+// the gains are kept incrementally -- a flip negates the vertex's own gain
+// and moves each neighbour's by 2 -- and each half-step is a grid-wide
+// argmax plus one row update in a single cooperative launch.
+//
+// Ordering: a flip of part[v] is deferred to the next phase (after a grid
+// barrier), so no thread reads part[v] while it is written; the argmax
+// phase reads gains only.  Four argmax slots rotate; the slot two
+// half-steps ahead is cleared while the current one is read.  Gains and
+// parts change between barriers on other SMs, so after the first phase
+// they are read with ld.global.cg (L2), never from a possibly stale L1 line.
+constexpr int kLSThreads = 512;
+
+struct LSArgs {
+    uint32_t n;
+    const uint32_t *rp, *col;
+    uint32_t *part;
+    int *gain;
+    uint32_t lo, mid, hi, max_swaps;
+    unsigned long long *key;   // [4], zero on entry
+    uint32_t *out;             // [0] swaps
+};
+
+namespace cgls = cooperative_groups;
+
+__global__ void __launch_bounds__(kLSThreads) k_local_search(LSArgs a) {
+    cgls::grid_group grid = cgls::this_grid();
+    const uint64_t tid = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const uint64_t nthreads = (uint64_t)gridDim.x * blockDim.x;
+    const unsigned lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    const bool leader = blockIdx.x == 0 && threadIdx.x == 0;
+    __shared__ unsigned long long wmax[kLSThreads / 32];
+    // gains, a warp per row
+    for (uint64_t u = tid >> 5; u < a.n; u += nthreads >> 5) {
+        const uint32_t pu = a.part[u];
+        int x = 0;
+        for (uint32_t j = a.rp[u] + lane; j < a.rp[u + 1]; j += 32) x += a.part[__ldg(a.col + j)] != pu ? 1 : -1;
+        x = warp_sum(x);
+        if (lane == 0) a.gain[u] = x;
+    }
+    grid.sync();
+    uint32_t pending = 0xFFFFFFFFu, first = 0xFFFFFFFFu, swaps = 0, slot = 0;
+    for (int half = 0;; half ^= 1) {
+        if (half == 0 && swaps >= a.max_swaps) break;
+        // ---- argmax of (gain, -id) over this half's range, gains > 0 only
+        if (leader && pending != 0xFFFFFFFFu) a.part[pending] = __ldcg(a.part + pending) ^ 1u;
+        pending = 0xFFFFFFFFu;
+        const uint32_t b = half == 0 ? a.lo : a.mid, e = half == 0 ? a.mid : a.hi;
+        unsigned long long best = 0;
+        for (uint64_t i = b + tid; i < e; i += nthreads) {
+            const int g = __ldcg(a.gain + i);
+            if (g > 0) {
+                const unsigned long long k = ((unsigned long long)(uint32_t)g << 32) | (0xFFFFFFFFu - (uint32_t)i);
+                best = k > best ? k : best;
+            }
+        }
+        best = warp_max(best);
+        if (lane == 0) wmax[wid] = best;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            unsigned long long m = 0;
+            for (int w = 0; w < kLSThreads / 32; w++) m = wmax[w] > m ? wmax[w] : m;
+            if (m) atomicMax(a.key + slot, m);
+        }
+        grid.sync();
+        // ---- apply: flip the winner (deferred) and move its neighbours' gains
+        const unsigned long long k = *(volatile unsigned long long *)(a.key + slot);
+        if (leader) a.key[(slot + 2) & 3] = 0;
+        slot = (slot + 1) & 3;
+        uint32_t v;
+        if (k == 0) {
+            if (half == 0) break;   // no first move: done
+            v = first;              // no second move: undo the first, then done
+        } else {
+            v = 0xFFFFFFFFu - (uint32_t)(k & 0xFFFFFFFFu);
+        }
+        const uint32_t old = __ldcg(a.part + v);
+        for (uint64_t j = a.rp[v] + tid; j < a.rp[v + 1]; j += nthreads) {
+            const uint32_t u = __ldg(a.col + j);
+            // rows hold u once: no other writer of gain[u] in this phase
+            a.gain[u] = __ldcg(a.gain + u) + (__ldcg(a.part + u) != old ? -2 : 2);
+        }
+        if (leader) a.gain[v] = -__ldcg(a.gain + v);
+        pending = v;
+        grid.sync();
+        if (k == 0) break;          // the undo above ends the search
+        if (half == 0) first = v;
+        else swaps++;
+    }
+    grid.sync();
+    if (leader) {
+        if (pending != 0xFFFFFFFFu) a.part[pending] = __ldcg(a.part + pending) ^ 1u;
+        a.out[0] = swaps;
+    }
+    grid.sync();
+    // part-0 size after the search (the moves need not balance)
+    uint32_t z = 0;
+    for (uint64_t i = tid; i < a.n; i += nthreads) z += __ldcg(a.part + i) == 0;
+    z = warp_sum(z);
+    if (lane == 0 && z) atomicAdd(a.out + 1, z);
+}
+
+int local_search_level(Context &C, const Level &L, uint32_t *part, uint32_t mid, uint32_t *swaps_out,
+                       uint32_t *part0_out) {
+    const uint32_t n = L.n;
+    if (n < 3) {
+        if (swaps_out) *swaps_out = 0;
+        if (part0_out) *part0_out = mid;
+        return SGP_B200_OK;
+    }
+    LSArgs a;
+    a.n = n;
+    a.rp = L.rp;
+    a.col = L.col;
+    a.part = part;
+    a.mid = mid;
+    a.lo = mid > n / 3 ? mid - n / 3 : 0;
+    a.hi = (uint64_t)mid + n / 3 < n ? mid + n / 3 : n;
+    a.max_swaps = n / 3;
+    SGPB_TRY(dalloc_t(C, &a.gain, n));
+    SGPB_TRY(dalloc_t(C, &a.key, 4));
+    SGPB_TRY(dalloc_t(C, &a.out, 2));
+    SGPB_TRY(dzero(C, a.out, 2 * sizeof(uint32_t)));
+    SGPB_TRY(dzero(C, a.key, 4 * sizeof(unsigned long long)));
+    int per_sm = 0;
+    SGPB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_local_search, kLSThreads, 0));
+    if (per_sm < 1) {
+        set_error("local-search kernel does not fit on an SM");
+        return SGP_B200_ERR_DEVICE;
+    }
+    // one block per SM at most: the per-move barriers cost less with fewer
+    // blocks, and a range of n/3 gains is a light scan
+    uint32_t grid = cdiv((uint64_t)n, 4096);
+    if (grid > (uint32_t)C.num_sms) grid = C.num_sms;
+    if (grid < 1) grid = 1;
+    void *args[] = {&a};
+    SGPB_CUDA(cudaLaunchCooperativeKernel((const void *)k_local_search, dim3(grid), dim3(kLSThreads), args, 0,
+                                          C.stream));
+    C.kernel_launches++;
+    uint32_t o[2] = {0, 0};
+    SGPB_TRY(read_u32(C, a.out, o, 2));
+    if (swaps_out) *swaps_out = o[0];
+    if (part0_out) *part0_out = o[1];
     return SGP_B200_OK;
 }
 

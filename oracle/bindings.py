@@ -76,7 +76,9 @@ def lib():
         L.orc_use_partition.argtypes = [c_u32, u32p, u32p, u32p, u32ref, u32p, u32p, u32ref, u32p, u32p]
         L.orc_use_partition.restype = c_int
         L.orc_partition_graph.argtypes = [c_u32, u32p, u32p, ctypes.c_void_p, c_u32, c_dbl,
-                                          u64ref, c_u64, c_int, c_int, c_int, u32p, u64ref, f64p, f64p]
+                                          u64ref, c_u64, c_int, c_int, c_int, c_int, u32p, u64ref, f64p, f64p]
+        L.orc_compute_partition_ls.argtypes = [c_u32, u32p, u32p, f64p, c_int, u32p, u64ref, u32ref]
+        L.orc_compute_partition_ls.restype = c_int
         L.orc_match_map.argtypes = [c_u32, u32p, u32p, ctypes.c_void_p, c_int, c_u64, u32p, u32ref, u32ref]
         L.orc_match_map.restype = c_int
         L.orc_set_map.argtypes = [c_u32, u32p, u32p, c_int, c_u64, u32p, u32ref, u32ref]
@@ -180,6 +182,18 @@ def compute_partition(row_ptr, col, evec, perc_imbalance: int = 0):
     return part, ec.value
 
 
+def compute_partition_ls(row_ptr, col, evec, local_search_alg: int = 1):
+    """The split plus the reference's local search -> (part, edgecut, swaps)."""
+    rp, cl = _u32(row_ptr), _u32(col)
+    n = rp.shape[0] - 1
+    part = np.zeros(n, dtype=np.uint32)
+    ec = ctypes.c_uint64(0)
+    sw = ctypes.c_uint32(0)
+    lib().orc_compute_partition_ls(n, rp, cl, np.ascontiguousarray(evec, dtype=np.float64), local_search_alg,
+                                   part, ctypes.byref(ec), ctypes.byref(sw))
+    return part, ec.value, sw.value
+
+
 def edge_cut(row_ptr, col, part) -> int:
     rp, cl = _u32(row_ptr), _u32(col)
     return int(lib().orc_edge_cut(rp.shape[0] - 1, rp, cl, _u32(part)))
@@ -221,7 +235,7 @@ def set_map(row_ptr, col, gosh: bool, seed: int):
 
 def partition_graph(row_ptr, col, w=None, cutoff: int = 50, tol: float = 1e-10,
                     rng_state: int = 42, rng_inc: int = 1, perc_imbalance: int = 0, refine_alg: int = 0,
-                    coarsener: int = 0):
+                    coarsener: int = 0, local_search_alg: int = 0):
     """Whole multilevel path.  Returns dict(part, edgecut, evec, levels,
     lambda, niter (finest), level_n, level_iters, rng_state)."""
     rp, cl = _u32(row_ptr), _u32(col)
@@ -233,7 +247,8 @@ def partition_graph(row_ptr, col, w=None, cutoff: int = 50, tol: float = 1e-10,
     ec = ctypes.c_uint64(0)
     keep, wp = _w64(w)
     if lib().orc_partition_graph(n, rp, cl, wp, cutoff, tol, ctypes.byref(s), rng_inc, perc_imbalance,
-                                 int(refine_alg), int(coarsener), part, ctypes.byref(ec), ev, stats):
+                                 int(refine_alg), int(coarsener), int(local_search_alg), part, ctypes.byref(ec), ev,
+                                 stats):
         raise RuntimeError("oracle coarsener left a vertex outside every aggregate")
     nl = int(stats[0])
     return dict(part=part, edgecut=ec.value, evec=ev, levels=nl, **{"lambda": stats[1]},
@@ -266,6 +281,7 @@ def ref(kind: str = "serial", cutoff: int = 50):
         L.ref_power_iter.argtypes = [c_u32, u32p, u32p, vp, c_int, f64p, c_dbl, c_int]
         L.ref_power_iter_nl.argtypes = [c_u32, u32p, u32p, vp, f64p, c_dbl, c_int]
         L.ref_compute_partition.argtypes = [c_u32, u32p, u32p, f64p, c_int, u32p, u64ref, c_int]
+        L.ref_compute_partition_ls.argtypes = [c_u32, u32p, u32p, f64p, c_int, c_int, u32p, u64ref, c_int]
         L.ref_build_coarse_msd.argtypes = [c_u32, u32p, u32p, vp, c_int, c_int, u32p, c_u32,
                                            u32p, u32p, u32p, u32p, u64ref]
         L.ref_coarsen_hec.argtypes = [c_u32, u32p, u32p, vp, c_int, u64ref, c_u64, u32p, u32ref]
@@ -304,6 +320,17 @@ def ref_compute_partition(row_ptr, col, evec, perc_imbalance: int = 0, kind: str
     ec = ctypes.c_uint64(0)
     ref(kind).ref_compute_partition(n, rp, cl, np.ascontiguousarray(evec, dtype=np.float64).copy(),
                                     perc_imbalance, part, ctypes.byref(ec), 1)
+    return part, ec.value
+
+
+def ref_compute_partition_ls(row_ptr, col, evec, local_search_alg: int = 1, kind: str = "serial"):
+    """The reference's sgp_compute_partition with its local search."""
+    rp, cl = _u32(row_ptr), _u32(col)
+    n = rp.shape[0] - 1
+    part = np.zeros(n, np.uint32)
+    ec = ctypes.c_uint64(0)
+    ref(kind).ref_compute_partition_ls(n, rp, cl, np.ascontiguousarray(evec, dtype=np.float64).copy(), 0,
+                                       local_search_alg, part, ctypes.byref(ec), 1)
     return part, ec.value
 
 

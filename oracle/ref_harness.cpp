@@ -134,6 +134,19 @@ int ref_compute_partition(uint32_t n, const uint32_t *row_ptr, const uint32_t *c
     return rc;
 }
 
+/* sgpar.h:1969-2170 with a local search: the split followed by the
+ * reference's greedy swap search over vertex-id ranges (local_search_alg != 0). */
+int ref_compute_partition_ls(uint32_t n, const uint32_t *row_ptr, const uint32_t *col,
+                             double *evec, int perc_imbalance_allowed, int local_search_alg,
+                             uint32_t *part, uint64_t *edgecut, int quiet) {
+    Quiet q(quiet);
+    sgp_graph_t g = make_graph(n, row_ptr, col);
+    sgp_eid_t ec = 0;
+    int rc = sgp_compute_partition(part, 2, &ec, perc_imbalance_allowed, local_search_alg, evec, g);
+    *edgecut = ec;
+    return rc;
+}
+
 /* sgpar.h:1223 sgp_build_coarse_graph_msd on a given mapping.  Output is the
  * reference's bucketed layout: offsets[nc+1] (bucket starts), counts[nc]
  * (deduplicated row lengths), cols / wgts sized offsets[nc] <= row_ptr[n]. */

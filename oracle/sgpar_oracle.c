@@ -17,7 +17,8 @@
  *   - shifted-Laplacian power iteration deflated against the constant vector,
  *     in the serial reference's exact floating-point operation order
  *     (sgpar.h:1790-1948, vector kernels sgpar.h:1687-1730)
- *   - median split + one-vertex sweep + edge cut (sgpar.h:1969-2071)
+ *   - median split + one-vertex sweep + edge cut (sgpar.h:1969-2071) and the
+ *     local search after it (sgpar.h:2080-2170)
  *   - induced sub-graphs for 4-way recursion (sgpar.h:2666-2752)
  *   - the level loop of sgp_generate_coarse_graphs (coarsen_kokkos.h:1165-1234)
  *     and sgp_eigensolve (eigensolve_kokkos.h:1493-1595)
@@ -489,6 +490,75 @@ int orc_compute_partition(uint32_t n, const uint32_t *row_ptr, const uint32_t *c
     return 0;
 }
 
+/* sgpar.h:2080-2170: the local search after the split.  With curr_split the
+ * part-0 size left by the split, it alternates: among vertex ids
+ * [curr_split - n/3, curr_split) the first id of largest positive gain
+ * (cross minus same-side neighbours) is flipped, then among
+ * [curr_split, curr_split + n/3) likewise; a missing second move undoes the
+ * first and ends the search, as does a missing first move or n/3 completed
+ * pairs.  Gains are kept incrementally here (the reference recomputes them
+ * per candidate); the values are the same integers.  Returns the swaps. */
+uint32_t orc_local_search(uint32_t n, const uint32_t *row_ptr, const uint32_t *col, uint32_t *part,
+                          uint32_t curr_split) {
+    int64_t *g = (int64_t *)malloc(((size_t)n + 1) * sizeof(int64_t));
+    for (uint32_t i = 0; i < n; i++) {
+        int64_t x = 0;
+        for (uint32_t j = row_ptr[i]; j < row_ptr[i + 1]; j++) x += part[col[j]] != part[i] ? 1 : -1;
+        g[i] = x;
+    }
+    int64_t lo = (int64_t)curr_split - n / 3, hi = (int64_t)curr_split + n / 3;
+    if (lo < 0) lo = 0;
+    if (hi > (int64_t)n) hi = n;
+    uint32_t swaps = 0, max_swaps = n / 3;
+    while (swaps < max_swaps) {
+        uint32_t pick[2];
+        int side;
+        for (side = 0; side < 2; side++) {
+            int64_t a = side == 0 ? lo : curr_split, b = side == 0 ? (int64_t)curr_split : hi;
+            int64_t best = 0;
+            pick[side] = ORC_UNASSIGNED;
+            for (int64_t i = a; i < b; i++)
+                if (g[i] > best) { best = g[i]; pick[side] = (uint32_t)i; }
+            if (pick[side] == ORC_UNASSIGNED) break;
+            uint32_t v = pick[side], old = part[v];
+            part[v] = 1 - old;
+            g[v] = -g[v];
+            for (uint32_t j = row_ptr[v]; j < row_ptr[v + 1]; j++) g[col[j]] += part[col[j]] != old ? -2 : 2;
+        }
+        if (side == 0) break;
+        if (side == 1) {   /* roll the first move back */
+            uint32_t v = pick[0], old = part[v];
+            part[v] = 1 - old;
+            g[v] = -g[v];
+            for (uint32_t j = row_ptr[v]; j < row_ptr[v + 1]; j++) g[col[j]] += part[col[j]] != old ? -2 : 2;
+            break;
+        }
+        swaps++;
+    }
+    free(g);
+    return swaps;
+}
+
+/* The split of orc_compute_partition followed by the local search; the
+ * part-0 size after the split is the reference's curr_split when
+ * perc_imbalance_allowed is 0 (the sweep range holds at most one vertex). */
+int orc_compute_partition_ls(uint32_t n, const uint32_t *row_ptr, const uint32_t *col, const double *evec,
+                             int local_search_alg, uint32_t *part, uint64_t *edgecut, uint32_t *swaps_out) {
+    orc_compute_partition(n, row_ptr, col, evec, 0, part, edgecut);
+    uint32_t swaps = 0;
+    if (local_search_alg) {
+        uint32_t p0 = 0;
+        for (uint32_t i = 0; i < n; i++) p0 += part[i] == 0;
+        swaps = orc_local_search(n, row_ptr, col, part, p0);
+        uint64_t c = 0;
+        for (uint32_t i = 0; i < n; i++)
+            for (uint32_t j = row_ptr[i]; j < row_ptr[i + 1]; j++) c += part[col[j]] != part[i];
+        *edgecut = c / 2;
+    }
+    if (swaps_out) *swaps_out = swaps;
+    return 0;
+}
+
 /* Edge cut of an arbitrary 2-way partition (directed cross entries / 2). */
 uint64_t orc_edge_cut(uint32_t n, const uint32_t *row_ptr, const uint32_t *col, const uint32_t *part) {
     uint64_t c = 0;
@@ -720,7 +790,7 @@ typedef struct { uint32_t n; uint32_t *rp; uint32_t *col; uint64_t *w; uint32_t 
 int orc_partition_graph(uint32_t n, const uint32_t *row_ptr, const uint32_t *col,
                         const uint64_t *w64, uint32_t cutoff, double tol,
                         uint64_t *rng_state, uint64_t rng_inc,
-                        int perc_imbalance_allowed, int normlap, int coarsener,
+                        int perc_imbalance_allowed, int normlap, int coarsener, int local_search_alg,
                         uint32_t *part, uint64_t *edgecut, double *evec_out, double *stats) {
     orc_level_t L[202];
     int nl = 1;
@@ -786,7 +856,10 @@ int orc_partition_graph(uint32_t n, const uint32_t *row_ptr, const uint32_t *col
         vec = fine;
     }
     if (stats) stats[1] = lambda;
-    orc_compute_partition(n, row_ptr, col, vec, perc_imbalance_allowed, part, edgecut);
+    if (local_search_alg)
+        orc_compute_partition_ls(n, row_ptr, col, vec, local_search_alg, part, edgecut, NULL);
+    else
+        orc_compute_partition(n, row_ptr, col, vec, perc_imbalance_allowed, part, edgecut);
     if (evec_out) memcpy(evec_out, vec, (size_t)n * sizeof(double));
     free(vec);
     for (int l = 0; l < nl; l++) {

@@ -171,3 +171,20 @@ def test_split_matches_reference_directly():
     p1, c1 = O.compute_partition(g.row_ptr, g.col, ev)
     p2, c2 = O.ref_compute_partition(g.row_ptr, g.col, ev)
     assert np.array_equal(p1, p2) and c1 == c2
+
+
+@pytest.mark.parametrize("case", ["grid", "holes", "er", "rmat"])
+def test_local_search_matches_reference(case):
+    """sgpar.h:2080-2170: the oracle's incremental-gain local search gives
+    the reference's own serial build's partition and cut exactly, from random
+    and from spectral vectors."""
+    if not O.ref_available("serial"):
+        pytest.skip("reference build not present")
+    from ipdps_2021_graph_coarsening_b200 import graphs as Gm
+    g = {"grid": lambda: Gm.grid2d(30, 20), "holes": lambda: Gm.grid2d_holes(40, 40, 0.1, 2),
+         "er": lambda: Gm.erdos_renyi(900, 4.0, seed=3), "rmat": lambda: Gm.rmat(10, seed=2)}[case]()
+    rng = np.random.default_rng(1)
+    for ev in (rng.standard_normal(g.n), O.partition_graph(g.row_ptr, g.col, None, rng_state=5)["evec"]):
+        p1, c1, _ = O.compute_partition_ls(g.row_ptr, g.col, ev)
+        p2, c2 = O.ref_compute_partition_ls(g.row_ptr, g.col, ev)
+        assert np.array_equal(p1, p2) and c1 == c2
