@@ -162,6 +162,8 @@ typedef struct {
                                    without deflation in the loop, as eigensolve_kokkos.h:103-206 */
     int local_search_alg;       /* != 0: the reference's local search after the split
                                    (sgpar.h:2080-2170), as config_t.local_search_alg */
+    uint32_t fm_passes;         /* > 0: up to this many FM passes on the final bisection
+                                   (sgp_b200_fm_refine); 0 = none (the reference's spectral path) */
     int coarsener;              /* SGP_B200_COARSEN_*: the reference's compile-time coarsener
                                    choice (coarsen_kokkos.h:1138-1150); | SGP_B200_COARSEN_NONE
                                    skips coarsening, | SGP_B200_COARSEN_RATIO_STOP stops after a
@@ -195,6 +197,8 @@ typedef struct {
     uint32_t kernel_launches;
     float ms_map, ms_build;     /* coarsening split into HEC mapping and coarse builds */
     uint32_t ls_swaps;          /* local-search move pairs (local_search_alg != 0) */
+    uint32_t fm_passes_run;     /* FM passes run (fm_passes > 0) */
+    uint64_t fm_moves;          /* FM moves applied */
 } sgp_b200_result_t;
 
 void sgp_b200_default_options(sgp_b200_options_t *opt);
@@ -278,6 +282,17 @@ int sgp_b200_power_iter(sgp_b200_ctx_t *ctx, uint32_t n, const uint32_t *row_ptr
 
 /* Median split + edge cut (sgpar.h:1969-2071) of a device eigenvector;
  * part is a device array of n entries. */
+/* FM refinement of a bisection (device arrays; part[n] in {0, 1}, updated in
+ * place): passes of gain-ordered moves in the structure of the reference's
+ * parallel FM (eigensolve_kokkos.h:695-971) with the serial FM's balance
+ * rule and imbalance target (:1073-1140), made deterministic -- each side's
+ * positive-gain vertices by (gain clamped to 1023 descending, id), the sides
+ * interleaved for balance, sequential gains, the best prefix within
+ * max(|balance| / 10, 20) applied -- until a pass does not lower the cut or
+ * max_passes.  Edges count 1 (the finest level).  *cut receives the cut. */
+int sgp_b200_fm_refine(sgp_b200_ctx_t *ctx, uint32_t n, const uint32_t *row_ptr, const uint32_t *col,
+                       uint32_t *part, uint32_t max_passes, uint64_t *cut, uint32_t *passes, uint64_t *moves);
+
 /* One level's mapping by an alternative coarsener (coarsener MATCH, MIS2 or
  * GOSH; the HEC mapping is sgp_b200_hec) on device arrays: vcmap[n] receives
  * the coarse vertex of each vertex, *nc the coarse count, *rounds the

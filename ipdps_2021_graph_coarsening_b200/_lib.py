@@ -45,7 +45,7 @@ class sgp_b200_graph_t(ctypes.Structure):
 class sgp_b200_options_t(ctypes.Structure):
     _fields_ = [("cutoff", c_u32), ("tol", c_dbl), ("mixed", c_int), ("perc_imbalance", c_int),
                 ("iter_cap", c_u64), ("rng_state", c_u64), ("rng_inc", c_u64), ("part_mem", c_int),
-                ("refine_alg", c_int), ("local_search_alg", c_int), ("coarsener", c_int)]
+                ("refine_alg", c_int), ("local_search_alg", c_int), ("fm_passes", c_u32), ("coarsener", c_int)]
 
 
 class sgp_b200_result_t(ctypes.Structure):
@@ -56,7 +56,8 @@ class sgp_b200_result_t(ctypes.Structure):
                 ("iter_max_reached", c_int),
                 ("rng_state", c_u64), ("ms_total", c_flt), ("ms_h2d", c_flt), ("ms_coarsen", c_flt),
                 ("ms_eigen", c_flt), ("ms_split", c_flt), ("ms_d2h", c_flt), ("kernel_launches", c_u32),
-                ("ms_map", c_flt), ("ms_build", c_flt), ("ls_swaps", c_u32)]
+                ("ms_map", c_flt), ("ms_build", c_flt), ("ls_swaps", c_u32), ("fm_passes_run", c_u32),
+                ("fm_moves", c_u64)]
 
 
 class sgp_b200_mtx_info_t(ctypes.Structure):
@@ -105,6 +106,7 @@ _SIGS = {
     "sgp_b200_power_iter": (c_int, [c_vp, c_u32, c_vp, c_vp, c_vp, c_int, c_vp, c_vp, c_vp, c_dbl, c_u64,
                                     c_int, P(c_u64), P(c_dbl), P(c_dbl)]),
     "sgp_b200_split": (c_int, [c_vp, c_u32, c_vp, c_vp, c_vp, c_int, c_vp, P(c_u64)]),
+    "sgp_b200_fm_refine": (c_int, [c_vp, c_u32, c_vp, c_vp, c_vp, c_u32, P(c_u64), P(c_u32), P(c_u64)]),
     "sgp_b200_coarsen_map": (c_int, [c_vp, c_u32, c_vp, c_vp, c_vp, c_int, c_int, c_int, c_u64, c_vp, P(c_u32),
                                      P(c_int)]),
     "sgp_b200_last_timing": (c_int, [c_vp, P(c_flt), P(c_flt), P(c_flt), P(c_flt)]),

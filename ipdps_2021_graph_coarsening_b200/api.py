@@ -182,6 +182,8 @@ class Result:
     ms_map: float = 0.0
     ms_build: float = 0.0
     ls_swaps: int = 0           # local-search move pairs
+    fm_passes: int = 0          # FM passes run
+    fm_moves: int = 0           # FM moves applied
     raw: object = None          # the C result struct (for write_metrics)
 
 
@@ -260,7 +262,8 @@ class Partitioner:
 
     @staticmethod
     def _options(cutoff, tol, mixed, rng_state, rng_inc, iter_cap, perc_imbalance,
-                 refine_alg: int = 0, coarsener: int = 0, local_search_alg: int = 0) -> L.sgp_b200_options_t:
+                 refine_alg: int = 0, coarsener: int = 0, local_search_alg: int = 0,
+                 fm_passes: int = 0) -> L.sgp_b200_options_t:
         o = L.sgp_b200_options_t()
         L.lib().sgp_b200_default_options(ctypes.byref(o))
         o.cutoff, o.tol, o.mixed, o.perc_imbalance = cutoff, tol, int(mixed), perc_imbalance
@@ -268,6 +271,7 @@ class Partitioner:
         o.refine_alg = refine_alg
         o.coarsener = coarsener
         o.local_search_alg = local_search_alg
+        o.fm_passes = fm_passes
         return o
 
     @staticmethod
@@ -289,12 +293,13 @@ class Partitioner:
                       list(res.level_hec_rounds[:nl]), list(res.level_pi_ms[:nl]), bool(res.iter_max_reached),
                       res.rng_state,
                       res.ms_total, res.ms_h2d, res.ms_coarsen, res.ms_eigen, res.ms_split, res.ms_d2h,
-                      res.kernel_launches, res.ms_map, res.ms_build, res.ls_swaps, res)
+                      res.kernel_launches, res.ms_map, res.ms_build, res.ls_swaps, res.fm_passes_run, res.fm_moves,
+                      res)
 
     def partition(self, g, cutoff: int = 50, tol: float = 1e-10, mixed: bool = False,
                   rng_state: int = 0x853C49E6748FEA9B, rng_inc: int = 1, iter_cap: int = 0,
                   perc_imbalance: int = 0, part_out=None, refine_alg: int = 0, coarsener: int = 0,
-                  local_search_alg: int = 0) -> Result:
+                  local_search_alg: int = 0, fm_passes: int = 0) -> Result:
         """Partition ``g``: a host :class:`CSR` (numpy) or a dict of CUDA torch
         tensors ``{"row_ptr", "col", "w"}`` (device-resident input).  The
         partition is written to ``part_out`` (numpy or CUDA tensor) when
@@ -302,7 +307,7 @@ class Partitioner:
         keep = []
         dg = self._graph(g, keep)
         o = self._options(cutoff, tol, mixed, rng_state, rng_inc, iter_cap, perc_imbalance, refine_alg, coarsener,
-                          local_search_alg)
+                          local_search_alg, fm_passes)
         res = L.sgp_b200_result_t()
         part_out, res.part = self._part_target(dg.n, part_out, o)
         L.check(L.lib().sgp_b200_partition(self._ctx, ctypes.byref(dg), ctypes.byref(o), ctypes.byref(res)),
@@ -348,6 +353,17 @@ class Partitioner:
         return [self._result(res[i], parts[i]) for i in range(len(graphs))]
 
     # -- per-kernel entry points (CUDA torch tensors)
+    def fm_refine(self, row_ptr, col, part, max_passes: int = 16):
+        """FM passes on a device bisection ``part`` (CUDA int32 tensor, updated
+        in place): returns (cut, passes, moves)."""
+        n = row_ptr.numel() - 1
+        cut, passes, moves = ctypes.c_uint64(0), ctypes.c_uint32(0), ctypes.c_uint64(0)
+        self._sync()
+        L.check(L.lib().sgp_b200_fm_refine(self._ctx, n, _dptr(row_ptr), _dptr(col), _dptr(part), max_passes,
+                                           ctypes.byref(cut), ctypes.byref(passes), ctypes.byref(moves)),
+                "sgp_b200_fm_refine")
+        return cut.value, passes.value, moves.value
+
     def coarsen_map(self, row_ptr, col, w=None, coarsener: int = 1, random_level: bool = False, seed: int = 1):
         """One level's mapping by an alternative coarsener (MATCH / MIS2 /
         GOSH): returns (vcmap CUDA tensor, nc, rounds)."""

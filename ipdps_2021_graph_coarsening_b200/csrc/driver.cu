@@ -279,6 +279,12 @@ static int partition_staged(Context &C, const Level &L0, const sgp_b200_options_
         SGPB_TRY(local_search_level(C, levels[0], part_d, p0, &res->ls_swaps, &p0));
         SGPB_TRY(edge_cut_device(C, levels[0], part_d, &cut));
     }
+    res->fm_passes_run = 0;
+    res->fm_moves = 0;
+    if (opt->fm_passes) {
+        SGPB_TRY(fm_refine_level(C, levels[0], part_d, opt->fm_passes, &cut, &res->fm_passes_run, &res->fm_moves));
+        SGPB_TRY(count_part0(C, part_d, levels[0].n, &p0));
+    }
     SGPB_CUDA(cudaEventRecord(ev[4], C.stream));
     res->edgecut = cut;
     res->part0_size = p0;
@@ -433,6 +439,7 @@ void sgp_b200_default_options(sgp_b200_options_t *o) {
     o->refine_alg = 0;
     o->coarsener = SGP_B200_COARSEN_HEC;
     o->local_search_alg = 0;
+    o->fm_passes = 0;
 }
 
 int sgp_b200_partition(sgp_b200_ctx_t *x, const sgp_b200_graph_t *g, const sgp_b200_options_t *opt,
@@ -664,6 +671,25 @@ int sgp_b200_coarsen_map(sgp_b200_ctx_t *x, uint32_t n, const uint32_t *rp, cons
         else rc = set_map_level(*C, L, coarsener == SGP_B200_COARSEN_GOSH, seed, vcmap, nc, &r);
     }
     if (rounds) *rounds = r;
+    cudaStreamSynchronize(C->stream);
+    release_all(*C);
+    return rc;
+}
+
+int sgp_b200_fm_refine(sgp_b200_ctx_t *x, uint32_t n, const uint32_t *rp, const uint32_t *col, uint32_t *part,
+                       uint32_t max_passes, uint64_t *cut, uint32_t *passes, uint64_t *moves) {
+    Context *C = ctx_get(x);
+    if (!C || !rp || !col || !part) { set_error("null argument"); return SGP_B200_ERR_INVALID; }
+    cudaSetDevice(C->device);
+    Level L;
+    L.n = n; L.rp = (uint32_t *)rp; L.col = (uint32_t *)col; L.w = nullptr; L.wbytes = 0;
+    uint32_t mm = 0;
+    int rc = n ? read_u32(*C, rp + n, &mm) : 0;
+    L.m = mm;
+    uint64_t c = 0;
+    if (rc == SGP_B200_OK) rc = edge_cut_device(*C, L, part, &c);
+    if (rc == SGP_B200_OK) rc = fm_refine_level(*C, L, part, max_passes, &c, passes, moves);
+    if (rc == SGP_B200_OK && cut) *cut = c;
     cudaStreamSynchronize(C->stream);
     release_all(*C);
     return rc;

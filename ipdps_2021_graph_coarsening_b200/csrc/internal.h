@@ -137,6 +137,10 @@ int edge_cut_device(Context &C, const Level &L, const uint32_t *part, uint64_t *
 // the part-0 size the split left
 int local_search_level(Context &C, const Level &L, uint32_t *part, uint32_t mid, uint32_t *swaps_out,
                        uint32_t *part0_out);
+// FM passes on a bisection of the finest level (fm.cu); *cut_out = its cut
+int fm_refine_level(Context &C, const Level &L, uint32_t *part, uint32_t max_passes, uint64_t *cut_out,
+                    uint32_t *passes_out, uint64_t *moves_out);
+int count_part0(Context &C, const uint32_t *part, uint32_t n, uint32_t *out);
 // map0 / map1 (optional): vertex i of L -> its id in g1 (part 0) / g2
 int induced_subgraphs(Context &C, const Level &L, const uint32_t *part, Level *g1, Level *g2,
                       uint32_t **map0 = nullptr, uint32_t **map1 = nullptr);

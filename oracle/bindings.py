@@ -79,6 +79,8 @@ def lib():
                                           u64ref, c_u64, c_int, c_int, c_int, c_int, u32p, u64ref, f64p, f64p]
         L.orc_compute_partition_ls.argtypes = [c_u32, u32p, u32p, f64p, c_int, u32p, u64ref, u32ref]
         L.orc_compute_partition_ls.restype = c_int
+        L.orc_fm_refine.argtypes = [c_u32, u32p, u32p, ctypes.c_void_p, u32p, c_u32, u64ref, u64ref]
+        L.orc_fm_refine.restype = c_u32
         L.orc_match_map.argtypes = [c_u32, u32p, u32p, ctypes.c_void_p, c_int, c_u64, u32p, u32ref, u32ref]
         L.orc_match_map.restype = c_int
         L.orc_set_map.argtypes = [c_u32, u32p, u32p, c_int, c_u64, u32p, u32ref, u32ref]
@@ -192,6 +194,18 @@ def compute_partition_ls(row_ptr, col, evec, local_search_alg: int = 1):
     lib().orc_compute_partition_ls(n, rp, cl, np.ascontiguousarray(evec, dtype=np.float64), local_search_alg,
                                    part, ctypes.byref(ec), ctypes.byref(sw))
     return part, ec.value, sw.value
+
+
+def fm_refine(row_ptr, col, w, part, max_passes: int = 16):
+    """FM passes on a partition -> (part, cut, passes, moves)."""
+    rp, cl = _u32(row_ptr), _u32(col)
+    n = rp.shape[0] - 1
+    p = np.ascontiguousarray(part, dtype=np.uint32).copy()
+    keep, wp = _w64(w)
+    cut = ctypes.c_uint64(edge_cut(rp, cl, p) if w is None else 0)
+    mv = ctypes.c_uint64(0)
+    passes = lib().orc_fm_refine(n, rp, cl, wp, p, max_passes, ctypes.byref(cut), ctypes.byref(mv))
+    return p, cut.value, int(passes), mv.value
 
 
 def edge_cut(row_ptr, col, part) -> int:

@@ -19,6 +19,8 @@
  *     (sgpar.h:1790-1948, vector kernels sgpar.h:1687-1730)
  *   - median split + one-vertex sweep + edge cut (sgpar.h:1969-2071) and the
  *     local search after it (sgpar.h:2080-2170)
+ *   - a deterministic parallel-form FM pass (structure of fm_refine_par,
+ *     eigensolve_kokkos.h:695-971, acceptance target of fm_refine :1073)
  *   - induced sub-graphs for 4-way recursion (sgpar.h:2666-2752)
  *   - the level loop of sgp_generate_coarse_graphs (coarsen_kokkos.h:1165-1234)
  *     and sgp_eigensolve (eigensolve_kokkos.h:1493-1595)
@@ -557,6 +559,112 @@ int orc_compute_partition_ls(uint32_t n, const uint32_t *row_ptr, const uint32_t
     }
     if (swaps_out) *swaps_out = swaps;
     return 0;
+}
+
+/* ------------------------------------------------------ FM refinement -- */
+/* A deterministic, parallel-form FM pass after the split, following the
+ * structure of the reference's parallel FM (eigensolve_kokkos.h:695-971,
+ * fm_refine_par) and the acceptance target of its serial FM
+ * (:1073-1076: target imbalance max(|balance| / 10, 20)):
+ *   1. gain(u) = sum over neighbours of w * (+1 across the cut, -1 inside);
+ *   2. the vertices of positive gain of each side, ordered by (gain clamped
+ *      to ORC_FM_BUCKETS - 1, descending; id ascending);
+ *   3. the two lists interleaved by the serial FM's balance rule
+ *      (:1105-1140): take from side 0 while the balance (part-0 minus part-1
+ *      vertices) is positive, from side 1 while negative, at zero the head of
+ *      larger gain (side 0 on a tie), the other list once one runs out;
+ *   4. sequential gains: gain of u given that every vertex before it in the
+ *      order has moved; cut after k moves = cut - sum of the first k;
+ *   5. k* = the k (0 included) of least cut among those whose |balance| is
+ *      within the target, the largest such k on a tie (the serial FM's
+ *      "<="); the first k* moves are applied.
+ * Passes repeat until one applies no move or leaves the cut unchanged, at
+ * most max_passes.  Vertex weights are 1 (the finest level).  Returns the
+ * passes run; *moves_out the moves applied in all. */
+#define ORC_FM_BUCKETS 1024
+typedef struct { int64_t g; uint32_t u; } orc_fmc_t;
+static int orc_fm_cmp(const void *a, const void *b) {
+    const orc_fmc_t *x = (const orc_fmc_t *)a, *y = (const orc_fmc_t *)b;
+    int64_t gx = x->g < ORC_FM_BUCKETS - 1 ? x->g : ORC_FM_BUCKETS - 1;
+    int64_t gy = y->g < ORC_FM_BUCKETS - 1 ? y->g : ORC_FM_BUCKETS - 1;
+    if (gx != gy) return gx > gy ? -1 : 1;
+    return x->u < y->u ? -1 : (x->u > y->u);
+}
+
+uint32_t orc_fm_refine(uint32_t n, const uint32_t *row_ptr, const uint32_t *col, const uint64_t *w,
+                       uint32_t *part, uint32_t max_passes, uint64_t *cut_io, uint64_t *moves_out) {
+    int64_t *gain = (int64_t *)malloc(((size_t)n + 1) * sizeof(int64_t));
+    uint32_t *rank = (uint32_t *)malloc(((size_t)n + 1) * sizeof(uint32_t));
+    uint32_t *seq = (uint32_t *)malloc(((size_t)n + 1) * sizeof(uint32_t));
+    int64_t *gseq = (int64_t *)malloc(((size_t)n + 1) * sizeof(int64_t));
+    orc_fmc_t *A = (orc_fmc_t *)malloc(((size_t)n + 1) * sizeof(orc_fmc_t));
+    orc_fmc_t *B = (orc_fmc_t *)malloc(((size_t)n + 1) * sizeof(orc_fmc_t));
+    uint64_t moves = 0;
+    uint32_t pass = 0;
+    for (; pass < max_passes; pass++) {
+        int64_t cut = 0, bal = 0;
+        uint32_t na = 0, nb = 0;
+        for (uint32_t u = 0; u < n; u++) {
+            int64_t g = 0;
+            for (uint32_t j = row_ptr[u]; j < row_ptr[u + 1]; j++) {
+                int64_t x = (int64_t)(w ? w[j] : 1);
+                if (part[col[j]] != part[u]) { g += x; cut += x; } else g -= x;
+            }
+            gain[u] = g;
+            bal += part[u] == 0 ? 1 : -1;
+            rank[u] = ORC_UNASSIGNED;
+            if (g > 0) {
+                if (part[u] == 0) { A[na].g = g; A[na].u = u; na++; }
+                else { B[nb].g = g; B[nb].u = u; nb++; }
+            }
+        }
+        cut /= 2;
+        qsort(A, na, sizeof(orc_fmc_t), orc_fm_cmp);
+        qsort(B, nb, sizeof(orc_fmc_t), orc_fm_cmp);
+        /* interleave (serial FM balance rule) */
+        uint32_t ia = 0, ib = 0, k = 0;
+        int64_t b = bal;
+        while (ia < na || ib < nb) {
+            int take_a;
+            if (ia == na) take_a = 0;
+            else if (ib == nb) take_a = 1;
+            else if (b > 0) take_a = 1;
+            else if (b < 0) take_a = 0;
+            else take_a = A[ia].g >= B[ib].g;
+            uint32_t u = take_a ? A[ia++].u : B[ib++].u;
+            b += take_a ? -2 : 2;
+            rank[u] = k;
+            seq[k++] = u;
+        }
+        /* sequential gains, prefix cut and balance, best prefix */
+        const int64_t abs0 = bal < 0 ? -bal : bal;
+        const int64_t target = abs0 / 10 > 20 ? abs0 / 10 : 20;
+        int64_t best_cut = cut, run = cut, rb = bal;
+        uint32_t best_k = 0;
+        for (uint32_t i = 0; i < k; i++) {
+            uint32_t u = seq[i];
+            int64_t g = 0;
+            for (uint32_t j = row_ptr[u]; j < row_ptr[u + 1]; j++) {
+                uint32_t v = col[j];
+                int64_t x = (int64_t)(w ? w[j] : 1);
+                int across = part[v] != part[u];
+                int moved = rank[v] < i;
+                g += (across ^ moved) ? x : -x;
+            }
+            gseq[i] = g;
+            run -= g;
+            rb += part[u] == 0 ? -2 : 2;
+            int64_t ab = rb < 0 ? -rb : rb;
+            if (ab <= target && run <= best_cut) { best_cut = run; best_k = i + 1; }
+        }
+        if (best_k == 0 || best_cut == cut) break;
+        for (uint32_t i = 0; i < best_k; i++) part[seq[i]] ^= 1u;
+        moves += best_k;
+        *cut_io = (uint64_t)best_cut;
+    }
+    if (moves_out) *moves_out = moves;
+    free(gain); free(rank); free(seq); free(gseq); free(A); free(B);
+    return pass;
 }
 
 /* Edge cut of an arbitrary 2-way partition (directed cross entries / 2). */

@@ -188,3 +188,27 @@ def test_local_search_matches_reference(case):
         p1, c1, _ = O.compute_partition_ls(g.row_ptr, g.col, ev)
         p2, c2 = O.ref_compute_partition_ls(g.row_ptr, g.col, ev)
         assert np.array_equal(p1, p2) and c1 == c2
+
+
+@pytest.mark.parametrize("case", ["grid", "holes", "er", "rmat", "rgg"])
+def test_fm_pass_properties(case):
+    """The oracle's FM passes (orc_fm_refine): the reported cut is the
+    partition's cut, it never rises, the balance ends within the serial FM's
+    target max(|d| / 10, 20), and a pass that cannot improve changes nothing."""
+    from ipdps_2021_graph_coarsening_b200 import graphs as Gm
+    g = {"grid": lambda: Gm.grid2d(60, 40), "holes": lambda: Gm.grid2d_holes(100, 80, 0.1, 2),
+         "er": lambda: Gm.erdos_renyi(5000, 5.0, seed=3), "rmat": lambda: Gm.rmat(13, seed=2),
+         "rgg": lambda: Gm.rgg3d(20000, seed=1)}[case]()
+    rng = np.random.default_rng(7)
+    starts = [O.partition_graph(g.row_ptr, g.col, None, rng_state=5)["part"],
+              (rng.permutation(g.n) < g.n // 2).astype(np.uint32)]
+    for p0 in starts:
+        c0 = O.edge_cut(g.row_ptr, g.col, p0)
+        p, c, passes, moves = O.fm_refine(g.row_ptr, g.col, None, p0)
+        assert c == O.edge_cut(g.row_ptr, g.col, p) <= c0
+        d0 = abs(2 * int((p0 == 0).sum()) - g.n)
+        assert abs(2 * int((p == 0).sum()) - g.n) <= max(d0 // 10, 20) or moves == 0
+        q, c2, passes2, moves2 = O.fm_refine(g.row_ptr, g.col, None, p, max_passes=64)
+        assert c2 <= c
+    # a random start improves a lot
+    assert O.fm_refine(g.row_ptr, g.col, None, starts[1])[1] < O.edge_cut(g.row_ptr, g.col, starts[1])
