@@ -10,6 +10,7 @@ duplicates merged, self loops dropped, largest connected component kept).
   e2e    the same through the public API with pinned host buffers: the CSR
          upload and the partition download are inside the timed region
   mixed  FP32-storage / FP64-reduction power iteration on the same graph
+  fm     the same partition followed by up to 16 FM passes (cut and time)
 
 Multi-GPU: the single-graph path does not shard (a row partition would need
 halo exchanges per iteration); N ranks run N independent replicas ("weak"),
@@ -264,6 +265,14 @@ def gpu_arm(args, rank: int, ws: int, local: int, distmod):
              "lambda_rel_err": abs(rm.lam - r.lam) / abs(r.lam) if r.lam else None,
              "residual": rm.residual, "speedup_vs_fp64": ms / ms_mx, "level_iters": rm.level_iters}
 
+    # FM refinement of the same bisection (fm_passes), timed the same way
+    p.partition(dg, rng_state=seed, part_out=part_d, fm_passes=16)
+    ms_fm, res_fm = timed(lambda: p.partition(dg, rng_state=seed, part_out=part_d, fm_passes=16), args.steps)
+    rf = res_fm[-1]
+    fm = {"ms_per_step": ms_fm, "fm_ms": ms_fm - ms, "edgecut": rf.edgecut, "edgecut_spectral": r.edgecut,
+          "cut_reduction": 1 - rf.edgecut / max(1, r.edgecut), "passes": rf.fm_passes, "moves": rf.fm_moves,
+          "part0_size": rf.part0_size}
+
     # roofline of the dominant kernel (power iteration) from this step's levels
     peak, peak_kind = load_peaks()
     byts = sum(it * algorithmic_pi_bytes(nl, ml, l > 0, 8)
@@ -296,7 +305,7 @@ def gpu_arm(args, rank: int, ws: int, local: int, distmod):
             "level_m": r.level_m,
             "level_iters": r.level_iters, "level_pi_ms": [round(x, 3) for x in r.level_pi_ms],
             "phase_ms": {"coarsen": r.ms_coarsen, "eigen": r.ms_eigen, "split": r.ms_split},
-            "clocks": clocks, "e2e": e2e, "mixed": mixed, "gpu_launches": r.kernel_launches * args.steps,
+            "clocks": clocks, "e2e": e2e, "mixed": mixed, "fm": fm, "gpu_launches": r.kernel_launches * args.steps,
             "roofline": roofline}
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline()
