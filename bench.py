@@ -440,10 +440,22 @@ def mtx_arm(args, rank: int, ws: int, local: int, distmod):
     # kernel; the phase split says where the rest of the step goes
     peak, peak_kind = load_peaks()
     parse_bytes = 2 * len(text) + 8 * lines
+    # DRAM traffic: the parse kernel's measured bytes per line (one ncu
+    # capture on the R-MAT 20 file, profiles/mtx_parse_traffic.json) scaled
+    # to this file, plus the count kernel's one streaming read of the text
+    traffic = None
+    tf = os.path.join(ROOT, "profiles", "mtx_parse_traffic.json")
+    if os.path.exists(tf):
+        try:
+            traffic = json.load(open(tf))["dram_bytes_per_line"] * lines + len(text)
+        except (OSError, ValueError, KeyError):
+            traffic = None
     roofline = {"bound": "hbm", "kernel": "k_mtx_count + k_mtx_parse (text pass)",
                 "algorithmic_bytes": parse_bytes, "kernel_ms": info["ms_parse"],
                 "achieved": parse_bytes / (info["ms_parse"] / 1e3) / 1e9, "peak": peak, "unit": "GB/s",
-                "peak_kind": peak_kind, "traffic": None}
+                "peak_kind": peak_kind, "traffic": traffic,
+                "note": "phase time incl. two scans and read-backs; the pass is instruction-bound "
+                        "(profiles/mtx_parse_rmat20.md); the step's largest kernel is the row sort"}
     roofline["frac"] = roofline["achieved"] / peak
     line = {"metric": MTX_METRIC, "value": value, "unit": "lines/s", "n_gpus": ws, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
