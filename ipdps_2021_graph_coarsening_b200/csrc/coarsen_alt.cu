@@ -8,6 +8,8 @@
 //          heuristics.h:8-80 (mis_2) and :218-310 (sgp_coarsen_mis_2)
 //   GOSH   aggregation around high-degree cluster centres: heuristics.h:81-216
 //          (GOSH_clusters) and :312-365 (sgp_coarsen_GOSH)
+//   HEC_V3 HEC's heavy neighbours with the pointer-jumping map construction
+//          of heuristics.h:766-834 (parallel_map_construct_v3)
 //
 // The reference draws its random keys from a time-seeded pool, numbers
 // aggregates with atomic counters and resolves some races by timing.  Here a
@@ -332,6 +334,75 @@ int match_map_level(Context &C, const Level &L, int random_level, uint64_t seed,
     *nc_out = out[0];
     *rounds_out = (int)out[1];
     return SGP_B200_OK;
+}
+
+// --------------------------------------------------------------- HEC_V3 --
+// heuristics.h:766-834: a vertex in a mutual heavy pair points to the pair's
+// smaller id; every heavy-neighbour target not in such a pair points to
+// itself; every other vertex points where its heavy neighbour points.  The
+// reference's compare-and-swap writes the same value from every thread, and
+// the join step reads only entries set before it, so the construction is
+// deterministic given the heavy neighbours.  Roots (m[u] == u) are numbered
+// in ascending order (the reference's scan over the dense map).
+__global__ void k_v3_pairs(uint32_t n, const uint32_t *__restrict__ hn, uint32_t *__restrict__ m) {
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    for (uint64_t u = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; u < n; u += stride) {
+        const uint32_t h = hn[u];
+        uint32_t x = kNone;
+        if (hn[h] == (uint32_t)u) x = h < u ? h : (uint32_t)u;
+        m[u] = x;
+    }
+}
+__global__ void k_v3_targets(uint32_t n, const uint32_t *__restrict__ hn, uint32_t *__restrict__ m) {
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    for (uint64_t u = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; u < n; u += stride) {
+        const uint32_t v = hn[u];
+        if (m[v] == kNone) m[v] = v;   // every writer stores v
+    }
+}
+__global__ void k_v3_join(uint32_t n, const uint32_t *__restrict__ hn, uint32_t *__restrict__ m,
+                          uint32_t *__restrict__ root) {
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    for (uint64_t u = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; u < n; u += stride) {
+        uint32_t x = m[u];
+        if (x == kNone) x = m[hn[u]];   // set by the steps above, not written here
+        root[u] = x;
+    }
+}
+__global__ void k_v3_flags(uint32_t n, const uint32_t *__restrict__ root, uint32_t *__restrict__ f) {
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    for (uint64_t u = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; u < n; u += stride)
+        f[u] = root[u] == (uint32_t)u;
+}
+__global__ void k_v3_number(uint32_t n, const uint32_t *__restrict__ root, const uint32_t *__restrict__ rank,
+                            uint32_t *__restrict__ vcmap) {
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    for (uint64_t u = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; u < n; u += stride) vcmap[u] = rank[root[u]];
+}
+
+int hec_v3_map_level(Context &C, const Level &L, int random_level, uint64_t seed, uint32_t *vcmap, uint32_t *nc_out) {
+    const uint32_t n = L.n;
+    if (n == 0) {
+        *nc_out = 0;
+        return SGP_B200_OK;
+    }
+    uint32_t *hn, *m, *root, *f, *rank;
+    SGPB_TRY(dalloc_t(C, &hn, n));
+    SGPB_TRY(dalloc_t(C, &m, n));
+    SGPB_TRY(dalloc_t(C, &root, n));
+    SGPB_TRY(dalloc_t(C, &f, n));
+    SGPB_TRY(dalloc_t(C, &rank, (size_t)n + 1));
+    SGPB_TRY(hec_hn_level(C, L, random_level, seed, hn));
+    const uint32_t g = rows_grid(C, n);
+    k_v3_pairs<<<g, 256, 0, C.stream>>>(n, hn, m);
+    k_v3_targets<<<g, 256, 0, C.stream>>>(n, hn, m);
+    k_v3_join<<<g, 256, 0, C.stream>>>(n, hn, m, root);
+    k_v3_flags<<<g, 256, 0, C.stream>>>(n, root, f);
+    SGPB_TRY(scan_u32(C, f, rank, n, nullptr));
+    k_v3_number<<<g, 256, 0, C.stream>>>(n, root, rank, vcmap);
+    C.kernel_launches += 5;
+    SGPB_CUDA(cudaGetLastError());
+    return read_u32(C, rank + n, nc_out);
 }
 
 // ---------------------------------------------------------- MIS-2 / GOSH --

@@ -246,12 +246,10 @@ static void launch_hn_heavy(Context &C, const Level &L, const W *w, uint64_t see
     C.kernel_launches++;
 }
 
-int hec_map_level(Context &C, const Level &L, int random_level, uint64_t seed, uint32_t *vcmap,
-                  uint32_t *hn_out, uint32_t *nc_out, int *rounds_out) {
+// the heavy-neighbour step alone (also used by the HEC_V3 mapping)
+int hec_hn_level(Context &C, const Level &L, int random_level, uint64_t seed, uint32_t *hn) {
     const uint32_t n = L.n;
-    if (n == 0) { *nc_out = 0; *rounds_out = 0; return SGP_B200_OK; }
-    uint32_t *hn = hn_out;
-    if (!hn) SGPB_TRY(dalloc_t(C, &hn, n));
+    if (n == 0) return SGP_B200_OK;
     if (random_level) {
         k_hn_random<<<cdiv(n, 256), 256, 0, C.stream>>>(n, L.rp, L.col, seed, hn);
         C.kernel_launches++;
@@ -261,6 +259,16 @@ int hec_map_level(Context &C, const Level &L, int random_level, uint64_t seed, u
         launch_hn_heavy<uint32_t>(C, L, (const uint32_t *)L.w, seed, hn);
     }
     SGPB_CUDA(cudaGetLastError());
+    return SGP_B200_OK;
+}
+
+int hec_map_level(Context &C, const Level &L, int random_level, uint64_t seed, uint32_t *vcmap,
+                  uint32_t *hn_out, uint32_t *nc_out, int *rounds_out) {
+    const uint32_t n = L.n;
+    if (n == 0) { *nc_out = 0; *rounds_out = 0; return SGP_B200_OK; }
+    uint32_t *hn = hn_out;
+    if (!hn) SGPB_TRY(dalloc_t(C, &hn, n));
+    SGPB_TRY(hec_hn_level(C, L, random_level, seed, hn));
 
     MapArgs a;
     a.n = n; a.hn = hn; a.seed = seed; a.vcmap = vcmap;

@@ -111,6 +111,9 @@ int build_coarse_level(Context &C, const Level &F, const uint32_t *vcmap, uint32
 // MIS-2 (gosh false) / GOSH (gosh true) aggregations
 int match_map_level(Context &C, const Level &L, int random_level, uint64_t seed, uint32_t *vcmap, uint32_t *nc_out,
                     int *rounds_out);
+// heavy neighbours of a level (hec.cu) and the HEC_V3 mapping built on them
+int hec_hn_level(Context &C, const Level &L, int random_level, uint64_t seed, uint32_t *hn);
+int hec_v3_map_level(Context &C, const Level &L, int random_level, uint64_t seed, uint32_t *vcmap, uint32_t *nc_out);
 int set_map_level(Context &C, const Level &L, bool gosh, uint64_t seed, uint32_t *vcmap, uint32_t *nc_out,
                   int *rounds_out);
 struct PowerIterOpts {

@@ -519,7 +519,17 @@ static int read_head(Context &C, MtxSource &src, MtxHead *h) {
 class HostPool {
   public:
     static HostPool &get() {
-        static HostPool *p = new HostPool();   // never destroyed: idle workers end with the process
+        // never destroyed: idle workers end with the process.  A forked
+        // child has none of the parent's workers, so it builds its own pool
+        // (the parent's object is left untouched).
+        static std::mutex mu;
+        static HostPool *p = nullptr;
+        static pid_t owner = 0;
+        std::lock_guard<std::mutex> lk(mu);
+        if (!p || owner != getpid()) {
+            p = new HostPool();
+            owner = getpid();
+        }
         return *p;
     }
     int width() const { return (int)th_.size() + 1; }

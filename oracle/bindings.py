@@ -83,6 +83,8 @@ def lib():
         L.orc_fm_refine.restype = c_u32
         L.orc_match_map.argtypes = [c_u32, u32p, u32p, ctypes.c_void_p, c_int, c_u64, u32p, u32ref, u32ref]
         L.orc_match_map.restype = c_int
+        L.orc_hec_v3_map.argtypes = [c_u32, u32p, u32p, u32ref]
+        L.orc_hec_v3_map.restype = c_int
         L.orc_set_map.argtypes = [c_u32, u32p, u32p, c_int, c_u64, u32p, u32ref, u32ref]
         L.orc_set_map.restype = c_int
         L.orc_partition_graph.restype = c_int
@@ -234,6 +236,17 @@ def match_map(row_ptr, col, w, random_level: bool, seed: int):
     nc, rounds = ctypes.c_uint32(0), ctypes.c_uint32(0)
     lib().orc_match_map(n, rp, cl, wp, int(random_level), seed, vc, ctypes.byref(nc), ctypes.byref(rounds))
     return vc[:n], nc.value, rounds.value
+
+
+def hec_v3_map(row_ptr, col, w, random_level: bool, seed: int):
+    """HEC_V3 mapping (HEC heavy neighbours, pointer-jumping construction)
+    -> (vcmap, nc)."""
+    hn = hec_heavy(row_ptr, col, w, random_level, seed)
+    n = hn.shape[0]
+    vc = np.zeros(max(n, 1), np.uint32)
+    nc = ctypes.c_uint32(0)
+    lib().orc_hec_v3_map(n, _u32(hn), vc, ctypes.byref(nc))
+    return vc[:n], nc.value
 
 
 def set_map(row_ptr, col, gosh: bool, seed: int):

@@ -797,6 +797,24 @@ int orc_match_map(uint32_t n, const uint32_t *rp, const uint32_t *col, const uin
     return 0;
 }
 
+/* heuristics.h:766-834 (parallel_map_construct_v3) on given heavy
+ * neighbours: mutual heavy pairs point to their smaller id, other heavy
+ * targets to themselves, the rest where their heavy neighbour points; roots
+ * numbered in ascending order. */
+int orc_hec_v3_map(uint32_t n, const uint32_t *hn, uint32_t *vcmap, uint32_t *nc_out) {
+    uint32_t *m = (uint32_t *)malloc(((size_t)n + 1) * sizeof(uint32_t));
+    for (uint32_t u = 0; u < n; u++) {
+        m[u] = ORC_UNASSIGNED;
+        if (hn[hn[u]] == u) m[u] = hn[u] < u ? hn[u] : u;
+    }
+    for (uint32_t u = 0; u < n; u++)
+        if (m[hn[u]] == ORC_UNASSIGNED) m[hn[u]] = hn[u];
+    for (uint32_t u = 0; u < n; u++) vcmap[u] = m[u] != ORC_UNASSIGNED ? m[u] : m[hn[u]];
+    *nc_out = orc_number_roots(n, vcmap);
+    free(m);
+    return 0;
+}
+
 typedef struct { int s; uint64_t k; uint32_t i; } orc_tup_t;
 static int orc_tup_gt(orc_tup_t x, orc_tup_t y) {
     return x.s > y.s || (x.s == y.s && (x.k > y.k || (x.k == y.k && x.i > y.i)));
@@ -905,7 +923,7 @@ int orc_partition_graph(uint32_t n, const uint32_t *row_ptr, const uint32_t *col
     const int kind = coarsener & 15;
     L[0].n = n; L[0].rp = (uint32_t *)row_ptr; L[0].col = (uint32_t *)col;
     L[0].w = (uint64_t *)w64; L[0].vcmap = NULL;
-    /* coarsener: 0 HEC, 1 MATCH, 2 MIS2, 3 GOSH; | 16 no coarsening, | 32 stop
+    /* coarsener: 0 HEC, 1 MATCH, 2 MIS2, 3 GOSH, 4 HEC_V3; | 16 no coarsening, | 32 stop
      * after a level keeping more than 0.9 of the vertices (sgpar.h:2466-2475) */
     while (!(coarsener & 16) && L[nl - 1].n > cutoff) {
         orc_level_t *f = &L[nl - 1];
@@ -921,6 +939,11 @@ int orc_partition_graph(uint32_t n, const uint32_t *row_ptr, const uint32_t *col
             free(hn);
         } else if (kind == 1) {
             orc_match_map(f->n, f->rp, f->col, f->w, random_level, seed, f->vcmap, &nc, &rounds);
+        } else if (kind == 4) {
+            uint32_t *hn = (uint32_t *)malloc((size_t)f->n * sizeof(uint32_t));
+            orc_hec_heavy(f->n, f->rp, f->col, f->w, random_level, seed, hn);
+            orc_hec_v3_map(f->n, hn, f->vcmap, &nc);
+            free(hn);
         } else {
             if (orc_set_map(f->n, f->rp, f->col, kind == 3, seed, f->vcmap, &nc, &rounds)) return 1;
         }

@@ -60,6 +60,17 @@ def test_set_map_bit_exact(partitioner, name, coarsener):
     assert np.array_equal(vc.cpu().numpy().view(np.uint32), ovc)
 
 
+@pytest.mark.parametrize("name", sorted(CASES))
+@pytest.mark.parametrize("random_level", [True, False])
+def test_hec_v3_map_bit_exact(partitioner, name, random_level):
+    g = CASES[name]
+    rp, col, w = dev(g)
+    seed = 0x1234ABCD
+    vc, nc, _ = partitioner.coarsen_map(rp, col, w, L.COARSEN_HEC_V3, random_level, seed)
+    ovc, onc = O.hec_v3_map(g.row_ptr, g.col, g.w, random_level, seed)
+    assert nc == onc and np.array_equal(vc.cpu().numpy().view(np.uint32), ovc)
+
+
 def test_coarsen_map_rejects_hec(partitioner):
     rp, col, _ = dev(CASES["grid"])
     with pytest.raises(L.SgparError):
@@ -71,7 +82,7 @@ def cut_of(g, labels):
     return int((labels[r] != labels[g.col]).sum()) // 2
 
 
-@pytest.mark.parametrize("coarsener", [L.COARSEN_MATCH, L.COARSEN_MIS2, L.COARSEN_GOSH,
+@pytest.mark.parametrize("coarsener", [L.COARSEN_MATCH, L.COARSEN_MIS2, L.COARSEN_GOSH, L.COARSEN_HEC_V3,
                                        L.COARSEN_MATCH | L.COARSEN_RATIO_STOP, L.COARSEN_NONE])
 @pytest.mark.parametrize("name", ["holes", "rmat14", "er_small"])
 def test_partition_with_coarsener(partitioner, coarsener, name):

@@ -152,3 +152,25 @@ def test_whole_path_with_each_coarsener(coarsener):
         # one fell below 10 vertices and was dropped (coarsen_kokkos.h:1226)
         ln = o["level_n"]
         assert o["levels"] > 1 and all(a > b for a, b in zip(ln, ln[1:]))
+
+
+@pytest.mark.parametrize("name", sorted(CASES))
+@pytest.mark.parametrize("random_level", [True, False])
+def test_hec_v3_aggregates(name, random_level):
+    """heuristics.h:766-834: roots are the smaller ends of mutual heavy pairs
+    and the other heavy-neighbour targets; every vertex that is neither joins
+    its heavy neighbour's aggregate, and a mutual pair shares one."""
+    g = CASES[name]
+    seed = 0x5151
+    hn = O.hec_heavy(g.row_ptr, g.col, g.w, random_level, seed)
+    vc, nc = O.hec_v3_map(g.row_ptr, g.col, g.w, random_level, seed)
+    assert sorted(set(vc.tolist())) == list(range(nc))
+    n = g.n
+    targeted = np.zeros(n, bool)
+    targeted[hn] = True
+    mutual = hn[hn] == np.arange(n)
+    plain = ~targeted & ~mutual
+    assert np.all(vc[plain] == vc[hn[plain]])
+    assert np.all(vc[mutual] == vc[hn[mutual]])
+    roots = (mutual & (np.arange(n) < hn)) | (targeted & ~mutual)
+    assert nc == int(roots.sum())
