@@ -175,6 +175,7 @@ typedef struct {
 #define SGP_B200_COARSEN_MIS2 2     /* distance-2 independent-set aggregation, heuristics.h:8-80, :218-310 */
 #define SGP_B200_COARSEN_GOSH 3     /* degree-keyed cluster aggregation, heuristics.h:81-216, :312-365 */
 #define SGP_B200_COARSEN_HEC_V3 4   /* HEC with the pointer-jumping map construction, heuristics.h:766-834 */
+#define SGP_B200_COARSEN_GOSH_V2 5  /* high-degree roots + joins + prefilled HEC rounds, heuristics.h:444-560 */
 #define SGP_B200_COARSEN_NONE 16
 #define SGP_B200_COARSEN_RATIO_STOP 32
 
@@ -295,7 +296,7 @@ int sgp_b200_fm_refine(sgp_b200_ctx_t *ctx, uint32_t n, const uint32_t *row_ptr,
                        uint32_t *part, uint32_t max_passes, uint64_t *cut, uint32_t *passes, uint64_t *moves);
 
 /* One level's mapping by an alternative coarsener (coarsener MATCH, MIS2,
- * GOSH or HEC_V3; the HEC mapping is sgp_b200_hec) on device arrays: vcmap[n] receives
+ * GOSH, HEC_V3 or GOSH_V2; the HEC mapping is sgp_b200_hec) on device arrays: vcmap[n] receives
  * the coarse vertex of each vertex, *nc the coarse count, *rounds the
  * matching rounds or independent-set iterations. */
 int sgp_b200_coarsen_map(sgp_b200_ctx_t *ctx, uint32_t n, const uint32_t *row_ptr, const uint32_t *col,

@@ -19,7 +19,7 @@ P = ctypes.POINTER
 MAX_LEVELS = 202
 OK, FAIL, ERR_INVALID, ERR_DEVICE, ERR_TOO_LARGE, ERR_BUDGET = 0, 1, 2, 3, 4, 5
 HOST, DEVICE = 0, 1
-COARSEN_HEC, COARSEN_MATCH, COARSEN_MIS2, COARSEN_GOSH, COARSEN_HEC_V3 = 0, 1, 2, 3, 4
+COARSEN_HEC, COARSEN_MATCH, COARSEN_MIS2, COARSEN_GOSH, COARSEN_HEC_V3, COARSEN_GOSH_V2 = 0, 1, 2, 3, 4, 5
 COARSEN_NONE, COARSEN_RATIO_STOP = 16, 32
 
 

@@ -10,6 +10,8 @@
 //          (GOSH_clusters) and :312-365 (sgp_coarsen_GOSH)
 //   HEC_V3 HEC's heavy neighbours with the pointer-jumping map construction
 //          of heuristics.h:766-834 (parallel_map_construct_v3)
+//   GOSH_V2 high-degree roots, three joining passes, then the HEC map rounds
+//          with those aggregates prefilled: heuristics.h:444-560
 //
 // The reference draws its random keys from a time-seeded pool, numbers
 // aggregates with atomic counters and resolves some races by timing.  Here a
@@ -403,6 +405,96 @@ int hec_v3_map_level(Context &C, const Level &L, int random_level, uint64_t seed
     C.kernel_launches += 5;
     SGPB_CUDA(cudaGetLastError());
     return read_u32(C, rank + n, nc_out);
+}
+
+// -------------------------------------------------------------- GOSH_V2 --
+// heuristics.h:444-560 with every joining pass reading a snapshot of the one
+// before (the reference reads live values, so its result depends on thread
+// timing).  dst[u] = src[u]; an unassigned u joins the aggregate of the
+// neighbour picked among those assigned in src: mode 0 the largest edge
+// weight, mode 1 the largest degree (the last in row order on a tie, the
+// reference's ">="), mode 2 the first in row order.  One warp per row.
+template <typename W>
+__global__ void __launch_bounds__(256) k_gv2_join(uint32_t n, const uint32_t *__restrict__ rp,
+                                                  const uint32_t *__restrict__ col, const W *__restrict__ w, int mode,
+                                                  const uint32_t *__restrict__ src, uint32_t *__restrict__ dst) {
+    const unsigned lane = threadIdx.x & 31;
+    const uint64_t nw = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+    for (uint64_t u = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; u < n; u += nw) {
+        const uint32_t own = src[u];
+        if (own != kNone) {
+            if (lane == 0) dst[u] = own;
+            continue;
+        }
+        uint64_t bk = 0;
+        uint32_t bj = kNone;
+        for (uint32_t j = rp[u] + lane; j < rp[u + 1]; j += 32) {
+            const uint32_t v = __ldg(col + j);
+            if (src[v] == kNone) continue;
+            if (mode == 2) {
+                if (bj == kNone) bj = j;   // j ascends per lane
+                continue;
+            }
+            const uint64_t k = mode == 0 ? wload(w, j) : (uint64_t)(rp[v + 1] - rp[v]);
+            if (bj == kNone || k >= bk) {
+                bk = k;
+                bj = j;
+            }
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            const uint64_t ok = __shfl_xor_sync(0xFFFFFFFFu, bk, o);
+            const uint32_t oj = __shfl_xor_sync(0xFFFFFFFFu, bj, o);
+            bool take;
+            if (mode == 2) take = oj < bj;   // kNone is the largest
+            else take = oj != kNone && (bj == kNone || ok > bk || (ok == bk && oj > bj));
+            if (take) {
+                bk = ok;
+                bj = oj;
+            }
+        }
+        if (lane == 0) dst[u] = bj == kNone ? kNone : src[__ldg(col + bj)];
+    }
+}
+
+__global__ void k_gv2_roots(uint32_t n, const uint32_t *__restrict__ rp, uint64_t thr, uint32_t *__restrict__ vc) {
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    for (uint64_t u = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; u < n; u += stride)
+        vc[u] = (uint64_t)(rp[u + 1] - rp[u]) > thr ? (uint32_t)u : kNone;
+}
+
+int gosh_v2_map_level(Context &C, const Level &L, uint64_t seed, uint32_t *vcmap, uint32_t *nc_out, int *rounds_out) {
+    const uint32_t n = L.n;
+    if (n == 0) {
+        *nc_out = 0;
+        *rounds_out = 0;
+        return SGP_B200_OK;
+    }
+    uint64_t thr = L.m / n;
+    if (thr < 50) thr = 50;
+    uint32_t *a, *hn;
+    SGPB_TRY(dalloc_t(C, &a, n));
+    SGPB_TRY(dalloc_t(C, &hn, n));
+    k_gv2_roots<<<rows_grid(C, n), 256, 0, C.stream>>>(n, L.rp, thr, a);
+    const uint32_t gw = rows_grid(C, (uint64_t)n * 32);
+    // snapshots ping-pong between a and vcmap, ending in vcmap
+    uint32_t *src = a, *dst = vcmap;
+    for (int mode = 0; mode < 3; mode++) {
+        if (L.wbytes == 8)
+            k_gv2_join<unsigned long long><<<gw, 256, 0, C.stream>>>(n, L.rp, L.col, (const unsigned long long *)L.w,
+                                                                     mode, src, dst);
+        else
+            k_gv2_join<uint32_t><<<gw, 256, 0, C.stream>>>(n, L.rp, L.col, (const uint32_t *)L.w, mode, src, dst);
+        uint32_t *t = src;
+        src = dst;
+        dst = t;
+    }
+    // an odd number of passes: the last one wrote vcmap
+    if (src != vcmap) SGPB_CUDA(cudaMemcpyAsync(vcmap, src, sizeof(uint32_t) * n, cudaMemcpyDeviceToDevice, C.stream));
+    C.kernel_launches += 4;
+    SGPB_CUDA(cudaGetLastError());
+    SGPB_TRY(hec_hn_level(C, L, 0, seed, hn));
+    return hec_map_from_hn(C, n, hn, seed, vcmap, true, nc_out, rounds_out);
 }
 
 // ---------------------------------------------------------- MIS-2 / GOSH --

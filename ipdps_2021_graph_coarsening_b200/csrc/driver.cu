@@ -127,9 +127,9 @@ static int weight_width(Context &C, const Level &L0, int *wbytes) {
 static int generate(Context &C, const Level &L0, uint32_t cutoff, uint64_t *rng_state, uint64_t rng_inc,
                     std::vector<Level> &levels, int coarsener = SGP_B200_COARSEN_HEC) {
     const int kind = coarsener & 15;
-    if (kind > SGP_B200_COARSEN_HEC_V3 || (coarsener & ~(15 | SGP_B200_COARSEN_NONE | SGP_B200_COARSEN_RATIO_STOP))) {
-        set_error("coarsener %d: HEC 0, MATCH 1, MIS2 2, GOSH 3 or HEC_V3 4, optionally | NONE (16) | RATIO_STOP (32)",
-                  coarsener);
+    if (kind > SGP_B200_COARSEN_GOSH_V2 || (coarsener & ~(15 | SGP_B200_COARSEN_NONE | SGP_B200_COARSEN_RATIO_STOP))) {
+        set_error("coarsener %d: HEC 0, MATCH 1, MIS2 2, GOSH 3, HEC_V3 4 or GOSH_V2 5, optionally | NONE (16) | "
+                  "RATIO_STOP (32)", coarsener);
         return SGP_B200_ERR_INVALID;
     }
     levels.clear();
@@ -162,6 +162,8 @@ static int generate(Context &C, const Level &L0, uint32_t cutoff, uint64_t *rng_
             SGPB_TRY(match_map_level(C, F, random_level, seed, vcmap, &nc, &rounds));
         else if (kind == SGP_B200_COARSEN_HEC_V3)
             SGPB_TRY(hec_v3_map_level(C, F, random_level, seed, vcmap, &nc));
+        else if (kind == SGP_B200_COARSEN_GOSH_V2)
+            SGPB_TRY(gosh_v2_map_level(C, F, seed, vcmap, &nc, &rounds));
         else
             SGPB_TRY(set_map_level(C, F, kind == SGP_B200_COARSEN_GOSH, seed, vcmap, &nc, &rounds));
         F.vcmap = vcmap;
@@ -656,8 +658,9 @@ int sgp_b200_coarsen_map(sgp_b200_ctx_t *x, uint32_t n, const uint32_t *rp, cons
     Context *C = ctx_get(x);
     if (!C || !rp || !vcmap || !nc) { set_error("null argument"); return SGP_B200_ERR_INVALID; }
     if (wbytes != 0 && wbytes != 4 && wbytes != 8) { set_error("wbytes must be 0, 4 or 8"); return SGP_B200_ERR_INVALID; }
-    if (coarsener < SGP_B200_COARSEN_MATCH || coarsener > SGP_B200_COARSEN_HEC_V3) {
-        set_error("sgp_b200_coarsen_map takes MATCH (1), MIS2 (2), GOSH (3) or HEC_V3 (4); HEC is sgp_b200_hec");
+    if (coarsener < SGP_B200_COARSEN_MATCH || coarsener > SGP_B200_COARSEN_GOSH_V2) {
+        set_error("sgp_b200_coarsen_map takes MATCH (1), MIS2 (2), GOSH (3), HEC_V3 (4) or GOSH_V2 (5); HEC is "
+                  "sgp_b200_hec");
         return SGP_B200_ERR_INVALID;
     }
     cudaSetDevice(C->device);
@@ -671,6 +674,7 @@ int sgp_b200_coarsen_map(sgp_b200_ctx_t *x, uint32_t n, const uint32_t *rp, cons
     if (rc == SGP_B200_OK) {
         if (coarsener == SGP_B200_COARSEN_MATCH) rc = match_map_level(*C, L, random_level, seed, vcmap, nc, &r);
         else if (coarsener == SGP_B200_COARSEN_HEC_V3) rc = hec_v3_map_level(*C, L, random_level, seed, vcmap, nc);
+        else if (coarsener == SGP_B200_COARSEN_GOSH_V2) rc = gosh_v2_map_level(*C, L, seed, vcmap, nc, &r);
         else rc = set_map_level(*C, L, coarsener == SGP_B200_COARSEN_GOSH, seed, vcmap, nc, &r);
     }
     if (rounds) *rounds = r;

@@ -269,7 +269,15 @@ int hec_map_level(Context &C, const Level &L, int random_level, uint64_t seed, u
     uint32_t *hn = hn_out;
     if (!hn) SGPB_TRY(dalloc_t(C, &hn, n));
     SGPB_TRY(hec_hn_level(C, L, random_level, seed, hn));
+    return hec_map_from_hn(C, n, hn, seed, vcmap, false, nc_out, rounds_out);
+}
 
+// The map rounds on given heavy neighbours.  prefilled: vcmap already holds
+// aggregates (members hold their root vertex, roots themselves, the rest
+// kUnassigned), as parallel_map_construct_prefilled (heuristics.h:378-443)
+// takes them; the rounds only place the unassigned vertices.
+int hec_map_from_hn(Context &C, uint32_t n, const uint32_t *hn, uint64_t seed, uint32_t *vcmap, bool prefilled,
+                    uint32_t *nc_out, int *rounds_out) {
     MapArgs a;
     a.n = n; a.hn = hn; a.seed = seed; a.vcmap = vcmap;
     SGPB_TRY(dalloc_t(C, &a.claim0, n));
@@ -282,7 +290,7 @@ int hec_map_level(Context &C, const Level &L, int random_level, uint64_t seed, u
     SGPB_TRY(dzero(C, a.claim0, sizeof(unsigned long long) * n));
     SGPB_TRY(dzero(C, a.claim1, sizeof(unsigned long long) * n));
     SGPB_TRY(dzero(C, a.counters, sizeof(uint32_t) * 2));
-    SGPB_CUDA(cudaMemsetAsync(vcmap, 0xFF, sizeof(uint32_t) * n, C.stream));
+    if (!prefilled) SGPB_CUDA(cudaMemsetAsync(vcmap, 0xFF, sizeof(uint32_t) * n, C.stream));
     // Progress argument: each two rounds assign at least one vertex, so
     // 2n + 4 rounds always suffice; the cap only turns a bug into an error.
     a.round_cap = (uint32_t)((uint64_t)2 * n + 4 < 0xFFFFFFF0u ? 2 * (uint64_t)n + 4 : 0xFFFFFFF0u);

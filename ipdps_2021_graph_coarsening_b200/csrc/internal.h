@@ -114,6 +114,9 @@ int match_map_level(Context &C, const Level &L, int random_level, uint64_t seed,
 // heavy neighbours of a level (hec.cu) and the HEC_V3 mapping built on them
 int hec_hn_level(Context &C, const Level &L, int random_level, uint64_t seed, uint32_t *hn);
 int hec_v3_map_level(Context &C, const Level &L, int random_level, uint64_t seed, uint32_t *vcmap, uint32_t *nc_out);
+int hec_map_from_hn(Context &C, uint32_t n, const uint32_t *hn, uint64_t seed, uint32_t *vcmap, bool prefilled,
+                    uint32_t *nc_out, int *rounds_out);
+int gosh_v2_map_level(Context &C, const Level &L, uint64_t seed, uint32_t *vcmap, uint32_t *nc_out, int *rounds_out);
 int set_map_level(Context &C, const Level &L, bool gosh, uint64_t seed, uint32_t *vcmap, uint32_t *nc_out,
                   int *rounds_out);
 struct PowerIterOpts {

@@ -85,6 +85,8 @@ def lib():
         L.orc_match_map.restype = c_int
         L.orc_hec_v3_map.argtypes = [c_u32, u32p, u32p, u32ref]
         L.orc_hec_v3_map.restype = c_int
+        L.orc_gosh_v2_map.argtypes = [c_u32, u32p, u32p, ctypes.c_void_p, c_u64, u32p, u32ref]
+        L.orc_gosh_v2_map.restype = c_int
         L.orc_set_map.argtypes = [c_u32, u32p, u32p, c_int, c_u64, u32p, u32ref, u32ref]
         L.orc_set_map.restype = c_int
         L.orc_partition_graph.restype = c_int
@@ -246,6 +248,17 @@ def hec_v3_map(row_ptr, col, w, random_level: bool, seed: int):
     vc = np.zeros(max(n, 1), np.uint32)
     nc = ctypes.c_uint32(0)
     lib().orc_hec_v3_map(n, _u32(hn), vc, ctypes.byref(nc))
+    return vc[:n], nc.value
+
+
+def gosh_v2_map(row_ptr, col, w, seed: int):
+    """GOSH_V2 mapping -> (vcmap, nc)."""
+    rp, cl = _u32(row_ptr), _u32(col)
+    n = rp.shape[0] - 1
+    keep, wp = _w64(w)
+    vc = np.zeros(max(n, 1), np.uint32)
+    nc = ctypes.c_uint32(0)
+    lib().orc_gosh_v2_map(n, rp, cl, wp, seed, vc, ctypes.byref(nc))
     return vc[:n], nc.value
 
 

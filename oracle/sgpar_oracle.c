@@ -126,8 +126,11 @@ void orc_hec_heavy(uint32_t n, const uint32_t *row_ptr, const uint32_t *col,
  * coarse numbering does not depend on thread timing (the reference uses an
  * atomic counter, :657).
  * Returns the number of rounds; nc receives the coarse vertex count. */
-int orc_hec_map(uint32_t n, const uint32_t *hn, uint64_t seed,
-                uint32_t *vcmap, uint32_t *nc_out) {
+/* prefilled: vcmap already holds aggregates (members point to their root
+ * vertex, roots to themselves, the rest ORC_UNASSIGNED), as in
+ * parallel_map_construct_prefilled (heuristics.h:378-443) */
+int orc_hec_map_pre(uint32_t n, const uint32_t *hn, uint64_t seed, uint32_t *vcmap, uint32_t *nc_out,
+                    int prefilled) {
     const uint64_t JOIN_KEY = ~0ULL, SELF_KEY = ~0ULL - 1;
     uint64_t *claim[2];
     claim[0] = (uint64_t *)calloc(n ? n : 1, sizeof(uint64_t));
@@ -135,7 +138,10 @@ int orc_hec_map(uint32_t n, const uint32_t *hn, uint64_t seed,
     uint8_t *act = (uint8_t *)malloc(n ? n : 1);
     uint32_t *list = (uint32_t *)malloc((n ? n : 1) * sizeof(uint32_t));
     uint32_t *next = (uint32_t *)malloc((n ? n : 1) * sizeof(uint32_t));
-    for (uint32_t u = 0; u < n; u++) { vcmap[u] = ORC_UNASSIGNED; list[u] = u; }
+    for (uint32_t u = 0; u < n; u++) {
+        if (!prefilled) vcmap[u] = ORC_UNASSIGNED;
+        list[u] = u;
+    }
     uint32_t len = n;
     int swap = 1, round = 0;
     while (1) {
@@ -194,6 +200,10 @@ int orc_hec_map(uint32_t n, const uint32_t *hn, uint64_t seed,
     *nc_out = nc;
     free(rank); free(claim[0]); free(claim[1]); free(act); free(list); free(next);
     return round;
+}
+
+int orc_hec_map(uint32_t n, const uint32_t *hn, uint64_t seed, uint32_t *vcmap, uint32_t *nc_out) {
+    return orc_hec_map_pre(n, hn, seed, vcmap, nc_out, 0);
 }
 
 /* HEC validity (invariant of the serial form, sgpar.h:686-695):
@@ -815,6 +825,46 @@ int orc_hec_v3_map(uint32_t n, const uint32_t *hn, uint32_t *vcmap, uint32_t *nc
     return 0;
 }
 
+/* heuristics.h:444-560 (sgp_coarsen_GOSH_v2) with every step reading a
+ * snapshot of the one before (the reference reads live values, so its
+ * result depends on thread timing): vertices of degree above max(nnz/n, 50)
+ * are roots; the others join their root neighbour of largest edge weight
+ * (the last in row order on a tie, ">="); the rest their aggregated
+ * neighbour of largest degree (last on a tie); the rest their first
+ * aggregated neighbour in row order; what remains goes through the HEC map
+ * rounds with those aggregates prefilled, heavy neighbours by (weight,
+ * tie-break hash) over all neighbours. */
+int orc_gosh_v2_map(uint32_t n, const uint32_t *rp, const uint32_t *col, const uint64_t *w, uint64_t seed,
+                    uint32_t *vcmap, uint32_t *nc_out) {
+    uint64_t thr = n ? (uint64_t)rp[n] / n : 0;
+    if (thr < 50) thr = 50;
+    uint32_t *a = (uint32_t *)malloc(((size_t)n + 1) * sizeof(uint32_t));
+    for (uint32_t u = 0; u < n; u++) a[u] = (uint64_t)(rp[u + 1] - rp[u]) > thr ? u : ORC_UNASSIGNED;
+    for (int mode = 0; mode < 3; mode++) {
+        for (uint32_t u = 0; u < n; u++) {
+            vcmap[u] = a[u];
+            if (a[u] != ORC_UNASSIGNED) continue;
+            uint64_t bk = 0;
+            uint32_t bj = ORC_UNASSIGNED;
+            for (uint32_t j = rp[u]; j < rp[u + 1]; j++) {
+                uint32_t v = col[j];
+                if (a[v] == ORC_UNASSIGNED) continue;
+                if (mode == 2) { bj = j; break; }
+                uint64_t k = mode == 0 ? (w ? w[j] : 1) : (uint64_t)(rp[v + 1] - rp[v]);
+                if (bj == ORC_UNASSIGNED || k >= bk) { bk = k; bj = j; }
+            }
+            if (bj != ORC_UNASSIGNED) vcmap[u] = a[col[bj]];
+        }
+        memcpy(a, vcmap, (size_t)n * sizeof(uint32_t));
+    }
+    free(a);
+    uint32_t *hn = (uint32_t *)malloc(((size_t)n + 1) * sizeof(uint32_t));
+    orc_hec_heavy(n, rp, col, w, 0, seed, hn);
+    orc_hec_map_pre(n, hn, seed, vcmap, nc_out, 1);
+    free(hn);
+    return 0;
+}
+
 typedef struct { int s; uint64_t k; uint32_t i; } orc_tup_t;
 static int orc_tup_gt(orc_tup_t x, orc_tup_t y) {
     return x.s > y.s || (x.s == y.s && (x.k > y.k || (x.k == y.k && x.i > y.i)));
@@ -923,7 +973,7 @@ int orc_partition_graph(uint32_t n, const uint32_t *row_ptr, const uint32_t *col
     const int kind = coarsener & 15;
     L[0].n = n; L[0].rp = (uint32_t *)row_ptr; L[0].col = (uint32_t *)col;
     L[0].w = (uint64_t *)w64; L[0].vcmap = NULL;
-    /* coarsener: 0 HEC, 1 MATCH, 2 MIS2, 3 GOSH, 4 HEC_V3; | 16 no coarsening, | 32 stop
+    /* coarsener: 0 HEC, 1 MATCH, 2 MIS2, 3 GOSH, 4 HEC_V3, 5 GOSH_V2; | 16 no coarsening, | 32 stop
      * after a level keeping more than 0.9 of the vertices (sgpar.h:2466-2475) */
     while (!(coarsener & 16) && L[nl - 1].n > cutoff) {
         orc_level_t *f = &L[nl - 1];
@@ -939,6 +989,8 @@ int orc_partition_graph(uint32_t n, const uint32_t *row_ptr, const uint32_t *col
             free(hn);
         } else if (kind == 1) {
             orc_match_map(f->n, f->rp, f->col, f->w, random_level, seed, f->vcmap, &nc, &rounds);
+        } else if (kind == 5) {
+            orc_gosh_v2_map(f->n, f->rp, f->col, f->w, seed, f->vcmap, &nc);
         } else if (kind == 4) {
             uint32_t *hn = (uint32_t *)malloc((size_t)f->n * sizeof(uint32_t));
             orc_hec_heavy(f->n, f->rp, f->col, f->w, random_level, seed, hn);

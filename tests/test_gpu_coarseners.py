@@ -71,6 +71,16 @@ def test_hec_v3_map_bit_exact(partitioner, name, random_level):
     assert nc == onc and np.array_equal(vc.cpu().numpy().view(np.uint32), ovc)
 
 
+@pytest.mark.parametrize("name", sorted(CASES))
+def test_gosh_v2_map_bit_exact(partitioner, name):
+    g = CASES[name]
+    rp, col, w = dev(g)
+    seed = 0x77AB
+    vc, nc, _ = partitioner.coarsen_map(rp, col, w, L.COARSEN_GOSH_V2, False, seed)
+    ovc, onc = O.gosh_v2_map(g.row_ptr, g.col, g.w, seed)
+    assert nc == onc and np.array_equal(vc.cpu().numpy().view(np.uint32), ovc)
+
+
 def test_coarsen_map_rejects_hec(partitioner):
     rp, col, _ = dev(CASES["grid"])
     with pytest.raises(L.SgparError):
@@ -83,6 +93,7 @@ def cut_of(g, labels):
 
 
 @pytest.mark.parametrize("coarsener", [L.COARSEN_MATCH, L.COARSEN_MIS2, L.COARSEN_GOSH, L.COARSEN_HEC_V3,
+                                       L.COARSEN_GOSH_V2,
                                        L.COARSEN_MATCH | L.COARSEN_RATIO_STOP, L.COARSEN_NONE])
 @pytest.mark.parametrize("name", ["holes", "rmat14", "er_small"])
 def test_partition_with_coarsener(partitioner, coarsener, name):

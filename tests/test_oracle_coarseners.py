@@ -174,3 +174,22 @@ def test_hec_v3_aggregates(name, random_level):
     assert np.all(vc[mutual] == vc[hn[mutual]])
     roots = (mutual & (np.arange(n) < hn)) | (targeted & ~mutual)
     assert nc == int(roots.sum())
+
+
+@pytest.mark.parametrize("name", sorted(CASES))
+def test_gosh_v2_aggregates(name):
+    """heuristics.h:444-560: vertices above max(nnz / n, 50) degree are
+    roots of their own aggregates, every vertex ends in an aggregate with a
+    neighbour or alone, and the mapping is onto."""
+    g = CASES[name]
+    vc, nc = O.gosh_v2_map(g.row_ptr, g.col, g.w, seed=31)
+    assert sorted(set(vc.tolist())) == list(range(nc))
+    deg = np.diff(g.row_ptr).astype(np.int64)
+    thr = max(int(g.row_ptr[-1]) // g.n, 50)
+    big = np.flatnonzero(deg > thr)
+    assert len(set(vc[big].tolist())) == len(big)   # one root per aggregate
+    r = rows(g)
+    same = np.zeros(g.n, bool)
+    same[r[vc[r] == vc[g.col]]] = True
+    sizes = np.bincount(vc, minlength=nc)
+    assert np.all(same | (sizes[vc] == 1))
