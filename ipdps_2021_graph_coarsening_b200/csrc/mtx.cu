@@ -51,6 +51,7 @@
 //      the keep flags, so rows stay sorted.
 #include <stdlib.h>
 #include <string.h>
+#include <sys/mman.h>
 #include <sys/stat.h>
 
 #include <unistd.h>
@@ -726,6 +727,18 @@ static int fetch_line(Context &C, MtxSource &src, const uint8_t *dtext, uint64_t
     return SGP_B200_OK;
 }
 
+// Host arrays the caller frees with free(): large ones 2 MiB aligned and
+// advised for transparent huge pages, so that the first touch by the copy-out
+// faults once per 2 MiB instead of once per 4 KiB page.
+static void *host_alloc_large(size_t bytes) {
+    const size_t huge = (size_t)2 << 20;
+    if (bytes < 4 * huge) return malloc(bytes);
+    const size_t rounded = (bytes + huge - 1) / huge * huge;
+    void *p = aligned_alloc(huge, rounded);
+    if (p) madvise(p, rounded, MADV_HUGEPAGE);   // advisory: ignored where huge pages are off
+    return p;
+}
+
 static double now_ms() {
     return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now().time_since_epoch()).count();
 }
@@ -751,8 +764,8 @@ static int copy_out(Context &C, uint32_t n, uint64_t m, const uint32_t *rp, cons
             return SGP_B200_ERR_DEVICE;
         }
     } else {
-        orp = (uint32_t *)malloc(brp);
-        ocol = (uint32_t *)malloc(bcol);
+        orp = (uint32_t *)host_alloc_large(brp);
+        ocol = (uint32_t *)host_alloc_large(bcol);
         if (!orp || !ocol) {
             free(orp);
             free(ocol);

@@ -1,0 +1,50 @@
+"""The edge-case graphs (a single vertex, a single edge, two components, a long
+path, a star, a complete graph, an odd cycle) through the alternative
+coarseners, the local search and FM: the device path against the oracle
+(hierarchies, rng advance and FM moves exactly; local search bit-exact against
+the reference's own build where it is present)."""
+import numpy as np
+import pytest
+
+from ipdps_2021_graph_coarsening_b200 import _lib as L
+from ipdps_2021_graph_coarsening_b200 import api
+from oracle import bindings as O
+from tests.test_gpu_edge_cases import CASES, cut_of
+
+pytestmark = pytest.mark.gpu
+
+COARSENERS = [L.COARSEN_MATCH, L.COARSEN_MIS2, L.COARSEN_GOSH, L.COARSEN_HEC_V3, L.COARSEN_GOSH_V2]
+
+
+@pytest.mark.parametrize("name", sorted(CASES))
+@pytest.mark.parametrize("coarsener", COARSENERS)
+def test_coarseners_on_edge_cases(partitioner, name, coarsener):
+    g = CASES[name]()
+    o = O.partition_graph(g.row_ptr, g.col, None, rng_state=13, coarsener=coarsener)
+    r = partitioner.partition(g, rng_state=13, coarsener=coarsener)
+    assert r.level_n == o["level_n"] and r.rng_state == o["rng_state"]
+    part = np.asarray(r.part)
+    assert int((part == 0).sum()) in (g.n // 2, (g.n + 1) // 2)
+    assert r.edgecut == cut_of(g, part)
+
+
+@pytest.mark.parametrize("name", sorted(CASES))
+def test_fm_on_edge_cases(partitioner, name):
+    g = CASES[name]()
+    base = partitioner.partition(g, rng_state=13)
+    r = partitioner.partition(g, rng_state=13, fm_passes=8)
+    op, oc, opasses, omoves = O.fm_refine(g.row_ptr, g.col, None, np.asarray(base.part), 8)
+    assert np.array_equal(np.asarray(r.part), op) and r.edgecut == oc == cut_of(g, np.asarray(r.part))
+    assert r.edgecut <= base.edgecut and (r.fm_passes, r.fm_moves) == (opasses, omoves)
+
+
+@pytest.mark.parametrize("name", sorted(CASES))
+def test_local_search_on_edge_cases(name):
+    g = CASES[name]()
+    ev = O.partition_graph(g.row_ptr, g.col, None, rng_state=13)["evec"]
+    part, cut = api.compute_partition(ev, g, 2, 0, local_search_alg=1)
+    op, oc, _ = O.compute_partition_ls(g.row_ptr, g.col, ev)
+    assert np.array_equal(part, op) and cut == oc == cut_of(g, part)
+    if O.ref_available("serial"):
+        rp, rc = O.ref_compute_partition_ls(g.row_ptr, g.col, ev)
+        assert np.array_equal(part, rp) and cut == rc
