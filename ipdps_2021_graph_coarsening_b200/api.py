@@ -194,6 +194,28 @@ class _DevArray:
         self.__cuda_array_interface__ = {"shape": (n,), "typestr": typestr, "data": (ptr, False), "version": 3}
 
 
+class _GraphOwner:
+    """Frees a library-allocated graph (sgp_b200_graph_free) when the last
+    view of it goes away."""
+
+    def __init__(self, g: L.sgp_b200_graph_t):
+        self.g = g
+
+    def __del__(self):
+        try:
+            L.lib().sgp_b200_graph_free(ctypes.byref(self.g))
+        except Exception:
+            pass
+
+
+class _OwnedDevArray:
+    """__cuda_array_interface__ view (int32) that keeps its owner alive."""
+
+    def __init__(self, ptr: int, n: int, owner: _GraphOwner):
+        self.owner = owner
+        self.__cuda_array_interface__ = {"shape": (n,), "typestr": "<i4", "data": (ptr, False), "version": 3}
+
+
 def _dptr(t) -> Optional[int]:
     return None if t is None else int(t.data_ptr())
 
@@ -468,23 +490,23 @@ class Partitioner:
                                           ctypes.byref(info))
             where = "sgp_b200_mtx_read"
         L.check(rc, where)
+        n, m = out.n, out.m
+        if device_out:
+            # zero copy: the tensors share the library's allocation, which is
+            # released when both are gone
+            import torch
+            owner = _GraphOwner(out)
+            rp = torch.as_tensor(_OwnedDevArray(out.row_ptr, n + 1, owner), device="cuda")
+            col = torch.as_tensor(_OwnedDevArray(out.col, m, owner), device="cuda") if m else \
+                torch.zeros(0, dtype=torch.int32, device="cuda")
+            return (rp, col), _mtx_info(info)
         try:
-            n, m = out.n, out.m
-            if device_out:
-                import torch
-                rp = torch.as_tensor(_DevArray(out.row_ptr, n + 1, "<i4"), device="cuda").clone()
-                col = torch.as_tensor(_DevArray(out.col, m, "<i4"), device="cuda").clone() if m else \
-                    torch.zeros(0, dtype=torch.int32, device="cuda")
-                torch.cuda.synchronize()
-                g = (rp, col)
-            else:
-                rp = np.ctypeslib.as_array(ctypes.cast(out.row_ptr, _u32p), shape=(n + 1,)).copy()
-                col = np.ctypeslib.as_array(ctypes.cast(out.col, _u32p), shape=(m,)).copy() if m else \
-                    np.zeros(0, dtype=np.uint32)
-                g = CSR(rp, col)
+            rp = np.ctypeslib.as_array(ctypes.cast(out.row_ptr, _u32p), shape=(n + 1,)).copy()
+            col = np.ctypeslib.as_array(ctypes.cast(out.col, _u32p), shape=(m,)).copy() if m else \
+                np.zeros(0, dtype=np.uint32)
         finally:
             L.lib().sgp_b200_graph_free(ctypes.byref(out))
-        return g, _mtx_info(info)
+        return CSR(rp, col), _mtx_info(info)
 
     def mtx2csr(self, mtx_path: str, csr_path: str, id_bytes: int = 4) -> dict:
         """The reference command ``mtx2csr <MM file> <binary CSR file>``
