@@ -6,7 +6,8 @@
 // there) orders moves through atomics and picks the best prefix with a
 // non-associative scan.  This pass keeps fm_refine_par's structure with
 // deterministic rules (oracle/sgpar_oracle.c orc_fm_refine restates them):
-//   1. gain(u) = sum of w over neighbours across the cut minus those inside;
+//   1. gain(u) = neighbours across the cut minus those inside (the finest
+//      level's edges all weigh 1);
 //   2. each side's positive-gain vertices ordered by (gain clamped to
 //      kFmBuckets - 1 descending, id ascending) -- a stable counting sort of
 //      the id-ordered candidates;
@@ -36,10 +37,13 @@ constexpr int kFmBuckets = 1024;
 constexpr uint32_t kFmNone = 0xFFFFFFFFu;
 constexpr int kFmTile = 1024;   // candidates per block in the counting sort
 
-// gains, candidate flags, cut and balance
-template <int G, typename W>
+// gains, candidate flags, cut and balance.  Unit edge weights (the finest
+// level): a symmetric graph with fewer than 2^32 directed entries has every
+// degree below 2^31, so 32-bit sums are exact.  G lanes per row, four
+// entries per lane in flight (destinations, then the part gathers).
+template <int G>
 __global__ void __launch_bounds__(256) k_fm_gain(uint32_t n, const uint32_t *__restrict__ rp,
-                                                 const uint32_t *__restrict__ col, const W *__restrict__ w,
+                                                 const uint32_t *__restrict__ col,
                                                  const uint32_t *__restrict__ part, long long *__restrict__ gain,
                                                  uint8_t *__restrict__ f0, uint8_t *__restrict__ f1,
                                                  unsigned long long *__restrict__ sums /* [0] 2 cut, [1] bal */) {
@@ -49,28 +53,25 @@ __global__ void __launch_bounds__(256) k_fm_gain(uint32_t n, const uint32_t *__r
     unsigned long long cut2 = 0;
     long long bal = 0;
     for (uint64_t u = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) / G; u < n; u += ng) {
-        const uint32_t pu = part[u];
-        long long g = 0;
-        unsigned long long c = 0;
-        for (uint32_t j = rp[u] + lane; j < rp[u + 1]; j += G) {
-            const long long x = (long long)wload(w, j);
-            if (part[__ldg(col + j)] != pu) {
-                g += x;
-                c += (unsigned long long)x;
-            } else {
-                g -= x;
-            }
-        }
+        const uint32_t pu = __ldg(part + u);
+        const uint32_t b = __ldg(rp + u), e = __ldg(rp + u + 1);
+        int across = 0;
+        for (uint32_t j0 = b + lane; j0 < e; j0 += 4 * G) {
+            uint32_t v[4];
 #pragma unroll
-        for (int o = G / 2; o > 0; o >>= 1) {
-            g += __shfl_xor_sync(gm, g, o);
-            c += __shfl_xor_sync(gm, c, o);
+            for (int q = 0; q < 4; q++) v[q] = j0 + q * G < e ? __ldg(col + j0 + q * G) : 0xFFFFFFFFu;
+#pragma unroll
+            for (int q = 0; q < 4; q++)
+                if (v[q] != 0xFFFFFFFFu) across += __ldg(part + v[q]) != pu;
         }
+        across = group_sum<G>(across);
         if (lane == 0) {
+            const int deg = (int)(e - b);
+            const int g = 2 * across - deg;   // across minus inside
             gain[u] = g;
             f0[u] = pu == 0 && g > 0;
             f1[u] = pu != 0 && g > 0;
-            cut2 += c;
+            cut2 += (unsigned)across;
             bal += pu == 0 ? 1 : -1;
         }
     }
@@ -174,28 +175,32 @@ __global__ void k_fm_interleave(uint32_t na, uint32_t nb, const uint32_t *__rest
     }
 }
 
-// sequential gain of the i-th move
-template <int G, typename W>
+// sequential gain of the i-th move (unit weights, 32-bit sums as above)
+template <int G>
 __global__ void __launch_bounds__(256) k_fm_seqgain(uint32_t k, const uint32_t *__restrict__ rp,
-                                                    const uint32_t *__restrict__ col, const W *__restrict__ w,
+                                                    const uint32_t *__restrict__ col,
                                                     const uint32_t *__restrict__ part,
                                                     const uint32_t *__restrict__ order,
                                                     const uint32_t *__restrict__ rank, long long *__restrict__ gseq) {
-    const unsigned gm = group_mask<G>();
     const uint32_t lane = threadIdx.x & (G - 1);
     const uint64_t ng = ((uint64_t)gridDim.x * blockDim.x) / G;
     for (uint64_t i = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) / G; i < k; i += ng) {
-        const uint32_t u = order[i], pu = part[u];
-        long long g = 0;
-        for (uint32_t j = rp[u] + lane; j < rp[u + 1]; j += G) {
-            const uint32_t v = __ldg(col + j);
-            const long long x = (long long)wload(w, j);
-            const bool across = part[v] != pu, moved = rank[v] < (uint32_t)i;
-            g += (across != moved) ? x : -x;
-        }
+        const uint32_t u = __ldg(order + i), pu = __ldg(part + u);
+        const uint32_t b = __ldg(rp + u), e = __ldg(rp + u + 1);
+        int plus = 0;   // neighbours counting +1: across xor moved before
+        for (uint32_t j0 = b + lane; j0 < e; j0 += 4 * G) {
+            uint32_t v[4];
 #pragma unroll
-        for (int o = G / 2; o > 0; o >>= 1) g += __shfl_xor_sync(gm, g, o);
-        if (lane == 0) gseq[i] = g;
+            for (int q = 0; q < 4; q++) v[q] = j0 + q * G < e ? __ldg(col + j0 + q * G) : 0xFFFFFFFFu;
+#pragma unroll
+            for (int q = 0; q < 4; q++) {
+                if (v[q] == 0xFFFFFFFFu) continue;
+                const bool across = __ldg(part + v[q]) != pu, moved = __ldg(rank + v[q]) < (uint32_t)i;
+                plus += across != moved;
+            }
+        }
+        plus = group_sum<G>(plus);
+        if (lane == 0) gseq[i] = 2 * plus - (int)(e - b);
     }
 }
 
@@ -315,7 +320,7 @@ static int fm_impl(Context &C, const Level &L, const W *w, uint32_t *part, uint3
     uint32_t pass = 0;
     for (; pass < max_passes; pass++) {
         SGPB_TRY(dzero(C, sums, 2 * sizeof(unsigned long long)));
-#define SGPB_FMG(G) k_fm_gain<G, W><<<fm_grid(C, (uint64_t)n * G), 256, 0, C.stream>>>(n, L.rp, L.col, w, part, gain, f0, f1, sums)
+#define SGPB_FMG(G) k_fm_gain<G><<<fm_grid(C, (uint64_t)n * G), 256, 0, C.stream>>>(n, L.rp, L.col, part, gain, f0, f1, sums)
         if (avg <= 4) SGPB_FMG(4);
         else if (avg <= 16) SGPB_FMG(16);
         else SGPB_FMG(32);
@@ -346,7 +351,7 @@ static int fm_impl(Context &C, const Level &L, const W *w, uint32_t *part, uint3
         SGPB_CUDA(cudaMemsetAsync(rank, 0xFF, sizeof(uint32_t) * n, C.stream));
         k_fm_interleave<<<fm_grid(C, na > nb ? na : nb), 256, 0, C.stream>>>(na, nb, sa, sb, gain, bal0, order, rank,
                                                                              side);
-#define SGPB_FMS(G) k_fm_seqgain<G, W><<<fm_grid(C, (uint64_t)k * G), 256, 0, C.stream>>>(k, L.rp, L.col, w, part, order, rank, gseq)
+#define SGPB_FMS(G) k_fm_seqgain<G><<<fm_grid(C, (uint64_t)k * G), 256, 0, C.stream>>>(k, L.rp, L.col, part, order, rank, gseq)
         if (avg <= 4) SGPB_FMS(4);
         else if (avg <= 16) SGPB_FMS(16);
         else SGPB_FMS(32);
