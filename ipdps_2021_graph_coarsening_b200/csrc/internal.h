@@ -155,5 +155,14 @@ int induced_subgraphs(Context &C, const Level &L, const uint32_t *part, Level *g
 // their multiplicities in tw (build.cu)
 int dedupe_buckets_unit(Context &C, uint32_t nc, const uint32_t *boff, uint32_t *bdst, uint32_t *tw,
                         uint32_t *dcnt);
+// stable LSD radix sort by the low `bits` bits of 64-bit keys, 8 bits per
+// pass, optional payload; tmp buffers hold n entries; *in_tmp: the result is
+// in the tmp buffers (sort.cu)
+int radix_sort_keys(Context &C, unsigned long long *keys, uint64_t n, int bits, unsigned long long *keys_tmp,
+                    bool *in_tmp);
+int radix_sort_pairs_u32(Context &C, unsigned long long *keys, uint32_t *vals, uint64_t n, int bits,
+                         unsigned long long *keys_tmp, uint32_t *vals_tmp, bool *in_tmp);
+int radix_sort_pairs_u64(Context &C, unsigned long long *keys, unsigned long long *vals, uint64_t n, int bits,
+                         unsigned long long *keys_tmp, unsigned long long *vals_tmp, bool *in_tmp);
 
 }  // namespace sgpb

@@ -75,6 +75,7 @@ constexpr int kMtxThreads = 256;
 constexpr int kMtxBytes = 32;                                   // bytes per thread
 constexpr uint64_t kMtxTile = (uint64_t)kMtxThreads * kMtxBytes;  // bytes per block
 constexpr uint32_t kNoEdge = 0xFFFFFFFFu;
+constexpr unsigned long long kNoKey = ~0ull;   // sorts after every entry key
 constexpr int kMaxBanners = 16;
 constexpr int kStageSlots = 4;
 constexpr size_t kStageSlotBytes = (size_t)32 << 20;
@@ -132,8 +133,9 @@ struct MtxParse {
     uint32_t rows, cols;         // bounds of the two ids
     uint32_t shift;              // bipartite: row id i is vertex cols + i - 1; else 0
     int drop_loops;
-    uint32_t *eu, *ev;           // per line; kNoEdge when the line adds nothing
-    uint32_t *deg;
+    unsigned long long *keys;    // per line two keys, (u << b | v) and (v << b | u), kNoKey when it adds nothing
+    int b;                       // bits per id in a key
+    uint32_t *valid;             // lines that add an entry
     unsigned long long *err;     // min over failing lines of (line << 8 | reason)
     unsigned long long *banner;  // [0] count, [1..kMaxBanners] offsets of banner lines
 };
@@ -203,67 +205,51 @@ __global__ void __launch_bounds__(kMtxThreads) k_mtx_parse(MtxParse a) {
     const uint32_t mine = __popc(m);
     uint64_t tot;
     uint32_t k = a.tile_base[blockIdx.x] + (uint32_t)(block_scan_u64(mine, sm, &tot) - mine);
-    // one line per lane per round, so the degree atomics aggregate over the warp
-    const uint32_t rounds = warp_max(mine);
-    for (uint32_t r = 0; r < rounds; r++) {
+    uint32_t valid = 0;
+    while (m) {
+        const int b = __ffs(m) - 1;
+        m &= m - 1;
         uint32_t u = kNoEdge, v = kNoEdge;
-        if (m) {
-            const int b = __ffs(m) - 1;
-            m &= m - 1;
-            parse_line(a, base + b + 1, k, u, v);
-            a.eu[k] = u;
-            a.ev[k] = v;
-            k++;
-        }
-        add_one(a.deg, u);
-        add_one(a.deg, v);
-    }
-}
-
-// Slot boff[x] + (rank among this call's x in the bucket), one atomic per
-// distinct x in the warp.  All 32 lanes must call it.
-__device__ __forceinline__ uint32_t bucket_slot(uint32_t x, const uint32_t *__restrict__ boff, uint32_t *fill) {
-    const unsigned lane = threadIdx.x & 31;
-    const unsigned act = __ballot_sync(0xFFFFFFFFu, x != kNoEdge);
-    uint32_t slot = 0;
-    if (x != kNoEdge) {
-        const unsigned peers = __match_any_sync(act, x);
-        const int leader = __ffs(peers) - 1;
-        uint32_t b = 0;
-        if ((int)lane == leader) b = atomicAdd(fill + x, (uint32_t)__popc(peers));
-        b = __shfl_sync(peers, b, leader);
-        slot = __ldg(boff + x) + b + __popc(peers & ((1u << lane) - 1u));
-    }
-    return slot;
-}
-
-__global__ void __launch_bounds__(256) k_mtx_scatter(uint32_t nl, const uint32_t *__restrict__ eu,
-                                                     const uint32_t *__restrict__ ev,
-                                                     const uint32_t *__restrict__ boff, uint32_t *__restrict__ fill,
-                                                     uint32_t *__restrict__ bdst) {
-    const unsigned lane = threadIdx.x & 31;
-    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
-    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i - lane < nl; i += stride) {
-        const uint32_t u = i < nl ? __ldg(eu + i) : kNoEdge;
-        const uint32_t v = i < nl ? __ldg(ev + i) : kNoEdge;   // kNoEdge together with u
-        const uint32_t su = bucket_slot(u, boff, fill);
-        const uint32_t sv = bucket_slot(v, boff, fill);
+        parse_line(a, base + b + 1, k, u, v);
+        unsigned long long k0 = kNoKey, k1 = kNoKey;
         if (u != kNoEdge) {
-            bdst[su] = v;
-            bdst[sv] = u;
+            k0 = ((unsigned long long)u << a.b) | v;
+            k1 = ((unsigned long long)v << a.b) | u;
+            valid++;
         }
+        reinterpret_cast<ulonglong2 *>(a.keys)[k] = make_ulonglong2(k0, k1);
+        k++;
     }
+    valid = warp_sum(valid);
+    if ((threadIdx.x & 31) == 0 && valid) atomicAdd(a.valid, valid);
 }
 
-// bucket heads (sorted, distinct) -> contiguous rows
-__global__ void __launch_bounds__(256) k_mtx_compact(uint32_t n, const uint32_t *__restrict__ boff,
-                                                     const uint32_t *__restrict__ rp,
-                                                     const uint32_t *__restrict__ bdst, uint32_t *__restrict__ col) {
+// Sorted keys -> CSR: a key that differs from its predecessor starts a run
+// (duplicates merged); heads are numbered by a scan, and since the keys are
+// sorted by (row, column) the heads are the CSR entries in order.
+__global__ void __launch_bounds__(256) k_mtx_heads(uint64_t cnt, const unsigned long long *__restrict__ keys,
+                                                   uint32_t *__restrict__ head) {
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < cnt; i += stride)
+        head[i] = i == 0 || __ldg(keys + i) != __ldg(keys + i - 1);
+}
+
+// col[pos] = the head's column; rows[row] counts heads (one atomic per run of
+// equal rows within a warp: the keys are sorted)
+__global__ void __launch_bounds__(256) k_mtx_emit(uint64_t cnt, const unsigned long long *__restrict__ keys,
+                                                  const uint32_t *__restrict__ head, const uint32_t *__restrict__ pos,
+                                                  int b, uint32_t *__restrict__ col, uint32_t *__restrict__ rows) {
     const unsigned lane = threadIdx.x & 31;
-    const uint64_t nw = ((uint64_t)gridDim.x * blockDim.x) >> 5;
-    for (uint64_t r = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; r < n; r += nw) {
-        const uint32_t src = boff[r], dst = rp[r], len = rp[r + 1] - dst;
-        for (uint32_t i = lane; i < len; i += 32) col[dst + i] = __ldg(bdst + src + i);
+    const unsigned long long mask = (1ull << b) - 1;
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i - lane < cnt; i += stride) {
+        uint32_t r = kNoEdge;
+        if (i < cnt && head[i]) {
+            const unsigned long long k = __ldg(keys + i);
+            col[pos[i]] = (uint32_t)(k & mask);
+            r = (uint32_t)(k >> b);
+        }
+        add_one(rows, r);
     }
 }
 
@@ -872,10 +858,15 @@ static int mtx_impl(Context &C, MtxSource &src, int out_mem, sgp_b200_graph_t *o
     SGPB_CUDA(cudaEventRecord(ev[0], C.stream));
 
     // 2-3. line starts, parse, degrees
-    uint32_t *deg, *eu = nullptr, *ev_ = nullptr;
+    // key layout: b = bit length of n, so every id (< n <= 2^b - 1) and every
+    // key stays below kNoKey in the sorted 2b bits
+    int kb = 1;
+    while (kb < 32 && ((uint64_t)1 << kb) <= (uint64_t)n) kb++;
+    unsigned long long *keys = nullptr;
+    uint32_t *valid;
+    SGPB_TRY(dalloc_t(C, &valid, 1));
+    SGPB_TRY(dzero(C, valid, 4));
     unsigned long long *flags;   // [0] err, [1] banner count, [2..] banner offsets
-    SGPB_TRY(dalloc_t(C, &deg, (size_t)n + 1));
-    SGPB_TRY(dzero(C, deg, sizeof(uint32_t) * ((size_t)n + 1)));
     SGPB_TRY(dalloc_t(C, &flags, 2 + kMaxBanners));
     SGPB_TRY(dzero(C, flags, sizeof(unsigned long long) * (2 + kMaxBanners)));
     SGPB_CUDA(cudaMemsetAsync(flags, 0xFF, sizeof(unsigned long long), C.stream));
@@ -897,8 +888,11 @@ static int mtx_impl(Context &C, MtxSource &src, int out_mem, sgp_b200_graph_t *o
             return SGP_B200_ERR_TOO_LARGE;
         }
         SGPB_TRY(read_u32(C, tbase + ntiles, &nl));
-        SGPB_TRY(dalloc_t(C, &eu, (size_t)nl + 1));
-        SGPB_TRY(dalloc_t(C, &ev_, (size_t)nl + 1));
+        if ((uint64_t)nl * 2 >= 0xFFFFFFFFull) {
+            set_error("more than 2^32 - 1 directed entries");
+            return SGP_B200_ERR_TOO_LARGE;
+        }
+        SGPB_TRY(dalloc_t(C, &keys, (size_t)2 * nl + 2));
         MtxParse a;
         a.s = s;
         a.tile_base = tbase;
@@ -906,9 +900,9 @@ static int mtx_impl(Context &C, MtxSource &src, int out_mem, sgp_b200_graph_t *o
         a.cols = (uint32_t)h.cols;
         a.shift = (uint32_t)shift;
         a.drop_loops = drop_loops;
-        a.eu = eu;
-        a.ev = ev_;
-        a.deg = deg;
+        a.keys = keys;
+        a.b = kb;
+        a.valid = valid;
         a.err = flags;
         a.banner = flags + 1;
         k_mtx_parse<<<(uint32_t)ntiles, kMtxThreads, 0, C.stream>>>(a);
@@ -941,42 +935,36 @@ static int mtx_impl(Context &C, MtxSource &src, int out_mem, sgp_b200_graph_t *o
     I.lines = nl;
     SGPB_CUDA(cudaEventRecord(ev[1], C.stream));
 
-    // 4. rows: bucket scatter, sort + merge, compaction
-    uint32_t *boff, *fill, *ovf2;
-    SGPB_TRY(dalloc_t(C, &boff, (size_t)n + 1));
-    SGPB_TRY(dalloc_t(C, &fill, (size_t)n + 1));
-    SGPB_TRY(dalloc_t(C, &ovf2, 1));
-    SGPB_TRY(dzero(C, fill, sizeof(uint32_t) * ((size_t)n + 1)));
-    SGPB_TRY(dzero(C, ovf2, 4));
-    SGPB_TRY(scan_u32(C, deg, boff, n, ovf2));
-    uint32_t tot[2];
-    SGPB_TRY(read_u32(C, ovf2, &tot[0]));
-    SGPB_TRY(read_u32(C, boff + n, &tot[1]));
-    if (tot[0]) {
-        set_error("more than 2^32 - 1 directed entries");
-        return SGP_B200_ERR_TOO_LARGE;
-    }
-    const uint32_t raw = tot[1];
-    uint32_t *bdst, *tw, *dcnt, *rp, *col;
-    SGPB_TRY(dalloc_t(C, &bdst, (size_t)raw + 1));
-    SGPB_TRY(dalloc_t(C, &tw, (size_t)raw + 1));
-    SGPB_TRY(dalloc_t(C, &dcnt, (size_t)n + 1));
-    if (raw) {
-        k_mtx_scatter<<<grid_for(C, nl, 256), 256, 0, C.stream>>>(nl, eu, ev_, boff, fill, bdst);
-        SGPB_CUDA(cudaGetLastError());
-        C.kernel_launches++;
-    }
-    SGPB_TRY(dedupe_buckets_unit(C, n, boff, bdst, tw, dcnt));
+    // 4. rows: one radix sort of all keys (the kNoKey of skipped lines sort
+    // last and are cut off), then run heads
+    uint32_t nvalid = 0;
+    SGPB_TRY(read_u32(C, valid, &nvalid));
+    const uint64_t cnt = 2ull * nvalid;
+    uint32_t *rp, *col, *rows;
     SGPB_TRY(dalloc_t(C, &rp, (size_t)n + 1));
-    SGPB_TRY(scan_u32(C, dcnt, rp, n, nullptr));
+    SGPB_TRY(dalloc_t(C, &rows, (size_t)n + 1));
+    SGPB_TRY(dzero(C, rows, sizeof(uint32_t) * ((size_t)n + 1)));
     uint32_t m_all = 0;
-    SGPB_TRY(read_u32(C, rp + n, &m_all));
-    SGPB_TRY(dalloc_t(C, &col, (size_t)m_all + 1));
-    if (n && m_all) {
-        k_mtx_compact<<<grid_for(C, (uint64_t)n * 32, 256), 256, 0, C.stream>>>(n, boff, rp, bdst, col);
+    if (cnt) {
+        unsigned long long *tmp;
+        SGPB_TRY(dalloc_t(C, &tmp, (size_t)2 * nl + 2));
+        bool in_tmp = false;
+        SGPB_TRY(radix_sort_keys(C, keys, 2ull * nl, 2 * kb, tmp, &in_tmp));
+        const unsigned long long *sk = in_tmp ? tmp : keys;
+        uint32_t *head, *pos;
+        SGPB_TRY(dalloc_t(C, &head, (size_t)cnt + 1));
+        SGPB_TRY(dalloc_t(C, &pos, (size_t)cnt + 1));
+        k_mtx_heads<<<grid_for(C, cnt, 256), 256, 0, C.stream>>>(cnt, sk, head);
+        SGPB_TRY(scan_u32(C, head, pos, (uint32_t)cnt, nullptr));
+        SGPB_TRY(read_u32(C, pos + cnt, &m_all));
+        SGPB_TRY(dalloc_t(C, &col, (size_t)m_all + 1));
+        k_mtx_emit<<<grid_for(C, cnt, 256), 256, 0, C.stream>>>(cnt, sk, head, pos, kb, col, rows);
         SGPB_CUDA(cudaGetLastError());
-        C.kernel_launches++;
+        C.kernel_launches += 2;
+    } else {
+        SGPB_TRY(dalloc_t(C, &col, 1));
     }
+    SGPB_TRY(scan_u32(C, rows, rp, n, nullptr));
     I.m_all = m_all;
     SGPB_CUDA(cudaEventRecord(ev[2], C.stream));
 
