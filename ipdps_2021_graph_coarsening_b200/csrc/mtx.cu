@@ -31,10 +31,11 @@
 //      thread, '\n' found with a SIMD byte compare) and the tile counts
 //      scanned;
 //   3. one pass parses every line -- line index = tile base + block prefix --
-//      into an endpoint pair and counts degrees with warp-aggregated atomics
-//      (files sorted by row or column repeat ids within a warp);
-//   4. a bucket scatter places both directions of every entry, the coarse
-//      build's sort + merge tiers sort each row and drop duplicates;
+//      into the two packed keys (u << b | v) and (v << b | u) of its entry;
+//   4. one stable radix sort of all keys (sort.cu) groups every row's
+//      entries in column order; the first key of each run of equal keys is
+//      a distinct entry, and the heads, numbered by a scan, are the CSR
+//      columns in order;
 //   5. a lock-free union-find labels components by their smallest vertex: a
 //      union hooks the larger of two roots under the smaller with a CAS,
 //      finds halve paths, and parent[x] <= x always holds, so every walk
