@@ -692,9 +692,4 @@ int build_coarse_into(Context &C, const Level &F, const uint32_t *vcmap, uint32_
     return build_impl<uint32_t, uint32_t>(C, F, (const uint32_t *)F.w, vcmap, nc, crp, &ccol, &w4, m_c, false);
 }
 
-int dedupe_buckets_unit(Context &C, uint32_t nc, const uint32_t *boff, uint32_t *bdst, uint32_t *tw,
-                        uint32_t *dcnt) {
-    return dedupe_buckets<uint32_t, uint32_t>(C, nc, boff, bdst, nullptr, tw, dcnt);
-}
-
 }  // namespace sgpb

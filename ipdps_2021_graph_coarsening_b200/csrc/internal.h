@@ -150,11 +150,6 @@ int count_part0(Context &C, const uint32_t *part, uint32_t n, uint32_t *out);
 // map0 / map1 (optional): vertex i of L -> its id in g1 (part 0) / g2
 int induced_subgraphs(Context &C, const Level &L, const uint32_t *part, Level *g1, Level *g2,
                       uint32_t **map0 = nullptr, uint32_t **map1 = nullptr);
-// sort + merge of unweighted buckets [boff[r], boff[r+1]) of bdst, r < nc:
-// the dcnt[r] distinct destinations of bucket r land ascending at its head,
-// their multiplicities in tw (build.cu)
-int dedupe_buckets_unit(Context &C, uint32_t nc, const uint32_t *boff, uint32_t *bdst, uint32_t *tw,
-                        uint32_t *dcnt);
 // stable LSD radix sort by the low `bits` bits of 64-bit keys, 8 bits per
 // pass, optional payload; tmp buffers hold n entries; *in_tmp: the result is
 // in the tmp buffers (sort.cu)

@@ -41,8 +41,11 @@ __global__ void __launch_bounds__(kRsThreads) k_rs_hist(const unsigned long long
     for (int b = threadIdx.x; b < kRsBins; b += blockDim.x) hist[(size_t)b * ntiles + blockIdx.x] = cnt[b];
 }
 
+// three blocks per SM (40 registers, a few spilled): more warps in flight for
+// the per-warp ranking chains beat spill-free code at two blocks (rows phase of
+// the converter 11.9 -> 10.3 ms on R-MAT 22)
 template <typename V>
-__global__ void __launch_bounds__(kRsThreads) k_rs_scatter(const unsigned long long *__restrict__ keys,
+__global__ void __launch_bounds__(kRsThreads, 3) k_rs_scatter(const unsigned long long *__restrict__ keys,
                                                            const V *__restrict__ vals, uint64_t n, int shift,
                                                            uint32_t ntiles, const uint32_t *__restrict__ off,
                                                            unsigned long long *__restrict__ keys_out,
