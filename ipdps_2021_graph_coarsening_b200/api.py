@@ -354,9 +354,12 @@ class Partitioner:
     def partition_batch(self, graphs: list, workers: int = 4, cutoff: int = 50, tol: float = 1e-10,
                         mixed: bool = False, rng_state: int = 0x853C49E6748FEA9B, rng_inc: int = 1,
                         iter_cap: int = 0, coarsener: int = 0) -> list:
-        """Partition independent host graphs, ``workers`` at a time on
-        separate streams (largest first); one :class:`Result` per graph, each
-        as if partitioned alone with the same options."""
+        """Partition independent host graphs: ``workers`` host threads on
+        separate streams coarsen them (largest first), one launch iterates the
+        small coarse levels of every hierarchy (a block per hierarchy at a
+        time), and the workers finish the larger levels and the splits.  One
+        :class:`Result` per graph, identical to partitioning it alone with the
+        same options."""
         keep = []
         cnt = max(1, len(graphs))
         arr = (L.sgp_b200_graph_t * cnt)()

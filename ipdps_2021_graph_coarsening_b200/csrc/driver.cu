@@ -12,6 +12,7 @@
 
 #include <algorithm>
 #include <atomic>
+#include <memory>
 #include <mutex>
 #include <string>
 #include <thread>
@@ -202,10 +203,19 @@ __global__ void k_normalize_guess(double *x, uint32_t n) {
     for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) x[i] *= inv;
 }
 
-// eigensolve_kokkos.h:1493-1595 without FM: coarsest guess, power iteration
-// per level, prolongation, final level.
-static int eigensolve(Context &C, std::vector<Level> &levels, uint64_t *rng_state, uint64_t rng_inc,
-                      const PowerIterOpts &o, double **evec_out, PowerIterResult *finest) {
+// eigensolve_kokkos.h:1493-1595 without FM, in two parts so that a batch can
+// run the small levels of all its hierarchies in one launch.  eigen_begin
+// draws and normalises the coarsest guess and plans the chain of small levels
+// from the coarsest one up (the levels stay in `levels`, which must not be
+// resized afterwards); the chain runs through power_iter_chains; eigen_finish
+// records its results and iterates the remaining levels, prolongating down.
+struct EigenState {
+    double *x0 = nullptr;
+    PIChain chain;
+};
+
+static int eigen_begin(Context &C, std::vector<Level> &levels, uint64_t *rng_state, uint64_t rng_inc,
+                       const PowerIterOpts &o, EigenState *E) {
     const int L = (int)levels.size();
     const uint32_t gn = levels[L - 1].n;
     std::vector<double> guess(gn);
@@ -216,8 +226,38 @@ static int eigensolve(Context &C, std::vector<Level> &levels, uint64_t *rng_stat
     SGPB_CUDA(cudaStreamSynchronize(C.stream));   // guess lives on the host stack
     k_normalize_guess<<<1, 256, 0, C.stream>>>(x, gn);
     C.kernel_launches++;
-    const double *xin = x;
-    for (int l = L - 1; l >= 0; l--) {
+    E->x0 = x;
+    E->chain.x0 = x;
+    E->chain.lev.clear();
+    for (int l = L - 1; l >= 0 && power_iter_small_ok(levels[l], o); l--) {
+        PIChainLevel cl;
+        cl.L = &levels[l];
+        cl.vcmap = (l == L - 1) ? nullptr : levels[l].vcmap;
+        SGPB_TRY(dalloc_t(C, &cl.x_out, levels[l].n));
+        E->chain.lev.push_back(cl);
+    }
+    return SGP_B200_OK;
+}
+
+static int eigen_finish(Context &C, std::vector<Level> &levels, const PowerIterOpts &o, const EigenState &E,
+                        double **evec_out, PowerIterResult *finest) {
+    const int L = (int)levels.size();
+    const int nc = (int)E.chain.lev.size();
+    for (int k = 0; k < nc; k++) {
+        Level &lv = levels[L - 1 - k];
+        const PowerIterResult &r = E.chain.lev[k].res;
+        lv.pi_iters = r.niter;
+        lv.pi_ms = r.kernel_ms;
+        lv.pi_capped = r.capped;
+        lv.pi_dot = r.dot;
+        lv.pi_lambda = r.lambda;
+        if (L - 1 - k == 0) {
+            *finest = r;
+            SGPB_TRY(level_residual(C, lv, E.chain.lev[k].x_out, o.normlap, finest));
+        }
+    }
+    const double *xin = nc ? E.chain.lev[nc - 1].x_out : E.x0;
+    for (int l = L - 1 - nc; l >= 0; l--) {
         Level &lv = levels[l];
         double *xo;
         SGPB_TRY(dalloc_t(C, &xo, lv.n));
@@ -240,34 +280,58 @@ static int eigensolve(Context &C, std::vector<Level> &levels, uint64_t *rng_stat
     return SGP_B200_OK;
 }
 
+static int eigensolve(Context &C, std::vector<Level> &levels, uint64_t *rng_state, uint64_t rng_inc,
+                      const PowerIterOpts &o, double **evec_out, PowerIterResult *finest) {
+    EigenState E;
+    SGPB_TRY(eigen_begin(C, levels, rng_state, rng_inc, o, &E));
+    SGPB_TRY(power_iter_chains(C, {&E.chain}, o));
+    return eigen_finish(C, levels, o, E, evec_out, finest);
+}
+
 static float ev_ms(cudaEvent_t a, cudaEvent_t b) {
     float ms = 0;
     cudaEventElapsedTime(&ms, a, b);
     return ms;
 }
 
-// The path on a staged level 0: hierarchy, eigenvector, split.  part_d is a
-// device array of L0.n entries; the caller copies it out.  ev[0] was recorded
-// before staging (the H2D window), ev[1..4] are recorded here.
-static int partition_staged(Context &C, const Level &L0, const sgp_b200_options_t *opt, sgp_b200_result_t *res,
-                            uint32_t *part_d, cudaEvent_t *ev) {
+// One graph between the phases of a partition: its hierarchy, rng state and
+// eigensolve plan.
+struct Staged {
+    std::vector<Level> levels;
+    uint64_t st = 0;
+    PowerIterOpts po;
+    EigenState es;
+};
+
+// The path on a staged level 0, in two halves around the run of the small
+// levels (partition_staged below for one graph, sgp_b200_partition_batch for
+// many).  partition_begin builds the hierarchy and plans the eigensolve;
+// partition_end finishes it and splits.  part_d is a device array of L0.n
+// entries; the caller copies it out.  ev[0] was recorded before staging (the
+// H2D window), ev[1..4] are recorded here.
+static int partition_begin(Context &C, const Level &L0, const sgp_b200_options_t *opt, cudaEvent_t *ev, Staged *S) {
     if (opt->refine_alg != 0 && opt->refine_alg != 1) {
         set_error("refine_alg %d: 0 (shifted combinatorial Laplacian) or 1 (normalized Laplacian)", opt->refine_alg);
         return SGP_B200_ERR_INVALID;
     }
     SGPB_CUDA(cudaEventRecord(ev[1], C.stream));
-    uint64_t st = opt->rng_state;
-    std::vector<Level> levels;
-    SGPB_TRY(generate(C, L0, opt->cutoff, &st, opt->rng_inc, levels, opt->coarsener));
+    S->st = opt->rng_state;
+    SGPB_TRY(generate(C, L0, opt->cutoff, &S->st, opt->rng_inc, S->levels, opt->coarsener));
     SGPB_CUDA(cudaEventRecord(ev[2], C.stream));
-    PowerIterOpts po;
-    po.tol = opt->tol;
-    po.iter_cap = opt->iter_cap;
-    po.mixed = opt->mixed;
-    po.normlap = opt->refine_alg == 1;
+    S->po.tol = opt->tol;
+    S->po.iter_cap = opt->iter_cap;
+    S->po.mixed = opt->mixed;
+    S->po.normlap = opt->refine_alg == 1;
+    SGPB_TRY(eigen_begin(C, S->levels, &S->st, opt->rng_inc, S->po, &S->es));
+    return SGP_B200_OK;
+}
+
+static int partition_end(Context &C, const sgp_b200_options_t *opt, sgp_b200_result_t *res, uint32_t *part_d,
+                         cudaEvent_t *ev, Staged &S) {
+    std::vector<Level> &levels = S.levels;
     double *evec = nullptr;
     PowerIterResult fin;
-    SGPB_TRY(eigensolve(C, levels, &st, opt->rng_inc, po, &evec, &fin));
+    SGPB_TRY(eigen_finish(C, levels, S.po, S.es, &evec, &fin));
     SGPB_CUDA(cudaEventRecord(ev[3], C.stream));
     uint64_t cut = 0;
     uint32_t p0 = 0;
@@ -304,8 +368,16 @@ static int partition_staged(Context &C, const Level &L0, const sgp_b200_options_
         res->level_pi_ms[l] = levels[l].pi_ms;
         res->iter_max_reached |= levels[l].pi_capped;
     }
-    res->rng_state = st;
+    res->rng_state = S.st;
     return SGP_B200_OK;
+}
+
+static int partition_staged(Context &C, const Level &L0, const sgp_b200_options_t *opt, sgp_b200_result_t *res,
+                            uint32_t *part_d, cudaEvent_t *ev) {
+    Staged S;
+    SGPB_TRY(partition_begin(C, L0, opt, ev, &S));
+    SGPB_TRY(power_iter_chains(C, {&S.es.chain}, S.po));
+    return partition_end(C, opt, res, part_d, ev, S);
 }
 
 struct Events {
@@ -497,35 +569,99 @@ int sgp_b200_partition_batch(sgp_b200_ctx_t *x, const sgp_b200_graph_t *graphs, 
     std::vector<int> order(count);
     for (int i = 0; i < count; i++) order[i] = i;
     std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return graphs[a].m > graphs[b].m; });
-    std::atomic<int> next(0);
     std::atomic<int> first_rc(SGP_B200_OK);
     std::mutex err_mu;
     std::string err;
-    auto work = [&](sgp_b200_ctx_t *wx) {
-        Context &W = *ctx_get(wx);
-        cudaSetDevice(W.device);
-        while (first_rc.load() == SGP_B200_OK) {
-            const int k = next.fetch_add(1);
-            if (k >= count) break;
-            const int i = order[k];
-            const int rc = partition_impl(W, &graphs[i], opt, &results[i]);
-            release_all(W);
-            if (rc != SGP_B200_OK) {
-                int expect = SGP_B200_OK;
-                if (first_rc.compare_exchange_strong(expect, rc)) {
-                    std::lock_guard<std::mutex> lk(err_mu);
-                    err = std::string("graph ") + std::to_string(i) + ": " + last_error();
-                }
-            }
+    auto fail = [&](int i, int rc) {
+        int expect = SGP_B200_OK;
+        if (first_rc.compare_exchange_strong(expect, rc)) {
+            std::lock_guard<std::mutex> lk(err_mu);
+            err = std::string("graph ") + std::to_string(i) + ": " + last_error();
         }
-        cudaStreamSynchronize(W.stream);
     };
-    std::vector<std::thread> th;
-    for (int t = 1; t < workers; t++) th.emplace_back(work, C->workers[t]);
-    work(C->workers[0]);
-    for (auto &t : th) t.join();
-    if (first_rc.load() != SGP_B200_OK) set_error("%s", err.c_str());
-    return first_rc.load();
+    // Waves of up to kWave graphs, three phases each: the workers stage and
+    // coarsen every graph of the wave (keeping the hierarchies), one launch
+    // iterates the small levels of all of them (a block per hierarchy at a
+    // time), then the workers iterate the remaining levels and split.  A
+    // graph's results are identical to a single call's: every level runs the
+    // same kernels with the same inputs.
+    constexpr int kWave = 1024;
+    struct Item {
+        Events E;
+        Level L0;
+        Staged S;
+        uint32_t *part_d = nullptr;
+        uint32_t launches = 0;
+        float t_map = 0, t_build = 0;
+    };
+    int rc_all = SGP_B200_OK;
+    for (int w0 = 0; w0 < count && first_rc.load() == SGP_B200_OK; w0 += kWave) {
+        const int w1 = count - w0 < kWave ? count : w0 + kWave;
+        std::unique_ptr<Item[]> items(new Item[w1 - w0]);
+        auto run_phase = [&](auto &&body) {
+            std::atomic<int> next(w0);
+            auto work = [&](sgp_b200_ctx_t *wx) {
+                Context &W = *ctx_get(wx);
+                cudaSetDevice(W.device);
+                while (first_rc.load() == SGP_B200_OK) {
+                    const int k = next.fetch_add(1);
+                    if (k >= w1) break;
+                    const int i = order[k];
+                    const int rc = body(W, items[k - w0], i);
+                    if (rc != SGP_B200_OK) fail(i, rc);
+                }
+                cudaStreamSynchronize(W.stream);
+            };
+            std::vector<std::thread> th;
+            for (int t = 1; t < workers; t++) th.emplace_back(work, C->workers[t]);
+            work(C->workers[0]);
+            for (auto &t : th) t.join();
+        };
+        // phase 1: stage, coarsen, draw the coarsest guess
+        run_phase([&](Context &W, Item &it, int i) -> int {
+            SGPB_TRY(it.E.create());
+            W.kernel_launches = 0;
+            SGPB_CUDA(cudaEventRecord(it.E.e[0], W.stream));
+            SGPB_TRY(stage_input(W, &graphs[i], &it.L0));
+            it.part_d = (opt->part_mem == SGP_B200_DEVICE) ? results[i].part : nullptr;
+            if (!it.part_d) SGPB_TRY(dalloc_t(W, &it.part_d, graphs[i].n));
+            SGPB_TRY(partition_begin(W, it.L0, opt, it.E.e, &it.S));
+            it.launches = W.kernel_launches + 1;   // and the shared launch of phase 2
+            it.t_map = W.t_map;
+            it.t_build = W.t_build;
+            return SGP_B200_OK;
+        });
+        // phase 2: the small levels of every hierarchy, one launch
+        if (first_rc.load() == SGP_B200_OK) {
+            std::vector<PIChain *> chains;
+            for (int k = 0; k < w1 - w0; k++) chains.push_back(&items[k].S.es.chain);
+            const int rc = power_iter_chains(*C, chains, items[0].S.po);
+            if (rc != SGP_B200_OK) fail(order[w0], rc);
+        }
+        // phase 3: the remaining levels, the split, the copy-out
+        if (first_rc.load() == SGP_B200_OK)
+            run_phase([&](Context &W, Item &it, int i) -> int {
+                sgp_b200_result_t *res = &results[i];
+                W.kernel_launches = it.launches;
+                SGPB_TRY(partition_end(W, opt, res, it.part_d, it.E.e, it.S));
+                if (opt->part_mem != SGP_B200_DEVICE)
+                    SGPB_CUDA(cudaMemcpyAsync(res->part, it.part_d, sizeof(uint32_t) * graphs[i].n,
+                                              cudaMemcpyDeviceToHost, W.stream));
+                SGPB_CUDA(cudaEventRecord(it.E.e[5], W.stream));
+                SGPB_CUDA(cudaStreamSynchronize(W.stream));
+                W.t_map = it.t_map;
+                W.t_build = it.t_build;
+                fill_times(W, it.E, res);
+                return SGP_B200_OK;
+            });
+        for (int t = 0; t < workers; t++) release_all(*ctx_get(C->workers[t]));
+        release_all(*C);
+    }
+    if (first_rc.load() != SGP_B200_OK) {
+        set_error("%s", err.c_str());
+        rc_all = first_rc.load();
+    }
+    return rc_all;
 }
 
 int sgp_b200_last_timing(sgp_b200_ctx_t *x, float *t, float *c, float *e, float *s) {

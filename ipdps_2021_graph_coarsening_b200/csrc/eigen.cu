@@ -34,6 +34,7 @@
 #include <stdlib.h>
 #include <string.h>
 
+#include <algorithm>
 #include <type_traits>
 
 #include "common.cuh"
@@ -1087,8 +1088,12 @@ static size_t small_level_bytes(uint32_t n, uint64_t m, bool weighted) {
     return b;
 }
 
+// The whole computation of one small level by the calling block, shared by the
+// single-level kernel and the chained one (not inlined, so both run the same
+// code): the level (offsets, destinations, weights, degrees) and both
+// iterates are staged in shared memory.
 template <typename W, typename V>
-__global__ void __launch_bounds__(kSmallThreads, 1) k_power_iter_small(PIArgs a) {
+__device__ __noinline__ void small_level(const PIArgs &a) {
     typedef typename std::conditional<sizeof(V) == 8, double, float>::type ACC;
     __shared__ double sm[256];
     extern __shared__ __align__(16) unsigned char dyn_smem[];
@@ -1244,6 +1249,52 @@ __global__ void __launch_bounds__(kSmallThreads, 1) k_power_iter_small(PIArgs a)
         mu = mu_n;
         inv_nu = inv_nu_n;
         V *t = src; src = dst; dst = t;
+    }
+}
+
+template <typename W, typename V>
+__global__ void __launch_bounds__(kSmallThreads, 1) k_power_iter_small(PIArgs a) {
+    small_level<W, V>(a);
+}
+
+// A chain: the consecutive small levels of one hierarchy from its coarsest
+// level up, each level reading the previous one's result through its vcmap.
+struct PIChainDesc {
+    PIArgs a;
+    int wbytes;   // 0, 4 or 8
+};
+
+__device__ __forceinline__ unsigned long long global_ns() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+// Work queue over chains (the host orders them largest first): each block
+// takes the next chain from a counter and runs its levels in order, so one
+// launch iterates the small levels of a whole batch of hierarchies, one block
+// per SM.  Each level is the single-level kernel's computation; res[6] of a
+// level is its duration in ms by the device's global timer.
+__global__ void __launch_bounds__(kSmallThreads, 1) k_power_iter_chains(const PIChainDesc *__restrict__ lev,
+                                                                        const uint2 *__restrict__ chains,
+                                                                        uint32_t nchains, uint32_t *next) {
+    __shared__ uint32_t item;
+    while (true) {
+        __syncthreads();   // the previous chain is done with item
+        if (threadIdx.x == 0) item = atomicAdd(next, 1u);
+        __syncthreads();
+        const uint32_t c = item;
+        if (c >= nchains) return;
+        const uint2 ch = chains[c];
+        for (uint32_t k = 0; k < ch.y; k++) {
+            const PIChainDesc &d = lev[ch.x + k];
+            const unsigned long long t0 = global_ns();
+            if (d.wbytes == 8) small_level<unsigned long long, double>(d.a);
+            else small_level<uint32_t, double>(d.a);
+            // the result is visible to the next level, and shared memory free
+            __syncthreads();
+            if (threadIdx.x == 0) d.a.res[6] = (double)(global_ns() - t0) * 1e-6;
+        }
     }
 }
 
@@ -1643,10 +1694,34 @@ __global__ void k_max_deg(uint32_t n, const uint32_t *rp, uint32_t *out) {
 
 int hub_first_copy(Context &C, const Level &L, uint32_t **perm_out, uint32_t **inv_out, Level *out);
 
+// the reference's cap (eigensolve_kokkos.h:153) is 1e14 / n, unbounded in
+// practice for small levels; a default budget of 5e6 iterations turns a
+// non-converging level into a reported cap instead of an endless kernel.
+static uint64_t iter_budget(uint32_t n, const PowerIterOpts &o) {
+    uint64_t imax = 100000000000000ULL / (uint64_t)n;
+    const uint64_t cap = o.iter_cap ? o.iter_cap : 5000000ULL;
+    return imax > cap ? cap : imax;
+}
+
 int power_iter_level(Context &C, const Level &Lin, const double *x_in, const uint32_t *vcmap, double *x_out,
                      const PowerIterOpts &o, PowerIterResult *res, int want_residual) {
     const uint32_t n = Lin.n;
     if (n == 0) { *res = PowerIterResult(); return SGP_B200_OK; }
+    if (power_iter_small_ok(Lin, o)) {
+        // one block in shared memory: a chain of one level, none of the
+        // row-cost tables of the multi-block kernel
+        PIChain ch;
+        ch.x0 = x_in;
+        PIChainLevel cl;
+        cl.L = &Lin;
+        cl.vcmap = vcmap;
+        cl.x_out = x_out;
+        ch.lev.push_back(cl);
+        SGPB_TRY(power_iter_chains(C, {&ch}, o));
+        *res = ch.lev[0].res;
+        if (want_residual) SGPB_TRY(level_residual(C, Lin, x_out, o.normlap, res));
+        return SGP_B200_OK;
+    }
     PIArgs a;
     memset(&a, 0, sizeof(a));
     // A level whose whole iterate fits in 96 KB keeps it in shared memory.
@@ -1743,12 +1818,7 @@ int power_iter_level(Context &C, const Level &Lin, const double *x_in, const uin
     SGPB_TRY(scan_u32(C, cost_all, cpre_all, n, nullptr));
     a.heavy = heavy; a.n_heavy_ptr = nh; a.cpre = cpre; a.cpre_all = cpre_all;
     a.x_in = x_in; a.vcmap = vcmap; a.out = x_out;
-    // the reference's cap (eigensolve_kokkos.h:153) is 1e14 / n, unbounded in
-    // practice for small levels; a default budget of 5e6 iterations turns a
-    // non-converging level into a reported cap instead of an endless kernel.
-    uint64_t imax = 100000000000000ULL / (uint64_t)n;
-    const uint64_t cap = o.iter_cap ? o.iter_cap : 5000000ULL;
-    if (imax > cap) imax = cap;
+    const uint64_t imax = iter_budget(n, o);
     a.iter_max = imax;
     a.tol = o.tol;
     double *res_d;
@@ -1786,27 +1856,116 @@ int power_iter_level(Context &C, const Level &Lin, const double *x_in, const uin
     res->capped = rh[4] != 0.0;
     res->resid = 0;
     res->kernel_ms = kms;
-    if (want_residual) {
-        uint32_t nb = C.num_sms * 4;
-        double *part, *out2;
-        SGPB_TRY(dalloc_t(C, &part, 2 * (size_t)nb));
-        SGPB_TRY(dalloc_t(C, &out2, 2));
-        // the result is in the level's own numbering: use the level itself
-        if (Lin.wbytes == 8)
-            k_residual<unsigned long long><<<nb, 256, 0, C.stream>>>(n, Lin.rp, Lin.col,
-                                                                     (const unsigned long long *)Lin.w, x_out,
-                                                                     res->lambda, o.normlap, part);
-        else
-            k_residual<uint32_t><<<nb, 256, 0, C.stream>>>(n, Lin.rp, Lin.col, (const uint32_t *)Lin.w, x_out,
-                                                           res->lambda, o.normlap, part);
-        k_sum_pairs<<<1, 32, 0, C.stream>>>(part, nb, out2);
-        C.kernel_launches += 2;
-        SGPB_CUDA(cudaGetLastError());
-        SGPB_CUDA(cudaMemcpyAsync(C.h_pinned, out2, 2 * sizeof(double), cudaMemcpyDeviceToHost, C.stream));
-        SGPB_CUDA(cudaStreamSynchronize(C.stream));
-        double r2 = ((double *)C.h_pinned)[0], x2 = ((double *)C.h_pinned)[1];
-        const double scale = o.normlap ? 2.0 : (res->gb > 0 ? res->gb : 1);   // bound on the spectrum
-        res->resid = sqrt(r2 / (x2 > 0 ? x2 : 1)) / scale;
+    // the result is in the level's own numbering: use the level itself
+    if (want_residual) SGPB_TRY(level_residual(C, Lin, x_out, o.normlap, res));
+    return SGP_B200_OK;
+}
+
+int level_residual(Context &C, const Level &L, const double *x, int normlap, PowerIterResult *res) {
+    const uint32_t n = L.n;
+    uint32_t nb = C.num_sms * 4;
+    double *part, *out2;
+    SGPB_TRY(dalloc_t(C, &part, 2 * (size_t)nb));
+    SGPB_TRY(dalloc_t(C, &out2, 2));
+    if (L.wbytes == 8)
+        k_residual<unsigned long long><<<nb, 256, 0, C.stream>>>(n, L.rp, L.col, (const unsigned long long *)L.w, x,
+                                                                 res->lambda, normlap, part);
+    else
+        k_residual<uint32_t><<<nb, 256, 0, C.stream>>>(n, L.rp, L.col, (const uint32_t *)L.w, x, res->lambda,
+                                                       normlap, part);
+    k_sum_pairs<<<1, 32, 0, C.stream>>>(part, nb, out2);
+    C.kernel_launches += 2;
+    SGPB_CUDA(cudaGetLastError());
+    SGPB_CUDA(cudaMemcpyAsync(C.h_pinned, out2, 2 * sizeof(double), cudaMemcpyDeviceToHost, C.stream));
+    SGPB_CUDA(cudaStreamSynchronize(C.stream));
+    double r2 = ((double *)C.h_pinned)[0], x2 = ((double *)C.h_pinned)[1];
+    const double scale = normlap ? 2.0 : (res->gb > 0 ? res->gb : 1);   // bound on the spectrum
+    res->resid = sqrt(r2 / (x2 > 0 ? x2 : 1)) / scale;
+    return SGP_B200_OK;
+}
+
+bool power_iter_small_ok(const Level &L, const PowerIterOpts &o) {
+    const char *forced = getenv("SGPB_PI_MODE");
+    if (forced && *forced) return false;
+    if (L.n == 0 || L.m + 8ull * L.n > kSmallCost) return false;
+    if (!(L.wbytes == 0 || L.wbytes == 4 || L.wbytes == 8)) return false;
+    if (o.mixed && L.n >= 4096) return false;   // would start in FP32
+    return small_level_bytes<unsigned long long, double>(L.n, L.m, L.w != nullptr) <= kSmallSmemBytes;
+}
+
+int power_iter_chains(Context &C, const std::vector<PIChain *> &chains, const PowerIterOpts &o) {
+    std::vector<PIChainDesc> h;
+    std::vector<std::pair<uint64_t, uint2>> order;   // (cost, chain) for largest-first
+    size_t bytes = 0;
+    for (PIChain *ch : chains) {
+        if (!ch || ch->lev.empty()) continue;
+        uint2 c = make_uint2((uint32_t)h.size(), (uint32_t)ch->lev.size());
+        uint64_t cost = 0;
+        for (size_t k = 0; k < ch->lev.size(); k++) {
+            const PIChainLevel &cl = ch->lev[k];
+            const Level &L = *cl.L;
+            if (!power_iter_small_ok(L, o)) {
+                set_error("level of %u vertices and %llu entries is not a small level", L.n,
+                          (unsigned long long)L.m);
+                return SGP_B200_ERR_INVALID;
+            }
+            PIChainDesc d;
+            memset(&d, 0, sizeof(d));
+            d.a.n = L.n; d.a.m = L.m; d.a.rp = L.rp; d.a.col = L.col; d.a.w = L.w;
+            d.a.x_in = k == 0 ? ch->x0 : ch->lev[k - 1].x_out;
+            d.a.vcmap = cl.vcmap;
+            d.a.out = cl.x_out;
+            d.a.tol = o.tol;
+            d.a.iter_max = iter_budget(L.n, o);
+            d.a.normlap = o.normlap;
+            d.wbytes = L.wbytes;
+            h.push_back(d);
+            cost += L.m + 8ull * L.n;
+            const size_t b = L.wbytes == 8 ? small_level_bytes<unsigned long long, double>(L.n, L.m, L.w != nullptr)
+                                           : small_level_bytes<uint32_t, double>(L.n, L.m, L.w != nullptr);
+            bytes = b > bytes ? b : bytes;
+        }
+        order.push_back({cost, c});
+    }
+    if (h.empty()) return SGP_B200_OK;
+    std::stable_sort(order.begin(), order.end(), [](const auto &x, const auto &y) { return x.first > y.first; });
+    std::vector<uint2> hc(order.size());
+    for (size_t i = 0; i < order.size(); i++) hc[i] = order[i].second;
+    double *res_d;
+    SGPB_TRY(dalloc_t(C, &res_d, 8 * h.size()));
+    for (size_t i = 0; i < h.size(); i++) h[i].a.res = res_d + 8 * i;
+    PIChainDesc *lev_d;
+    uint2 *ch_d;
+    uint32_t *next;
+    SGPB_TRY(dalloc_t(C, &lev_d, h.size()));
+    SGPB_TRY(dalloc_t(C, &ch_d, hc.size()));
+    SGPB_TRY(dalloc_t(C, &next, 1));
+    SGPB_CUDA(cudaMemcpyAsync(lev_d, h.data(), sizeof(PIChainDesc) * h.size(), cudaMemcpyHostToDevice, C.stream));
+    SGPB_CUDA(cudaMemcpyAsync(ch_d, hc.data(), sizeof(uint2) * hc.size(), cudaMemcpyHostToDevice, C.stream));
+    SGPB_TRY(dzero(C, next, 4));
+    // one fixed bound for every launch (host threads share the attribute)
+    SGPB_CUDA(cudaFuncSetAttribute(k_power_iter_chains, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   (int)kSmallSmemBytes));
+    const uint32_t grid = (uint32_t)(hc.size() < (size_t)C.num_sms ? hc.size() : (size_t)C.num_sms);
+    k_power_iter_chains<<<grid, kSmallThreads, bytes, C.stream>>>(lev_d, ch_d, (uint32_t)hc.size(), next);
+    C.kernel_launches++;
+    SGPB_CUDA(cudaGetLastError());
+    std::vector<double> rh(8 * h.size());
+    SGPB_CUDA(cudaMemcpyAsync(rh.data(), res_d, sizeof(double) * rh.size(), cudaMemcpyDeviceToHost, C.stream));
+    SGPB_CUDA(cudaStreamSynchronize(C.stream));
+    size_t i = 0;
+    for (PIChain *ch : chains) {
+        if (!ch) continue;
+        for (PIChainLevel &cl : ch->lev) {
+            const double *r = &rh[8 * i++];
+            cl.res = PowerIterResult();
+            cl.res.niter = (uint64_t)r[0];
+            cl.res.dot = r[1];
+            cl.res.gb = r[2];
+            cl.res.lambda = r[3];
+            cl.res.capped = r[4] != 0.0;
+            cl.res.kernel_ms = (float)r[6];
+        }
     }
     return SGP_B200_OK;
 }

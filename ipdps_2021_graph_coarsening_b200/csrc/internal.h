@@ -136,6 +136,25 @@ struct PowerIterResult {
 // initial vector; x_out: n doubles (may alias nothing).
 int power_iter_level(Context &C, const Level &L, const double *x_in, const uint32_t *vcmap,
                      double *x_out, const PowerIterOpts &o, PowerIterResult *res, int want_residual);
+// |L x - lambda x| / (bound on the spectrum) of a level's result into res->resid
+int level_residual(Context &C, const Level &L, const double *x, int normlap, PowerIterResult *res);
+// Small levels (one block, the level in shared memory).  A chain is the
+// consecutive small levels of one hierarchy, coarsest first: the first reads
+// x0 (through its vcmap when set), each later one the previous result through
+// its own vcmap.  power_iter_chains runs any number of chains in one launch,
+// a block per chain at a time, and fills each level's result.
+bool power_iter_small_ok(const Level &L, const PowerIterOpts &o);
+struct PIChainLevel {
+    const Level *L = nullptr;
+    const uint32_t *vcmap = nullptr;   // this level's vertex -> vertex of the vector it starts from
+    double *x_out = nullptr;           // L->n doubles
+    PowerIterResult res;
+};
+struct PIChain {
+    const double *x0 = nullptr;
+    std::vector<PIChainLevel> lev;
+};
+int power_iter_chains(Context &C, const std::vector<PIChain *> &chains, const PowerIterOpts &o);
 int split_level(Context &C, const Level &L, const double *evec, int perc_imbalance, uint32_t *part,
                 uint64_t *edgecut, uint32_t *n_part0);
 int edge_cut_device(Context &C, const Level &L, const uint32_t *part, uint64_t *edgecut);

@@ -109,6 +109,38 @@ def test_batch_equals_single_calls(partitioner):
             assert r.level_iters == s.level_iters and r.rng_state == s.rng_state
 
 
+def same_result(a, b):
+    assert np.array_equal(a.part, b.part) and a.edgecut == b.edgecut
+    assert a.level_n == b.level_n and a.level_iters == b.level_iters and a.rng_state == b.rng_state
+    assert a.lam == b.lam and a.residual == b.residual
+
+
+def test_batch_of_small_hierarchies(partitioner):
+    """Graphs whose every level, level 0 included, is a small level: the
+    whole eigensolve of each is the batch's one chained launch (one block per
+    hierarchy), and the result equals a single call's bit for bit."""
+    gs = batch_graphs(40, seed=5, lo=40, hi=1500)
+    rs = partitioner.partition_batch(gs, workers=3, rng_state=2)
+    for g, r in zip(gs, rs):
+        same_result(r, partitioner.partition(g, rng_state=2))
+        assert r.edgecut == cut_of(g, r.part)
+    for g, r in list(zip(gs, rs))[:6]:
+        o = O.partition_graph(g.row_ptr, g.col, None, cutoff=50, tol=1e-10, rng_state=2)
+        assert r.level_n == o["level_n"] and r.rng_state == o["rng_state"]
+        assert abs(r.lam - o["lambda"]) <= 1e-6 * abs(o["lambda"])
+
+
+@pytest.mark.parametrize("mixed", [False, True])
+def test_batch_weighted_and_mixed_equal_single_calls(partitioner, mixed):
+    """64-bit coarse weights (total weight above 2^32) and the mixed-precision
+    path through the batch: each graph as a single call."""
+    gs = [G.chung_lu(n, wmax=1 << 22, seed=s) for n, s in ((3000, 1), (9000, 2), (600, 3))]
+    gs += batch_graphs(5, seed=41, lo=2000, hi=20000)
+    rs = partitioner.partition_batch(gs, workers=2, rng_state=8, mixed=mixed)
+    for g, r in zip(gs, rs):
+        same_result(r, partitioner.partition(g, rng_state=8, mixed=mixed))
+
+
 def test_batch_matches_oracle(partitioner):
     gs = batch_graphs(6, seed=23)
     rs = partitioner.partition_batch(gs, workers=3, rng_state=4)
