@@ -349,13 +349,14 @@ int sgpgen_rgg3d(uint32_t n, double radius, uint64_t seed, sgpgen_csr_t *out) {
 int sgpgen_chunglu(uint32_t n, double alpha, double dmin, double dmax, uint32_t wmax,
                    uint64_t seed, sgpgen_csr_t *out) {
     if (n < 2 || alpha <= 1.0 || dmin <= 0 || dmax < dmin) return 1;
-    // expected degrees: Pareto(alpha, dmin) capped at dmax
+    // expected degrees: Pareto with shape alpha and scale dmin (P(D > d) =
+    // (dmin / d)^alpha, mean alpha dmin / (alpha - 1)) capped at dmax
     std::vector<double> wdeg(n);
     #pragma omp parallel for schedule(static)
     for (int64_t i = 0; i < (int64_t)n; i++) {
         Rng r(mix64(seed ^ (0x9E3779B97F4A7C15ULL * ((uint64_t)i + 1))));
         double uu = 1.0 - r.unit();
-        double d = dmin * pow(uu, -1.0 / (alpha - 1.0));
+        double d = dmin * pow(uu, -1.0 / alpha);
         wdeg[i] = d > dmax ? dmax : d;
     }
     std::vector<double> cdf(n + 1, 0.0);

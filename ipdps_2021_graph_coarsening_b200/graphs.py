@@ -125,7 +125,8 @@ def rgg3d(n: int, mean_degree: float = 12.0, seed: int = 1, radius: Optional[flo
 
 def chung_lu(n: int, alpha: float = 2.1, dmin: float = 12.5, dmax: float = 50000.0,
              wmax: int = 100, seed: int = 1) -> CSR:
-    """Chung-Lu with Pareto(alpha, dmin) expected degrees capped at dmax and
+    """Chung-Lu with Pareto expected degrees (shape alpha, scale dmin: mean
+    alpha dmin / (alpha - 1), about 24 for the defaults) capped at dmax and
     integer edge weights uniform in [1, wmax] (0 = unit weights)."""
     return _call(_gen().sgpgen_chunglu, n, alpha, dmin, dmax, wmax, seed, name=f"chunglu{n}")
 
