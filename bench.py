@@ -297,7 +297,8 @@ def gpu_arm(args, rank: int, ws: int, local: int, distmod):
         except (OSError, ValueError):
             traffic = None
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                "traffic": traffic, "kernel": "k_power_iter", "peak_kind": peak_kind,
+                "traffic": traffic, "kernel": "k_power_iter (+ k_power_iter_chains on the small levels)",
+                "peak_kind": peak_kind,
                 "kernel_ms_per_step": pi_ms, "algorithmic_bytes_per_step": byts,
                 "kernel_share_of_step": pi_ms / ms if ms else None}
 

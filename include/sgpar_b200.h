@@ -223,11 +223,15 @@ int sgp_b200_partition_4way(sgp_b200_ctx_t *ctx, const sgp_b200_graph_t *g,
 /* No counterpart in the reference (its experiment runner starts one process
  * per graph).  Partitions graphs[0..count) independently, each with opt as
  * given (the same rng seeding for every graph), into results[i] (whose part
- * the caller sets, kind opt->part_mem).  `workers` graphs are in flight at
- * once, each on its own stream of the context's device, largest graphs
- * first; the worker contexts are kept by ctx for later calls.  Results do
- * not depend on `workers`.  On failure the first error is returned and the
- * message names the graph. */
+ * the caller sets, kind opt->part_mem).  In waves of up to 1024 graphs:
+ * `workers` host threads, each on its own stream of the context's device,
+ * coarsen the graphs (largest first) and keep the hierarchies; one launch
+ * then iterates the small coarse levels of every hierarchy (a block per
+ * hierarchy at a time); the workers finish the larger levels and the splits.
+ * The worker contexts are kept by ctx for later calls.  Results equal single
+ * calls' and do not depend on `workers`; the per-graph phase times include
+ * waiting for the shared launch.  On failure the first error is returned
+ * and the message names the graph. */
 int sgp_b200_partition_batch(sgp_b200_ctx_t *ctx, const sgp_b200_graph_t *graphs, int count,
                              const sgp_b200_options_t *opt, sgp_b200_result_t *results,
                              int workers);
