@@ -393,7 +393,11 @@ int sgp_b200_csr_write(const char *csr_path, const sgp_b200_graph_t *g, int id_b
 int sgp_b200_mtx2csr(sgp_b200_ctx_t *ctx, const char *mtx_path, const char *csr_path, int id_bytes,
                      sgp_b200_mtx_info_t *info);
 
-/* Milliseconds of the phases of the last sgp_b200_partition / eigensolve. */
+/* Milliseconds of the phases of the last sgp_b200_partition / eigensolve
+ * (CUDA events).  After sgp_b200_partition_batch: host wall time of its
+ * phases summed over the waves -- coarsening (ms_coarsen), the shared launch
+ * of the small levels (ms_eigen), the remaining levels and the splits
+ * (ms_split), and their sum (ms_total). */
 int sgp_b200_last_timing(sgp_b200_ctx_t *ctx, float *ms_total, float *ms_coarsen,
                          float *ms_eigen, float *ms_split);
 

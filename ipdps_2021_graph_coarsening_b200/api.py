@@ -377,6 +377,15 @@ class Partitioner:
                 "sgp_b200_partition_batch")
         return [self._result(res[i], parts[i]) for i in range(len(graphs))]
 
+    def last_timing(self) -> dict:
+        """Phase times (ms) of the last call on this partitioner: CUDA-event
+        phases of a partition, or the host wall times of a batch's phases
+        (coarsen, the shared small-level launch as ``eigen``, the rest as
+        ``split``)."""
+        t = [ctypes.c_float(0) for _ in range(4)]
+        L.check(L.lib().sgp_b200_last_timing(self._ctx, *[ctypes.byref(x) for x in t]), "sgp_b200_last_timing")
+        return dict(zip(("total", "coarsen", "eigen", "split"), (x.value for x in t)))
+
     # -- per-kernel entry points (CUDA torch tensors)
     def fm_refine(self, row_ptr, col, part, max_passes: int = 16):
         """FM passes on a device bisection ``part`` (CUDA int32 tensor, updated

@@ -12,6 +12,7 @@
 
 #include <algorithm>
 #include <atomic>
+#include <chrono>
 #include <memory>
 #include <mutex>
 #include <string>
@@ -595,6 +596,13 @@ int sgp_b200_partition_batch(sgp_b200_ctx_t *x, const sgp_b200_graph_t *graphs, 
         float t_map = 0, t_build = 0;
     };
     int rc_all = SGP_B200_OK;
+    // wall time of each phase, summed over the waves (the phases are
+    // separated by host synchronisation)
+    double ph[3] = {0, 0, 0};
+    auto now = [] { return std::chrono::steady_clock::now(); };
+    auto ms_since = [](std::chrono::steady_clock::time_point t0) {
+        return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    };
     for (int w0 = 0; w0 < count && first_rc.load() == SGP_B200_OK; w0 += kWave) {
         const int w1 = count - w0 < kWave ? count : w0 + kWave;
         std::unique_ptr<Item[]> items(new Item[w1 - w0]);
@@ -618,6 +626,7 @@ int sgp_b200_partition_batch(sgp_b200_ctx_t *x, const sgp_b200_graph_t *graphs, 
             for (auto &t : th) t.join();
         };
         // phase 1: stage, coarsen, draw the coarsest guess
+        auto t0 = now();
         run_phase([&](Context &W, Item &it, int i) -> int {
             SGPB_TRY(it.E.create());
             W.kernel_launches = 0;
@@ -631,14 +640,18 @@ int sgp_b200_partition_batch(sgp_b200_ctx_t *x, const sgp_b200_graph_t *graphs, 
             it.t_build = W.t_build;
             return SGP_B200_OK;
         });
+        ph[0] += ms_since(t0);
         // phase 2: the small levels of every hierarchy, one launch
+        t0 = now();
         if (first_rc.load() == SGP_B200_OK) {
             std::vector<PIChain *> chains;
             for (int k = 0; k < w1 - w0; k++) chains.push_back(&items[k].S.es.chain);
             const int rc = power_iter_chains(*C, chains, items[0].S.po);
             if (rc != SGP_B200_OK) fail(order[w0], rc);
         }
+        ph[1] += ms_since(t0);
         // phase 3: the remaining levels, the split, the copy-out
+        t0 = now();
         if (first_rc.load() == SGP_B200_OK)
             run_phase([&](Context &W, Item &it, int i) -> int {
                 sgp_b200_result_t *res = &results[i];
@@ -654,9 +667,14 @@ int sgp_b200_partition_batch(sgp_b200_ctx_t *x, const sgp_b200_graph_t *graphs, 
                 fill_times(W, it.E, res);
                 return SGP_B200_OK;
             });
+        ph[2] += ms_since(t0);
         for (int t = 0; t < workers; t++) release_all(*ctx_get(C->workers[t]));
         release_all(*C);
     }
+    C->t_coarsen = (float)ph[0];
+    C->t_eigen = (float)ph[1];
+    C->t_split = (float)ph[2];
+    C->t_total = (float)(ph[0] + ph[1] + ph[2]);
     if (first_rc.load() != SGP_B200_OK) {
         set_error("%s", err.c_str());
         rc_all = first_rc.load();
