@@ -5,8 +5,9 @@ properties that hold at any size (the oracle takes minutes to hours there):
   precision, balanced parts, the reported cut equal to the cut recomputed from
   the partition, the mixed cut within 1% of the FP64 cut;
 * weighted Chung-Lu, 8,388,608 vertices, ~1e8 edges, weights in [1, 100]:
-  the first coarse level's 64-bit weights conserve the fine weights exactly
-  (total and two position-weighted checksums over (coarse u, coarse v)), rows
+  the heavy-edge mapping passes the HEC validity check, and the coarse graph
+  built from it with 64-bit weights conserves the fine weights exactly (total
+  and two position-weighted checksums over (coarse u, coarse v)), rows
   strictly sorted with no self loops, the mapping onto [0, nc);
 * 3D random geometric graph, 2^24 points, mean degree ~12: the 4-way driver
   (balanced quarters, cut2 <= cut4, both recomputed);
@@ -32,11 +33,6 @@ def dev(a):
 def rows_of(row_ptr):
     deg = dev(np.diff(row_ptr.astype(np.int64)))
     return torch.repeat_interleave(torch.arange(deg.numel(), device="cuda"), deg)
-
-
-def u32(t):
-    """A uint32 device tensor (values below 2^31) as int64."""
-    return t.view(torch.int32).to(torch.int64)
 
 
 def cut_dev(g, labels):
@@ -67,36 +63,35 @@ def test_rmat22_fp64_and_mixed(partitioner):
 
 
 def test_chunglu23_weighted_coarse_weights_conserved(partitioner):
+    from oracle import bindings as O
     g = G.chung_lu(1 << 23, wmax=100, seed=1)
     assert 0.8e8 < g.m_directed // 2 < 1.2e8
-    h = partitioner.generate_coarse_graphs(g)
-    try:
-        fine, coarse = h.level(0), h.level(1)
-    finally:
-        h.free()
-    vc = u32(fine["vcmap"])
-    nc = coarse["n"]
+    i32 = lambda a: torch.from_numpy(np.ascontiguousarray(a).view(np.int32)).cuda()
+    rp, col, w32 = i32(g.row_ptr), i32(g.col), i32(g.w)
+    hn, vc32, nc, _ = partitioner.hec(rp, col, w32, random_level=False, seed=5)
+    assert O.hec_check(hn.cpu().numpy().view(np.uint32), vc32.cpu().numpy().view(np.uint32), nc) == 0
+    # 64-bit coarse weights: the total weight exceeds 2^32
+    crp, ccol, cw = partitioner.build_coarse(rp, col, w32, vc32, nc, out_wbytes=8)
+    vc = vc32.to(torch.int64)
     assert int(vc.max().item()) < nc and bool((torch.bincount(vc, minlength=nc) > 0).all())
-    assert coarse["wbytes"] == 8   # the total weight exceeds 2^32
     # fine entries mapped to coarse pairs, self loops of aggregates dropped
     cu = vc[rows_of(g.row_ptr)]
     cv = vc[dev(g.col)]
     w = dev(g.w)
     keep = cu != cv
     cu, cv, w = cu[keep], cv[keep], w[keep]
-    crp = u32(coarse["row_ptr"])
-    ccol = u32(coarse["col"])
-    cw = coarse["w"].view(torch.int64)
+    crp = crp.to(torch.int64)
+    ccol = ccol.to(torch.int64)
     crow = torch.repeat_interleave(torch.arange(nc, device="cuda"), crp[1:] - crp[:-1])
     assert bool((crow != ccol).all())
     same_row = crow[1:] == crow[:-1]
     assert bool((ccol[1:][same_row] > ccol[:-1][same_row]).all())
-    assert int(cw.min().item()) >= 1
+    assert int(cw.min().item()) >= 1 and int(cw.sum().item()) > 0xFFFFFFFF
     assert int(cw.sum().item()) == int(w.sum().item())
     for mul in (1000003, 7919):
         f = lambda a, b: (a * mul + b) & 0xFFFF
         assert int((cw * f(crow, ccol)).sum().item()) == int((w * f(cu, cv)).sum().item())
-    del cu, cv, w, crow, ccol, cw, vc
+    del cu, cv, w, crow, ccol, cw, vc, crp, rp, col, w32, hn, vc32
     r = partitioner.partition(g, rng_state=3)
     check_bisection(g, r)
 
