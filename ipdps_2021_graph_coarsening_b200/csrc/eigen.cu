@@ -1088,12 +1088,13 @@ static size_t small_level_bytes(uint32_t n, uint64_t m, bool weighted) {
     return b;
 }
 
-// The whole computation of one small level by the calling block, shared by the
-// single-level kernel and the chained one (not inlined, so both run the same
-// code): the level (offsets, destinations, weights, degrees) and both
-// iterates are staged in shared memory.
+// The whole computation of one small level by the calling block: the level
+// (offsets, destinations, weights, degrees) and both iterates are staged in
+// shared memory.  Every FP64 small level runs it inside the chained kernel
+// (single partitions and batches alike); the single-level kernel remains for
+// the FP32 start of a mixed-precision level.
 template <typename W, typename V>
-__device__ __noinline__ void small_level(const PIArgs &a) {
+__device__ __forceinline__ void small_level(const PIArgs &a) {
     typedef typename std::conditional<sizeof(V) == 8, double, float>::type ACC;
     __shared__ double sm[256];
     extern __shared__ __align__(16) unsigned char dyn_smem[];

@@ -742,11 +742,15 @@ static int copy_out(Context &C, uint32_t n, uint64_t m, const uint32_t *rp, cons
     uint32_t *orp = nullptr, *ocol = nullptr;
     const size_t brp = sizeof(uint32_t) * ((size_t)n + 1), bcol = sizeof(uint32_t) * (m ? m : 1);
     if (out_mem == SGP_B200_DEVICE) {
-        cudaError_t e1 = cudaMalloc((void **)&orp, brp);
-        cudaError_t e2 = cudaMalloc((void **)&ocol, bcol);
+        // from the device's stream-ordered pool, which keeps freed memory
+        // mapped (sgp_b200_create): a repeated conversion does not map and
+        // unmap half a gigabyte per call.  cudaFree in sgp_b200_graph_free
+        // returns it to the pool.
+        cudaError_t e1 = cudaMallocAsync((void **)&orp, brp, C.stream);
+        cudaError_t e2 = cudaMallocAsync((void **)&ocol, bcol, C.stream);
         if (e1 != cudaSuccess || e2 != cudaSuccess) {
-            cudaFree(orp);
-            cudaFree(ocol);
+            if (orp) cudaFreeAsync(orp, C.stream);
+            if (ocol) cudaFreeAsync(ocol, C.stream);
             set_error("device allocation of the output graph failed");
             return SGP_B200_ERR_DEVICE;
         }
@@ -775,8 +779,9 @@ static int copy_out(Context &C, uint32_t n, uint64_t m, const uint32_t *rp, cons
     }
     if (rc != SGP_B200_OK) {
         if (out_mem == SGP_B200_DEVICE) {
-            cudaFree(orp);
-            cudaFree(ocol);
+            cudaFreeAsync(orp, C.stream);
+            cudaFreeAsync(ocol, C.stream);
+            cudaStreamSynchronize(C.stream);
         } else {
             free(orp);
             free(ocol);
