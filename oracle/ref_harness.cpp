@@ -1,7 +1,7 @@
 /*
  * ref_harness.cpp -- C-ABI shim over the reference's own serial/OpenMP
  * implementation (cmg/sgpar.h, compiled from its sources where they lie; see
- * oracle/Makefile).  TEST AND BASELINE INFRASTRUCTURE ONLY: used by tests/ to
+ * oracle/Makefile).  TEST AND CPU-REFERENCE INFRASTRUCTURE ONLY: used by tests/ to
  * pin the oracle restatement and by bench.py's reference arm as the CPU
  * baseline.  Nothing here is shipped.
  *
