@@ -639,6 +639,161 @@ static int build_impl(Context &C, const Level &F, const WI *w, const uint32_t *v
     return SGP_B200_OK;
 }
 
+// -------------------------------------------------------- sorted build --
+// Unit-weight fine levels with many entries.  Every entry becomes the key
+// (vcmap[u] << b | vcmap[v]) -- all ones for an entry inside an aggregate --
+// and one stable LSD radix sort (csrc/sort.cu) orders the keys by coarse row
+// and destination.  Each run of equal keys is one coarse entry whose weight is
+// the run length: the RADIX build's output (rows sorted by destination,
+// duplicates summed, self loops dropped) with no per-row sorts.
+constexpr uint64_t kNoKey = ~0ull;
+
+template <int G>
+__global__ void __launch_bounds__(256) k_sb_keys(uint32_t n, const uint32_t *__restrict__ rp,
+                                                 const uint32_t *__restrict__ col,
+                                                 const uint32_t *__restrict__ vcmap, int b,
+                                                 unsigned long long *__restrict__ keys,
+                                                 unsigned long long *__restrict__ kept) {
+    __shared__ unsigned long long wsum[8];
+    const uint32_t lane = threadIdx.x & (G - 1);
+    const uint64_t gid = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) / G;
+    const uint64_t ngroups = ((uint64_t)gridDim.x * blockDim.x) / G;
+    unsigned long long c = 0;
+    for (uint64_t u = gid; u < n; u += ngroups) {
+        const unsigned long long cu = vcmap[u];
+        const uint32_t e = rp[u + 1];
+        for (uint32_t j = rp[u] + lane; j < e; j += G) {
+            const uint32_t cv = __ldg(vcmap + __ldg(col + j));
+            const bool keep = cv != cu;
+            keys[j] = keep ? (cu << b | cv) : kNoKey;
+            c += keep;
+        }
+    }
+    c = warp_sum(c);
+    if ((threadIdx.x & 31) == 0) wsum[threadIdx.x >> 5] = c;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        unsigned long long t = 0;
+        for (int k = 0; k < (int)(blockDim.x >> 5); k++) t += wsum[k];
+        if (t) atomicAdd(kept, t);
+    }
+}
+
+// flag[i] = 1 where a run of equal (valid) keys starts
+__global__ void __launch_bounds__(256) k_sb_heads(uint64_t m, const unsigned long long *__restrict__ s,
+                                                  uint32_t *__restrict__ flag) {
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < m; i += (uint64_t)gridDim.x * blockDim.x) {
+        const unsigned long long k = s[i];
+        flag[i] = (k != kNoKey && (i == 0 || s[i - 1] != k)) ? 1u : 0u;
+    }
+}
+
+// heads: destination, run start and the coarse row's entry count (rows are
+// sorted, so a warp's heads mostly share rows: one atomic per row per warp)
+__global__ void __launch_bounds__(256) k_sb_emit(uint64_t m, const unsigned long long *__restrict__ s,
+                                                 const uint32_t *__restrict__ pos, int b,
+                                                 uint32_t *__restrict__ ccol, uint32_t *__restrict__ start,
+                                                 uint32_t *__restrict__ rcnt) {
+    const unsigned long long mask = (1ull << b) - 1;
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    for (uint64_t i0 = (uint64_t)blockIdx.x * blockDim.x; i0 < m; i0 += stride) {
+        const uint64_t i = i0 + threadIdx.x;
+        const bool head = i < m && pos[i + 1] != pos[i];
+        uint32_t row = 0xFFFFFFFFu;
+        if (head) {
+            const unsigned long long k = s[i];
+            const uint32_t p = pos[i];
+            ccol[p] = (uint32_t)(k & mask);
+            start[p] = (uint32_t)i;
+            row = (uint32_t)(k >> b);
+        }
+        const unsigned act = __ballot_sync(0xFFFFFFFFu, head);
+        if (head) {
+            const unsigned peers = __match_any_sync(act, row);
+            if ((int)(threadIdx.x & 31) == __ffs(peers) - 1) atomicAdd(rcnt + row, (uint32_t)__popc(peers));
+        }
+    }
+}
+
+template <typename WO>
+__global__ void __launch_bounds__(256) k_sb_weights(uint32_t mc, const uint32_t *__restrict__ start, uint64_t nvalid,
+                                                    WO *__restrict__ cw) {
+    for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < mc; p += gridDim.x * blockDim.x) {
+        const uint64_t e = p + 1 < mc ? (uint64_t)start[p + 1] : nvalid;
+        cw[p] = (WO)(e - start[p]);
+    }
+}
+
+// unit-weight levels with at least this many entries take the sorted build
+// (SGPB_BUILD_SORTED=0 turns it off, =1 forces it for every unit-weight level)
+constexpr uint64_t kSortedBuildMin = 1ull << 22;
+
+static bool sorted_build_wanted(const Level &F) {
+    if (F.w || F.m == 0) return false;
+    const char *e = getenv("SGPB_BUILD_SORTED");
+    if (e && *e) return atoi(e) != 0;
+    return F.m >= kSortedBuildMin;
+}
+
+template <typename WO>
+static int build_sorted_unit(Context &C, const Level &F, const uint32_t *vcmap, uint32_t nc, uint32_t *crp,
+                             uint32_t **ccol_io, WO **cw_io, uint64_t *m_c, bool alloc_out) {
+    const uint32_t n = F.n;
+    const uint64_t m = F.m;
+    // 2^b > nc: a valid key's low 2b bits are never all ones, so the
+    // sentinels sort after every valid key
+    int b = 1;
+    while (b < 32 && (1ull << b) <= (uint64_t)nc) b++;
+    unsigned long long *keys, *tmp, *kept;
+    uint32_t *flag, *pos, *rcnt;
+    SGPB_TRY(dalloc_t(C, &keys, m));
+    SGPB_TRY(dalloc_t(C, &tmp, m));
+    SGPB_TRY(dalloc_t(C, &kept, 1));
+    SGPB_TRY(dalloc_t(C, &flag, m + 1));
+    SGPB_TRY(dalloc_t(C, &pos, m + 1));
+    SGPB_TRY(dalloc_t(C, &rcnt, (size_t)nc + 1));
+    SGPB_TRY(dzero(C, kept, 8));
+    SGPB_TRY(dzero(C, rcnt, sizeof(uint32_t) * ((size_t)nc + 1)));
+    const double avg = n ? (double)m / n : 0;
+    const uint32_t cap = (uint32_t)C.num_sms * 16;
+    auto rows_grid = [&](int G) {
+        uint32_t g = cdiv((uint64_t)n * G, 256);
+        return g > cap ? cap : (g ? g : 1u);
+    };
+    if (avg <= 4) k_sb_keys<4><<<rows_grid(4), 256, 0, C.stream>>>(n, F.rp, F.col, vcmap, b, keys, kept);
+    else if (avg <= 16) k_sb_keys<16><<<rows_grid(16), 256, 0, C.stream>>>(n, F.rp, F.col, vcmap, b, keys, kept);
+    else k_sb_keys<32><<<rows_grid(32), 256, 0, C.stream>>>(n, F.rp, F.col, vcmap, b, keys, kept);
+    C.kernel_launches++;
+    bool in_tmp = false;
+    SGPB_TRY(radix_sort_keys(C, keys, m, 2 * b, tmp, &in_tmp));
+    const unsigned long long *sk = in_tmp ? tmp : keys;
+    const uint32_t eg = (uint32_t)(cdiv(m, 256) > cap ? cap : cdiv(m, 256));
+    k_sb_heads<<<eg, 256, 0, C.stream>>>(m, sk, flag);
+    C.kernel_launches++;
+    SGPB_TRY(scan_u32(C, flag, pos, (uint32_t)m, nullptr));
+    uint32_t mc = 0;
+    uint64_t nvalid = 0;
+    SGPB_TRY(read_u32(C, pos + m, &mc));
+    SGPB_TRY(read_u64(C, (const uint64_t *)kept, &nvalid));
+    *m_c = mc;
+    if (alloc_out) {
+        SGPB_TRY(dalloc_t(C, ccol_io, (size_t)mc + 1));
+        SGPB_TRY(dalloc_t(C, cw_io, (size_t)mc + 1));
+    }
+    uint32_t *start;
+    SGPB_TRY(dalloc_t(C, &start, (size_t)mc + 1));
+    k_sb_emit<<<eg, 256, 0, C.stream>>>(m, sk, pos, b, *ccol_io, start, rcnt);
+    C.kernel_launches++;
+    SGPB_TRY(scan_u32(C, rcnt, crp, nc, nullptr));
+    if (mc) {
+        const uint32_t wg = (uint32_t)(cdiv(mc, 256) > cap ? cap : cdiv(mc, 256));
+        k_sb_weights<WO><<<wg, 256, 0, C.stream>>>(mc, start, nvalid, *cw_io);
+        C.kernel_launches++;
+    }
+    SGPB_CUDA(cudaGetLastError());
+    return SGP_B200_OK;
+}
+
 // Builds level `out` (allocating its arrays from the context) from F + vcmap.
 int build_coarse_level(Context &C, const Level &F, const uint32_t *vcmap, uint32_t nc, int out_wbytes,
                        Level *out) {
@@ -653,6 +808,20 @@ int build_coarse_level(Context &C, const Level &F, const uint32_t *vcmap, uint32
     if (F.wbytes == 8 && out_wbytes != 8) {
         set_error("coarse weights must be at least as wide as fine weights");
         return SGP_B200_ERR_INVALID;
+    }
+    if (sorted_build_wanted(F)) {
+        if (out_wbytes == 8) {
+            unsigned long long *cw = nullptr;
+            SGPB_TRY((build_sorted_unit<unsigned long long>(C, F, vcmap, nc, crp, &ccol, &cw, &mc, true)));
+            out->w = cw;
+        } else {
+            uint32_t *cw = nullptr;
+            SGPB_TRY((build_sorted_unit<uint32_t>(C, F, vcmap, nc, crp, &ccol, &cw, &mc, true)));
+            out->w = cw;
+        }
+        out->col = ccol;
+        out->m = mc;
+        return SGP_B200_OK;
     }
     if (out_wbytes == 8) {
         unsigned long long *cw = nullptr;
@@ -679,6 +848,14 @@ int build_coarse_into(Context &C, const Level &F, const uint32_t *vcmap, uint32_
     if (F.wbytes == 8 && out_wbytes != 8) {
         set_error("coarse weights must be at least as wide as fine weights");
         return SGP_B200_ERR_INVALID;
+    }
+    if (sorted_build_wanted(F)) {
+        if (out_wbytes == 8) {
+            unsigned long long *w8 = (unsigned long long *)cw;
+            return build_sorted_unit<unsigned long long>(C, F, vcmap, nc, crp, &ccol, &w8, m_c, false);
+        }
+        uint32_t *w4 = (uint32_t *)cw;
+        return build_sorted_unit<uint32_t>(C, F, vcmap, nc, crp, &ccol, &w4, m_c, false);
     }
     if (out_wbytes == 8) {
         unsigned long long *w8 = (unsigned long long *)cw;
