@@ -662,11 +662,22 @@ __global__ void __launch_bounds__(256) k_sb_keys(uint32_t n, const uint32_t *__r
     for (uint64_t u = gid; u < n; u += ngroups) {
         const unsigned long long cu = vcmap[u];
         const uint32_t e = rp[u + 1];
-        for (uint32_t j = rp[u] + lane; j < e; j += G) {
-            const uint32_t cv = __ldg(vcmap + __ldg(col + j));
-            const bool keep = cv != cu;
-            keys[j] = keep ? (cu << b | cv) : kNoKey;
-            c += keep;
+        // four entries per lane in flight: destinations, then their vcmap gathers
+        for (uint32_t j0 = rp[u] + lane; j0 < e; j0 += 4 * G) {
+            uint32_t d[4];
+#pragma unroll
+            for (int q = 0; q < 4; q++) d[q] = j0 + q * G < e ? __ldg(col + j0 + q * G) : 0u;
+            uint32_t cv[4];
+#pragma unroll
+            for (int q = 0; q < 4; q++) cv[q] = j0 + q * G < e ? __ldg(vcmap + d[q]) : 0u;
+#pragma unroll
+            for (int q = 0; q < 4; q++) {
+                if (j0 + q * G < e) {
+                    const bool keep = cv[q] != cu;
+                    keys[j0 + q * G] = keep ? (cu << b | cv[q]) : kNoKey;
+                    c += keep;
+                }
+            }
         }
     }
     c = warp_sum(c);
