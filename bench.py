@@ -9,7 +9,10 @@ duplicates merged, self loops dropped, largest connected component kept).
          device (FP64 path), whole job over all ranks
   e2e    the same through the public API with pinned host buffers: the CSR
          upload and the partition download are inside the timed region
-  mixed  FP32-storage / FP64-reduction power iteration on the same graph
+  mixed  the mixed-precision power iteration on the same graph (FP32
+         edge-difference SpMV arithmetic; FP64 iterate, shift, deflation,
+         normalisation, dot product and stopping test), its cut and its
+         Fiedler value against the FP64 run
   fm     the same partition followed by up to 16 FM passes (cut and time)
 
 Multi-GPU: the single-graph path does not shard (a row partition would need

@@ -151,8 +151,12 @@ typedef struct {
 typedef struct {
     uint32_t cutoff;            /* coarsen while n > cutoff (reference: 50) */
     double tol;                 /* power-iteration tolerance (reference: 1e-10) */
-    int mixed;                  /* 0: FP64 vectors; 1: FP32 vector storage and
-                                   gathers with FP64 reductions (+ FP64 polish) */
+    int mixed;                  /* 0: FP64 SpMV; 1: mixed precision -- on levels of
+                                   >= 4096 vertices the Laplacian is applied as
+                                   sum_j w_ij (x_i - x_j) with FP32 differences,
+                                   products and row sums; the iterate, shift,
+                                   deflation, normalisation, dot product and
+                                   stopping test stay FP64 */
     int perc_imbalance;         /* sgp_compute_partition's perc_imbalance_allowed */
     uint64_t iter_cap;          /* extra cap on power iterations per level, 0 = none */
     uint64_t rng_state, rng_inc;/* PCG32 seeding (advanced copy returned in result) */
@@ -204,6 +208,15 @@ typedef struct {
 } sgp_b200_result_t;
 
 void sgp_b200_default_options(sgp_b200_options_t *opt);
+
+/* The options sgp_partition_graph (sgpar.h:2363) runs with for a config_t:
+ * tolerance (the change_tol default when config->tol <= 0), refine_alg,
+ * local_search_alg, the coarsener coarsening_alg's bits select (bit 4: none;
+ * bit 0: heavy-edge matching with the 0.9 ratio stop; else HEC,
+ * sgpar.h:2457-2475), perc_imbalance_allowed and the rng's state.
+ * SGP_B200_ERR_INVALID for a refine_alg other than 0 or 1. */
+int sgp_b200_config_options(const config_t *config, int perc_imbalance_allowed, const sgp_pcg32_random_t *rng,
+                            sgp_b200_options_t *opt);
 
 /* The whole path on one graph (the body of sgp_partition_graph). */
 int sgp_b200_partition(sgp_b200_ctx_t *ctx, const sgp_b200_graph_t *g,
@@ -322,9 +335,12 @@ int sgp_b200_split(sgp_b200_ctx_t *ctx, uint32_t n, const uint32_t *row_ptr, con
  * SGP_B200_ERR_TOO_LARGE.  Asynchronous on `stream` (a cudaStream_t, NULL =
  * default stream): part (n entries) and result (device array: result[0] =
  * edge cut, result[1] = size of part 0) are valid once the stream has
- * reached the call.  The first call on a device looks up the scratch address
- * and should come before any stream capture.  All calls on a device share the
- * scratch: calls that overlap on the GPU race and must be serialised. */
+ * reached the call.  `stream` must belong to the current device
+ * (SGP_B200_ERR_INVALID otherwise).  The first call on a device looks up the
+ * scratch address and should come before any stream capture; the look-up is
+ * repeated when the device's context has changed (after cudaDeviceReset).
+ * All calls on a device share the scratch: calls that overlap on the GPU
+ * race and must be serialised. */
 int sgp_b200_split_noalloc(void *stream, uint32_t n, const uint32_t *row_ptr, const uint32_t *col,
                            const double *evec, uint32_t *part, uint64_t *result);
 

@@ -87,6 +87,7 @@ _SIGS = {
     "sgp_b200_last_error": (ctypes.c_char_p, []),
     "sgp_b200_stream": (c_vp, [c_vp]),
     "sgp_b200_default_options": (None, [P(sgp_b200_options_t)]),
+    "sgp_b200_config_options": (c_int, [P(config_t), c_int, P(sgp_pcg32_random_t), P(sgp_b200_options_t)]),
     "sgp_b200_partition": (c_int, [c_vp, P(sgp_b200_graph_t), P(sgp_b200_options_t), P(sgp_b200_result_t)]),
     "sgp_b200_partition_4way": (c_int, [c_vp, P(sgp_b200_graph_t), P(sgp_b200_options_t), c_vp, P(c_u64)]),
     "sgp_b200_partition_batch": (c_int, [c_vp, P(sgp_b200_graph_t), c_int, P(sgp_b200_options_t),

@@ -4,6 +4,9 @@
   ``include/sgpar_b200.h`` (``csrc/*.cu`` + ``csrc/io.cpp``), built with nvcc
   for ``arch=compute_100a,code=sm_100a``.
 * ``libsgpgen.so`` -- the synthetic graph generators (``csrc/graphgen.cpp``).
+* ``sgpar_b200`` -- the config-file driver command (``csrc/sgpar_main.c``,
+  the reference's ``sgpar.cpp`` main), linked against ``libsgpar_b200.so``
+  with an rpath to this directory.
 
 Objects go to ``_build/``; the libraries sit next to this file so that they
 travel with the source tree.  Rebuilds are skipped when outputs are newer than
@@ -23,6 +26,7 @@ CSRC = os.path.join(HERE, "csrc")
 BUILD = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "libsgpar_b200.so")
 GENLIB = os.path.join(HERE, "libsgpgen.so")
+DRIVER = os.path.join(HERE, "sgpar_b200")
 
 NVCC_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-lineinfo", "-std=c++17",
               "-Xcompiler", "-fPIC", "-Xcompiler", "-O3"]
@@ -89,9 +93,19 @@ def build_gen(force: bool = False) -> str:
     return GENLIB
 
 
+def build_driver(force: bool = False) -> str:
+    src = os.path.join(CSRC, "sgpar_main.c")
+    hdr = os.path.join(ROOT, "include", "sgpar_b200.h")
+    if force or _stale(DRIVER, [src, hdr, LIB]):
+        _run(["gcc", "-O2", "-std=c11", "-Wall", "-o", DRIVER, src, "-L" + HERE, "-lsgpar_b200",
+              "-Wl,-rpath,$ORIGIN"])
+    return DRIVER
+
+
 def build_all(force: bool = False, verbose: bool = False) -> None:
     build_gen(force)
     build_lib(verbose=verbose, force=force)
+    build_driver(force)
 
 
 if __name__ == "__main__":

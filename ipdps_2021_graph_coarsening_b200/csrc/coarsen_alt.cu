@@ -320,7 +320,7 @@ int match_map_level(Context &C, const Level &L, int random_level, uint64_t seed,
     SGPB_TRY(dzero(C, a.counters, sizeof(uint32_t) * 2));
     SGPB_CUDA(cudaMemsetAsync(vcmap, 0xFF, sizeof(uint32_t) * n, C.stream));
     // two rounds assign at least one pair while anything is listed
-    a.round_cap = (uint32_t)((uint64_t)n + 4 < 0xFFFFFFF0u ? n + 4 : 0xFFFFFFF0u);
+    a.round_cap = round_budget((uint64_t)n + 4);
     uint32_t grid = 1;
     SGPB_TRY(coop_grid_alt(C, (const void *)k_match_map, 512, n, &grid));
     SGPB_TRY(dalloc_t(C, &a.block_tot, grid));
@@ -695,7 +695,7 @@ static int set_iterations(Context &C, const Level &L, bool gosh, uint64_t seed, 
     const uint64_t thr = gosh ? L.m / n + 1 : 0;
     const double avg = (double)L.m / n;
     const int hops = gosh ? 1 : 2;
-    const uint32_t cap = 4 * n + 16;
+    const uint32_t cap = round_budget(4 * (uint64_t)n + 16);
     int it = 0;
     for (;; it++) {
         if ((uint32_t)it > cap) {

@@ -918,6 +918,32 @@ int sgp_b200_split(sgp_b200_ctx_t *x, uint32_t n, const uint32_t *rp, const uint
     return rc;
 }
 
+int sgp_b200_config_options(const config_t *config, int perc_imbalance_allowed, const sgp_pcg32_random_t *rng,
+                            sgp_b200_options_t *o) {
+    if (!config || !rng || !o) {
+        set_error("null argument");
+        return SGP_B200_ERR_INVALID;
+    }
+    if (config->refine_alg != 0 && config->refine_alg != 1) {
+        set_error("refine_alg must be 0 (shifted combinatorial Laplacian) or 1 (normalized Laplacian)");
+        return SGP_B200_ERR_INVALID;
+    }
+    sgp_b200_default_options(o);
+    o->tol = config->tol > 0 ? config->tol : g_tol;
+    o->refine_alg = config->refine_alg;
+    // sgpar.h:2457-2475: bit 4 skips coarsening, bit 0 picks heavy-edge
+    // matching with the 0.9 coarsening-ratio stop (bits 1-2 choose a dedupe
+    // method, which does not change the coarse graph)
+    o->coarsener = (config->coarsening_alg & 16) ? SGP_B200_COARSEN_NONE
+                   : (config->coarsening_alg & 1) ? (SGP_B200_COARSEN_MATCH | SGP_B200_COARSEN_RATIO_STOP)
+                                                  : SGP_B200_COARSEN_HEC;
+    o->perc_imbalance = perc_imbalance_allowed;
+    o->local_search_alg = config->local_search_alg;
+    o->rng_state = rng->state;
+    o->rng_inc = rng->inc;
+    return SGP_B200_OK;
+}
+
 // ------------------------------------------------------ sgpar.h API --
 int sgp_partition_graph(sgp_vid_t *part, sgp_eid_t *edge_cut, config_t *config, const int perc_imbalance_allowed,
                         const sgp_graph_t g, sgp_pcg32_random_t *rng) {
@@ -939,19 +965,7 @@ int sgp_partition_graph(sgp_vid_t *part, sgp_eid_t *edge_cut, config_t *config, 
     dg.w = g.eweights;
     dg.mem = SGP_B200_HOST;
     sgp_b200_options_t o;
-    sgp_b200_default_options(&o);
-    o.tol = config->tol > 0 ? config->tol : g_tol;
-    o.refine_alg = config->refine_alg;
-    // sgpar.h:2457-2475: bit 4 skips coarsening, bit 0 picks heavy-edge
-    // matching with the 0.9 coarsening-ratio stop (bits 1-2 choose a dedupe
-    // method, which does not change the coarse graph)
-    o.coarsener = (config->coarsening_alg & 16) ? SGP_B200_COARSEN_NONE
-                  : (config->coarsening_alg & 1) ? (SGP_B200_COARSEN_MATCH | SGP_B200_COARSEN_RATIO_STOP)
-                                                 : SGP_B200_COARSEN_HEC;
-    o.perc_imbalance = perc_imbalance_allowed;
-    o.local_search_alg = config->local_search_alg;
-    o.rng_state = rng->state;
-    o.rng_inc = rng->inc;
+    if (sgp_b200_config_options(config, perc_imbalance_allowed, rng, &o) != SGP_B200_OK) return 1;
     sgp_b200_result_t *r = (sgp_b200_result_t *)calloc(1, sizeof(sgp_b200_result_t));
     if (!r) return 1;
     r->part = part;

@@ -27,9 +27,17 @@
 // short-row graphs (grids, the finest R-MAT level) stream as well as dense
 // coarse levels.
 //
-// V is the vector storage type: double (plain FP64) or float (mixed
-// precision: FP32 storage, gathers and row sums; FP64 reductions, deflation,
-// normalisation and stopping test).
+// Precision.  The iterate is stored and gathered in FP64 (V = double).  MX
+// selects the SpMV arithmetic: false -- FP64 row sums of w_ij x_j (plain);
+// true -- mixed precision: the Laplacian is applied in edge-difference form,
+// (L x)_i = sum_j w_ij (x_i - x_j), each difference rounded to FP32 and the
+// products and row sums formed in FP32, while the shift gb u_i, the
+// deflation, the normalisation, the dot product and the stopping test stay
+// FP64.  The FP32 rounding then scales with |x_i - x_j| instead of with the
+// shifted iterate (about gb |u_i|), which keeps the mixed recurrence on the
+// FP64 trajectory: an FP32-stored iterate would add a relative noise of
+// about 6e-8 per element and iteration, and the shifted power iteration
+// amplifies such noise by roughly gb / (lambda_3 - lambda_2).
 #include <math.h>
 #include <stdlib.h>
 #include <string.h>
@@ -73,9 +81,7 @@ struct PIArgs {
     double *partials;             // [2][gridDim][kNP]
     double tol;
     uint64_t iter_max;
-    double stall_factor;          // > 0: stop when |d dot| has not halved within stall_window iterations
-    uint32_t stall_window;
-    double *res;                  // [0] niter [1] dot [2] gb [3] lambda [4] capped [5] stalled
+    double *res;                  // [0] niter [1] dot [2] gb [3] lambda [4] capped
     const uint32_t *inv;          // relabelled copy: new id -> level vertex id (null: identity)
     uint32_t kcache;              // leading iterate entries: shared-memory copy, or the L1 hub prefix
     int cache_ok;                 // host: 2 shared-memory copy when it fits, 3 L1 hub prefix, 0 none
@@ -122,19 +128,9 @@ __device__ __forceinline__ double ld_hub(const double *p) {
     asm volatile("ld.global.L1::evict_last.f64 %0, [%1];" : "=d"(v) : "l"(p));
     return v;
 }
-__device__ __forceinline__ float ld_hub(const float *p) {
-    float v;
-    asm volatile("ld.global.L1::evict_last.f32 %0, [%1];" : "=f"(v) : "l"(p));
-    return v;
-}
 __device__ __forceinline__ double ld_tail(const double *p) {
     double v;
     asm volatile("ld.global.L1::no_allocate.f64 %0, [%1];" : "=d"(v) : "l"(p));
-    return v;
-}
-__device__ __forceinline__ float ld_tail(const float *p) {
-    float v;
-    asm volatile("ld.global.L1::no_allocate.f32 %0, [%1];" : "=f"(v) : "l"(p));
     return v;
 }
 template <typename V>
@@ -195,35 +191,6 @@ __device__ __forceinline__ uint32_t lower_bound_u32(const uint32_t *pre, uint32_
     return lo;
 }
 
-// acc += sum_j w_j src[col_j] over j = j0, j0 + s, ... < e, four predicated
-// entries in flight per thread (used for block-wide rows).  S is the iterate
-// source: a plain pointer, or an XView when a shared-memory cache is in use.
-template <typename W, typename V, typename ACC, typename S>
-__device__ __forceinline__ void row_accum(const uint32_t *__restrict__ col, const W *__restrict__ w, const S &src,
-                                          uint32_t j, uint32_t e, uint32_t s, ACC &acc) {
-    for (; j < e; j += 4 * s) {
-        const bool p1 = j + s < e, p2 = j + 2 * s < e, p3 = j + 3 * s < e;
-        const uint32_t c0 = __ldg(col + j);
-        const uint32_t c1 = p1 ? __ldg(col + j + s) : 0u;
-        const uint32_t c2 = p2 ? __ldg(col + j + 2 * s) : 0u;
-        const uint32_t c3 = p3 ? __ldg(col + j + 3 * s) : 0u;
-        V x0 = src[c0];
-        V x1 = p1 ? src[c1] : (V)0;
-        V x2 = p2 ? src[c2] : (V)0;
-        V x3 = p3 ? src[c3] : (V)0;
-        if (w) {
-            x0 *= (V)__ldg(w + j);
-            if (p1) x1 *= (V)__ldg(w + j + s);
-            if (p2) x2 *= (V)__ldg(w + j + 2 * s);
-            if (p3) x3 *= (V)__ldg(w + j + 3 * s);
-        }
-        acc += (ACC)x0;
-        acc += (ACC)x1;
-        acc += (ACC)x2;
-        acc += (ACC)x3;
-    }
-}
-
 // Streaming loads of the matrix (destinations, weights): read-only and read
 // once per iteration, so they bypass L1 allocation and leave L1 to the
 // gathered vector entries (NA = true).
@@ -265,16 +232,31 @@ __device__ __forceinline__ unsigned long long ld_stream(const unsigned long long
     return __ldg(p);
 }
 
-// acc += sum_j w_j src[col_j] (and dsum += sum_j w_j) over the row entries
-// j = j0, j0 + 32, ... < e of one warp (j0 = row start + lane): U predicated
-// entries in flight per lane, destinations and weights first, then the U
-// gathers.
-template <int U, bool NA, typename W, typename V, typename ACC, typename S>
+// One SpMV term of row i for destination value xj and weight wt (weighted:
+// HAS_W): plain, w_ij x_j in the iterate type; mixed (MX), the edge
+// difference w_ij (x_i - x_j) with the difference rounded to FP32 and the
+// product formed in FP32.
+template <bool MX, typename ACC, typename V, typename W>
+__device__ __forceinline__ ACC spmv_term(bool HAS_W, V xi, V xj, W wt) {
+    if constexpr (MX) {
+        const float dx = (float)(xi - xj);
+        return HAS_W ? (float)wt * dx : dx;
+    } else {
+        return (ACC)(HAS_W ? (V)wt * xj : xj);
+    }
+}
+
+// acc += sum_j term(w_j, src[col_j]) (and dsum += sum_j w_j) over the row
+// entries j = j0, j0 + 32, ... < e of one warp (j0 = row start + lane): U
+// predicated entries in flight per lane, destinations and weights first,
+// then the U gathers.  xi: the row's own iterate value (used when MX).
+template <int U, bool NA, bool MX, typename W, typename V, typename ACC, typename S>
 __device__ __forceinline__ void warp_row_accum(const uint32_t *__restrict__ col, const W *__restrict__ w,
-                                               const S &src, uint32_t j, uint32_t e, ACC &acc, uint64_t &dsum) {
+                                               const S &src, uint32_t j, uint32_t e, V xi, ACC &acc,
+                                               uint64_t &dsum) {
     for (; j < e; j += 32 * U) {
         uint32_t c[U];
-        V x[U];
+        ACC x[U];
 #pragma unroll
         for (int k = 0; k < U; k++) c[k] = (j + 32 * k < e) ? ld_stream<NA>(col + j + 32 * k) : 0u;
         if (w) {
@@ -283,15 +265,15 @@ __device__ __forceinline__ void warp_row_accum(const uint32_t *__restrict__ col,
             for (int k = 0; k < U; k++) wt[k] = (j + 32 * k < e) ? ld_stream<NA>(w + j + 32 * k) : (W)0;
 #pragma unroll
             for (int k = 0; k < U; k++) {
-                x[k] = (j + 32 * k < e) ? (V)wt[k] * src[c[k]] : (V)0;
+                x[k] = (j + 32 * k < e) ? spmv_term<MX, ACC>(true, xi, src[c[k]], wt[k]) : (ACC)0;
                 dsum += (uint64_t)wt[k];
             }
         } else {
 #pragma unroll
-            for (int k = 0; k < U; k++) x[k] = (j + 32 * k < e) ? src[c[k]] : (V)0;
+            for (int k = 0; k < U; k++) x[k] = (j + 32 * k < e) ? spmv_term<MX, ACC>(false, xi, src[c[k]], (W)0) : (ACC)0;
         }
 #pragma unroll
-        for (int k = 0; k < U; k++) acc += (ACC)x[k];
+        for (int k = 0; k < U; k++) acc += x[k];
     }
 }
 
@@ -299,9 +281,10 @@ __device__ __forceinline__ void warp_row_accum(const uint32_t *__restrict__ col,
 // software-pipelined: the destinations and weights of the next trip (in the
 // same row or the next processed row) are loaded before the gathers of the
 // current trip, so DRAM latency overlaps the L2 gathers; a row's own value
-// and weighted degree are loaded with its first trip.  Rows for which
-// skip(len) holds are left out.  fin(i, sum, d, xi) on lane 0 once per row.
-template <bool NA, typename W, typename V, typename ACC, typename S, typename Skip, typename Fin>
+// and weighted degree are loaded with its first trip (by every lane when MX,
+// whose terms use it).  Rows for which skip(len) holds are left out.
+// fin(i, sum, d, xi) on lane 0 once per row.
+template <bool NA, bool MX, typename W, typename V, typename ACC, typename S, typename Skip, typename Fin>
 __device__ __forceinline__ void warp_rows_pipelined(const uint32_t *__restrict__ rp, const uint32_t *__restrict__ col,
                                                     const W *__restrict__ w, const S &src, const double *deg,
                                                     uint32_t r0, uint32_t r1, Skip skip, Fin &fin) {
@@ -327,11 +310,9 @@ __device__ __forceinline__ void warp_rows_pipelined(const uint32_t *__restrict__
         c_cur[k] = j < ce ? ld_stream<NA>(col + j) : 0u;
         if (w) w_cur[k] = j < ce ? ld_stream<NA>(w + j) : (W)0;
     }
-    double cx = 0, cd = 0;   // own value and weighted degree of row ci (lane 0)
-    if (lane == 0) {
-        cx = (double)src[ci];
-        cd = w ? deg[ci] : (double)(ce - cb);
-    }
+    double cx = 0, cd = 0;   // own value and weighted degree of row ci (lane 0; cx on every lane when MX)
+    if (MX || lane == 0) cx = (double)src[ci];
+    if (lane == 0) cd = w ? deg[ci] : (double)(ce - cb);
     ACC acc = 0;
     while (true) {
         // position of the next trip
@@ -352,17 +333,21 @@ __device__ __forceinline__ void warp_rows_pipelined(const uint32_t *__restrict__
             if (w) w_nxt[k] = ok ? ld_stream<NA>(w + j) : (W)0;
         }
         double nx = cx, nd = cd;
-        if (row_ends && have_next && lane == 0) {
-            nx = (double)src[ni];
-            nd = w ? deg[ni] : (double)(ne - nb);
+        if (row_ends && have_next) {
+            if (MX || lane == 0) nx = (double)src[ni];
+            if (lane == 0) nd = w ? deg[ni] : (double)(ne - nb);
         }
         // gathers of the current trip
 #pragma unroll
         for (int k = 0; k < 4; k++) {
             const bool ok = cj + lane + 32 * k < ce;
-            V x = ok ? src[c_cur[k]] : (V)0;
-            if (w) x *= (V)w_cur[k];
-            acc += (ACC)x;
+            if constexpr (MX) {
+                if (ok) acc += spmv_term<true, ACC>(w != nullptr, (V)cx, src[c_cur[k]], w ? w_cur[k] : (W)0);
+            } else {
+                V x = ok ? src[c_cur[k]] : (V)0;
+                if (w) x *= (V)w_cur[k];
+                acc += (ACC)x;
+            }
         }
         if (row_ends) {
             const ACC t = warp_sum(acc);
@@ -433,7 +418,7 @@ __device__ __forceinline__ void load4(const uint32_t *__restrict__ col, const W 
 // Stream the rows [ra, rb) (all non-empty, none block-wide) through one warp.
 // fin(i, sum, degree, own value) is called exactly once per row, by one lane.
 // win: this warp's kWin-entry shared-memory window of row offsets.
-template <bool NA, typename W, typename V, typename ACC, typename S, typename Fin>
+template <bool NA, bool MX, typename W, typename V, typename ACC, typename S, typename Fin>
 __device__ __forceinline__ void warp_stream(const uint32_t *__restrict__ rp, const uint32_t *__restrict__ col,
                                             const W *__restrict__ w, const S &src, uint64_t m, bool vec,
                                             uint32_t ra, uint32_t rb, const double *deg, uint32_t *win, V *winx,
@@ -464,13 +449,12 @@ __device__ __forceinline__ void warp_stream(const uint32_t *__restrict__ rp, con
         uint32_t cc[4];
         W ww[4];
         load4<NA, W>(col, w, p, m, vec, cc, ww);
-        V prod[4];
+        V xg[4];
         bool valid[4];
 #pragma unroll
         for (int k = 0; k < 4; k++) {
             valid[k] = (p + k >= Ea) && (p + k < Eb);
-            V x = valid[k] ? src[cc[k]] : (V)0;
-            prod[k] = w ? (V)ww[k] * x : x;
+            xg[k] = valid[k] ? src[cc[k]] : (V)0;
         }
         __syncwarp();
         const uint32_t first = (Ea > c ? Ea : c);
@@ -500,6 +484,13 @@ __device__ __forceinline__ void warp_stream(const uint32_t *__restrict__ rp, con
                 slot[k] = s;
                 nvalid++;
             }
+        }
+        // the entries' terms (mixed: edge differences to the row's own value)
+        ACC prod[4];
+#pragma unroll
+        for (int k = 0; k < 4; k++) {
+            if constexpr (MX) prod[k] = valid[k] ? spmv_term<true, ACC>(w != nullptr, winx[slot[k]], xg[k], w ? ww[k] : (W)0) : (ACC)0;
+            else prod[k] = (ACC)(w ? (V)ww[k] * xg[k] : xg[k]);
         }
         // row slot s of this tile is complete with sum t
         auto done = [&](uint32_t s, ACC t) {
@@ -542,18 +533,18 @@ __device__ __forceinline__ void warp_stream(const uint32_t *__restrict__ rp, con
         const uint32_t prev_s3 = __shfl_up_sync(0xFFFFFFFFu, s3, 1);
         const int prev_v = __shfl_up_sync(0xFFFFFFFFu, (int)lv, 1);
         const bool cont_prev = lv && lane > 0 && prev_v && lane != lane_first && prev_s3 == s0;
-        ACC S = lv ? B : (ACC)0;
+        ACC Sc = lv ? B : (ACC)0;
         int F = (!lv || multi || !cont_prev) ? 1 : 0;
 #pragma unroll
         for (int d = 1; d < 32; d <<= 1) {
-            const ACC t = __shfl_up_sync(0xFFFFFFFFu, S, d);
+            const ACC t = __shfl_up_sync(0xFFFFFFFFu, Sc, d);
             const int tf = __shfl_up_sync(0xFFFFFFFFu, F, d);
             if (lane >= (unsigned)d) {
-                if (!F) S += t;
+                if (!F) Sc += t;
                 F |= tf;
             }
         }
-        const ACC S_prev = __shfl_up_sync(0xFFFFFFFFu, S, 1);
+        const ACC S_prev = __shfl_up_sync(0xFFFFFFFFu, Sc, 1);
         const uint32_t next_s0 = __shfl_down_sync(0xFFFFFFFFu, s0, 1);
         const int next_v = __shfl_down_sync(0xFFFFFFFFu, (int)lv, 1);
         // first run of a multi-run lane ends here
@@ -561,11 +552,11 @@ __device__ __forceinline__ void warp_stream(const uint32_t *__restrict__ rp, con
         // last run: ends here unless the next lane or the next tile continues it
         const bool next_cont = lane < 31 && next_v && next_s0 == s3;
         const bool tile_cont = lane == 31 && lv && win[s3 + 1] > c + kTile;
-        if (lv && !next_cont && !tile_cont) done(s3, S);
+        if (lv && !next_cont && !tile_cont) done(s3, Sc);
         // next tile starts in row cur + s3 of lane 31 (continued) or the row after
         const int tc = __shfl_sync(0xFFFFFFFFu, (int)tile_cont, 31);
         const uint32_t s31 = __shfl_sync(0xFFFFFFFFu, s3, 31);
-        const ACC S31 = __shfl_sync(0xFFFFFFFFu, S, 31);
+        const ACC S31 = __shfl_sync(0xFFFFFFFFu, Sc, 31);
         __syncwarp();
         if (tc) {
             cur += s31;
@@ -711,6 +702,23 @@ __device__ __forceinline__ void panel_rows32(const uint32_t *__restrict__ offp, 
     __syncwarp();
 }
 
+// The next raw iterate value r_i of row i from u_i = (x_i - mu) / nu and
+// its row sum acc (plain: sum_j w_ij x_j; MX: sum_j w_ij (x_i - x_j)):
+// shifted Laplacian r = (gb - d) u + A u = gb u - L u, or the lazy random
+// walk r = u / 2 + (A u)_i / (2 d) of the normalized variant (r = u / 2 for
+// an isolated vertex).  All in FP64.
+template <bool MX>
+__device__ __forceinline__ double next_value(int normlap, double gb, double mu, double inv_nu, double ui, double acc,
+                                             double d) {
+    if constexpr (MX) {
+        const double lu = acc * inv_nu;   // (L u)_i; the mean cancels in the differences
+        return normlap ? (d > 0 ? ui - 0.5 * lu / d : 0.5 * ui) : gb * ui - lu;
+    } else {
+        const double au = (acc - mu * d) * inv_nu;   // (A u)_i
+        return normlap ? 0.5 * ui + (d > 0 ? 0.5 * au / d : 0.0) : (gb - d) * ui + au;
+    }
+}
+
 template <int CACHE, typename V>
 __device__ __forceinline__ auto make_src(const V *g, const V *s, uint32_t k) {
     if constexpr (CACHE == kCachePrefix) return XView<V>{g, s, k};
@@ -724,8 +732,9 @@ __device__ __forceinline__ auto make_src(const V *g, const V *s, uint32_t k) {
 // NA: matrix loads bypass L1 allocation.  CACHE: kCachePrefix -- gathers read
 // the block's shared-memory copy of a small level's iterate; kCacheSplit --
 // gathers below kcache (the hub prefix of a relabelled level) use L1
-// evict-last priority, the others bypass L1 allocation.
-template <typename W, typename V, int MODE, bool NA, int CACHE>
+// evict-last priority, the others bypass L1 allocation.  MX: mixed-precision
+// arithmetic (FP32 edge-difference row sums; never with column panels).
+template <typename W, typename V, int MODE, bool NA, int CACHE, bool MX>
 __global__ void __launch_bounds__(kPIThreads, 2) k_power_iter(PIArgs a) {
     constexpr bool STREAM = MODE == 0;
     cg::grid_group grid = cg::this_grid();
@@ -735,7 +744,9 @@ __global__ void __launch_bounds__(kPIThreads, 2) k_power_iter(PIArgs a) {
     // per-row staging of the stream windows (unused by the warp-row variants)
     __shared__ V swinx[STREAM ? kPIWarps : 1][kTile];
     __shared__ double swind[STREAM ? kPIWarps : 1][kTile];
-    typedef typename std::conditional<sizeof(V) == 8, double, float>::type ACC;
+    static_assert(sizeof(V) == 8, "the iterate is stored in FP64");
+    static_assert(!(MX && MODE == 6), "column panels have no mixed-precision form");
+    typedef typename std::conditional<MX, float, double>::type ACC;
     // panels: per-warp row sums of a 32-row group, group counters (two, used
     // by alternate panels so one can be reset while the other is in use)
     constexpr bool PANEL = MODE == 6;
@@ -885,8 +896,6 @@ __global__ void __launch_bounds__(kPIThreads, 2) k_power_iter(PIArgs a) {
 
     // ---- iterations
     double dot = 0, last = 1;
-    double best_delta = 1e300;
-    uint64_t best_at = 0;
     uint64_t niter = 0;
     V *src = va, *dst = vb;
     uint32_t panel_seq = 0;   // panels processed so far: selects the group counter
@@ -904,12 +913,12 @@ __global__ void __launch_bounds__(kPIThreads, 2) k_power_iter(PIArgs a) {
             __syncthreads();
         }
         const auto xv = make_src<CACHE, V>(src, xs, kc);
-        // finalise row i from its sum of w_ij * src_j, its weighted degree d
-        // and its own raw iterate value xi
+        // finalise row i from its row sum acc (plain: sum_j w_ij src_j; MX:
+        // sum_j w_ij (src_i - src_j)), its weighted degree d and its own raw
+        // iterate value xi
         auto fin = [&](uint32_t i, ACC acc, double d, double xi) {
             const double ui = (xi - mu) * inv_nu;
-            const double au = ((double)acc - mu * d) * inv_nu;   // (A u)_i
-            const double r = a.normlap ? 0.5 * ui + (d > 0 ? 0.5 * au / d : 0.0) : (gb - d) * ui + au;
+            const double r = next_value<MX>(a.normlap, gb, mu, inv_nu, ui, (double)acc, d);
             const V rs = (V)r;
             dst[i] = rs;
             const double rd = (double)rs;
@@ -921,10 +930,11 @@ __global__ void __launch_bounds__(kPIThreads, 2) k_power_iter(PIArgs a) {
             uint32_t seg = w_r0;
             for (uint32_t h = wh0; h < wh1; h++) {
                 const uint32_t hr = a.heavy[h];
-                warp_stream<NA, W, V, ACC>(a.rp, a.col, w, xv, a.m, a.vec_ok, seg, hr, a.deg, win, winx, wind, fin);
+                warp_stream<NA, MX, W, V, ACC>(a.rp, a.col, w, xv, a.m, a.vec_ok, seg, hr, a.deg, win, winx, wind,
+                                               fin);
                 seg = hr + 1;
             }
-            warp_stream<NA, W, V, ACC>(a.rp, a.col, w, xv, a.m, a.vec_ok, seg, w_r1, a.deg, win, winx, wind, fin);
+            warp_stream<NA, MX, W, V, ACC>(a.rp, a.col, w, xv, a.m, a.vec_ok, seg, w_r1, a.deg, win, winx, wind, fin);
         } else if (PANEL) {
             // column panels: the block copies panel p of the iterate into
             // shared memory, then its warps take 32-row groups of the block's
@@ -970,7 +980,7 @@ __global__ void __launch_bounds__(kPIThreads, 2) k_power_iter(PIArgs a) {
         } else if (MODE == 5) {
             const uint32_t T = a.heavy_T;
             auto skip = [T](uint32_t len) { return len > T || len == 0; };
-            warp_rows_pipelined<NA, W, V, ACC>(a.rp, a.col, w, xv, a.deg, w_r0, w_r1, skip, fin);
+            warp_rows_pipelined<NA, MX, W, V, ACC>(a.rp, a.col, w, xv, a.deg, w_r0, w_r1, skip, fin);
         } else {
             uint32_t e = w_r0 < w_r1 ? a.rp[w_r0] : 0;
             for (uint32_t i = w_r0; i < w_r1; i++) {
@@ -979,10 +989,10 @@ __global__ void __launch_bounds__(kPIThreads, 2) k_power_iter(PIArgs a) {
                 if (e - b > a.heavy_T || e == b) continue;   // block-wide rows
                 // the row's own value is loaded before its entries so the
                 // latency overlaps; the weighted degree is summed on the way
-                const double xi = lane == 0 ? (double)src[i] : 0.0;
+                const double xi = (MX || lane == 0) ? (double)src[i] : 0.0;
                 ACC acc = 0;
                 uint64_t ds = 0;
-                warp_row_accum<(MODE == 8 ? 8 : 4), NA, W, V, ACC>(a.col, w, xv, b + lane, e, acc, ds);
+                warp_row_accum<(MODE == 8 ? 8 : 4), NA, MX, W, V, ACC>(a.col, w, xv, b + lane, e, (V)xi, acc, ds);
                 acc = warp_sum(acc);
                 if (w) ds = warp_sum(ds);
                 if (lane == 0) fin(i, acc, w ? (double)ds : (double)(e - b), xi);
@@ -1003,9 +1013,10 @@ __global__ void __launch_bounds__(kPIThreads, 2) k_power_iter(PIArgs a) {
                 const uint32_t e = a.rp[i + 1];
                 const uint32_t b = a.rp[i] + ((sg - a.hseg[i]) << a.seg_shift);
                 const uint32_t e2 = e - b > (1u << a.seg_shift) ? b + (1u << a.seg_shift) : e;
+                const V xi = MX ? src[i] : (V)0;
                 ACC acc = 0;
                 uint64_t ds = 0;
-                warp_row_accum<8, NA, W, V, ACC>(a.col, w, xv, b + lane, e2, acc, ds);
+                warp_row_accum<8, NA, MX, W, V, ACC>(a.col, w, xv, b + lane, e2, xi, acc, ds);
                 acc = warp_sum(acc);
                 if (lane == 0) a.hpart[sg] = (double)acc;
             }
@@ -1019,8 +1030,7 @@ __global__ void __launch_bounds__(kPIThreads, 2) k_power_iter(PIArgs a) {
             for (uint32_t sg = a.hseg[i]; sg < a.hseg[i + 1]; sg++) acc += a.hpart[sg];
             const double d = w ? (e > b ? a.deg[i] : 0.0) : (double)(e - b);
             const double ui = ((double)src[i] - mu) * inv_nu;
-            const double au = (acc - mu * d) * inv_nu;
-            const double r = a.normlap ? 0.5 * ui + (d > 0 ? 0.5 * au / d : 0.0) : (gb - d) * ui + au;
+            const double r = next_value<MX>(a.normlap, gb, mu, inv_nu, ui, acc, d);
             const V rs = (V)r;
             dst[i] = rs;
             const double rd = (double)rs;
@@ -1041,10 +1051,7 @@ __global__ void __launch_bounds__(kPIThreads, 2) k_power_iter(PIArgs a) {
         dot = (S[2] - mu_n * S[3]) * inv_nu_n;
         niter++;
         const double delta = fabs(dot - last);
-        if (niter > 2 && delta < best_delta * a.stall_factor) { best_delta = delta; best_at = niter; }
-        const bool converged = !(delta > a.tol && niter < a.iter_max);
-        const bool stalled = a.stall_factor > 0 && niter > 2 && niter - best_at > a.stall_window;
-        if (converged || stalled) {
+        if (!(delta > a.tol && niter < a.iter_max)) {
             // the reference returns u of the last iteration: (src - mu) / nu
             for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
                  i += (uint64_t)gridDim.x * blockDim.x)
@@ -1057,7 +1064,6 @@ __global__ void __launch_bounds__(kPIThreads, 2) k_power_iter(PIArgs a) {
                 // random-walk Laplacian from the lazy walk's quotient
                 a.res[3] = a.normlap ? 2.0 * (1.0 - S[2] / S[4]) : (gb * S[4] - S[2]) / S[4];
                 a.res[4] = niter >= a.iter_max ? 1.0 : 0.0;
-                a.res[5] = converged ? 0.0 : 1.0;
             }
             return;
         }
@@ -1090,12 +1096,12 @@ static size_t small_level_bytes(uint32_t n, uint64_t m, bool weighted) {
 
 // The whole computation of one small level by the calling block: the level
 // (offsets, destinations, weights, degrees) and both iterates are staged in
-// shared memory.  Every FP64 small level runs it inside the chained kernel
-// (single partitions and batches alike); the single-level kernel remains for
-// the FP32 start of a mixed-precision level.
+// shared memory.  Every small level runs it inside the chained kernel
+// (single partitions and batches alike), in FP64 also in a mixed-precision
+// partition (these levels are latency-bound).
 template <typename W, typename V>
 __device__ __forceinline__ void small_level(const PIArgs &a) {
-    typedef typename std::conditional<sizeof(V) == 8, double, float>::type ACC;
+    typedef double ACC;
     __shared__ double sm[256];
     extern __shared__ __align__(16) unsigned char dyn_smem[];
     const uint32_t n = a.n;
@@ -1174,8 +1180,8 @@ __device__ __forceinline__ void small_level(const PIArgs &a) {
     __syncthreads();
     double inv_nu = 1.0 / sqrt(sm[200]);
     __syncthreads();
-    double dot = 0, last = 1, best_delta = 1e300;
-    uint64_t best_at = 0, niter = 0;
+    double dot = 0, last = 1;
+    uint64_t niter = 0;
     V *src = xa, *dst = xb;
     // rows of at least 8 entries on average: one warp per row, else one thread
     const bool warp_rows = m >= 8ull * n;
@@ -1230,10 +1236,7 @@ __device__ __forceinline__ void small_level(const PIArgs &a) {
         dot = (S[2] - mu_n * S[3]) * inv_nu_n;
         niter++;
         const double delta = fabs(dot - last);
-        if (niter > 2 && delta < best_delta * a.stall_factor) { best_delta = delta; best_at = niter; }
-        const bool converged = !(delta > a.tol && niter < a.iter_max);
-        const bool stalled = a.stall_factor > 0 && niter > 2 && niter - best_at > a.stall_window;
-        if (converged || stalled) {
+        if (!(delta > a.tol && niter < a.iter_max)) {
             for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) a.out[i] = ((double)src[i] - mu) * inv_nu;
             if (threadIdx.x == 0) {
                 a.res[0] = (double)niter;
@@ -1243,7 +1246,6 @@ __device__ __forceinline__ void small_level(const PIArgs &a) {
                 // random-walk Laplacian from the lazy walk's quotient
                 a.res[3] = a.normlap ? 2.0 * (1.0 - S[2] / S[4]) : (gb * S[4] - S[2]) / S[4];
                 a.res[4] = niter >= a.iter_max ? 1.0 : 0.0;
-                a.res[5] = converged ? 0.0 : 1.0;
             }
             return;
         }
@@ -1547,16 +1549,16 @@ static bool panels_wanted(const Level &L, const PIArgs &a) {
     return s && !strcmp(s, "panel");
 }
 
-template <typename W, typename V, int CACHE>
+template <typename W, typename V, int CACHE, bool MX>
 static const void *pi_kernel_c(int mode) {
-    if (mode == 0) return (const void *)k_power_iter<W, V, 0, true, CACHE>;
-    if (mode == 5) return (const void *)k_power_iter<W, V, 5, true, CACHE>;
-    if constexpr (sizeof(W) >= 4)
-        if (mode == 6) return (const void *)k_power_iter<W, V, 6, true, kCacheNone>;
-    return (const void *)k_power_iter<W, V, 4, true, CACHE>;
+    if (mode == 0) return (const void *)k_power_iter<W, V, 0, true, CACHE, MX>;
+    if (mode == 5) return (const void *)k_power_iter<W, V, 5, true, CACHE, MX>;
+    if constexpr (sizeof(W) >= 4 && !MX)
+        if (mode == 6) return (const void *)k_power_iter<W, V, 6, true, kCacheNone, false>;
+    return (const void *)k_power_iter<W, V, 4, true, CACHE, MX>;
 }
 
-template <typename W, typename V>
+template <typename W, typename V, bool MX>
 static int launch_pi(Context &C, PIArgs &a, uint32_t grid) {
     const PIVariant var = pi_variant(a);
     const size_t cache_bytes = var.mode == 0 ? kCacheBytesStream : kCacheBytesRows;
@@ -1574,10 +1576,11 @@ static int launch_pi(Context &C, PIArgs &a, uint32_t grid) {
             set_error("narrow weights outside a relabelled copy");
             return SGP_B200_ERR_INVALID;
         }
-        k = pi_kernel_c<W, V, kCacheSplit>(var.mode);
+        k = pi_kernel_c<W, V, kCacheSplit, MX>(var.mode);
     } else {
-        k = split ? pi_kernel_c<W, V, kCacheSplit>(var.mode)
-                  : a.kcache ? pi_kernel_c<W, V, kCachePrefix>(var.mode) : pi_kernel_c<W, V, kCacheNone>(var.mode);
+        k = split ? pi_kernel_c<W, V, kCacheSplit, MX>(var.mode)
+                  : a.kcache ? pi_kernel_c<W, V, kCachePrefix, MX>(var.mode)
+                             : pi_kernel_c<W, V, kCacheNone, MX>(var.mode);
     }
     const size_t dyn = var.mode == 6 ? (size_t)a.PW * sizeof(V) : split ? 0 : (size_t)a.kcache * sizeof(V);
     if (var.mode == 6)
@@ -1602,21 +1605,17 @@ static int launch_pi(Context &C, PIArgs &a, uint32_t grid) {
     return SGP_B200_OK;
 }
 
-// panels[0] / panels[1]: layouts for FP32 / FP64 iterates, built on first use
-// when want_panels is set
-static int run_pi(Context &C, const Level &L, PIArgs a, int mixed, double *res_d, double res_h[6], float *ms,
-                  bool want_panels, PanelLayout (&panels)[2], bool (&built)[2]) {
+// Runs one level's iterations: the one-block shared-memory kernel for small
+// levels, else the cooperative kernel (column panels when a layout is given).
+// mixed: FP32 edge-difference arithmetic (never with panels or small levels).
+static int run_pi(Context &C, const Level &L, PIArgs a, bool mixed, const PanelLayout *panels, double *res_d,
+                  double res_h[5], float *ms) {
     const uint32_t grid = pi_grid(C, L.n, L.m);
     a.res = res_d;
     a.P = 0;
-    if (want_panels) {
-        const int k = mixed ? 0 : 1;
-        if (!built[k]) {
-            SGPB_TRY(build_panels(C, L, a.heavy_T, mixed ? sizeof(float) : sizeof(double), &panels[k]));
-            built[k] = true;
-        }
-        const PanelLayout &pl = panels[k];
-        a.P = pl.P; a.PW = pl.PW; a.poff = pl.off; a.pcol = pl.col; a.pw = pl.w; a.yacc = pl.yacc;
+    if (panels) {
+        a.P = panels->P; a.PW = panels->PW; a.poff = panels->off; a.pcol = panels->col; a.pw = panels->w;
+        a.yacc = panels->yacc;
     }
     int rc;
     cudaEvent_t e0, e1;
@@ -1625,56 +1624,46 @@ static int run_pi(Context &C, const Level &L, PIArgs a, int mixed, double *res_d
     // levels of at most kSmallCost cost units that fit in shared memory (not
     // when SGPB_PI_MODE forces a variant of the main kernel)
     const char *forced = getenv("SGPB_PI_MODE");
-    const bool small = !(forced && *forced) && !a.P && !a.inv && L.m + 8ull * L.n <= kSmallCost &&
+    const bool small = !mixed && !(forced && *forced) && !a.P && !a.inv && L.m + 8ull * L.n <= kSmallCost &&
                        (L.wbytes == 0 || L.wbytes == 4 || L.wbytes == 8) &&
-                       (mixed ? small_level_bytes<unsigned long long, float>(L.n, L.m, L.w != nullptr)
-                              : small_level_bytes<unsigned long long, double>(L.n, L.m, L.w != nullptr)) <=
-                           kSmallSmemBytes;
+                       small_level_bytes<unsigned long long, double>(L.n, L.m, L.w != nullptr) <= kSmallSmemBytes;
     if (small) {
-        auto launch_small = [&](auto wtag, auto vtag) -> int {
+        auto launch_small = [&](auto wtag) -> int {
             using Wt = decltype(wtag);
-            using Vt = decltype(vtag);
-            const size_t bytes = small_level_bytes<Wt, Vt>(L.n, L.m, L.w != nullptr);
-            const void *k = (const void *)k_power_iter_small<Wt, Vt>;
+            const size_t bytes = small_level_bytes<Wt, double>(L.n, L.m, L.w != nullptr);
+            const void *k = (const void *)k_power_iter_small<Wt, double>;
             // the limit is a property of the function, shared by every host
             // thread (batch workers): always the same bound, never this
             // launch's size, so no thread lowers it under another's launch
             SGPB_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmallSmemBytes));
             SGPB_CUDA(cudaEventRecord(e0, C.stream));
-            k_power_iter_small<Wt, Vt><<<1, kSmallThreads, bytes, C.stream>>>(a);
+            k_power_iter_small<Wt, double><<<1, kSmallThreads, bytes, C.stream>>>(a);
             C.kernel_launches++;
             return SGP_B200_OK;
         };
-        if (mixed) rc = L.wbytes == 8 ? launch_small((unsigned long long)0, 0.0f) : launch_small((uint32_t)0, 0.0f);
-        else rc = L.wbytes == 8 ? launch_small((unsigned long long)0, 0.0) : launch_small((uint32_t)0, 0.0);
-    } else if (mixed) {
-        float *va, *vb;
-        SGPB_TRY(dalloc_t(C, &va, L.n));
-        SGPB_TRY(dalloc_t(C, &vb, L.n));
-        a.va = va; a.vb = vb;
-        // partials are allocated inside launch_pi; the events bracket the launch
-        SGPB_CUDA(cudaEventRecord(e0, C.stream));
-        if (L.wbytes == 8) rc = launch_pi<unsigned long long, float>(C, a, grid);
-        else if (L.wbytes == 2) rc = launch_pi<uint16_t, float>(C, a, grid);
-        else if (L.wbytes == 1) rc = launch_pi<uint8_t, float>(C, a, grid);
-        else rc = launch_pi<uint32_t, float>(C, a, grid);
+        rc = L.wbytes == 8 ? launch_small((unsigned long long)0) : launch_small((uint32_t)0);
     } else {
         double *va, *vb;
         SGPB_TRY(dalloc_t(C, &va, L.n));
         SGPB_TRY(dalloc_t(C, &vb, L.n));
         a.va = va; a.vb = vb;
+        // partials are allocated inside launch_pi; the events bracket the launch
         SGPB_CUDA(cudaEventRecord(e0, C.stream));
-        if (L.wbytes == 8) rc = launch_pi<unsigned long long, double>(C, a, grid);
-        else if (L.wbytes == 2) rc = launch_pi<uint16_t, double>(C, a, grid);
-        else if (L.wbytes == 1) rc = launch_pi<uint8_t, double>(C, a, grid);
-        else rc = launch_pi<uint32_t, double>(C, a, grid);
+        auto go = [&](auto mx) -> int {
+            constexpr bool M = decltype(mx)::value;
+            if (L.wbytes == 8) return launch_pi<unsigned long long, double, M>(C, a, grid);
+            if (L.wbytes == 2) return launch_pi<uint16_t, double, M>(C, a, grid);
+            if (L.wbytes == 1) return launch_pi<uint8_t, double, M>(C, a, grid);
+            return launch_pi<uint32_t, double, M>(C, a, grid);
+        };
+        rc = mixed ? go(std::true_type()) : go(std::false_type());
     }
     cudaEventRecord(e1, C.stream);
     if (rc != SGP_B200_OK) { cudaEventDestroy(e0); cudaEventDestroy(e1); return rc; }
     SGPB_CUDA(cudaGetLastError());
-    SGPB_CUDA(cudaMemcpyAsync(C.h_pinned, res_d, 6 * sizeof(double), cudaMemcpyDeviceToHost, C.stream));
+    SGPB_CUDA(cudaMemcpyAsync(C.h_pinned, res_d, 5 * sizeof(double), cudaMemcpyDeviceToHost, C.stream));
     SGPB_CUDA(cudaStreamSynchronize(C.stream));
-    memcpy(res_h, C.h_pinned, 6 * sizeof(double));
+    memcpy(res_h, C.h_pinned, 5 * sizeof(double));
     float t = 0;
     cudaEventElapsedTime(&t, e0, e1);
     *ms += t;
@@ -1759,8 +1748,11 @@ int power_iter_level(Context &C, const Level &Lin, const double *x_in, const uin
     a.n = n; a.m = L.m; a.rp = L.rp; a.col = L.col; a.w = L.w;
     a.normlap = o.normlap;
     a.vec_ok = (((uintptr_t)L.col | (uintptr_t)L.w) & 15u) == 0;
+    // mixed-precision arithmetic for levels of at least 4096 vertices (the
+    // smaller ones are latency-bound and run in FP64)
+    const bool mixed = o.mixed && n >= 4096;
     // the variant decides the heavy-row threshold and the cost model
-    bool want_panels = panels_wanted(L, a);
+    bool want_panels = !mixed && panels_wanted(L, a);
     if (want_panels && !L.sorted) {
         uint32_t *bad, hbad = 0;
         SGPB_TRY(dalloc_t(C, &bad, 1));
@@ -1824,32 +1816,12 @@ int power_iter_level(Context &C, const Level &Lin, const double *x_in, const uin
     a.tol = o.tol;
     double *res_d;
     SGPB_TRY(dalloc_t(C, &res_d, 8));
-    double rh[6];
+    double rh[5];
     float kms = 0;
-    PanelLayout panels[2];
-    bool built[2] = {false, false};
-    uint64_t total_iters = 0;
-    // Mixed precision: FP32 vector storage and gathers under the reference's
-    // stopping rule.  When |d dot| stops shrinking before reaching tol (the
-    // FP32 noise floor), the FP32 iterate seeds FP64 iterations that finish
-    // the level at the requested tolerance.  Levels below 4096 vertices are
-    // latency-bound and run in FP64 directly.
-    bool done = false;
-    if (o.mixed && n >= 4096) {
-        a.stall_factor = 0.5;
-        a.stall_window = 64;
-        SGPB_TRY(run_pi(C, L, a, 1, res_d, rh, &kms, want_panels, panels, built));
-        total_iters += (uint64_t)rh[0];
-        done = rh[5] == 0.0;
-        a.x_in = x_out;
-        a.vcmap = nullptr;
-        a.stall_factor = 0;
-        a.iter_max = imax > total_iters ? imax - total_iters : 1;
-    }
-    if (!done) {
-        SGPB_TRY(run_pi(C, L, a, 0, res_d, rh, &kms, want_panels, panels, built));
-        total_iters += (uint64_t)rh[0];
-    }
+    PanelLayout panels;
+    if (want_panels) SGPB_TRY(build_panels(C, L, a.heavy_T, sizeof(double), &panels));
+    SGPB_TRY(run_pi(C, L, a, mixed, want_panels ? &panels : nullptr, res_d, rh, &kms));
+    const uint64_t total_iters = (uint64_t)rh[0];
     res->niter = total_iters;
     res->dot = rh[1];
     res->gb = rh[2];
@@ -1890,7 +1862,6 @@ bool power_iter_small_ok(const Level &L, const PowerIterOpts &o) {
     if (forced && *forced) return false;
     if (L.n == 0 || L.m + 8ull * L.n > kSmallCost) return false;
     if (!(L.wbytes == 0 || L.wbytes == 4 || L.wbytes == 8)) return false;
-    if (o.mixed && L.n >= 4096) return false;   // would start in FP32
     return small_level_bytes<unsigned long long, double>(L.n, L.m, L.w != nullptr) <= kSmallSmemBytes;
 }
 

@@ -293,7 +293,7 @@ int hec_map_from_hn(Context &C, uint32_t n, const uint32_t *hn, uint64_t seed, u
     if (!prefilled) SGPB_CUDA(cudaMemsetAsync(vcmap, 0xFF, sizeof(uint32_t) * n, C.stream));
     // Progress argument: each two rounds assign at least one vertex, so
     // 2n + 4 rounds always suffice; the cap only turns a bug into an error.
-    a.round_cap = (uint32_t)((uint64_t)2 * n + 4 < 0xFFFFFFF0u ? 2 * (uint64_t)n + 4 : 0xFFFFFFF0u);
+    a.round_cap = round_budget(2 * (uint64_t)n + 4);
     uint32_t grid = 1;
     SGPB_TRY(coop_grid(C, (const void *)k_hec_map, kMapThreads, 0, n, &grid));
     SGPB_TRY(dalloc_t(C, &a.block_tot, grid));

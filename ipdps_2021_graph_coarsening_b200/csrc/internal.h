@@ -77,6 +77,12 @@ int compact_flags(Context &C, const uint8_t *flags, uint32_t n, uint32_t *out_id
 // read a few device scalars (synchronises the stream)
 int read_u32(Context &C, const uint32_t *d, uint32_t *h, int count = 1);
 int read_u64(Context &C, const uint64_t *d, uint64_t *h, int count = 1);
+// Round or iteration budget of a coarsening construction whose natural bound
+// (a progress argument) is `natural`: that bound, clamped to 32 bits, or the
+// smaller positive value of the environment variable SGPB_ROUND_CAP -- a test
+// hook that makes the give-up path (SGP_B200_ERR_BUDGET) reachable; it never
+// raises a bound.
+uint32_t round_budget(uint64_t natural);
 
 inline uint32_t cdiv(uint64_t a, uint64_t b) { return (uint32_t)((a + b - 1) / b); }
 
@@ -122,7 +128,7 @@ int set_map_level(Context &C, const Level &L, bool gosh, uint64_t seed, uint32_t
 struct PowerIterOpts {
     double tol = 1e-10;
     uint64_t iter_cap = 0;   // 0: the reference's 1e14 / n only
-    int mixed = 0;           // 1: float vector storage / gathers, fp64 reductions
+    int mixed = 0;           // 1: FP32 edge-difference SpMV arithmetic, FP64 iterate and reductions
     int allow_relabel = 1;   // skewed levels may iterate on a hub-first relabelled copy
     int normlap = 0;         // refine_alg 1: normalized-Laplacian (lazy random walk) iteration
 };

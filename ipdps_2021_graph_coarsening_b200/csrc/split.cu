@@ -232,26 +232,67 @@ constexpr size_t kNoAllocOutOff = kNoAllocCutOff + 2 * (size_t)kNoAllocMaxBlocks
 constexpr size_t kNoAllocBytes = kNoAllocOutOff + 4 * sizeof(unsigned long long);
 static __device__ __align__(256) unsigned char g_split_scratch[kNoAllocBytes];
 
-// Per-device set-up, done once by the first call on that device: the host
+// Per-device set-up, done by the first call on that device: the host
 // address of g_split_scratch is only a stand-in, so the device address comes
-// from cudaGetSymbolAddress with the device current.
+// from cudaGetSymbolAddress with the device current.  The address belongs to
+// the context that loaded the module: after cudaDeviceReset (or any new
+// context on the device) the cached one is stale, so the set-up is keyed by
+// the current context's id and redone when that id changes.
 struct NoAllocDevice {
     unsigned char *scratch = nullptr;
     int num_sms = 0;
     int per_sm = 0;
+    unsigned long long ctx_id = 0;
     bool ready = false;
 };
 static std::mutex g_noalloc_mu;
 static NoAllocDevice g_noalloc_dev[64];
+
+// Unique id of the calling thread's current context (cuCtxGetCurrent and
+// cuCtxGetId through the runtime's driver entry points, so the library does
+// not link the driver library itself).  Every context ever created in the
+// process gets a distinct id.
+typedef int (*CtxGetCurrentFn)(void **ctx);
+typedef int (*CtxGetIdFn)(void *ctx, unsigned long long *id);
+static int current_ctx_id(int device, unsigned long long *id) {
+    static CtxGetCurrentFn get_current = nullptr;
+    static CtxGetIdFn get_id = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void *f = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            get_current = (CtxGetCurrentFn)f;
+        if (cudaGetDriverEntryPoint("cuCtxGetId", &f, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            get_id = (CtxGetIdFn)f;
+    });
+    if (!get_current || !get_id) {
+        set_error("the CUDA driver does not provide cuCtxGetCurrent / cuCtxGetId");
+        return SGP_B200_ERR_DEVICE;
+    }
+    // makes the device's primary context current if no context is yet
+    SGPB_CUDA(cudaSetDevice(device));
+    void *ctx = nullptr;
+    if (get_current(&ctx) != 0 || !ctx || get_id(ctx, id) != 0) {
+        set_error("no current CUDA context on device %d", device);
+        return SGP_B200_ERR_DEVICE;
+    }
+    return SGP_B200_OK;
+}
 
 static int noalloc_setup(int device, NoAllocDevice **out) {
     if (device < 0 || device >= 64) {
         set_error("device %d out of range for the no-allocation entry point", device);
         return SGP_B200_ERR_INVALID;
     }
+    unsigned long long id = 0;
+    SGPB_TRY(current_ctx_id(device, &id));
     std::lock_guard<std::mutex> lock(g_noalloc_mu);
     NoAllocDevice &d = g_noalloc_dev[device];
-    if (!d.ready) {
+    if (!d.ready || d.ctx_id != id) {
+        d.ready = false;
         void *p = nullptr;
         SGPB_CUDA(cudaGetSymbolAddress(&p, g_split_scratch));
         SGPB_CUDA(cudaDeviceGetAttribute(&d.num_sms, cudaDevAttrMultiProcessorCount, device));
@@ -261,6 +302,7 @@ static int noalloc_setup(int device, NoAllocDevice **out) {
             return SGP_B200_ERR_DEVICE;
         }
         d.scratch = (unsigned char *)p;
+        d.ctx_id = id;
         d.ready = true;
     }
     *out = &d;
@@ -549,10 +591,12 @@ using namespace sgpb;
 // device memory at that point: a host application that owns every device
 // allocation through its own pool, code running inside an out-of-memory
 // handler, or a plug-in whose allocation calls are forbidden by its host.
-// The first call on a device fetches the scratch address (see
-// noalloc_setup); make that first call before any stream capture.  Calls that
-// overlap on the GPU (different streams, or graphs replayed concurrently)
-// share the scratch and race; serialise them.
+// The first call on a device (and the first after the device's context
+// changed, e.g. after cudaDeviceReset) fetches the scratch address (see
+// noalloc_setup); make that first call before any stream capture.  The stream
+// must belong to the current device.  Calls that overlap on the GPU
+// (different streams, or graphs replayed concurrently) share the scratch and
+// race; serialise them.
 extern "C" int sgp_b200_split_noalloc(void *stream, uint32_t n, const uint32_t *row_ptr, const uint32_t *col,
                                       const double *evec, uint32_t *part, uint64_t *result) {
     if (!row_ptr || !col || !evec || !part || !result) {
@@ -566,9 +610,19 @@ extern "C" int sgp_b200_split_noalloc(void *stream, uint32_t n, const uint32_t *
     }
     int device = 0;
     SGPB_CUDA(cudaGetDevice(&device));
+    cudaStream_t s = (cudaStream_t)stream;
+    if (s) {
+        int sdev = -1;
+        SGPB_CUDA(cudaStreamGetDevice(s, &sdev));
+        if (sdev != device) {
+            set_error("sgp_b200_split_noalloc: the stream belongs to device %d but device %d is current; "
+                      "make the stream's device current",
+                      sdev, device);
+            return SGP_B200_ERR_INVALID;
+        }
+    }
     NoAllocDevice *d = nullptr;
     SGPB_TRY(noalloc_setup(device, &d));
-    cudaStream_t s = (cudaStream_t)stream;
     SplitArgs a;
     a.n = n;
     a.rp = row_ptr;

@@ -1,5 +1,6 @@
 // util.cu -- context, stream-ordered allocation, device scan and compaction.
 #include <stdarg.h>
+#include <stdlib.h>
 #include <string.h>
 
 #include "common.cuh"
@@ -33,6 +34,15 @@ int dalloc(Context &C, void **p, size_t bytes) {
     }
     C.owned.push_back(*p);
     return SGP_B200_OK;
+}
+
+uint32_t round_budget(uint64_t natural) {
+    uint64_t cap = natural < 0xFFFFFFF0ull ? natural : 0xFFFFFFF0ull;
+    if (const char *e = getenv("SGPB_ROUND_CAP")) {
+        const unsigned long long t = strtoull(e, nullptr, 10);
+        if (t > 0 && t < cap) cap = t;
+    }
+    return (uint32_t)cap;
 }
 
 int dzero(Context &C, void *p, size_t bytes) {

@@ -126,3 +126,38 @@ def test_metrics_file_has_the_reference_layout(tmp_path):
         assert [x["number-vertices"] for x in lv] == [40, 300, 1000]      # coarsest first
         assert [x["unrefined-edge-cut"] for x in lv] == [0, 0, 100 + k]  # the finest carries the cut
         assert [x["refine-iterations"] for x in lv] == [700, 40, 12]
+
+
+def test_config_options_follow_sgp_partition_graph():
+    """coarsening_alg's bits select the coarsener as sgpar.h:2457-2475 reads
+    them; the tolerance, refine and local-search choices and the rng pass
+    through; refine_alg outside {0, 1} is rejected."""
+    import ctypes
+    cases = [(4, L.COARSEN_HEC), (1, L.COARSEN_MATCH | L.COARSEN_RATIO_STOP), (5, L.COARSEN_MATCH | L.COARSEN_RATIO_STOP),
+             (16, L.COARSEN_NONE), (17, L.COARSEN_NONE)]
+    for alg, want in cases:
+        c = L.config_t(coarsening_alg=alg, refine_alg=1, local_search_alg=1, num_iter=3, tol=1e-8,
+                       num_partitions=2)
+        rng = L.sgp_pcg32_random_t(state=77, inc=5)
+        o = L.sgp_b200_options_t()
+        assert L.lib().sgp_b200_config_options(ctypes.byref(c), 0, ctypes.byref(rng), ctypes.byref(o)) == L.OK
+        assert o.coarsener == want and o.refine_alg == 1 and o.local_search_alg == 1 and o.tol == 1e-8
+        assert o.rng_state == 77 and o.rng_inc == 5 and o.perc_imbalance == 0 and o.cutoff == 50
+    c = L.config_t(coarsening_alg=4, refine_alg=2, local_search_alg=0, num_iter=1, tol=1e-10, num_partitions=2)
+    rng = L.sgp_pcg32_random_t(state=1, inc=1)
+    assert L.lib().sgp_b200_config_options(ctypes.byref(c), 0, ctypes.byref(rng),
+                                           ctypes.byref(L.sgp_b200_options_t())) == L.ERR_INVALID
+
+
+DRIVER = os.path.join(os.path.dirname(L.LIB_PATH), "sgpar_b200")
+
+
+def test_driver_command_usage():
+    """The config-file driver command is built and prints the reference's
+    usage line, exiting EXIT_FAILURE, when arguments are missing."""
+    import subprocess
+    assert os.path.exists(DRIVER)
+    p = subprocess.run([DRIVER, "only-one"], capture_output=True, text=True, timeout=60)
+    assert p.returncode == 1
+    assert "You input 2 args" in p.stdout
+    assert "csr_filename metrics_filename config_file" in p.stderr

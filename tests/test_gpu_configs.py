@@ -223,8 +223,13 @@ def test_normalized_laplacian_variant(partitioner, name):
     if name == "rmat12":
         assert abs(r.lam) < 1e-4 and abs(o["lambda"]) < 1e-4
     else:
-        assert abs(r.lam - o["lambda"]) <= 1e-3 * o["lambda"]
+        # same hierarchy and iteration counts as the oracle: FP64 agrees to
+        # rounding, mixed precision within the 1e-6 bound of the other tests
+        assert r.level_iters == o["level_iters"]
+        assert abs(r.lam - o["lambda"]) <= 1e-8 * o["lambda"]
         assert abs(r.edgecut - o["edgecut"]) <= 0.05 * o["edgecut"] + 4
+        rm = partitioner.partition(g, rng_state=77, refine_alg=1, mixed=True)
+        assert abs(rm.lam - o["lambda"]) <= 1e-6 * o["lambda"]
         # and it differs from the combinatorial variant's eigenvalue
         c = partitioner.partition(g, rng_state=77)
         assert abs(c.lam - r.lam) > 0.5 * r.lam

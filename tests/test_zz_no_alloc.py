@@ -72,6 +72,39 @@ def test_noalloc_matches_split_on_consecutive_calls(partitioner):
     assert np.array_equal(outs[0][0], outs[2][0]) and outs[0][1] == outs[2][1]
 
 
+def path_graph(n):
+    """A path of n vertices (n = 1: a single isolated vertex)."""
+    deg = np.full(n, 2, np.uint32)
+    if n == 1:
+        deg[0] = 0
+    else:
+        deg[0] = deg[-1] = 1
+    rp = np.zeros(n + 1, np.uint32)
+    rp[1:] = np.cumsum(deg)
+    col = np.empty(int(rp[-1]), np.uint32)
+    i = np.arange(n, dtype=np.uint32)
+    left = rp[1:n] if n > 1 else np.zeros(0, np.uint32)    # slot of the entry i -> i - 1 in rows 1..n-1
+    col[left] = i[1:] - 1
+    right = rp[:n - 1] + (np.arange(n - 1) > 0)             # slot of the entry i -> i + 1 in rows 0..n-2
+    col[right] = i[:n - 1] + 1
+    return G.CSR(rp, col)
+
+
+@pytest.mark.parametrize("n", [1, 1 << 20])
+def test_noalloc_smallest_and_largest_inputs(partitioner, n):
+    """One vertex (the sweep vertex is the only vertex) and exactly
+    SGP_B200_NOALLOC_MAX_N vertices, which fills the keys region up to the
+    histograms; each twice in a row, equal to the allocating split."""
+    g = path_graph(n)
+    ev = vector(n, 3, True)
+    ref_part, ref_cut = split_allocating(partitioner, g, ev)
+    for _ in range(2):
+        rc, part, cut, p0 = split_noalloc(g, ev)
+        assert rc == L.OK, L.last_error()
+        assert cut == ref_cut and np.array_equal(part, ref_part)
+        assert p0 == int((part == 0).sum())
+
+
 def test_noalloc_rejects_sizes_beyond_its_scratch():
     small = torch.zeros(4, dtype=torch.int64, device="cuda")
     p = small.data_ptr()
