@@ -335,7 +335,8 @@ int sgp_b200_split(sgp_b200_ctx_t *ctx, uint32_t n, const uint32_t *row_ptr, con
  * SGP_B200_ERR_TOO_LARGE.  Asynchronous on `stream` (a cudaStream_t, NULL =
  * default stream): part (n entries) and result (device array: result[0] =
  * edge cut, result[1] = size of part 0) are valid once the stream has
- * reached the call.  `stream` must belong to the current device
+ * reached the call (col may be NULL when the graph has no edges).  `stream`
+ * must belong to the current device
  * (SGP_B200_ERR_INVALID otherwise).  The first call on a device looks up the
  * scratch address and should come before any stream capture; the look-up is
  * repeated when the device's context has changed (after cudaDeviceReset).

@@ -599,7 +599,8 @@ using namespace sgpb;
 // race; serialise them.
 extern "C" int sgp_b200_split_noalloc(void *stream, uint32_t n, const uint32_t *row_ptr, const uint32_t *col,
                                       const double *evec, uint32_t *part, uint64_t *result) {
-    if (!row_ptr || !col || !evec || !part || !result) {
+    // col may be NULL for a graph without edges, as for sgp_b200_split
+    if (!row_ptr || !evec || !part || !result) {
         set_error("null argument");
         return SGP_B200_ERR_INVALID;
     }

@@ -34,6 +34,17 @@ def build() -> None:
     subprocess.run(["make", "-s", "-C", HERE, "oracle", "ref"], check=True)
 
 
+def reference_root() -> str:
+    """The reference checkout oracle/Makefile compiles from: the environment's
+    REFERENCE_ROOT, else the Makefile's default (the one place that names it)."""
+    if os.environ.get("REFERENCE_ROOT"):
+        return os.environ["REFERENCE_ROOT"]
+    import re
+    with open(os.path.join(HERE, "Makefile")) as f:
+        m = re.search(r"^REFERENCE_ROOT\s*\?=\s*(\S+)", f.read(), flags=re.M)
+    return m.group(1) if m else ""
+
+
 _orc = None
 
 
