@@ -34,9 +34,10 @@ def test_grid256_cutoff32(partitioner):
     assert abs(r.lam - o["lambda"]) <= 1e-6 * o["lambda"]
     assert abs(r.edgecut - o["edgecut"]) <= 0.05 * o["edgecut"] + 4
     # the finest iterate approximates the Fiedler pair of the grid:
-    # lambda_2 = 2 - 2 cos(pi / 256)
+    # lambda_2 = 2 - 2 cos(pi / 256); the reference's stopping rule ends
+    # within 5% of it (3.2% for this seed)
     lam2 = 2 - 2 * np.cos(np.pi / 256)
-    assert abs(r.lam - lam2) / lam2 < 0.1
+    assert 0 <= (r.lam - lam2) / lam2 < 0.05
 
 
 def oracle_4way(g, rng_state, cutoff=50):
