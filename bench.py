@@ -20,7 +20,10 @@ halo exchanges per iteration); N ranks run N independent replicas ("weak"),
 value = total edges of all replicas / max over ranks of the step time.
 
 `--impl reference` times the reference's own OpenMP path (cmg/sgpar.h built
-by oracle/Makefile) on the host cores on a bounded R-MAT sample.
+by oracle/Makefile) on the host cores: the timed steps partition a bounded
+sample (R-MAT scale 18 from the same generator; a scale-22 partition takes
+minutes there), and one partition of the scale-22 graph itself follows,
+reported as `full_size`.
 
 `--workload mtx2csr` measures the MatrixMarket converter instead (the
 reference's cmg/mtx2csr.cpp): one step = one conversion of the R-MAT scale-22
@@ -156,6 +159,18 @@ def reference_arm(args, rank: int, ws: int):
     value = g.m_undirected / sec
     sample = (f"R-MAT scale {REF_SAMPLE_SCALE} (same generator, {g.n} vertices, {g.m_undirected} edges), "
               f"one partition per step, reference OpenMP build of cmg/sgpar.h with {cores} threads")
+    # one partition of the full-size graph, outside the timed steps: a
+    # scale-22 partition takes minutes on the host cores, so the steps use
+    # the bounded sample above
+    full = None
+    if not args.no_full_size:
+        g22 = rmat_graph(SCALE)
+        t = time.perf_counter()
+        _, cut22, _ = O.ref_partition_graph(g22.row_ptr, g22.col, rng_state=1000, kind="omp")
+        sec22 = time.perf_counter() - t
+        full = {"workload": f"rmat{SCALE} bisection ({g22.n} vertices, {g22.m_undirected} edges)",
+                "sec_per_partition": sec22, "edges_per_s": g22.m_undirected / sec22, "edgecut": int(cut22),
+                "threads": cores, "kind": "reference OpenMP build of cmg/sgpar.h, one partition"}
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "edges/s", "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": sec * 1e3, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
@@ -164,7 +179,7 @@ def reference_arm(args, rank: int, ws: int):
             "cpu_baseline": {"value": value, "unit": "edges/s", "cores": cores, "kind": "reference",
                              "sample": sample},
             "e2e": {"value": value, "unit": "edges/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
-            "edgecut_median": float(np.median(cuts))}
+            "edgecut_median": float(np.median(cuts)), "full_size": full}
     print(json.dumps(line))
 
 
@@ -504,6 +519,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-full-size", action="store_true",
+                    help="with --impl reference: skip the one full-size reference partition")
     ap.add_argument("--scale", type=int, default=SCALE, help="R-MAT scale (the benchmark is 22)")
     ap.add_argument("--single", action="store_true",
                     help="one partition (or, with --workload mtx2csr, two conversions) of --scale and exit (profiling)")

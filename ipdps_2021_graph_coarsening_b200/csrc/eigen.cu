@@ -93,6 +93,7 @@ struct PIArgs {
     const uint16_t *pcol;         // destination minus p*PW
     const void *pw;               // weights (same width as w), null when unweighted
     void *yacc;                   // [n] row sums over the panels so far (iterate type)
+    uint32_t *err;                // staged rows (mode 7): set when a bulk copy did not complete in time
 };
 
 // dynamic shared memory for the iterate cache, per block (two blocks per SM)
@@ -568,6 +569,227 @@ __device__ __forceinline__ void warp_stream(const uint32_t *__restrict__ rp, con
     }
 }
 
+// ------------------------------------------ staged warp rows (MODE 7) --
+// The matrix stream of a warp's rows is copied into a per-warp ring of
+// shared-memory chunks by 1-D bulk copies (cp.async.bulk, completion counted
+// on an mbarrier per slot), issued by lane 0 ahead of use.  The warp then
+// reads destinations and weights from shared memory, so its registers hold
+// only the gathers: eight per lane in flight instead of four plus the
+// prefetched stream.  Chunks are kStageCh consecutive entries at multiples of
+// kStageCh in the level's arrays (16-byte aligned); the arrays of a level
+// that runs this mode are padded by kStagePad entries, so every chunk copy
+// is in bounds.  Only this GPU's own memory is read, and no copy uses cluster
+// multicast.
+constexpr uint32_t kStageCh = kStagePad;
+constexpr int kStageU = 8;                       // entries per lane per trip (32 * 8 = kStageCh)
+constexpr uint32_t kStageWaitLimit = 1u << 22;   // bounded mbarrier polls before giving up
+template <typename W>
+struct StageCfg {
+    static constexpr uint32_t R = sizeof(W) == 8 ? 2 : (sizeof(W) == 4 ? 3 : 4);   // ring slots per warp
+    // destinations, weights, mbarriers, chunk ids; 16-byte multiple
+    static constexpr size_t warp_bytes = ((size_t)R * kStageCh * (4 + sizeof(W)) + 12 * R + 15) & ~(size_t)15;
+};
+
+__device__ __forceinline__ uint32_t smem_addr(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
+__device__ __forceinline__ void mbar_init(uint64_t *b) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(b)) : "memory");
+}
+__device__ __forceinline__ void mbar_fence_init() { asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory"); }
+__device__ __forceinline__ void mbar_expect_tx(uint64_t *b, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(b)), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ bool mbar_test(uint64_t *b, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(smem_addr(b)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+// bounded wait for the phase of the given parity to complete
+__device__ __forceinline__ bool mbar_wait(uint64_t *b, uint32_t parity) {
+    for (uint32_t k = 0; k < kStageWaitLimit; k++)
+        if (mbar_test(b, parity)) return true;
+    return false;
+}
+__device__ __forceinline__ void bulk_load(void *dst, const void *src, uint32_t bytes, uint64_t *b) {
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                     smem_addr(dst)),
+                 "l"(src), "r"(bytes), "r"(smem_addr(b))
+                 : "memory");
+}
+// generic-proxy reads of a slot are ordered before the next bulk copy into it
+__device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+
+// A warp's ring in dynamic shared memory: slot s holds chunk ids[s].  Copies
+// are numbered in issue order (seq): slot = seq % R, and the phase parity of
+// a copy is (seq / R) & 1.  seq persists across the iterations of a launch
+// (the barriers are set up once, by stage_init).
+template <typename W>
+struct StageRing {
+    uint32_t *col;   // [R][kStageCh]
+    W *w;            // [R][kStageCh]
+    uint64_t *bar;   // [R]
+    uint32_t *ids;   // [R]
+};
+
+template <typename W>
+__device__ __forceinline__ StageRing<W> stage_ring(unsigned char *base, uint32_t warp) {
+    constexpr uint32_t R = StageCfg<W>::R;
+    unsigned char *p = base + (size_t)warp * StageCfg<W>::warp_bytes;
+    StageRing<W> r;
+    r.col = (uint32_t *)p;
+    r.w = (W *)(p + (size_t)R * kStageCh * 4);
+    r.bar = (uint64_t *)(p + (size_t)R * kStageCh * (4 + sizeof(W)));
+    r.ids = (uint32_t *)(r.bar + R);
+    return r;
+}
+
+template <typename W>
+__device__ __forceinline__ void stage_init(const StageRing<W> &r) {
+    if ((threadIdx.x & 31) == 0) {
+        for (uint32_t s = 0; s < StageCfg<W>::R; s++) mbar_init(&r.bar[s]);
+        mbar_fence_init();
+    }
+    __syncwarp();
+}
+
+// One warp, rows [r0, r1) (rows with skip(len) left out), one after another
+// in trips of up to kStageCh entries of one row (kStageU per lane), the
+// destinations and weights read from the ring.  fin(i, sum, d, xi) on lane 0
+// once per row.  seq: the warp's copy counter (in/out).  Returns false when a
+// copy did not complete within the wait limit, or the ring's bookkeeping
+// failed a check (the caller reports the error); every copy issued has then
+// been waited for once more, with the same limit.
+template <bool MX, typename W, typename V, typename ACC, typename S, typename Skip, typename Fin>
+__device__ __forceinline__ bool warp_rows_staged(const uint32_t *__restrict__ rp, const uint32_t *__restrict__ col,
+                                                 const W *__restrict__ w, const S &src, const double *deg,
+                                                 uint32_t r0, uint32_t r1, Skip skip, Fin &fin,
+                                                 const StageRing<W> &ring, uint32_t &seq) {
+    constexpr uint32_t R = StageCfg<W>::R;
+    const unsigned lane = threadIdx.x & 31;
+    // producer: the chunks of the processed rows of [r0, r1), in order, each
+    // once; [pc, pend) are the current producer row's chunks not yet issued
+    uint32_t pr = r0, pc = 0, pend = 0;
+    auto prod_next = [&]() -> bool {
+        while (pc >= pend) {
+            if (pr >= r1) return false;
+            const uint32_t b = rp[pr], e = rp[pr + 1];
+            pr++;
+            if (skip(e - b)) continue;
+            pend = (e + kStageCh - 1) / kStageCh;
+            if (pc < b / kStageCh) pc = b / kStageCh;
+        }
+        return true;
+    };
+    uint32_t iss = seq, rel = seq;   // copies [rel, iss) hold chunks not yet consumed
+    auto fill = [&]() {
+        __syncwarp();   // every lane is done reading the released slots
+        while (iss - rel < R && prod_next()) {
+            const uint32_t slot = iss % R;
+            if (lane == 0) {
+                ring.ids[slot] = pc;
+                fence_proxy_async();
+                const uint32_t bytes = kStageCh * 4 + (w ? kStageCh * (uint32_t)sizeof(W) : 0u);
+                mbar_expect_tx(&ring.bar[slot], bytes);
+                bulk_load(ring.col + (size_t)slot * kStageCh, col + (size_t)pc * kStageCh, kStageCh * 4,
+                          &ring.bar[slot]);
+                if (w)
+                    bulk_load(ring.w + (size_t)slot * kStageCh, w + (size_t)pc * kStageCh,
+                              kStageCh * (uint32_t)sizeof(W), &ring.bar[slot]);
+            }
+            pc++;
+            iss++;
+        }
+        __syncwarp();   // ids[] visible to every lane
+    };
+    // consumer: the current row ci = [cb, ce), entry j, own value cx, degree cd
+    auto next_row = [&](uint32_t i, uint32_t &b, uint32_t &e) -> uint32_t {
+        for (; i < r1; i++) {
+            b = rp[i];
+            e = rp[i + 1];
+            if (!skip(e - b)) return i;
+        }
+        return r1;
+    };
+    uint32_t cb = 0, ce = 0;
+    uint32_t ci = next_row(r0, cb, ce);
+    double cx = 0, cd = 0;
+    if (ci < r1) {
+        if (MX || lane == 0) cx = (double)src[ci];
+        if (lane == 0) cd = w ? deg[ci] : (double)(ce - cb);
+    }
+    uint32_t cseq = seq;   // the copy holding the chunk of entry j
+    uint32_t j = cb;
+    ACC acc = 0;
+    bool ok = true;
+    while (ci < r1) {
+        const uint32_t tend = ce - j > kStageCh ? j + kStageCh : ce;
+        const uint32_t c0 = j / kStageCh, c1 = (tend - 1) / kStageCh;
+        // the copies before the one holding c0 are consumed: release them
+        fill();
+        while (cseq < iss && ring.ids[cseq % R] != c0) {
+            cseq++;
+            rel = cseq;
+            fill();
+        }
+        // the trip's chunks are copies cseq (and cseq + 1), issued in order
+        if (cseq >= iss || (c1 != c0 && (cseq + 1 >= iss || ring.ids[(cseq + 1) % R] != c1))) { ok = false; break; }
+        if (!mbar_wait(&ring.bar[cseq % R], (cseq / R) & 1u)) { ok = false; break; }
+        if (c1 != c0 && !mbar_wait(&ring.bar[(cseq + 1) % R], ((cseq + 1) / R) & 1u)) { ok = false; break; }
+        // the next processed row's own value and degree load during the gathers
+        const bool row_ends = tend == ce;
+        uint32_t ni = ci, nb = cb, ne = ce;
+        double nx = cx, nd = cd;
+        if (row_ends) {
+            ni = next_row(ci + 1, nb, ne);
+            if (ni < r1) {
+                if (MX || lane == 0) nx = (double)src[ni];
+                if (lane == 0) nd = w ? deg[ni] : (double)(ne - nb);
+            }
+        }
+        uint32_t c[kStageU];
+        W wt[kStageU];
+#pragma unroll
+        for (int k = 0; k < kStageU; k++) {
+            const uint32_t e = j + lane + 32 * k;
+            const uint32_t slot = (e / kStageCh == c0 ? cseq : cseq + 1) % R;
+            const uint32_t off = slot * kStageCh + e % kStageCh;
+            c[k] = e < tend ? ring.col[off] : 0u;
+            wt[k] = (w && e < tend) ? ring.w[off] : (W)0;
+        }
+        V x[kStageU];
+#pragma unroll
+        for (int k = 0; k < kStageU; k++) x[k] = (j + lane + 32 * k < tend) ? src[c[k]] : (V)0;
+#pragma unroll
+        for (int k = 0; k < kStageU; k++) {
+            if (j + lane + 32 * k < tend) {
+                if constexpr (MX) acc += spmv_term<true, ACC>(w != nullptr, (V)cx, x[k], wt[k]);
+                else acc += (ACC)(w ? (V)wt[k] * x[k] : x[k]);
+            }
+        }
+        if (row_ends) {
+            const ACC t = warp_sum(acc);
+            if (lane == 0) fin(ci, t, cd, cx);
+            acc = 0;
+            ci = ni; cb = nb; ce = ne; cx = nx; cd = nd;
+            j = cb;
+        } else {
+            j = tend;
+        }
+    }
+    if (!ok) {
+        // every copy issued lands before the ring is given up
+        for (uint32_t q = rel; q < iss; q++) mbar_wait(&ring.bar[q % R], (q / R) & 1u);
+    }
+    seq = iss;
+    __syncwarp();
+    return ok;
+}
+
 // Destinations of four consecutive panel entries (16-bit, panel-relative).
 template <bool NA>
 __device__ __forceinline__ void ld_pcol4(const uint16_t *p, uint32_t (&c)[4]) {
@@ -728,7 +950,9 @@ __device__ __forceinline__ auto make_src(const V *g, const V *s, uint32_t k) {
 
 // MODE 0: normal rows streamed in warp tiles (short-row levels); MODE 4: one
 // warp per row with 4 loads in flight per lane; MODE 5: one warp per row,
-// trips software-pipelined across rows (dense levels); MODE 6: column panels.
+// trips software-pipelined across rows (dense levels); MODE 6: column panels;
+// MODE 7: one warp per row, the matrix stream staged in shared memory by bulk
+// copies (dense levels of a padded relabelled copy).
 // NA: matrix loads bypass L1 allocation.  CACHE: kCachePrefix -- gathers read
 // the block's shared-memory copy of a small level's iterate; kCacheSplit --
 // gathers below kcache (the hub prefix of a relabelled level) use L1
@@ -740,7 +964,8 @@ __global__ void __launch_bounds__(kPIThreads, 2) k_power_iter(PIArgs a) {
     cg::grid_group grid = cg::this_grid();
     // [0, 160): block_sum_d scratch (5 x 32), [200, 202): broadcast, [210, 226): warp maxima
     __shared__ double sm[256];
-    __shared__ uint32_t swin[kPIWarps][kWin + 3];
+    constexpr bool WIN = MODE == 0 || MODE == 6;   // row-offset windows: streaming and panels only
+    __shared__ uint32_t swin[WIN ? kPIWarps : 1][kWin + 3];
     // per-row staging of the stream windows (unused by the warp-row variants)
     __shared__ V swinx[STREAM ? kPIWarps : 1][kTile];
     __shared__ double swind[STREAM ? kPIWarps : 1][kTile];
@@ -759,6 +984,14 @@ __global__ void __launch_bounds__(kPIThreads, 2) k_power_iter(PIArgs a) {
     const W *w = (const W *)a.w;
     const unsigned lane = threadIdx.x & 31;
     const uint32_t n_heavy = *a.n_heavy_ptr;
+    extern __shared__ __align__(16) unsigned char dyn_smem[];
+    constexpr bool STAGED = MODE == 7;
+    StageRing<W> ring;
+    uint32_t stage_seq = 0;
+    if constexpr (STAGED) {
+        ring = stage_ring<W>(dyn_smem, threadIdx.x >> 5);
+        stage_init(ring);
+    }
     // Work split, fixed for the whole launch: block b owns the rows whose
     // cost prefix (all rows) starts in the b-th equal share; inside the block,
     // block-wide rows are processed by all threads and the remaining rows are
@@ -899,10 +1132,9 @@ __global__ void __launch_bounds__(kPIThreads, 2) k_power_iter(PIArgs a) {
     uint64_t niter = 0;
     V *src = va, *dst = vb;
     uint32_t panel_seq = 0;   // panels processed so far: selects the group counter
-    uint32_t *win = swin[wk];
+    uint32_t *win = swin[WIN ? wk : 0];
     V *winx = swinx[STREAM ? wk : 0];
     double *wind = swind[STREAM ? wk : 0];
-    extern __shared__ __align__(16) unsigned char dyn_smem[];
     V *xs = reinterpret_cast<V *>(dyn_smem);
     const uint32_t kc = a.kcache < n ? a.kcache : n;
     while (true) {
@@ -981,6 +1213,14 @@ __global__ void __launch_bounds__(kPIThreads, 2) k_power_iter(PIArgs a) {
             const uint32_t T = a.heavy_T;
             auto skip = [T](uint32_t len) { return len > T || len == 0; };
             warp_rows_pipelined<NA, MX, W, V, ACC>(a.rp, a.col, w, xv, a.deg, w_r0, w_r1, skip, fin);
+        } else if constexpr (STAGED) {
+            const uint32_t T = a.heavy_T;
+            auto skip = [T](uint32_t len) { return len > T || len == 0; };
+            if (!warp_rows_staged<MX, W, V, ACC>(a.rp, a.col, w, xv, a.deg, w_r0, w_r1, skip, fin, ring, stage_seq) &&
+                lane == 0) {
+                atomicExch(a.err, 1u);
+                __threadfence();
+            }
         } else {
             uint32_t e = w_r0 < w_r1 ? a.rp[w_r0] : 0;
             for (uint32_t i = w_r0; i < w_r1; i++) {
@@ -1051,6 +1291,15 @@ __global__ void __launch_bounds__(kPIThreads, 2) k_power_iter(PIArgs a) {
         dot = (S[2] - mu_n * S[3]) * inv_nu_n;
         niter++;
         const double delta = fabs(dot - last);
+        if (STAGED && *(volatile uint32_t *)a.err) {
+            // a bulk copy did not complete: every block leaves here (the flag
+            // was set before the barrier), the host reports the error
+            if (blockIdx.x == 0 && threadIdx.x == 0) {
+                a.res[0] = (double)niter;
+                a.res[5] = 1.0;
+            }
+            return;
+        }
         if (!(delta > a.tol && niter < a.iter_max)) {
             // the reference returns u of the last iteration: (src - mu) / nu
             for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
@@ -1064,6 +1313,7 @@ __global__ void __launch_bounds__(kPIThreads, 2) k_power_iter(PIArgs a) {
                 // random-walk Laplacian from the lazy walk's quotient
                 a.res[3] = a.normlap ? 2.0 * (1.0 - S[2] / S[4]) : (gb * S[4] - S[2]) / S[4];
                 a.res[4] = niter >= a.iter_max ? 1.0 : 0.0;
+                a.res[5] = 0.0;
             }
             return;
         }
@@ -1246,6 +1496,7 @@ __device__ __forceinline__ void small_level(const PIArgs &a) {
                 // random-walk Laplacian from the lazy walk's quotient
                 a.res[3] = a.normlap ? 2.0 * (1.0 - S[2] / S[4]) : (gb * S[4] - S[2]) / S[4];
                 a.res[4] = niter >= a.iter_max ? 1.0 : 0.0;
+                a.res[5] = 0.0;
             }
             return;
         }
@@ -1523,9 +1774,13 @@ constexpr double kStreamMaxAvgDegree = 64.0;
 // it, else CSR streaming below kStreamMaxAvgDegree and pipelined warp rows
 // above; SGPB_PI_MODE = stream | row4 | rowp | panel overrides the rule.
 struct PIVariant {
-    int mode;   // 0 stream, 4 warp rows, 5 pipelined warp rows, 6 column panels
+    int mode;   // 0 stream, 4 warp rows, 5 pipelined warp rows, 6 column panels, 7 staged warp rows
     bool na;
 };
+// Staged warp rows (mode 7) run only when SGPB_PI_MODE=staged asks for them,
+// on a relabelled copy (whose arrays are padded for whole chunks): their ring
+// of shared memory takes L1 capacity from the hub prefix of the gathers, and
+// R-MAT scale 22's level 1 went from 173.5 to 393.7 ms with them.
 static PIVariant pi_variant(const PIArgs &a) {
     PIVariant v;
     v.mode = (a.n && (double)a.m / a.n <= kStreamMaxAvgDegree) ? 0 : 5;
@@ -1534,6 +1789,7 @@ static PIVariant pi_variant(const PIArgs &a) {
         if (!strcmp(s, "stream")) v.mode = 0;
         else if (!strcmp(s, "row4")) v.mode = 4;
         else if (!strcmp(s, "rowp")) v.mode = 5;
+        else if (!strcmp(s, "staged") && a.cache_ok == 3 && a.vec_ok) v.mode = 7;
     }
     if (a.P) v.mode = 6;
     return v;
@@ -1553,6 +1809,8 @@ template <typename W, typename V, int CACHE, bool MX>
 static const void *pi_kernel_c(int mode) {
     if (mode == 0) return (const void *)k_power_iter<W, V, 0, true, CACHE, MX>;
     if (mode == 5) return (const void *)k_power_iter<W, V, 5, true, CACHE, MX>;
+    if constexpr (CACHE == kCacheSplit)
+        if (mode == 7) return (const void *)k_power_iter<W, V, 7, true, kCacheSplit, MX>;
     if constexpr (sizeof(W) >= 4 && !MX)
         if (mode == 6) return (const void *)k_power_iter<W, V, 6, true, kCacheNone, false>;
     return (const void *)k_power_iter<W, V, 4, true, CACHE, MX>;
@@ -1582,8 +1840,13 @@ static int launch_pi(Context &C, PIArgs &a, uint32_t grid) {
                   : a.kcache ? pi_kernel_c<W, V, kCachePrefix, MX>(var.mode)
                              : pi_kernel_c<W, V, kCacheNone, MX>(var.mode);
     }
-    const size_t dyn = var.mode == 6 ? (size_t)a.PW * sizeof(V) : split ? 0 : (size_t)a.kcache * sizeof(V);
-    if (var.mode == 6)
+    const size_t dyn = var.mode == 7   ? (size_t)kPIWarps * StageCfg<W>::warp_bytes
+                       : var.mode == 6 ? (size_t)a.PW * sizeof(V)
+                       : split         ? 0
+                                       : (size_t)a.kcache * sizeof(V);
+    if (var.mode == 7)
+        SGPB_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn));
+    else if (var.mode == 6)
         SGPB_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kPanelBytes));
     else if (a.kcache && !split)
         SGPB_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)cache_bytes));
@@ -1599,6 +1862,8 @@ static int launch_pi(Context &C, PIArgs &a, uint32_t grid) {
     }
     if ((uint64_t)grid > (uint64_t)per_sm * C.num_sms) grid = per_sm * C.num_sms;
     SGPB_TRY(dalloc_t(C, &a.partials, (size_t)2 * grid * kNP));
+    SGPB_TRY(dalloc_t(C, &a.err, 1));
+    SGPB_TRY(dzero(C, a.err, sizeof(uint32_t)));
     void *args[] = {&a};
     SGPB_CUDA(cudaLaunchCooperativeKernel(k, dim3(grid), dim3(kPIThreads), args, dyn, C.stream));
     C.kernel_launches++;
@@ -1661,9 +1926,15 @@ static int run_pi(Context &C, const Level &L, PIArgs a, bool mixed, const PanelL
     cudaEventRecord(e1, C.stream);
     if (rc != SGP_B200_OK) { cudaEventDestroy(e0); cudaEventDestroy(e1); return rc; }
     SGPB_CUDA(cudaGetLastError());
-    SGPB_CUDA(cudaMemcpyAsync(C.h_pinned, res_d, 5 * sizeof(double), cudaMemcpyDeviceToHost, C.stream));
+    SGPB_CUDA(cudaMemcpyAsync(C.h_pinned, res_d, 6 * sizeof(double), cudaMemcpyDeviceToHost, C.stream));
     SGPB_CUDA(cudaStreamSynchronize(C.stream));
     memcpy(res_h, C.h_pinned, 5 * sizeof(double));
+    if (!small && ((const double *)C.h_pinned)[5] != 0.0) {
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        set_error("power iteration: a staged bulk copy of the matrix did not complete within its wait limit");
+        return SGP_B200_ERR_DEVICE;
+    }
     float t = 0;
     cudaEventElapsedTime(&t, e0, e1);
     *ms += t;
@@ -1785,8 +2056,8 @@ int power_iter_level(Context &C, const Level &Lin, const double *x_in, const uin
     SGPB_TRY(dalloc_t(C, &a.deg, (size_t)n + 1));
     k_heavy_flags<<<cdiv(n, 256), 256, 0, C.stream>>>(n, L.rp, a.heavy_T, flags);
     // the cost total is kept in 32 bits
-    const uint32_t qs = (mode == 4 || mode == 5) ? 7u : 0u;
-    const uint32_t over = (mode == 4 || mode == 5) ? 32u : 8u;
+    const uint32_t qs = (mode == 4 || mode == 5) ? 7u : mode == 7 ? 8u : 0u;   // trip of 128 / 256 entries
+    const uint32_t over = (mode == 4 || mode == 5 || mode == 7) ? 32u : 8u;
     uint32_t shift = 0;
     while ((L.m + ((1ull << qs) + over + 1) * (uint64_t)n) >> shift >= 0xFFFFFFF0ull) shift++;
     k_row_cost<<<cdiv(n, 256), 256, 0, C.stream>>>(n, L.rp, a.heavy_T, qs, over, shift, cost, cost_all);

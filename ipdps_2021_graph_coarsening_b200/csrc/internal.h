@@ -125,6 +125,11 @@ int hec_map_from_hn(Context &C, uint32_t n, const uint32_t *hn, uint64_t seed, u
 int gosh_v2_map_level(Context &C, const Level &L, uint64_t seed, uint32_t *vcmap, uint32_t *nc_out, int *rounds_out);
 int set_map_level(Context &C, const Level &L, bool gosh, uint64_t seed, uint32_t *vcmap, uint32_t *nc_out,
                   int *rounds_out);
+// Entries of padding behind the destination and weight arrays of a
+// relabelled power-iteration copy: its staged SpMV copies whole chunks of this
+// many entries (16-byte aligned), so the last chunk stays in bounds.
+constexpr uint32_t kStagePad = 256;
+
 struct PowerIterOpts {
     double tol = 1e-10;
     uint64_t iter_cap = 0;   // 0: the reference's 1e14 / n only

@@ -105,7 +105,7 @@ __global__ void __launch_bounds__(256) k_perm_fill(uint32_t n, const uint32_t *_
 template <typename WI, typename WO>
 static int fill_impl(Context &C, const Level &L, const uint32_t *perm, const uint32_t *inv, Level *out) {
     WO *nw = nullptr;
-    if (L.w) SGPB_TRY(dalloc_t(C, &nw, (size_t)L.m + 16));
+    if (L.w) SGPB_TRY(dalloc_t(C, &nw, (size_t)L.m + kStagePad));
     uint32_t blocks = cdiv((uint64_t)L.n * 32, 256);
     if (blocks > (uint32_t)C.num_sms * 16) blocks = C.num_sms * 16;
     k_perm_fill<WI, WO><<<blocks ? blocks : 1, 256, 0, C.stream>>>(L.n, L.rp, L.col, (const WI *)L.w, perm, inv,
@@ -141,7 +141,7 @@ int hub_first_copy(Context &C, const Level &L, uint32_t **perm_out, uint32_t **i
     *out = L;
     out->vcmap = nullptr;
     SGPB_TRY(dalloc_t(C, &out->rp, (size_t)n + 1));
-    SGPB_TRY(dalloc_t(C, &out->col, (size_t)L.m + 4));
+    SGPB_TRY(dalloc_t(C, &out->col, (size_t)L.m + kStagePad));
     SGPB_TRY(scan_u32(C, deg, out->rp, n, nullptr));
     if (L.wbytes == 8) {
         SGPB_TRY((fill_impl<unsigned long long, unsigned long long>(C, L, perm, inv, out)));

@@ -250,23 +250,31 @@ def rmat18_level1():
     return O.build_coarse(g.row_ptr, g.col, None, vc, nc)
 
 
-@pytest.mark.parametrize("variant,wscale", [("auto", 1), ("row4", 1), ("stream", 1), ("auto", 300),
-                                            ("stream", 300), ("auto", 100000)])
-def test_power_iter_hub_first_copy(partitioner, monkeypatch, variant, wscale):
+@pytest.mark.parametrize("variant,wscale,wide", [("auto", 1, False), ("staged", 1, False), ("row4", 1, False),
+                                                 ("stream", 1, False), ("auto", 300, False), ("staged", 300, False),
+                                                 ("stream", 300, False), ("auto", 100000, False),
+                                                 ("staged", 100000, False), ("auto", 7, True), ("staged", 7, True)])
+@pytest.mark.parametrize("mixed", [False, True])
+def test_power_iter_hub_first_copy(partitioner, monkeypatch, variant, wscale, wide, mixed):
     """A skewed level above 16384 vertices iterates on a hub-first
     relabelled copy whose leading entries are gathered through L1 and whose
     weights are stored in 8 bits (wscale 1: all weights <= 255), 16 bits
-    (wscale 300) or 32 bits (wscale 100000); the result (mapped back to the
-    level's numbering) matches the run without the copy and the oracle."""
+    (wscale 300), 32 bits (wscale 100000) or 64 bits (wide); its dense rows
+    run on the register-pipelined warp rows by default ("auto") or on the
+    staged ones ("staged": the matrix stream copied into shared memory by
+    bulk copies).  The result (mapped back to the level's numbering) matches
+    the run without the copy and the oracle, in both precisions."""
     rp, col, w = rmat18_level1()
     w = w * wscale
     assert int(w.max()) <= 0xFFFFFFFF and ((int(w.max()) <= 255) == (wscale == 1))
     n = rp.shape[0] - 1
     assert n > 16384
+    assert rp[-1] > 64 * n   # dense: the warp-row variants
     if variant != "auto":
         monkeypatch.setenv("SGPB_PI_MODE", variant)
     x0 = torch.from_numpy(np.random.default_rng(n).random(n)).cuda()
-    args = (dev_u32(rp), dev_u32(col), dev_u32(w), x0, None, 1e-10, 400)
+    wd = dev_u64(w) if wide else dev_u32(w)
+    args = (dev_u32(rp), dev_u32(col), wd, x0, None, 1e-10, 400, mixed)
     u_r, it_r, lam_r, res_r = partitioner.power_iter(*args)
     monkeypatch.setenv("SGPB_PI_RELABEL", "0")
     u_p, it_p, lam_p, _ = partitioner.power_iter(*args)
@@ -278,6 +286,21 @@ def test_power_iter_hub_first_copy(partitioner, monkeypatch, variant, wscale):
     assert abs(it_r - it_o) <= max(2, it_o // 50)
     assert abs(lam_r - lam_o) <= 1e-6 * abs(lam_o)
     assert res_r >= 0
+
+
+def test_power_iter_staged_unweighted(partitioner, monkeypatch):
+    """Staged warp rows on an unweighted relabelled level (only destinations
+    are copied), forced on the R-MAT 18 input graph, against the oracle."""
+    g = G.rmat(18, seed=2)
+    monkeypatch.setenv("SGPB_PI_MODE", "staged")
+    x0 = np.random.default_rng(3).random(g.n)
+    u_g, it_g, lam_g, _ = partitioner.power_iter(dev_u32(g.row_ptr), dev_u32(g.col), None,
+                                                 torch.from_numpy(x0).cuda(), None, 1e-10, 300)
+    u_o, it_o, lam_o = O.power_iter(g.row_ptr, g.col, None, x0, 1e-10, 300)
+    assert abs(it_g - it_o) <= max(2, it_o // 50)
+    assert abs(lam_g - lam_o) <= 1e-6 * abs(lam_o)
+    if it_g == it_o:
+        assert 1 - abs(float(np.dot(u_g.cpu().numpy(), u_o))) <= 1e-8
 
 
 def test_partition_with_and_without_hub_first_copy(partitioner, monkeypatch):
