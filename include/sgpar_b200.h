@@ -264,6 +264,11 @@ int sgp_b200_hierarchy_levels(const sgp_b200_hierarchy_t *h);
 int sgp_b200_hierarchy_level(const sgp_b200_hierarchy_t *h, int l, uint32_t *n, uint64_t *m,
                              const uint32_t **row_ptr, const uint32_t **col, const void **w,
                              int *wbytes, const uint32_t **vcmap);
+/* Vertex weights of level l (device array of n entries): the number of
+ * input vertices each vertex stands for, i.e. the fine weights summed over
+ * each aggregate (coarsen_kokkos.h:1098 c_vtx_w); NULL for level 0, whose
+ * vertices weigh 1. */
+int sgp_b200_hierarchy_vertex_weights(const sgp_b200_hierarchy_t *h, int l, const uint32_t **vtx_w);
 /* Fiedler vector of the finest level: coarsest guess from rng, power
  * iteration per level, prolongation; eigenvec has n_0 entries of kind mem. */
 int sgp_b200_eigensolve(sgp_b200_ctx_t *ctx, sgp_b200_hierarchy_t *h, sgp_pcg32_random_t *rng,
@@ -409,6 +414,22 @@ int sgp_b200_csr_write(const char *csr_path, const sgp_b200_graph_t *g, int id_b
 /* The command `mtx2csr <MM file> <binary CSR file>`: read + write. */
 int sgp_b200_mtx2csr(sgp_b200_ctx_t *ctx, const char *mtx_path, const char *csr_path, int id_bytes,
                      sgp_b200_mtx_info_t *info);
+
+/* The power iteration's autotuner (no counterpart in the reference, whose
+ * SpMV launch shape follows fixed rules, kokkos-kernels
+ * KokkosSparse_spmv_impl.hpp:222-258).  The first time a level of a given
+ * shape (weight width, relabelled or not, precision, octave of the vertex
+ * count, half octave of the mean degree) and at least 2^18 cost units is
+ * iterated on a kind of device, candidate work splits -- SpMV variant, long-row
+ * threshold, grid size -- run ten trial iterations each into scratch memory
+ * and the fastest is kept for every later level of that shape, in memory and
+ * in the file the environment variable SGPB_TUNE_CACHE names (default
+ * $HOME/.cache/sgpar_b200/pi_tune.txt; empty: memory only).  Results then depend
+ * on the kept split only through the order of floating-point sums, and are
+ * reproducible while it stays.  SGPB_AUTOTUNE=0 uses the built-in rules.
+ * sgp_b200_autotune_clear forgets this process's splits (they are read from
+ * the file, or tuned, again). */
+void sgp_b200_autotune_clear(void);
 
 /* Milliseconds of the phases of the last sgp_b200_partition / eigensolve
  * (CUDA events).  After sgp_b200_partition_batch: host wall time of its

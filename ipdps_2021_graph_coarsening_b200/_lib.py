@@ -97,6 +97,7 @@ _SIGS = {
     "sgp_b200_hierarchy_levels": (c_int, [c_vp]),
     "sgp_b200_hierarchy_level": (c_int, [c_vp, c_int, P(c_u32), P(c_u64), P(c_vp), P(c_vp), P(c_vp),
                                          P(c_int), P(c_vp)]),
+    "sgp_b200_hierarchy_vertex_weights": (c_int, [c_vp, c_int, P(c_vp)]),
     "sgp_b200_eigensolve": (c_int, [c_vp, c_vp, P(sgp_pcg32_random_t), c_dbl, c_int, c_u64, c_vp, c_int,
                                     P(sgp_b200_result_t)]),
     "sgp_b200_hierarchy_free": (None, [c_vp]),
@@ -110,6 +111,7 @@ _SIGS = {
     "sgp_b200_fm_refine": (c_int, [c_vp, c_u32, c_vp, c_vp, c_vp, c_u32, P(c_u64), P(c_u32), P(c_u64)]),
     "sgp_b200_coarsen_map": (c_int, [c_vp, c_u32, c_vp, c_vp, c_vp, c_int, c_int, c_int, c_u64, c_vp, P(c_u32),
                                      P(c_int)]),
+    "sgp_b200_autotune_clear": (None, []),
     "sgp_b200_last_timing": (c_int, [c_vp, P(c_flt), P(c_flt), P(c_flt), P(c_flt)]),
     "sgp_b200_write_metrics": (c_int, [ctypes.c_char_p, P(sgp_b200_result_t), c_u64, c_u64, c_int, c_int]),
     "sgp_b200_split_noalloc": (c_int, [c_vp, c_u32, c_vp, c_vp, c_vp, c_vp, c_vp]),

@@ -571,9 +571,12 @@ class Hierarchy:
             if not p.value or cnt == 0:
                 return None
             return torch.as_tensor(_DevArray(p.value, cnt, ts), device="cuda").clone()
+        vw = ctypes.c_void_p()
+        L.check(L.lib().sgp_b200_hierarchy_vertex_weights(self.h, l, ctypes.byref(vw)),
+                "sgp_b200_hierarchy_vertex_weights")
         out = {"n": n.value, "m": m.value, "row_ptr": view(rp, n.value + 1, "<u4"), "col": view(col, m.value, "<u4"),
                "wbytes": wb.value, "w": view(w, m.value, "<u4" if wb.value == 4 else "<u8"),
-               "vcmap": view(vc, n.value, "<u4")}
+               "vcmap": view(vc, n.value, "<u4"), "vtx_w": view(vw, n.value, "<u4")}
         return out
 
     def eigensolve(self, rng: Optional[PCG32] = None, tol: float = 1e-10, mixed: bool = False,

@@ -1,7 +1,7 @@
 """In-tree build of the native libraries.
 
 * ``libsgpar_b200.so`` -- the sm_100a kernels and the C ABI of
-  ``include/sgpar_b200.h`` (``csrc/*.cu`` + ``csrc/io.cpp``), built with nvcc
+  ``include/sgpar_b200.h`` (``csrc/*.cu``, ``csrc/io.cpp``, ``csrc/tune.cpp``), built with nvcc
   for ``arch=compute_100a,code=sm_100a``.
 * ``libsgpgen.so`` -- the synthetic graph generators (``csrc/graphgen.cpp``).
 * ``sgpar_b200`` -- the config-file driver command (``csrc/sgpar_main.c``,
@@ -64,7 +64,8 @@ def build_lib(verbose: bool = False, force: bool = False) -> str:
     os.makedirs(BUILD, exist_ok=True)
     headers = glob.glob(os.path.join(CSRC, "*.cuh")) + glob.glob(os.path.join(CSRC, "*.h")) + \
         [os.path.join(ROOT, "include", "sgpar_b200.h")]
-    srcs = sorted(glob.glob(os.path.join(CSRC, "*.cu"))) + [os.path.join(CSRC, "io.cpp")]
+    srcs = sorted(glob.glob(os.path.join(CSRC, "*.cu"))) + [os.path.join(CSRC, "io.cpp"),
+                                                             os.path.join(CSRC, "tune.cpp")]
     nvcc = _nvcc()
     jobs = []
     objs = []

@@ -806,6 +806,27 @@ static int build_sorted_unit(Context &C, const Level &F, const uint32_t *vcmap, 
 }
 
 // Builds level `out` (allocating its arrays from the context) from F + vcmap.
+// c_vtx_w[vcmap[u]] += vtx_w[u] over the fine vertices u (unit weights when
+// fw is null); integer atomics, so the sums do not depend on their order
+__global__ void k_vertex_weights(uint32_t n, const uint32_t *__restrict__ vcmap, const uint32_t *__restrict__ fw,
+                                 uint32_t *cw) {
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
+        atomicAdd(&cw[vcmap[i]], fw ? fw[i] : 1u);
+}
+
+int coarse_vertex_weights(Context &C, const Level &F, const uint32_t *vcmap, uint32_t nc, uint32_t **out) {
+    uint32_t *cw;
+    SGPB_TRY(dalloc_t(C, &cw, (size_t)nc + 1));
+    SGPB_TRY(dzero(C, cw, sizeof(uint32_t) * ((size_t)nc + 1)));
+    uint32_t blocks = cdiv(F.n, 256);
+    if (blocks > (uint32_t)C.num_sms * 8) blocks = C.num_sms * 8;
+    if (F.n) k_vertex_weights<<<blocks, 256, 0, C.stream>>>(F.n, vcmap, F.vtx_w, cw);
+    C.kernel_launches++;
+    SGPB_CUDA(cudaGetLastError());
+    *out = cw;
+    return SGP_B200_OK;
+}
+
 int build_coarse_level(Context &C, const Level &F, const uint32_t *vcmap, uint32_t nc, int out_wbytes,
                        Level *out) {
     uint32_t *crp;

@@ -173,6 +173,7 @@ static int generate(Context &C, const Level &L0, uint32_t cutoff, uint64_t *rng_
         SGPB_CUDA(cudaEventRecord(ev[1], C.stream));
         Level Cl;
         SGPB_TRY(build_coarse_level(C, F, vcmap, nc, out_wbytes, &Cl));
+        SGPB_TRY(coarse_vertex_weights(C, F, vcmap, nc, &Cl.vtx_w));
         SGPB_CUDA(cudaEventRecord(ev[2], C.stream));
         SGPB_CUDA(cudaEventSynchronize(ev[2]));
         float a = 0, b = 0;
@@ -734,6 +735,15 @@ int sgp_b200_hierarchy_level(const sgp_b200_hierarchy_t *h, int l, uint32_t *n, 
     if (w) *w = L.w;
     if (wbytes) *wbytes = L.wbytes;
     if (vcmap) *vcmap = L.vcmap;
+    return SGP_B200_OK;
+}
+
+int sgp_b200_hierarchy_vertex_weights(const sgp_b200_hierarchy_t *h, int l, const uint32_t **vtx_w) {
+    if (!h || !vtx_w || l < 0 || l >= (int)h->levels.size()) {
+        set_error("level index out of range");
+        return SGP_B200_ERR_INVALID;
+    }
+    *vtx_w = h->levels[l].vtx_w;
     return SGP_B200_OK;
 }
 

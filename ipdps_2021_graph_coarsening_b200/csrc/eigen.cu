@@ -1756,13 +1756,13 @@ static int build_panels(Context &C, const Level &L, uint32_t T, size_t vbytes, P
     return SGP_B200_OK;
 }
 
-static uint32_t pi_grid(const Context &C, uint64_t n, uint64_t m) {
+static uint32_t pi_grid(const Context &C, uint64_t n, uint64_t m, uint32_t units) {
     const uint64_t maxg = (uint64_t)2 * C.num_sms;   // two resident blocks per SM (launch bounds)
-    // 16 cost units per thread: mid-size levels are latency-bound, and more
-    // warps shorten each warp's serial chain of rows (a 50k-vertex
-    // Erdos-Renyi graph: 63 -> 31 ms); levels large enough to fill the GPU
-    // are unaffected
-    const uint64_t want = cdiv(m + 8 * n, (uint64_t)kPIThreads * 16);
+    // `units` cost units per thread (16 by the built-in rule): mid-size
+    // levels are latency-bound, and more warps shorten each warp's serial
+    // chain of rows (a 50k-vertex Erdos-Renyi graph: 63 -> 31 ms going from 64
+    // to 16); levels large enough to fill the GPU are unaffected
+    const uint64_t want = cdiv(m + 8 * n, (uint64_t)kPIThreads * units);
     uint64_t grid = want < maxg ? want : maxg;
     return (uint32_t)(grid < 1 ? 1 : grid);
 }
@@ -1817,8 +1817,10 @@ static const void *pi_kernel_c(int mode) {
 }
 
 template <typename W, typename V, bool MX>
-static int launch_pi(Context &C, PIArgs &a, uint32_t grid) {
-    const PIVariant var = pi_variant(a);
+static int launch_pi(Context &C, PIArgs &a, uint32_t grid, int mode) {
+    PIVariant var;
+    var.mode = a.P ? 6 : mode;
+    var.na = true;
     const size_t cache_bytes = var.mode == 0 ? kCacheBytesStream : kCacheBytesRows;
     const uint64_t kmax = cache_bytes / sizeof(V);
     // cache_ok: 2 = the whole iterate in shared memory when it fits, 3 =
@@ -1874,8 +1876,7 @@ static int launch_pi(Context &C, PIArgs &a, uint32_t grid) {
 // levels, else the cooperative kernel (column panels when a layout is given).
 // mixed: FP32 edge-difference arithmetic (never with panels or small levels).
 static int run_pi(Context &C, const Level &L, PIArgs a, bool mixed, const PanelLayout *panels, double *res_d,
-                  double res_h[5], float *ms) {
-    const uint32_t grid = pi_grid(C, L.n, L.m);
+                  double res_h[5], float *ms, uint32_t grid, int mode) {
     a.res = res_d;
     a.P = 0;
     if (panels) {
@@ -1916,10 +1917,10 @@ static int run_pi(Context &C, const Level &L, PIArgs a, bool mixed, const PanelL
         SGPB_CUDA(cudaEventRecord(e0, C.stream));
         auto go = [&](auto mx) -> int {
             constexpr bool M = decltype(mx)::value;
-            if (L.wbytes == 8) return launch_pi<unsigned long long, double, M>(C, a, grid);
-            if (L.wbytes == 2) return launch_pi<uint16_t, double, M>(C, a, grid);
-            if (L.wbytes == 1) return launch_pi<uint8_t, double, M>(C, a, grid);
-            return launch_pi<uint32_t, double, M>(C, a, grid);
+            if (L.wbytes == 8) return launch_pi<unsigned long long, double, M>(C, a, grid, mode);
+            if (L.wbytes == 2) return launch_pi<uint16_t, double, M>(C, a, grid, mode);
+            if (L.wbytes == 1) return launch_pi<uint8_t, double, M>(C, a, grid, mode);
+            return launch_pi<uint32_t, double, M>(C, a, grid, mode);
         };
         rc = mixed ? go(std::true_type()) : go(std::false_type());
     }
@@ -1962,6 +1963,142 @@ static uint64_t iter_budget(uint32_t n, const PowerIterOpts &o) {
     uint64_t imax = 100000000000000ULL / (uint64_t)n;
     const uint64_t cap = o.iter_cap ? o.iter_cap : 5000000ULL;
     return imax > cap ? cap : imax;
+}
+
+// The work split of a level for variant t.mode (0 streaming, 5 or 7 warp
+// rows, 6 panels): rows longer than a warp's cost share / t.heavy_div are
+// block-wide (cut into 2^kSegShift-entry segments shared by the block's
+// warps), the others are cut into equal-cost warp ranges; per-row costs
+// count whole trips of the variant plus a row overhead.  Sets a.heavy_T,
+// a.heavy, a.n_heavy_ptr, a.hseg, a.seg_row, a.hpart, a.cpre, a.cpre_all
+// and allocates a.deg.
+static int setup_split(Context &C, const Level &L, const PITune &t, PIArgs &a) {
+    const uint32_t n = L.n;
+    const int mode = t.mode;
+    const uint64_t nwarps = (uint64_t)pi_grid(C, n, L.m, t.units) * kPIWarps;
+    uint64_t T = (L.m + 8ull * n) / nwarps / (t.heavy_div ? t.heavy_div : 1);
+    if (T < 4ull * kTile) T = 4ull * kTile;
+    if (T > 0xFFFFFFFFull) T = 0xFFFFFFFFull;
+    a.heavy_T = (uint32_t)T;
+    uint8_t *flags;
+    uint32_t *heavy, *nh, *cost, *cpre, *cost_all, *cpre_all;
+    SGPB_TRY(dalloc_t(C, &flags, n));
+    SGPB_TRY(dalloc_t(C, &heavy, (size_t)n + 1));
+    SGPB_TRY(dalloc_t(C, &nh, 1));
+    SGPB_TRY(dalloc_t(C, &cost, (size_t)n + 1));
+    SGPB_TRY(dalloc_t(C, &cpre, (size_t)n + 1));
+    SGPB_TRY(dalloc_t(C, &cost_all, (size_t)n + 1));
+    SGPB_TRY(dalloc_t(C, &cpre_all, (size_t)n + 1));
+    SGPB_TRY(dalloc_t(C, &a.deg, (size_t)n + 1));
+    k_heavy_flags<<<cdiv(n, 256), 256, 0, C.stream>>>(n, L.rp, a.heavy_T, flags);
+    // the cost total is kept in 32 bits
+    const uint32_t qs = (mode == 4 || mode == 5) ? 7u : mode == 7 ? 8u : 0u;   // trip of 128 / 256 entries
+    const uint32_t over = (mode == 4 || mode == 5 || mode == 7) ? 32u : 8u;
+    uint32_t shift = 0;
+    while ((L.m + ((1ull << qs) + over + 1) * (uint64_t)n) >> shift >= 0xFFFFFFF0ull) shift++;
+    k_row_cost<<<cdiv(n, 256), 256, 0, C.stream>>>(n, L.rp, a.heavy_T, qs, over, shift, cost, cost_all);
+    C.kernel_launches += 2;
+    SGPB_TRY(compact_flags(C, flags, n, heavy, nh));
+    {
+        // rows longer than T have more than 512 entries: at most m / 512 of them
+        const uint64_t max_segs = (L.m >> kSegShift) + L.m / (4ull * kTile) + 1;
+        uint32_t *segc, *hseg, *seg_row;
+        double *hpart;
+        SGPB_TRY(dalloc_t(C, &segc, (size_t)n + 1));
+        SGPB_TRY(dalloc_t(C, &hseg, (size_t)n + 1));
+        SGPB_TRY(dalloc_t(C, &seg_row, max_segs));
+        SGPB_TRY(dalloc_t(C, &hpart, max_segs));
+        k_seg_counts<<<cdiv(n, 256), 256, 0, C.stream>>>(n, L.rp, a.heavy_T, kSegShift, segc);
+        SGPB_TRY(scan_u32(C, segc, hseg, n, nullptr));
+        k_seg_rows<<<cdiv(n, 256), 256, 0, C.stream>>>(n, hseg, seg_row);
+        C.kernel_launches += 2;
+        a.hseg = hseg; a.seg_row = seg_row; a.hpart = hpart; a.seg_shift = kSegShift;
+    }
+    SGPB_TRY(scan_u32(C, cost, cpre, n, nullptr));
+    SGPB_TRY(scan_u32(C, cost_all, cpre_all, n, nullptr));
+    a.heavy = heavy; a.n_heavy_ptr = nh; a.cpre = cpre; a.cpre_all = cpre_all;
+    return SGP_B200_OK;
+}
+
+// levels below this cost (entries + 8 per vertex) keep the built-in rule
+constexpr uint64_t kTuneMinCost = 1ull << 18;
+constexpr uint64_t kTuneIters = 10;   // trial iterations per candidate split
+
+// Shape of a level for the autotuner's cache: weight width, relabelled copy
+// or not, arithmetic, and the octave of the vertex count and the half octave
+// of the mean degree.
+static std::string tune_key(const Level &L, const PIArgs &a, bool mixed) {
+    const double avg = L.n ? (double)L.m / L.n : 0;
+    int ln = 0;
+    while ((1ull << (ln + 1)) <= L.n) ln++;
+    const int ld = avg >= 1 ? (int)floor(2.0 * log2(avg)) : 0;
+    char k[96];
+    snprintf(k, sizeof(k), "w%d_r%d_x%d_n%d_d%d", L.wbytes, a.cache_ok == 3 ? 1 : 0, mixed ? 1 : 0, ln, ld);
+    return k;
+}
+
+// The first time a level of this shape is met on this device: run each
+// candidate split for kTuneIters iterations from the level's start vector
+// (into a scratch output, so the level's own run is untouched) and keep the
+// fastest.  Candidates: both variants where the mean degree leaves the choice
+// open (8 .. 512), long-row divisors of half, one and two times the rule's,
+// then grid units of 8 and 32 for the best of those.  `t` holds the rule on
+// entry and the choice on return.
+static int autotune_level(Context &C, const Level &L, const PIArgs &a0, bool mixed, const PowerIterOpts &o,
+                          PITune &t) {
+    const std::string key = tune_key(L, a0, mixed);
+    if (tune_lookup(C, key, &t)) return SGP_B200_OK;
+    tune_lock();
+    struct Unlock {
+        ~Unlock() { tune_unlock(); }
+    } unlock;
+    if (tune_lookup(C, key, &t)) return SGP_B200_OK;   // tuned by another thread meanwhile
+    const PITune rule = t;
+    double *scratch, *res_d;
+    SGPB_TRY(dalloc_t(C, &scratch, L.n));
+    SGPB_TRY(dalloc_t(C, &res_d, 8));
+    auto trial = [&](const PITune &c, double *ms) -> int {
+        PIArgs a = a0;
+        SGPB_TRY(setup_split(C, L, c, a));
+        a.out = scratch;
+        a.iter_max = kTuneIters;
+        a.tol = -1.0;   // run exactly kTuneIters iterations
+        double rh[5];
+        float k = 0;
+        SGPB_TRY(run_pi(C, L, a, mixed, nullptr, res_d, rh, &k, pi_grid(C, L.n, L.m, c.units), c.mode));
+        *ms = k;
+        return SGP_B200_OK;
+    };
+    const double avg = (double)L.m / L.n;
+    std::vector<int> modes;
+    if (avg >= 8.0 && avg <= 512.0) modes = {0, 5};
+    else modes = {rule.mode};
+    PITune best = rule;
+    double best_ms = 1e300, rule_ms = 0;
+    for (int m : modes) {
+        const uint32_t base = (uint32_t)(m == 0 ? kHeavyDivStream : kHeavyDivRows);
+        for (uint32_t div : {base / 2, base, base * 2}) {
+            PITune c;
+            c.mode = m;
+            c.heavy_div = div;
+            c.units = 16;
+            double ms = 0;
+            SGPB_TRY(trial(c, &ms));
+            if (c.mode == rule.mode && c.heavy_div == rule.heavy_div && c.units == rule.units) rule_ms = ms;
+            if (ms < best_ms) { best_ms = ms; best = c; }
+        }
+    }
+    for (uint32_t u : {8u, 32u}) {
+        PITune c = best;
+        c.units = u;
+        double ms = 0;
+        SGPB_TRY(trial(c, &ms));
+        if (ms < best_ms) { best_ms = ms; best = c; }
+    }
+    (void)o;
+    t = best;
+    tune_store(C, key, best, best_ms, rule_ms);
+    return SGP_B200_OK;
 }
 
 int power_iter_level(Context &C, const Level &Lin, const double *x_in, const uint32_t *vcmap, double *x_out,
@@ -2035,53 +2172,20 @@ int power_iter_level(Context &C, const Level &Lin, const double *x_in, const uin
         SGPB_TRY(read_u32(C, bad, &hbad));
         want_panels = hbad == 0;
     }
-    const int mode = want_panels ? 6 : pi_variant(a).mode;
-    // rows longer than a fraction of one warp's share of the cost are cut
-    // into segments shared by the block's warps (streaming profits from a
-    // lower threshold than warp rows: measured on R-MAT levels)
-    const uint64_t nwarps = (uint64_t)pi_grid(C, n, L.m) * kPIWarps;
-    uint64_t T = (L.m + 8ull * n) / nwarps / (mode == 0 ? kHeavyDivStream : kHeavyDivRows);
-    if (T < 4ull * kTile) T = 4ull * kTile;
-    if (T > 0xFFFFFFFFull) T = 0xFFFFFFFFull;
-    a.heavy_T = (uint32_t)T;
-    uint8_t *flags;
-    uint32_t *heavy, *nh, *cost, *cpre, *cost_all, *cpre_all;
-    SGPB_TRY(dalloc_t(C, &flags, n));
-    SGPB_TRY(dalloc_t(C, &heavy, (size_t)n + 1));
-    SGPB_TRY(dalloc_t(C, &nh, 1));
-    SGPB_TRY(dalloc_t(C, &cost, (size_t)n + 1));
-    SGPB_TRY(dalloc_t(C, &cpre, (size_t)n + 1));
-    SGPB_TRY(dalloc_t(C, &cost_all, (size_t)n + 1));
-    SGPB_TRY(dalloc_t(C, &cpre_all, (size_t)n + 1));
-    SGPB_TRY(dalloc_t(C, &a.deg, (size_t)n + 1));
-    k_heavy_flags<<<cdiv(n, 256), 256, 0, C.stream>>>(n, L.rp, a.heavy_T, flags);
-    // the cost total is kept in 32 bits
-    const uint32_t qs = (mode == 4 || mode == 5) ? 7u : mode == 7 ? 8u : 0u;   // trip of 128 / 256 entries
-    const uint32_t over = (mode == 4 || mode == 5 || mode == 7) ? 32u : 8u;
-    uint32_t shift = 0;
-    while ((L.m + ((1ull << qs) + over + 1) * (uint64_t)n) >> shift >= 0xFFFFFFF0ull) shift++;
-    k_row_cost<<<cdiv(n, 256), 256, 0, C.stream>>>(n, L.rp, a.heavy_T, qs, over, shift, cost, cost_all);
-    C.kernel_launches += 2;
-    SGPB_TRY(compact_flags(C, flags, n, heavy, nh));
-    {
-        // rows longer than T have more than 512 entries: at most m / 512 of them
-        const uint64_t max_segs = (L.m >> kSegShift) + L.m / (4ull * kTile) + 1;
-        uint32_t *segc, *hseg, *seg_row;
-        double *hpart;
-        SGPB_TRY(dalloc_t(C, &segc, (size_t)n + 1));
-        SGPB_TRY(dalloc_t(C, &hseg, (size_t)n + 1));
-        SGPB_TRY(dalloc_t(C, &seg_row, max_segs));
-        SGPB_TRY(dalloc_t(C, &hpart, max_segs));
-        k_seg_counts<<<cdiv(n, 256), 256, 0, C.stream>>>(n, L.rp, a.heavy_T, kSegShift, segc);
-        SGPB_TRY(scan_u32(C, segc, hseg, n, nullptr));
-        k_seg_rows<<<cdiv(n, 256), 256, 0, C.stream>>>(n, hseg, seg_row);
-        C.kernel_launches += 2;
-        a.hseg = hseg; a.seg_row = seg_row; a.hpart = hpart; a.seg_shift = kSegShift;
-    }
-    SGPB_TRY(scan_u32(C, cost, cpre, n, nullptr));
-    SGPB_TRY(scan_u32(C, cost_all, cpre_all, n, nullptr));
-    a.heavy = heavy; a.n_heavy_ptr = nh; a.cpre = cpre; a.cpre_all = cpre_all;
-    a.x_in = x_in; a.vcmap = vcmap; a.out = x_out;
+    const int rule_mode = want_panels ? 6 : pi_variant(a).mode;
+    a.x_in = x_in; a.vcmap = vcmap;
+    // the work split: the built-in rule, or the autotuner's choice for
+    // levels of this shape on this device (trial iterations the first time)
+    PITune tune;
+    tune.mode = rule_mode;
+    tune.heavy_div = (uint32_t)(rule_mode == 0 ? kHeavyDivStream : kHeavyDivRows);
+    tune.units = 16;
+    const char *forced = getenv("SGPB_PI_MODE");
+    if (!want_panels && !(forced && *forced) && (rule_mode == 0 || rule_mode == 5) && autotune_enabled() &&
+        L.m + 8ull * n >= kTuneMinCost)
+        SGPB_TRY(autotune_level(C, L, a, mixed, o, tune));
+    SGPB_TRY(setup_split(C, L, tune, a));
+    a.out = x_out;
     const uint64_t imax = iter_budget(n, o);
     a.iter_max = imax;
     a.tol = o.tol;
@@ -2091,7 +2195,8 @@ int power_iter_level(Context &C, const Level &Lin, const double *x_in, const uin
     float kms = 0;
     PanelLayout panels;
     if (want_panels) SGPB_TRY(build_panels(C, L, a.heavy_T, sizeof(double), &panels));
-    SGPB_TRY(run_pi(C, L, a, mixed, want_panels ? &panels : nullptr, res_d, rh, &kms));
+    SGPB_TRY(run_pi(C, L, a, mixed, want_panels ? &panels : nullptr, res_d, rh, &kms, pi_grid(C, n, L.m, tune.units),
+                    tune.mode));
     const uint64_t total_iters = (uint64_t)rh[0];
     res->niter = total_iters;
     res->dot = rh[1];

@@ -57,6 +57,7 @@ struct Context {
     float t_total = 0, t_coarsen = 0, t_eigen = 0, t_split = 0, t_h2d = 0, t_d2h = 0;
     float t_map = 0, t_build = 0;   // coarsening of the last partition: HEC mapping / coarse builds
     uint32_t kernel_launches = 0;
+    std::string dev_key;            // device name, SM count and compute capability (autotuner cache key)
 };
 
 Context *ctx_get(sgp_b200_ctx_t *c);
@@ -99,6 +100,7 @@ struct Level {
     int wbytes = 0;
     int sorted = 0;              // 1: every row ascending by destination (coarse levels)
     uint32_t *vcmap = nullptr;   // this level -> next coarser level
+    uint32_t *vtx_w = nullptr;   // vertex weights; null: every vertex weighs 1 (the input level)
     uint32_t max_deg = 0;
     uint32_t seed_hi = 0, seed_lo = 0;
     int hec_rounds = 0;
@@ -113,6 +115,10 @@ int hec_map_level(Context &C, const Level &L, int random_level, uint64_t seed, u
                   uint32_t *hn_out, uint32_t *nc_out, int *rounds_out);
 int build_coarse_level(Context &C, const Level &F, const uint32_t *vcmap, uint32_t nc, int out_wbytes,
                        Level *out);
+// Vertex weights of the coarse level of F under vcmap: the sum of the fine
+// vertex weights of each aggregate (coarsen_kokkos.h:1098), into *out (nc
+// entries, allocated here).
+int coarse_vertex_weights(Context &C, const Level &F, const uint32_t *vcmap, uint32_t nc, uint32_t **out);
 // the alternative coarseners (coarsen_alt.cu): heavy-edge matching, and the
 // MIS-2 (gosh false) / GOSH (gosh true) aggregations
 int match_map_level(Context &C, const Level &L, int random_level, uint64_t seed, uint32_t *vcmap, uint32_t *nc_out,
@@ -125,6 +131,27 @@ int hec_map_from_hn(Context &C, uint32_t n, const uint32_t *hn, uint64_t seed, u
 int gosh_v2_map_level(Context &C, const Level &L, uint64_t seed, uint32_t *vcmap, uint32_t *nc_out, int *rounds_out);
 int set_map_level(Context &C, const Level &L, bool gosh, uint64_t seed, uint32_t *vcmap, uint32_t *nc_out,
                   int *rounds_out);
+// Work split of one level's power iteration, chosen per level shape by the
+// autotuner (tune.cpp): the SpMV variant (0 CSR streaming, 5 pipelined warp
+// rows), the divisor of a warp's cost share above which a row is cut into
+// block-shared segments, and the cost units per thread that size the grid.
+struct PITune {
+    int mode = 5;
+    uint32_t heavy_div = 16;
+    uint32_t units = 16;
+};
+// The tuned split cached for level-shape key `key` on the context's device;
+// false when none is cached.  Thread-safe; the cache lives for the process
+// and in the file SGPB_TUNE_CACHE names (default
+// $HOME/.cache/sgpar_b200/pi_tune.txt; an empty value keeps it in memory).
+bool tune_lookup(const Context &C, const std::string &key, PITune *t);
+void tune_store(const Context &C, const std::string &key, const PITune &t, double ms_best, double ms_rule);
+// serialises the tuning of a level shape across host threads (batch workers)
+void tune_lock();
+void tune_unlock();
+// SGPB_AUTOTUNE=0 turns the autotuner off (the built-in rules then decide)
+bool autotune_enabled();
+
 // Entries of padding behind the destination and weight arrays of a
 // relabelled power-iteration copy: its staged SpMV copies whole chunks of this
 // many entries (16-byte aligned), so the last chunk stays in bounds.

@@ -211,6 +211,13 @@ sgp_b200_ctx_t *sgp_b200_create(int device) {
     C.device = device;
     C.num_sms = prop.multiProcessorCount;
     C.smem_optin = prop.sharedMemPerBlockOptin;
+    {
+        char key[160];
+        snprintf(key, sizeof(key), "%s|sm%d%d|%dSMs", prop.name, prop.major, prop.minor, prop.multiProcessorCount);
+        for (char *c = key; *c; c++)
+            if (*c == ' ') *c = '_';
+        C.dev_key = key;
+    }
     if (cudaStreamCreateWithFlags(&C.stream, cudaStreamNonBlocking) != cudaSuccess ||
         cudaMallocHost((void **)&C.h_pinned, 4096) != cudaSuccess) {
         set_error("stream / pinned buffer creation failed");
