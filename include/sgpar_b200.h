@@ -172,6 +172,12 @@ typedef struct {
                                    choice (coarsen_kokkos.h:1138-1150); | SGP_B200_COARSEN_NONE
                                    skips coarsening, | SGP_B200_COARSEN_RATIO_STOP stops after a
                                    level keeping more than 0.9 of the vertices (sgpar.h:2466-2475) */
+    uint32_t cluster_max_log2;  /* power-iteration levels above one block's shared memory and of at
+                                   most 2^k cost units (entries + 8 per vertex) run on a cluster of
+                                   8 blocks (one cluster barrier per iteration, several levels at
+                                   once); larger ones on the whole GPU.  0 = the default: 17 for
+                                   single partitions, 23 for sgp_b200_partition_batch, whose levels
+                                   of many graphs then share the GPU.  Equal values give equal bits. */
 } sgp_b200_options_t;
 
 #define SGP_B200_COARSEN_HEC 0      /* heavy-edge coarsening, heuristics.h:930-1031 (default) */

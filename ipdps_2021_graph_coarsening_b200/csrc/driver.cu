@@ -206,14 +206,17 @@ __global__ void k_normalize_guess(double *x, uint32_t n) {
 }
 
 // eigensolve_kokkos.h:1493-1595 without FM, in two parts so that a batch can
-// run the small levels of all its hierarchies in one launch.  eigen_begin
-// draws and normalises the coarsest guess and plans the chain of small levels
-// from the coarsest one up (the levels stay in `levels`, which must not be
-// resized afterwards); the chain runs through power_iter_chains; eigen_finish
-// records its results and iterates the remaining levels, prolongating down.
+// run the small and mid-size levels of all its hierarchies in two launches.
+// eigen_begin draws and normalises the coarsest guess and plans the chain of
+// small levels from the coarsest one up, then the chain of mid-size levels
+// above it (the levels stay in `levels`, which must not be resized
+// afterwards); the chains run through power_iter_chains and
+// power_iter_mid_chains (run_chains); eigen_finish records their results and
+// iterates the remaining levels, prolongating down.
 struct EigenState {
     double *x0 = nullptr;
-    PIChain chain;
+    PIChain chain;   // small levels
+    PIChain mid;     // mid-size levels, starting from the small chain's result
 };
 
 static int eigen_begin(Context &C, std::vector<Level> &levels, uint64_t *rng_state, uint64_t rng_inc,
@@ -231,23 +234,48 @@ static int eigen_begin(Context &C, std::vector<Level> &levels, uint64_t *rng_sta
     E->x0 = x;
     E->chain.x0 = x;
     E->chain.lev.clear();
-    for (int l = L - 1; l >= 0 && power_iter_small_ok(levels[l], o); l--) {
+    int l = L - 1;
+    for (; l >= 0 && power_iter_small_ok(levels[l], o); l--) {
         PIChainLevel cl;
         cl.L = &levels[l];
         cl.vcmap = (l == L - 1) ? nullptr : levels[l].vcmap;
         SGPB_TRY(dalloc_t(C, &cl.x_out, levels[l].n));
         E->chain.lev.push_back(cl);
     }
+    E->mid.x0 = E->chain.lev.empty() ? x : E->chain.lev.back().x_out;
+    E->mid.lev.clear();
+    for (; l >= 0 && power_iter_mid_ok(levels[l], o); l--) {
+        PIChainLevel cl;
+        cl.L = &levels[l];
+        cl.vcmap = (l == L - 1) ? nullptr : levels[l].vcmap;
+        SGPB_TRY(dalloc_t(C, &cl.x_out, levels[l].n));
+        E->mid.lev.push_back(cl);
+    }
     return SGP_B200_OK;
+}
+
+// the small-level chains of every hierarchy in one launch, then their
+// mid-size chains in another
+static int run_chains(Context &C, const std::vector<EigenState *> &es, const PowerIterOpts &o) {
+    std::vector<PIChain *> small, mid;
+    for (EigenState *e : es) {
+        small.push_back(&e->chain);
+        mid.push_back(&e->mid);
+    }
+    SGPB_TRY(power_iter_chains(C, small, o));
+    return power_iter_mid_chains(C, mid, o);
 }
 
 static int eigen_finish(Context &C, std::vector<Level> &levels, const PowerIterOpts &o, const EigenState &E,
                         double **evec_out, PowerIterResult *finest) {
     const int L = (int)levels.size();
-    const int nc = (int)E.chain.lev.size();
+    std::vector<const PIChainLevel *> done;   // chain levels from the coarsest one down
+    for (const PIChainLevel &cl : E.chain.lev) done.push_back(&cl);
+    for (const PIChainLevel &cl : E.mid.lev) done.push_back(&cl);
+    const int nc = (int)done.size();
     for (int k = 0; k < nc; k++) {
         Level &lv = levels[L - 1 - k];
-        const PowerIterResult &r = E.chain.lev[k].res;
+        const PowerIterResult &r = done[k]->res;
         lv.pi_iters = r.niter;
         lv.pi_ms = r.kernel_ms;
         lv.pi_capped = r.capped;
@@ -255,10 +283,10 @@ static int eigen_finish(Context &C, std::vector<Level> &levels, const PowerIterO
         lv.pi_lambda = r.lambda;
         if (L - 1 - k == 0) {
             *finest = r;
-            SGPB_TRY(level_residual(C, lv, E.chain.lev[k].x_out, o.normlap, finest));
+            SGPB_TRY(level_residual(C, lv, done[k]->x_out, o.normlap, finest));
         }
     }
-    const double *xin = nc ? E.chain.lev[nc - 1].x_out : E.x0;
+    const double *xin = nc ? done[nc - 1]->x_out : E.x0;
     for (int l = L - 1 - nc; l >= 0; l--) {
         Level &lv = levels[l];
         double *xo;
@@ -286,7 +314,7 @@ static int eigensolve(Context &C, std::vector<Level> &levels, uint64_t *rng_stat
                       const PowerIterOpts &o, double **evec_out, PowerIterResult *finest) {
     EigenState E;
     SGPB_TRY(eigen_begin(C, levels, rng_state, rng_inc, o, &E));
-    SGPB_TRY(power_iter_chains(C, {&E.chain}, o));
+    SGPB_TRY(run_chains(C, {&E}, o));
     return eigen_finish(C, levels, o, E, evec_out, finest);
 }
 
@@ -311,7 +339,8 @@ struct Staged {
 // partition_end finishes it and splits.  part_d is a device array of L0.n
 // entries; the caller copies it out.  ev[0] was recorded before staging (the
 // H2D window), ev[1..4] are recorded here.
-static int partition_begin(Context &C, const Level &L0, const sgp_b200_options_t *opt, cudaEvent_t *ev, Staged *S) {
+static int partition_begin(Context &C, const Level &L0, const sgp_b200_options_t *opt, cudaEvent_t *ev, Staged *S,
+                           bool batch = false) {
     if (opt->refine_alg != 0 && opt->refine_alg != 1) {
         set_error("refine_alg %d: 0 (shifted combinatorial Laplacian) or 1 (normalized Laplacian)", opt->refine_alg);
         return SGP_B200_ERR_INVALID;
@@ -324,6 +353,11 @@ static int partition_begin(Context &C, const Level &L0, const sgp_b200_options_t
     S->po.iter_cap = opt->iter_cap;
     S->po.mixed = opt->mixed;
     S->po.normlap = opt->refine_alg == 1;
+    // the cluster kernel's share of the levels: up to 2^17 cost units for a
+    // single partition (latency), 2^23 in a batch (many levels at once)
+    const uint32_t lg = opt->cluster_max_log2 ? (opt->cluster_max_log2 < 40 ? opt->cluster_max_log2 : 40u)
+                                              : (batch ? 23u : 17u);
+    S->po.mid_limit = 1ull << lg;
     SGPB_TRY(eigen_begin(C, S->levels, &S->st, opt->rng_inc, S->po, &S->es));
     return SGP_B200_OK;
 }
@@ -378,7 +412,7 @@ static int partition_staged(Context &C, const Level &L0, const sgp_b200_options_
                             uint32_t *part_d, cudaEvent_t *ev) {
     Staged S;
     SGPB_TRY(partition_begin(C, L0, opt, ev, &S));
-    SGPB_TRY(power_iter_chains(C, {&S.es.chain}, S.po));
+    SGPB_TRY(run_chains(C, {&S.es}, S.po));
     return partition_end(C, opt, res, part_d, ev, S);
 }
 
@@ -567,6 +601,10 @@ int sgp_b200_partition_batch(sgp_b200_ctx_t *x, const sgp_b200_graph_t *graphs, 
         if (!w) return SGP_B200_ERR_DEVICE;
         C->workers.push_back(w);
     }
+    {
+        const char *gc = getenv("SGPB_BATCH_GRID");
+        for (sgp_b200_ctx_t *w : C->workers) ctx_get(w)->grid_cap = gc ? (uint32_t)atoi(gc) : 0u;
+    }
     // largest graphs first (LPT): the workers take the next index of this order
     std::vector<int> order(count);
     for (int i = 0; i < count; i++) order[i] = i;
@@ -635,19 +673,20 @@ int sgp_b200_partition_batch(sgp_b200_ctx_t *x, const sgp_b200_graph_t *graphs, 
             SGPB_TRY(stage_input(W, &graphs[i], &it.L0));
             it.part_d = (opt->part_mem == SGP_B200_DEVICE) ? results[i].part : nullptr;
             if (!it.part_d) SGPB_TRY(dalloc_t(W, &it.part_d, graphs[i].n));
-            SGPB_TRY(partition_begin(W, it.L0, opt, it.E.e, &it.S));
-            it.launches = W.kernel_launches + 1;   // and the shared launch of phase 2
+            SGPB_TRY(partition_begin(W, it.L0, opt, it.E.e, &it.S, true));
+            it.launches = W.kernel_launches + 2;   // and the shared launches of phase 2
             it.t_map = W.t_map;
             it.t_build = W.t_build;
             return SGP_B200_OK;
         });
         ph[0] += ms_since(t0);
-        // phase 2: the small levels of every hierarchy, one launch
+        // phase 2: the small levels of every hierarchy in one launch, then
+        // their mid-size levels in another
         t0 = now();
         if (first_rc.load() == SGP_B200_OK) {
-            std::vector<PIChain *> chains;
-            for (int k = 0; k < w1 - w0; k++) chains.push_back(&items[k].S.es.chain);
-            const int rc = power_iter_chains(*C, chains, items[0].S.po);
+            std::vector<EigenState *> es;
+            for (int k = 0; k < w1 - w0; k++) es.push_back(&items[k].S.es);
+            const int rc = run_chains(*C, es, items[0].S.po);
             if (rc != SGP_B200_OK) fail(order[w0], rc);
         }
         ph[1] += ms_since(t0);

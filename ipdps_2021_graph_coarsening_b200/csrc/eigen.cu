@@ -1552,6 +1552,244 @@ __global__ void __launch_bounds__(kSmallThreads, 1) k_power_iter_chains(const PI
     }
 }
 
+// --------------------------------------------------- mid-size levels --
+// Levels too large for one block's shared memory but small enough that the
+// cooperative kernel's grid barriers dominate (about 13 us per iteration
+// whatever the level's size) run on a cluster of kMidCTAs blocks: the
+// iterate stays in global memory (L2-resident at these sizes), the five sums
+// of an iteration are exchanged through distributed shared memory, and one
+// cluster barrier per iteration replaces the grid barrier.  Clusters take
+// chains of consecutive mid-size levels (one hierarchy each, coarsest first)
+// from a work queue, so one launch iterates these levels of a whole batch of
+// hierarchies, a cluster per hierarchy at a time.  The recurrence, stopping
+// rule and result are the cooperative kernel's; the work split (rows by
+// entry count over the cluster's blocks, then over their warps, CSR
+// streaming) depends only on the level.
+constexpr int kMidCTAs = 8;
+constexpr int kMidThreads = 512;
+constexpr int kMidWarps = kMidThreads / 32;
+// m + 8n of the largest level run here by default: above it one level on the
+// whole GPU is faster (measured on grids: at 2^17 both take ~12 us per
+// iteration; at 3*10^5, 26 vs 9 us); batches raise it (options.cluster_max_log2)
+constexpr uint64_t kMidCost = 1ull << 17;
+
+struct MidLevelDesc {
+    uint32_t n;
+    uint64_t m;
+    const uint32_t *rp;
+    const uint32_t *col;
+    const void *w;
+    int wbytes;              // 0, 4 or 8
+    int mixed;               // FP32 edge-difference arithmetic
+    int normlap;
+    int vec_ok;              // col / w 16-byte aligned
+    const double *x_in;      // start vector, read through vcmap when set
+    const uint32_t *vcmap;
+    double *out;             // normalised result (n)
+    double *va, *vb, *deg;   // iterate buffers and weighted degrees (n each)
+    double tol;
+    uint64_t iter_max;
+    double *res;             // [0] niter [1] dot [2] gb [3] lambda [4] capped [6] ms
+};
+
+// first row i in [lo, hi] with rp[i] >= t
+__device__ __forceinline__ uint32_t rows_at(const uint32_t *rp, uint32_t lo, uint32_t hi, uint64_t t) {
+    return lower_bound_u32(rp, lo, hi, t);
+}
+
+// Cluster-wide sums of NV values: every block adds its partials to slot
+// `buf` of its shared memory; after the cluster barrier lane r < kMidCTAs of
+// the first warp reads block r's slot, lane 0 adds them in rank order and
+// broadcasts through shared memory, so every block holds the same totals
+// (and only kMidCTAs remote reads per value and block cross the cluster).
+template <int NV>
+__device__ __forceinline__ void cluster_sum(double (&v)[NV], double (*slot)[8], int buf, double *sm,
+                                            cg::cluster_group &cl) {
+    block_sum_d<NV>(v, sm);
+    if (threadIdx.x == 0)
+#pragma unroll
+        for (int k = 0; k < NV; k++) slot[buf][k] = v[k];
+    cl.sync();
+    if (threadIdx.x < 32) {
+        const unsigned lane = threadIdx.x;
+        double mine[NV];
+        const double *rs = cl.map_shared_rank(&slot[buf][0], lane < kMidCTAs ? lane : 0u);
+#pragma unroll
+        for (int k = 0; k < NV; k++) mine[k] = lane < kMidCTAs ? rs[k] : 0.0;
+#pragma unroll
+        for (int k = 0; k < NV; k++) {
+            double t = 0;
+            for (int r = 0; r < kMidCTAs; r++) t += __shfl_sync(0xFFFFFFFFu, mine[k], r);
+            if (lane == 0) sm[220 + k] = t;
+        }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int k = 0; k < NV; k++) v[k] = sm[220 + k];
+    __syncthreads();   // sm is reused by the next sum
+}
+
+template <typename W, bool MX>
+__device__ __forceinline__ void mid_level(const MidLevelDesc &d, cg::cluster_group &cl, double *sm,
+                                          double (*slot)[8], uint32_t *win, double *winx, double *wind) {
+    typedef typename std::conditional<MX, float, double>::type ACC;
+    const uint32_t n = d.n;
+    const uint64_t m = d.m;
+    const uint32_t *rp = d.rp;
+    const W *w = (const W *)d.w;
+    const unsigned rank = cl.block_rank();
+    const unsigned lane = threadIdx.x & 31, wk = threadIdx.x >> 5;
+    // rows of this block and of this warp: equal shares of the entries
+    const uint32_t R0 = rank == 0 ? 0u : rows_at(rp, 0, n, m * rank / kMidCTAs);
+    const uint32_t R1 = rank + 1 == kMidCTAs ? n : rows_at(rp, 0, n, m * (rank + 1) / kMidCTAs);
+    const uint64_t E0 = rp[R0], E1 = rp[R1];
+    const uint32_t w0 = wk == 0 ? R0 : rows_at(rp, R0, R1, E0 + (E1 - E0) * wk / kMidWarps);
+    const uint32_t w1 = wk + 1 == kMidWarps ? R1 : rows_at(rp, R0, R1, E0 + (E1 - E0) * (wk + 1) / kMidWarps);
+    // ---- phase 0: start vector (prolongated), weighted degrees, shift
+    double p[4] = {0, 0, 0, 0};   // sum x, sum x d, sum d (normlap mean), max d
+    bool empty_rows = false;
+    for (uint32_t i = w0; i < w1; i++) {
+        const uint32_t b = rp[i], e = rp[i + 1];
+        double dg = (double)(e - b);
+        if (w) {
+            uint64_t sw = 0;
+            for (uint32_t j = b + lane; j < e; j += 32) sw += (uint64_t)__ldg(w + j);
+            dg = (double)warp_sum(sw);
+        }
+        empty_rows |= e == b;
+        if (lane == 0) {
+            const double x = d.vcmap ? d.x_in[d.vcmap[i]] : d.x_in[i];
+            d.va[i] = x;
+            d.deg[i] = dg;
+            p[0] += x;
+            p[1] += x * dg;
+            p[2] += dg;
+            p[3] = dg > p[3] ? dg : p[3];
+        }
+    }
+    double mx = warp_max(p[3]);
+    if (lane == 0) sm[210 + wk] = mx;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double t = 0;
+        for (int k = 0; k < kMidWarps; k++) t = sm[210 + k] > t ? sm[210 + k] : t;
+        slot[1][4] = t;
+    }
+    double s3[3] = {p[0], p[1], p[2]};
+    block_sum_d<3>(s3, sm);
+    if (threadIdx.x == 0) { slot[1][0] = s3[0]; slot[1][1] = s3[1]; slot[1][2] = s3[2]; }
+    cl.sync();
+    if (threadIdx.x == 0) {
+        double a = 0, b = 0, c = 0, mxd = 0;
+        for (int r = 0; r < kMidCTAs; r++) {
+            const double *rs = cl.map_shared_rank(&slot[1][0], r);
+            a += rs[0];
+            b += rs[1];
+            c += rs[2];
+            mxd = rs[4] > mxd ? rs[4] : mxd;
+        }
+        sm[220] = a; sm[221] = b; sm[222] = c; sm[223] = mxd;
+    }
+    __syncthreads();
+    const double S0 = sm[220], Sxd = sm[221], Sd = sm[222], maxd = sm[223];
+    __syncthreads();
+    double gb = 2.0 * maxd;
+    if (gb < 2.0) gb = 2.0;
+    double mu = d.normlap ? (Sd > 0 ? Sxd / Sd : 0.0) : S0 / (double)n;
+    double q[1] = {0};
+    for (uint32_t i = R0 + threadIdx.x; i < R1; i += blockDim.x) {
+        const double x = d.va[i] - mu;
+        q[0] += x * x;
+    }
+    cluster_sum<1>(q, slot, 0, sm, cl);
+    double inv_nu = 1.0 / sqrt(q[0]);
+    // ---- iterations
+    double dot = 0, last = 1;
+    uint64_t niter = 0;
+    double *src = d.va, *dst = d.vb;
+    while (true) {
+        double P[kNP] = {0, 0, 0, 0, 0};
+        auto fin = [&](uint32_t i, ACC acc, double dg, double xi) {
+            const double ui = (xi - mu) * inv_nu;
+            const double r = next_value<MX>(d.normlap, gb, mu, inv_nu, ui, (double)acc, dg);
+            dst[i] = r;
+            P[0] += r; P[1] += r * r; P[2] += ui * r; P[3] += ui; P[4] += ui * ui;
+        };
+        if (w1 > w0)
+            warp_stream<true, MX, W, double, ACC>(rp, d.col, w, (const double *)src, m, d.vec_ok != 0, w0, w1,
+                                                  d.deg, win, winx, wind, fin);
+        // rows without entries are not streamed: r = (gb - 0) u_i (u_i / 2
+        // for the normalized walk)
+        if (empty_rows && lane == 0)
+            for (uint32_t i = w0; i < w1; i++)
+                if (rp[i] == rp[i + 1]) fin(i, (ACC)0, 0.0, src[i]);
+        // consecutive exchanges alternate slots (phase 0 used 1, then 0)
+        cluster_sum<kNP>(P, slot, (int)((niter + 1) & 1), sm, cl);
+        const double mu_n = d.normlap ? 0.0 : P[0] / (double)n;
+        const double nsq = P[1] - mu_n * P[0];
+        const double inv_nu_n = 1.0 / sqrt(nsq);
+        last = dot;
+        dot = (P[2] - mu_n * P[3]) * inv_nu_n;
+        niter++;
+        const double delta = fabs(dot - last);
+        if (!(delta > d.tol && niter < d.iter_max)) {
+            for (uint32_t i = R0 + threadIdx.x; i < R1; i += blockDim.x) d.out[i] = (src[i] - mu) * inv_nu;
+            if (rank == 0 && threadIdx.x == 0) {
+                d.res[0] = (double)niter;
+                d.res[1] = dot;
+                d.res[2] = gb;
+                d.res[3] = d.normlap ? 2.0 * (1.0 - P[2] / P[4]) : (gb * P[4] - P[2]) / P[4];
+                d.res[4] = niter >= d.iter_max ? 1.0 : 0.0;
+            }
+            break;
+        }
+        mu = mu_n;
+        inv_nu = inv_nu_n;
+        double *t = src; src = dst; dst = t;
+    }
+}
+
+__global__ void __cluster_dims__(kMidCTAs, 1, 1) __launch_bounds__(kMidThreads, 1)
+    k_power_iter_mid(const MidLevelDesc *__restrict__ lev, const uint2 *__restrict__ chains, uint32_t nchains,
+                     uint32_t *next) {
+    cg::cluster_group cl = cg::this_cluster();
+    __shared__ double sm[256];
+    __shared__ double slot[2][8];
+    __shared__ uint32_t swin[kMidWarps][kWin + 3];
+    __shared__ double swinx[kMidWarps][kTile];
+    __shared__ double swind[kMidWarps][kTile];
+    __shared__ uint32_t item;
+    const unsigned wk = threadIdx.x >> 5;
+    while (true) {
+        if (cl.block_rank() == 0 && threadIdx.x == 0) item = atomicAdd(next, 1u);
+        cl.sync();
+        if (threadIdx.x == 0) sm[230] = (double)*cl.map_shared_rank(&item, 0);
+        __syncthreads();
+        const uint32_t c = (uint32_t)sm[230];
+        // every block has read rank 0's `item` before any block can exit (a
+        // block's shared memory must not be read after it has exited) or
+        // rank 0 writes the next one
+        cl.sync();
+        if (c >= nchains) return;
+        const uint2 ch = chains[c];
+        for (uint32_t k = 0; k < ch.y; k++) {
+            const MidLevelDesc &dsc = lev[ch.x + k];
+            const unsigned long long t0 = global_ns();
+            if (dsc.wbytes == 8) {
+                if (dsc.mixed) mid_level<unsigned long long, true>(dsc, cl, sm, slot, swin[wk], swinx[wk], swind[wk]);
+                else mid_level<unsigned long long, false>(dsc, cl, sm, slot, swin[wk], swinx[wk], swind[wk]);
+            } else {
+                if (dsc.mixed) mid_level<uint32_t, true>(dsc, cl, sm, slot, swin[wk], swinx[wk], swind[wk]);
+                else mid_level<uint32_t, false>(dsc, cl, sm, slot, swin[wk], swinx[wk], swind[wk]);
+            }
+            // every block's part of the result is written before the next
+            // level reads it, and every read of another block's slots is done
+            cl.sync();
+            if (cl.block_rank() == 0 && threadIdx.x == 0) dsc.res[6] = (double)(global_ns() - t0) * 1e-6;
+        }
+    }
+}
+
 // ----------------------------------------------------------- residual --
 // |L x - lambda x|^2 partial sums per block (x unit-norm FP64 vector).
 // normlap: the random-walk Laplacian I - D^-1 A instead of L = D - A.
@@ -1764,6 +2002,7 @@ static uint32_t pi_grid(const Context &C, uint64_t n, uint64_t m, uint32_t units
     // to 16); levels large enough to fill the GPU are unaffected
     const uint64_t want = cdiv(m + 8 * n, (uint64_t)kPIThreads * units);
     uint64_t grid = want < maxg ? want : maxg;
+    if (C.grid_cap && grid > C.grid_cap) grid = C.grid_cap;
     return (uint32_t)(grid < 1 ? 1 : grid);
 }
 
@@ -2120,6 +2359,20 @@ int power_iter_level(Context &C, const Level &Lin, const double *x_in, const uin
         if (want_residual) SGPB_TRY(level_residual(C, Lin, x_out, o.normlap, res));
         return SGP_B200_OK;
     }
+    if (power_iter_mid_ok(Lin, o)) {
+        // one cluster: a mid-size chain of one level
+        PIChain ch;
+        ch.x0 = x_in;
+        PIChainLevel cl;
+        cl.L = &Lin;
+        cl.vcmap = vcmap;
+        cl.x_out = x_out;
+        ch.lev.push_back(cl);
+        SGPB_TRY(power_iter_mid_chains(C, {&ch}, o));
+        *res = ch.lev[0].res;
+        if (want_residual) SGPB_TRY(level_residual(C, Lin, x_out, o.normlap, res));
+        return SGP_B200_OK;
+    }
     PIArgs a;
     memset(&a, 0, sizeof(a));
     // A level whose whole iterate fits in 96 KB keeps it in shared memory.
@@ -2296,6 +2549,101 @@ int power_iter_chains(Context &C, const std::vector<PIChain *> &chains, const Po
                                    (int)kSmallSmemBytes));
     const uint32_t grid = (uint32_t)(hc.size() < (size_t)C.num_sms ? hc.size() : (size_t)C.num_sms);
     k_power_iter_chains<<<grid, kSmallThreads, bytes, C.stream>>>(lev_d, ch_d, (uint32_t)hc.size(), next);
+    C.kernel_launches++;
+    SGPB_CUDA(cudaGetLastError());
+    std::vector<double> rh(8 * h.size());
+    SGPB_CUDA(cudaMemcpyAsync(rh.data(), res_d, sizeof(double) * rh.size(), cudaMemcpyDeviceToHost, C.stream));
+    SGPB_CUDA(cudaStreamSynchronize(C.stream));
+    size_t i = 0;
+    for (PIChain *ch : chains) {
+        if (!ch) continue;
+        for (PIChainLevel &cl : ch->lev) {
+            const double *r = &rh[8 * i++];
+            cl.res = PowerIterResult();
+            cl.res.niter = (uint64_t)r[0];
+            cl.res.dot = r[1];
+            cl.res.gb = r[2];
+            cl.res.lambda = r[3];
+            cl.res.capped = r[4] != 0.0;
+            cl.res.kernel_ms = (float)r[6];
+        }
+    }
+    return SGP_B200_OK;
+}
+
+bool power_iter_mid_ok(const Level &L, const PowerIterOpts &o) {
+    const char *forced = getenv("SGPB_PI_MODE");
+    if (forced && *forced) return false;
+    if (const char *e = getenv("SGPB_PI_MID"))
+        if (atoi(e) == 0) return false;
+    if (L.n == 0 || power_iter_small_ok(L, o)) return false;
+    if (!(L.wbytes == 0 || L.wbytes == 4 || L.wbytes == 8)) return false;
+    return L.m + 8ull * L.n <= (o.mid_limit ? o.mid_limit : kMidCost);
+}
+
+int power_iter_mid_chains(Context &C, const std::vector<PIChain *> &chains, const PowerIterOpts &o) {
+    std::vector<MidLevelDesc> h;
+    std::vector<std::pair<uint64_t, uint2>> order;   // (cost, chain) for largest-first
+    for (PIChain *ch : chains) {
+        if (!ch || ch->lev.empty()) continue;
+        uint2 c = make_uint2((uint32_t)h.size(), (uint32_t)ch->lev.size());
+        uint64_t cost = 0;
+        for (size_t k = 0; k < ch->lev.size(); k++) {
+            const PIChainLevel &cl = ch->lev[k];
+            const Level &L = *cl.L;
+            if (!power_iter_mid_ok(L, o)) {
+                set_error("level of %u vertices and %llu entries is not a mid-size level", L.n,
+                          (unsigned long long)L.m);
+                return SGP_B200_ERR_INVALID;
+            }
+            MidLevelDesc d;
+            memset(&d, 0, sizeof(d));
+            d.n = L.n; d.m = L.m; d.rp = L.rp; d.col = L.col; d.w = L.w; d.wbytes = L.wbytes;
+            d.mixed = o.mixed && L.n >= 4096;
+            d.normlap = o.normlap;
+            d.vec_ok = (((uintptr_t)L.col | (uintptr_t)L.w) & 15u) == 0;
+            d.x_in = k == 0 ? ch->x0 : ch->lev[k - 1].x_out;
+            d.vcmap = cl.vcmap;
+            d.out = cl.x_out;
+            SGPB_TRY(dalloc_t(C, &d.va, L.n));
+            SGPB_TRY(dalloc_t(C, &d.vb, L.n));
+            SGPB_TRY(dalloc_t(C, &d.deg, L.n));
+            d.tol = o.tol;
+            d.iter_max = iter_budget(L.n, o);
+            h.push_back(d);
+            cost += L.m + 8ull * L.n;
+        }
+        order.push_back({cost, c});
+    }
+    if (h.empty()) return SGP_B200_OK;
+    std::stable_sort(order.begin(), order.end(), [](const auto &x, const auto &y) { return x.first > y.first; });
+    std::vector<uint2> hc(order.size());
+    for (size_t i = 0; i < order.size(); i++) hc[i] = order[i].second;
+    double *res_d;
+    SGPB_TRY(dalloc_t(C, &res_d, 8 * h.size()));
+    for (size_t i = 0; i < h.size(); i++) h[i].res = res_d + 8 * i;
+    MidLevelDesc *lev_d;
+    uint2 *ch_d;
+    uint32_t *next;
+    SGPB_TRY(dalloc_t(C, &lev_d, h.size()));
+    SGPB_TRY(dalloc_t(C, &ch_d, hc.size()));
+    SGPB_TRY(dalloc_t(C, &next, 1));
+    SGPB_CUDA(cudaMemcpyAsync(lev_d, h.data(), sizeof(MidLevelDesc) * h.size(), cudaMemcpyHostToDevice, C.stream));
+    SGPB_CUDA(cudaMemcpyAsync(ch_d, hc.data(), sizeof(uint2) * hc.size(), cudaMemcpyHostToDevice, C.stream));
+    SGPB_TRY(dzero(C, next, 4));
+    // as many clusters as fit at once (the queue balances the rest)
+    cudaLaunchConfig_t cfg;
+    memset(&cfg, 0, sizeof(cfg));
+    cfg.gridDim = dim3(kMidCTAs);
+    cfg.blockDim = dim3(kMidThreads);
+    int max_clusters = 0;
+    SGPB_CUDA(cudaOccupancyMaxActiveClusters(&max_clusters, (const void *)k_power_iter_mid, &cfg));
+    if (max_clusters < 1) {
+        set_error("the mid-size power-iteration cluster does not fit on the device");
+        return SGP_B200_ERR_DEVICE;
+    }
+    const uint32_t nclu = (uint32_t)(hc.size() < (size_t)max_clusters ? hc.size() : (size_t)max_clusters);
+    k_power_iter_mid<<<nclu * kMidCTAs, kMidThreads, 0, C.stream>>>(lev_d, ch_d, (uint32_t)hc.size(), next);
     C.kernel_launches++;
     SGPB_CUDA(cudaGetLastError());
     std::vector<double> rh(8 * h.size());

@@ -58,6 +58,7 @@ struct Context {
     float t_map = 0, t_build = 0;   // coarsening of the last partition: HEC mapping / coarse builds
     uint32_t kernel_launches = 0;
     std::string dev_key;            // device name, SM count and compute capability (autotuner cache key)
+    uint32_t grid_cap = 0;          // > 0: at most this many blocks per power-iteration launch
 };
 
 Context *ctx_get(sgp_b200_ctx_t *c);
@@ -163,6 +164,7 @@ struct PowerIterOpts {
     int mixed = 0;           // 1: FP32 edge-difference SpMV arithmetic, FP64 iterate and reductions
     int allow_relabel = 1;   // skewed levels may iterate on a hub-first relabelled copy
     int normlap = 0;         // refine_alg 1: normalized-Laplacian (lazy random walk) iteration
+    uint64_t mid_limit = 0;  // largest cost (m + 8n) of a level on the cluster kernel; 0 = 2^17
 };
 struct PowerIterResult {
     uint64_t niter = 0;
@@ -193,6 +195,11 @@ struct PIChain {
     std::vector<PIChainLevel> lev;
 };
 int power_iter_chains(Context &C, const std::vector<PIChain *> &chains, const PowerIterOpts &o);
+// Mid-size levels (a cluster of blocks, the iterate in global memory, one
+// cluster barrier per iteration): chains of consecutive such levels, coarsest
+// first, one cluster per chain at a time, in one launch.
+bool power_iter_mid_ok(const Level &L, const PowerIterOpts &o);
+int power_iter_mid_chains(Context &C, const std::vector<PIChain *> &chains, const PowerIterOpts &o);
 int split_level(Context &C, const Level &L, const double *evec, int perc_imbalance, uint32_t *part,
                 uint64_t *edgecut, uint32_t *n_part0);
 int edge_cut_device(Context &C, const Level &L, const uint32_t *part, uint64_t *edgecut);

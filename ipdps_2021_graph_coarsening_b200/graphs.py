@@ -187,3 +187,20 @@ def mtx_of(g: CSR, symmetry: str = "symmetric", field: str = "pattern", seed: Op
         rows, cols = rows[p], cols[p]
     n = g.n + extra_vertices
     return mtx_text(rows, cols, n, n, field=field, symmetry=symmetry, **kw)
+
+
+def batch_graphs(count: int = 2048, seed: int = 2048, lo: int = 1000, hi: int = 250000) -> list:
+    """The batch configuration: vertex counts log-uniform in [lo, hi] from a
+    fixed seed; even indices are near-square 2D grids with 10% of the vertices
+    removed (largest component kept), odd ones Erdos-Renyi graphs of mean
+    degree 8 (largest component), unit weights."""
+    rng = np.random.default_rng(seed)
+    sizes = np.exp(rng.uniform(np.log(lo), np.log(hi), count)).astype(int)
+    out = []
+    for i, s in enumerate(sizes):
+        if i % 2 == 0:
+            nx = int(math.sqrt(s))
+            out.append(grid2d_holes(nx, max(2, int(s) // nx), seed=i + 1))
+        else:
+            out.append(erdos_renyi(int(s), 8.0, seed=i + 1))
+    return out

@@ -98,12 +98,17 @@ def batch_graphs(count, seed=17, lo=1000, hi=12000):
     return out
 
 
+# a batch runs levels of up to 2^23 cost units on the cluster kernel (single
+# calls: 2^17); with the same cluster_max_log2 a single call gives equal bits
+BATCH_CLUSTER = 23
+
+
 def test_batch_equals_single_calls(partitioner):
     gs = batch_graphs(12)
     many = partitioner.partition_batch(gs, workers=4, rng_state=9)
     one = partitioner.partition_batch(gs, workers=1, rng_state=9)
     for g, a, b in zip(gs, many, one):
-        s = partitioner.partition(g, rng_state=9)
+        s = partitioner.partition(g, rng_state=9, cluster_max_log2=BATCH_CLUSTER)
         for r in (a, b):
             assert np.array_equal(r.part, s.part)
             assert r.edgecut == s.edgecut == cut_of(g, r.part)
@@ -123,7 +128,7 @@ def test_batch_of_small_hierarchies(partitioner):
     gs = batch_graphs(40, seed=5, lo=40, hi=1500)
     rs = partitioner.partition_batch(gs, workers=3, rng_state=2)
     for g, r in zip(gs, rs):
-        same_result(r, partitioner.partition(g, rng_state=2))
+        same_result(r, partitioner.partition(g, rng_state=2, cluster_max_log2=BATCH_CLUSTER))
         assert r.edgecut == cut_of(g, r.part)
     for g, r in list(zip(gs, rs))[:6]:
         o = O.partition_graph(g.row_ptr, g.col, None, cutoff=50, tol=1e-10, rng_state=2)
@@ -139,7 +144,20 @@ def test_batch_weighted_and_mixed_equal_single_calls(partitioner, mixed):
     gs += batch_graphs(5, seed=41, lo=2000, hi=20000)
     rs = partitioner.partition_batch(gs, workers=2, rng_state=8, mixed=mixed)
     for g, r in zip(gs, rs):
-        same_result(r, partitioner.partition(g, rng_state=8, mixed=mixed))
+        same_result(r, partitioner.partition(g, rng_state=8, mixed=mixed, cluster_max_log2=BATCH_CLUSTER))
+
+
+def test_batch_default_and_single_default_agree(partitioner):
+    """Default settings: the batch's mid-size levels run on the cluster kernel
+    and a single call's larger ones on the whole GPU; the hierarchy and rng
+    are the same, the Fiedler values agree to rounding and the cuts to 1%."""
+    gs = batch_graphs(6, seed=29, lo=5000, hi=40000)
+    rs = partitioner.partition_batch(gs, workers=3, rng_state=12)
+    for g, r in zip(gs, rs):
+        s = partitioner.partition(g, rng_state=12)
+        assert r.level_n == s.level_n and r.rng_state == s.rng_state
+        assert abs(r.lam - s.lam) <= 1e-8 * abs(s.lam)
+        assert abs(r.edgecut - s.edgecut) <= 0.01 * s.edgecut and r.edgecut == cut_of(g, r.part)
 
 
 def test_batch_matches_oracle(partitioner):
@@ -184,7 +202,7 @@ def test_sharded_batch_on_one_rank(partitioner):
     gs = batch_graphs(5, seed=31)
     out = shard.partition_sharded(gs, lambda l: partitioner.partition_batch(l, workers=2, rng_state=6), 0, 1)
     for g, r in zip(gs, out):
-        s = partitioner.partition(g, rng_state=6)
+        s = partitioner.partition(g, rng_state=6, cluster_max_log2=BATCH_CLUSTER)
         assert np.array_equal(r.part, s.part) and r.edgecut == s.edgecut
 
 

@@ -485,3 +485,57 @@ def test_malformed_graph_is_rejected(partitioner):
     with pytest.raises(L.SgparError) as e:
         partitioner.partition(bad)
     assert e.value.code == L.ERR_INVALID
+
+
+def with_isolated(g, k, seed=0):
+    """g plus k isolated vertices at random positions (rows without entries)."""
+    rng = np.random.default_rng(seed)
+    n2 = g.n + k
+    old = np.sort(rng.choice(n2, g.n, replace=False)).astype(np.uint32)   # new id of each old vertex
+    deg = np.zeros(n2, np.int64)
+    deg[old] = np.diff(g.row_ptr).astype(np.int64)
+    rp = np.zeros(n2 + 1, np.uint32)
+    rp[1:] = np.cumsum(deg)
+    col = np.empty(len(g.col), np.uint32)
+    for i in range(g.n):
+        col[rp[old[i]]:rp[old[i] + 1]] = old[g.col[g.row_ptr[i]:g.row_ptr[i + 1]]]
+    return G.CSR(rp, col)
+
+
+@pytest.mark.parametrize("name", ["er7k", "grid100", "er7k_isolated", "chunglu_w"])
+@pytest.mark.parametrize("mixed", [False, True])
+def test_power_iter_mid_size_cluster(partitioner, monkeypatch, name, mixed):
+    """Mid-size levels (more than one block's shared memory, at most 2^17
+    cost units) run on a cluster of blocks with the iterate in global memory
+    and one cluster barrier per iteration: against the oracle, and against the
+    cooperative kernel (SGPB_PI_MID=0), including rows without entries."""
+    if name == "er7k":
+        g = G.erdos_renyi(7500, 8.0, seed=7)
+        rp, col, w = g.row_ptr, g.col, None
+    elif name == "grid100":
+        g = G.grid2d(100, 90)
+        rp, col, w = g.row_ptr, g.col, None
+    elif name == "er7k_isolated":
+        g = with_isolated(G.erdos_renyi(7000, 8.0, seed=8), 200, seed=1)
+        rp, col, w = g.row_ptr, g.col, None
+    else:
+        g = G.chung_lu(4000, wmax=50, seed=5)
+        rp, col, w = g.row_ptr, g.col, g.w
+    n = rp.shape[0] - 1
+    assert 32768 < int(rp[-1]) + 8 * n <= (1 << 17)
+    x0 = np.random.default_rng(n).random(n)
+    args = (dev_u32(rp), dev_u32(col), None if w is None else dev_u32(w), torch.from_numpy(x0).cuda(), None,
+            1e-10, 3000, mixed)
+    u_c, it_c, lam_c, res_c = partitioner.power_iter(*args)
+    u_o, it_o, lam_o = O.power_iter(rp, col, w, x0, 1e-10, 3000)
+    assert abs(it_c - it_o) <= max(2, it_o // 50)
+    assert abs(lam_c - lam_o) <= 1e-6 * abs(lam_o)
+    if it_c == it_o:
+        assert 1 - abs(float(np.dot(u_c.cpu().numpy(), u_o))) <= 1e-8
+    u = u_c.cpu().numpy()
+    assert abs(np.linalg.norm(u) - 1) < 1e-9 and abs(u.sum()) < 1e-8 * np.sqrt(n)
+    monkeypatch.setenv("SGPB_PI_MID", "0")
+    u_p, it_p, lam_p, _ = partitioner.power_iter(*args)
+    # the two kernels add the FP32 partial sums of the mixed path in
+    # different orders (isolated vertices make lambda ~1e-5: an absolute floor)
+    assert abs(it_p - it_c) <= 2 and abs(lam_p - lam_c) <= (1e-8 if mixed else 1e-9) * abs(lam_c) + 1e-13
