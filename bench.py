@@ -14,6 +14,8 @@ duplicates merged, self loops dropped, largest connected component kept).
          normalisation, dot product and stopping test), its cut and its
          Fiedler value against the FP64 run
   fm     the same partition followed by up to 16 FM passes (cut and time)
+  batch  the 2,048-graph batch configuration through the batched entry point
+         (FP64 and mixed; edges/s of the whole batch, phase split)
 
 Multi-GPU: the single-graph path does not shard (a row partition would need
 halo exchanges per iteration); N ranks run N independent replicas ("weak"),
@@ -127,6 +129,21 @@ def algorithmic_pi_bytes(n: int, m: int, weighted: bool, s: int) -> int:
     return 4 * (n + 1) + 4 * m + (4 * m if weighted else 0) + s * n + s * n + 4 * n
 
 
+def algorithmic_coarsen_bytes(level_n, level_m, level_rounds, wbytes: int = 4) -> int:
+    """Bytes the coarsening of a hierarchy must move (the per-level model):
+    the heavy-neighbour scan 4(n+1) + 4m + w*m (weighted levels) + 4n, the map
+    construction 3*4n per round, and the coarse build 4(n+1) + 4m + w*m + 4n
+    (vcmap) + 4(nc+1) + (4 + w)*mc; level 0 is unweighted."""
+    total = 0
+    for l in range(len(level_n) - 1):
+        n, m, nc, mc = level_n[l], level_m[l], level_n[l + 1], level_m[l + 1]
+        wm = wbytes * m if l > 0 else 0
+        total += 4 * (n + 1) + 4 * m + wm + 4 * n
+        total += 12 * n * max(1, level_rounds[l])
+        total += 4 * (n + 1) + 4 * m + wm + 4 * n + 4 * (nc + 1) + (4 + wbytes) * mc
+    return total
+
+
 def dist_setup():
     ws = int(os.environ.get("WORLD_SIZE", "1"))
     if ws <= 1:
@@ -202,6 +219,51 @@ def cpu_baseline():
     sec = time.perf_counter() - t
     return {"value": g.m_undirected / sec, "unit": "edges/s", "cores": 1, "kind": "port",
             "sample": f"R-MAT scale {REF_SAMPLE_SCALE}, 1 partition, oracle C restatement"}
+
+
+def batch_graphs_cached():
+    from ipdps_2021_graph_coarsening_b200 import graphs as G
+    cache = os.path.join("/tmp", "sgpb_batch2048.npz")
+    if os.path.exists(cache):
+        d = np.load(cache)
+        off_r, off_c = d["off_r"], d["off_c"]
+        return [G.CSR(d["rp"][off_r[i]:off_r[i + 1]], d["col"][off_c[i]:off_c[i + 1]])
+                for i in range(len(off_r) - 1)]
+    gs = G.batch_graphs(2048)
+    try:
+        off_r = np.cumsum([0] + [g.n + 1 for g in gs])
+        off_c = np.cumsum([0] + [g.m_directed for g in gs])
+        np.savez(cache, rp=np.concatenate([g.row_ptr for g in gs]), col=np.concatenate([g.col for g in gs]),
+                 off_r=off_r, off_c=off_c)
+    except OSError:
+        pass
+    return gs
+
+
+def batch_leg(p, single_value):
+    """The batch configuration (2,048 graphs of 10^3..2.5*10^5 vertices,
+    grids with holes and Erdos-Renyi graphs, log-uniform sizes): one batched
+    call, host graphs in and host partitions out, FP64 and mixed precision,
+    after one warm-up call on 64 of the graphs; wall clock around the call
+    (it synchronises), phases from sgp_b200_last_timing."""
+    gs = batch_graphs_cached()
+    m_und = sum(g.m_undirected for g in gs)
+    p.partition_batch(gs[:64], workers=16)
+    out = {"workload": "batch2048 (log-uniform 1e3..2.5e5 vertices; grids with 10% holes and ER mean degree 8; "
+                       "LCC; unit weights)", "graphs": len(gs), "n": int(sum(g.n for g in gs)),
+           "m_undirected": int(m_und), "workers": 16}
+    for name, mixed in (("fp64", False), ("mixed", True)):
+        t = time.perf_counter()
+        rs = p.partition_batch(gs, workers=16, mixed=mixed)
+        sec = time.perf_counter() - t
+        ph = p.last_timing()
+        out[name] = {"value": m_und / sec, "unit": "edges/s", "s": sec,
+                     "phases_ms": {"coarsen": ph["coarsen"], "small_and_mid_levels": ph["eigen"],
+                                   "large_levels_and_split": ph["split"]},
+                     "edgecut_sum": int(sum(r.edgecut for r in rs))}
+    out["mixed_speedup_vs_fp64"] = out["fp64"]["s"] / out["mixed"]["s"]
+    out["fp64_vs_single_rmat22"] = out["fp64"]["value"] / single_value
+    return out
 
 
 def gpu_arm(args, rank: int, ws: int, local: int, distmod):
@@ -297,6 +359,11 @@ def gpu_arm(args, rank: int, ws: int, local: int, distmod):
           "cut_reduction": 1 - rf.edgecut / max(1, r.edgecut), "passes": rf.fm_passes, "moves": rf.fm_moves,
           "part0_size": rf.part0_size}
 
+    # the batch configuration: 2,048 graphs through the batched entry point
+    batch = None
+    if ws == 1 and not args.no_batch:
+        batch = batch_leg(p, value)
+
     # roofline of the dominant kernel (power iteration) from this step's levels
     peak, peak_kind = load_peaks()
     byts = sum(it * algorithmic_pi_bytes(nl, ml, l > 0, 8)
@@ -314,6 +381,13 @@ def gpu_arm(args, rank: int, ws: int, local: int, distmod):
             traffic = ratio * byts if ratio else None
         except (OSError, ValueError):
             traffic = None
+    cbytes = algorithmic_coarsen_bytes(r.level_n, r.level_m, r.level_hec_rounds)
+    roofline_coarsen = {"bound": "hbm", "algorithmic_bytes_per_step": cbytes, "ms_per_step": r.ms_coarsen,
+                        "achieved": cbytes / (r.ms_coarsen / 1e3) / 1e9 if r.ms_coarsen else 0.0,
+                        "peak": peak, "unit": "GB/s", "peak_kind": peak_kind,
+                        "map_ms": r.ms_map, "build_ms": r.ms_build,
+                        "kernels": "HEC scan + map rounds + coarse builds of every level"}
+    roofline_coarsen["frac"] = roofline_coarsen["achieved"] / peak
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                 "traffic": traffic, "kernel": "k_power_iter (+ k_power_iter_chains on the small levels)",
                 "peak_kind": peak_kind,
@@ -330,8 +404,9 @@ def gpu_arm(args, rank: int, ws: int, local: int, distmod):
             "level_m": r.level_m,
             "level_iters": r.level_iters, "level_pi_ms": [round(x, 3) for x in r.level_pi_ms],
             "phase_ms": {"coarsen": r.ms_coarsen, "eigen": r.ms_eigen, "split": r.ms_split},
-            "clocks": clocks, "e2e": e2e, "mixed": mixed, "fm": fm, "gpu_launches": r.kernel_launches * args.steps,
-            "roofline": roofline}
+            "clocks": clocks, "e2e": e2e, "mixed": mixed, "fm": fm, "batch": batch,
+            "gpu_launches": r.kernel_launches * args.steps, "roofline": roofline,
+            "roofline_coarsen": roofline_coarsen}
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline()
     if rank == 0:
@@ -519,6 +594,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-batch", action="store_true", help="skip the 2,048-graph batch leg")
     ap.add_argument("--no-full-size", action="store_true",
                     help="with --impl reference: skip the one full-size reference partition")
     ap.add_argument("--scale", type=int, default=SCALE, help="R-MAT scale (the benchmark is 22)")
