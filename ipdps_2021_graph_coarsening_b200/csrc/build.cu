@@ -11,8 +11,10 @@
 //   tier 1 (<= 32 entries)   one warp, bitonic sort in registers
 //   tier 2 (<= kT1 entries)  a 64-thread block, bitonic sort in shared memory
 //   tier 2 (<= kT2 entries)  a kT2Threads block, bitonic sort in shared memory
-//   tier 3 (larger)          dense accumulation over [0, nc) in global memory
-//                            (bitmap + weight array, L2-resident), compacted in
+//   tier 3 (larger)          dense accumulation over [0, nc): in one block's
+//                            shared memory when nc weights and their bitmap fit
+//                            (a block per row at a time), else in global memory
+//                            (bitmap + weight array, L2-resident); compacted in
 //                            ascending destination order
 #include "common.cuh"
 #include "internal.h"
@@ -116,18 +118,21 @@ __global__ void __launch_bounds__(256) k_build_scatter(uint32_t n, const uint32_
 constexpr uint32_t kT1 = 256;
 constexpr int kT1Threads = 64;
 
+// buckets above this many entries are split over many blocks (tier 4)
+constexpr uint32_t kGiant = 1u << 18;
+
 __global__ void k_classify(uint32_t nc, const uint32_t *__restrict__ boff, uint32_t *__restrict__ dcnt,
-                           uint32_t *__restrict__ lists /* 4 x nc */, uint32_t *__restrict__ tcount /* 4 */) {
+                           uint32_t *__restrict__ lists /* 5 x nc */, uint32_t *__restrict__ tcount /* 5 */) {
     const uint32_t c = blockIdx.x * blockDim.x + threadIdx.x;
     const unsigned lane = threadIdx.x & 31;
     int t = -1;
     if (c < nc) {
         const uint32_t sz = boff[c + 1] - boff[c];
         if (sz == 0) dcnt[c] = 0;
-        else t = sz <= 32 ? 0 : sz <= kT1 ? 1 : sz <= (uint32_t)kT2 ? 2 : 3;
+        else t = sz <= 32 ? 0 : sz <= kT1 ? 1 : sz <= (uint32_t)kT2 ? 2 : sz <= kGiant ? 3 : 4;
     }
 #pragma unroll
-    for (int q = 0; q < 4; q++) {
+    for (int q = 0; q < 5; q++) {
         const unsigned m = __ballot_sync(0xFFFFFFFFu, t == q);
         if (!m) continue;   // warp-uniform
         const int leader = __ffs(m) - 1;
@@ -377,6 +382,103 @@ __global__ void __launch_bounds__(256) k_dense_add(const uint32_t *__restrict__ 
     }
 }
 
+// Tier 3 in shared memory: a block per row at a time accumulates the row's
+// weights over [0, nc) with shared-memory atomics (integer sums, so the order
+// does not matter), then writes the destinations with a non-zero sum (every
+// weight is positive) in ascending order with their sums to the bucket's
+// head.  When nc is small the block keeps R copies of the accumulator (thread
+// t adds to copy t mod R, up to one per thread) so that rows of millions of
+// entries over a few dozen destinations do not serialise on the same words;
+// with one copy a bitmap of the touched destinations keeps the compaction
+// from scanning all nc sums.
+constexpr int kDenseSmemThreads = 1024;
+
+template <typename WO>
+static size_t dense_smem_bytes(uint32_t nc, uint32_t R) {
+    const size_t acc = (((size_t)R * nc * sizeof(WO)) + 15) & ~(size_t)15;
+    return acc + (R == 1 ? (((size_t)nc + 31) / 32) * 4 : 0);
+}
+
+template <typename WI, typename WO>
+__global__ void __launch_bounds__(kDenseSmemThreads, 1)
+    k_dense_smem(const uint32_t *__restrict__ list, const uint32_t *__restrict__ nrows_ptr,
+                 const uint32_t *__restrict__ boff, uint32_t *__restrict__ bdst, const WI *__restrict__ bw,
+                 WO *__restrict__ tw, uint32_t *__restrict__ dcnt, uint32_t nc, uint32_t R) {
+    extern __shared__ __align__(16) unsigned char dyn[];
+    WO *acc = reinterpret_cast<WO *>(dyn);
+    uint32_t *bits = reinterpret_cast<uint32_t *>(dyn + ((((size_t)R * nc * sizeof(WO)) + 15) & ~(size_t)15));
+    __shared__ uint32_t warp_tot[kDenseSmemThreads / 32];
+    const bool use_bits = R == 1;
+    const uint32_t words = (nc + 31) / 32;
+    const uint32_t nrows = *nrows_ptr;
+    const unsigned lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    WO *mine = acc + (size_t)(threadIdx.x % R) * nc;
+    // compaction units: bitmap words, or accumulator entries; contiguous per
+    // thread so that the output order is the thread order
+    const uint32_t units = use_bits ? words : nc;
+    const uint32_t upt = (units + kDenseSmemThreads - 1) / kDenseSmemThreads;
+    for (uint32_t r = blockIdx.x; r < nrows; r += gridDim.x) {
+        const uint32_t c = list[r];
+        const uint32_t b = boff[c], e = boff[c + 1];
+        for (uint32_t i = threadIdx.x; i < R * nc; i += blockDim.x) acc[i] = (WO)0;
+        if (use_bits)
+            for (uint32_t i = threadIdx.x; i < words; i += blockDim.x) bits[i] = 0u;
+        __syncthreads();
+        for (uint32_t j = b + threadIdx.x; j < e; j += blockDim.x) {
+            const uint32_t v = bdst[j];
+            atomicAdd(&mine[v], bw ? (WO)bw[j] : (WO)1);
+            if (use_bits) atomicOr(&bits[v >> 5], 1u << (v & 31));
+        }
+        __syncthreads();
+        if (R > 1) {   // the copies' sums into copy 0
+            for (uint32_t i = threadIdx.x; i < nc; i += blockDim.x) {
+                WO t = acc[i];
+                for (uint32_t q = 1; q < R; q++) t += acc[(size_t)q * nc + i];
+                acc[i] = t;
+            }
+            __syncthreads();
+        }
+        const uint32_t u0 = threadIdx.x * upt;
+        uint32_t cnt = 0;
+        for (uint32_t k = 0; k < upt && u0 + k < units; k++)
+            cnt += use_bits ? __popc(bits[u0 + k]) : (acc[u0 + k] != (WO)0);
+        // exclusive prefix of cnt over the block
+        uint32_t incl = cnt;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t y = __shfl_up_sync(0xFFFFFFFFu, incl, o);
+            if (lane >= (unsigned)o) incl += y;
+        }
+        if (lane == 31) warp_tot[wid] = incl;
+        __syncthreads();
+        uint32_t base = 0, total = 0;
+        for (uint32_t k = 0; k < kDenseSmemThreads / 32; k++) {
+            if (k < wid) base += warp_tot[k];
+            total += warp_tot[k];
+        }
+        uint32_t pos = b + base + incl - cnt;
+        for (uint32_t k = 0; k < upt && u0 + k < units; k++) {
+            if (use_bits) {
+                uint32_t word = bits[u0 + k];
+                while (word) {
+                    const int bit = __ffs(word) - 1;
+                    word &= word - 1;
+                    const uint32_t v = (u0 + k) * 32 + bit;
+                    bdst[pos] = v;
+                    tw[pos] = acc[v];
+                    pos++;
+                }
+            } else if (acc[u0 + k] != (WO)0) {
+                bdst[pos] = u0 + k;
+                tw[pos] = acc[u0 + k];
+                pos++;
+            }
+        }
+        if (threadIdx.x == 0) dcnt[c] = total;
+        __syncthreads();   // the next row clears acc, bits and warp_tot
+    }
+}
+
 // Compaction of the dense slots in ascending destination order, clearing
 // them for reuse.  A slot's bitmap is cut into chunks of kChunkWords words,
 // one block per (chunk, slot): k_dense_count counts the bits of each chunk,
@@ -508,9 +610,9 @@ template <typename WI, typename WO>
 static int dedupe_buckets(Context &C, uint32_t nc, const uint32_t *boff, uint32_t *bdst, const WI *bw, WO *tw,
                           uint32_t *dcnt) {
     uint32_t *lists, *tcount;
-    SGPB_TRY(dalloc_t(C, &lists, (size_t)4 * nc + 4));
-    SGPB_TRY(dalloc_t(C, &tcount, 4));
-    SGPB_TRY(dzero(C, tcount, sizeof(uint32_t) * 4));
+    SGPB_TRY(dalloc_t(C, &lists, (size_t)5 * nc + 4));
+    SGPB_TRY(dalloc_t(C, &tcount, 5));
+    SGPB_TRY(dzero(C, tcount, sizeof(uint32_t) * 5));
     if (nc) {
         k_classify<<<cdiv(nc, 256), 256, 0, C.stream>>>(nc, boff, dcnt, lists, tcount);
         uint32_t g1 = cdiv(nc, 8);
@@ -540,14 +642,17 @@ static int dedupe_buckets(Context &C, uint32_t nc, const uint32_t *boff, uint32_
         }
         C.kernel_launches += 4;
         SGPB_CUDA(cudaGetLastError());
-        uint32_t n3 = 0;
-        SGPB_TRY(read_u32(C, tcount + 3, &n3));
-        if (n3) {
+        uint32_t n34[2] = {0, 0};
+        SGPB_TRY(read_u32(C, tcount + 3, n34, 2));
+        const uint32_t n3 = n34[0], n4 = n34[1];
+        // dense accumulation in global memory (L2-resident slots) of the rows
+        // of `list`, `per_row` blocks per row
+        auto dense_global = [&](const uint32_t *list, uint32_t nrows, uint32_t per_row) -> int {
             const size_t words = ((size_t)nc + 31) / 32;
             const size_t slot_bytes = (size_t)nc * sizeof(WO) + words * 4;
             size_t slots = ((size_t)1 << 30) / (slot_bytes ? slot_bytes : 1);
             if (slots < 1) slots = 1;
-            if (slots > n3) slots = n3;
+            if (slots > nrows) slots = nrows;
             if (slots > 65535) slots = 65535;
             WO *acc;
             uint32_t *bits, *chunk_cnt;
@@ -557,17 +662,39 @@ static int dedupe_buckets(Context &C, uint32_t nc, const uint32_t *boff, uint32_
             SGPB_TRY(dalloc_t(C, &chunk_cnt, slots * nchunks));
             SGPB_TRY(dzero(C, acc, slots * nc * sizeof(WO)));
             SGPB_TRY(dzero(C, bits, slots * words * 4));
-            for (uint32_t r0 = 0; r0 < n3; r0 += (uint32_t)slots) {
-                uint32_t nr = n3 - r0 < slots ? n3 - r0 : (uint32_t)slots;
-                dim3 ga(8, nr), gc(nchunks, nr);
-                k_dense_add<WI, WO><<<ga, 256, 0, C.stream>>>(lists + 3 * (size_t)nc, r0, boff, bdst, bw, nc, acc, bits);
+            for (uint32_t r0 = 0; r0 < nrows; r0 += (uint32_t)slots) {
+                uint32_t nr = nrows - r0 < slots ? nrows - r0 : (uint32_t)slots;
+                dim3 ga(per_row, nr), gc(nchunks, nr);
+                k_dense_add<WI, WO><<<ga, 256, 0, C.stream>>>(list, r0, boff, bdst, bw, nc, acc, bits);
                 k_dense_count<<<gc, 256, 0, C.stream>>>(nc, bits, chunk_cnt);
-                k_dense_collect<WO><<<gc, 256, 0, C.stream>>>(lists + 3 * (size_t)nc, r0, boff, nc, acc, bits,
-                                                             chunk_cnt, bdst, tw, dcnt);
+                k_dense_collect<WO><<<gc, 256, 0, C.stream>>>(list, r0, boff, nc, acc, bits, chunk_cnt, bdst, tw, dcnt);
                 C.kernel_launches += 3;
             }
             SGPB_CUDA(cudaGetLastError());
+            return SGP_B200_OK;
+        };
+        // tier 3: one block's shared memory per row when nc fits, else global
+        // memory; accumulator copies that fit in one block's shared memory
+        const size_t budget = C.smem_optin - 8 * 1024;
+        uint32_t R = nc ? (uint32_t)(budget / ((size_t)nc * sizeof(WO))) : 1u;
+        if (R > (uint32_t)kDenseSmemThreads) R = kDenseSmemThreads;
+        while (R > 1 && dense_smem_bytes<WO>(nc, R) > budget) R--;
+        const size_t dsm = R ? dense_smem_bytes<WO>(nc, R) : 0;
+        if (n3 && R >= 1 && dsm <= budget) {
+            SGPB_CUDA(cudaFuncSetAttribute(k_dense_smem<WI, WO>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                           (int)dsm));
+            const uint32_t g3 = n3 < (uint32_t)C.num_sms ? n3 : (uint32_t)C.num_sms;
+            k_dense_smem<WI, WO><<<g3, kDenseSmemThreads, dsm, C.stream>>>(lists + 3 * (size_t)nc, tcount + 3, boff,
+                                                                          bdst, bw, tw, dcnt, nc, R);
+            C.kernel_launches++;
+            SGPB_CUDA(cudaGetLastError());
+        } else if (n3) {
+            SGPB_TRY(dense_global(lists + 3 * (size_t)nc, n3, 8));
         }
+        // tier 4: rows of more than kGiant entries (the hub aggregates of
+        // skewed graphs, millions of entries each) on 64 blocks per row, so
+        // that one row does not hold one SM for the whole build
+        if (n4) SGPB_TRY(dense_global(lists + 4 * (size_t)nc, n4, 64));
     }
     return SGP_B200_OK;
 }

@@ -121,10 +121,13 @@ def test_build_bit_exact(partitioner, graph, out_wbytes):
     assert np.array_equal(gw.astype(np.uint64), w2)
 
 
-@pytest.mark.parametrize("n_leaves,ring", [(12000, 4000), (90000, 30000)])
-def test_build_large_rows_dense_tier(partitioner, n_leaves, ring):
-    """Buckets above 4096 entries (the dense tier), with 6001 and 60001
-    coarse vertices."""
+@pytest.mark.parametrize("n_leaves,ring", [(12000, 4000), (67500, 22500), (90000, 30000)])
+@pytest.mark.parametrize("out_wbytes", [4, 8])
+def test_build_large_rows_dense_tier(partitioner, n_leaves, ring, out_wbytes):
+    """Buckets above 4096 entries (the dense tier), with 8002 coarse vertices
+    (several accumulator copies in one block's shared memory), 45002 (one
+    copy and a bitmap with 32-bit weights; global memory with 64-bit ones)
+    and 60002 (global memory), 32- and 64-bit coarse weights."""
     g = star_plus_ring(n_leaves, ring)
     # map everything in the first half to one aggregate: one huge bucket
     n = g.n
@@ -132,11 +135,34 @@ def test_build_large_rows_dense_tier(partitioner, n_leaves, ring):
     vc[n // 2:] = np.arange(1, n - n // 2 + 1, dtype=np.uint32)
     nc = int(vc.max()) + 1
     rp_o, col_o, w_o = O.build_coarse(g.row_ptr, g.col, None, vc, nc)
-    crp, ccol, cw = partitioner.build_coarse(dev_u32(g.row_ptr), dev_u32(g.col), None, dev_u32(vc), nc, 4)
+    crp, ccol, cw = partitioner.build_coarse(dev_u32(g.row_ptr), dev_u32(g.col), None, dev_u32(vc), nc, out_wbytes)
     assert int(np.diff(rp_o).max()) > 4096
     assert np.array_equal(host_u32(crp), rp_o)
     assert np.array_equal(host_u32(ccol), col_o)
-    assert np.array_equal(host_u32(cw).astype(np.uint64), w_o)
+    cwh = host_u32(cw).astype(np.uint64) if out_wbytes == 4 else host_u64(cw)
+    assert np.array_equal(cwh, w_o)
+
+
+@pytest.mark.parametrize("nc_tail", [20000, 70000])
+@pytest.mark.parametrize("out_wbytes", [4, 8])
+def test_build_giant_rows(partitioner, nc_tail, out_wbytes):
+    """A bucket of more than 2^18 entries (split over many blocks) beside
+    rows of the other tiers; the remaining vertices folded onto nc_tail
+    coarse vertices (the shared-memory or the global dense tier)."""
+    g = star_plus_ring(220000, 60000)
+    n = g.n
+    vc = np.zeros(n, np.uint32)
+    vc[n // 2:] = 1 + (np.arange(n - n // 2, dtype=np.uint32) % nc_tail)
+    nc = int(vc.max()) + 1
+    rp_o, col_o, w_o = O.build_coarse(g.row_ptr, g.col, None, vc, nc)
+    assert int(np.diff(rp_o).max()) > 0
+    sizes = np.bincount(vc, weights=np.diff(g.row_ptr).astype(np.int64), minlength=nc)
+    assert sizes.max() > (1 << 18)
+    crp, ccol, cw = partitioner.build_coarse(dev_u32(g.row_ptr), dev_u32(g.col), None, dev_u32(vc), nc, out_wbytes)
+    assert np.array_equal(host_u32(crp), rp_o)
+    assert np.array_equal(host_u32(ccol), col_o)
+    cwh = host_u32(cw).astype(np.uint64) if out_wbytes == 4 else host_u64(cw)
+    assert np.array_equal(cwh, w_o)
 
 
 # ---------------------------------------------------------------- split --
