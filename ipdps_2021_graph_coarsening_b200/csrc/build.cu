@@ -24,15 +24,42 @@ namespace sgpb {
 constexpr int kT2 = 4096;
 constexpr uint32_t kSentinel = 0xFFFFFFFFu;
 
+// Rows longer than kLongRowT entries (the hubs of skewed graphs, up to
+// hundreds of thousands of entries) would hold one group for the whole of a
+// rows-strided kernel: the count and key kernels list them and leave them to
+// a kernel that gives each such row a block.
+constexpr uint32_t kLongRowT = 8192;
+constexpr int kLongThreads = 1024;
+
+__device__ __forceinline__ void list_long_row(uint32_t *long_list, uint32_t *long_cnt, uint32_t u) {
+    long_list[atomicAdd(long_cnt, 1u)] = u;
+}
+
+// block-wide sum for the long-row kernels (result on thread 0)
+template <typename T>
+__device__ __forceinline__ T block_sum_long(T v, T *sm /* kLongThreads / 32 */) {
+    v = warp_sum(v);
+    if ((threadIdx.x & 31) == 0) sm[threadIdx.x >> 5] = v;
+    __syncthreads();
+    T t = 0;
+    if (threadIdx.x == 0)
+        for (int k = 0; k < (int)(blockDim.x >> 5); k++) t += sm[k];
+    __syncthreads();
+    return t;
+}
+
 // ---------------------------------------------------------------- count --
 // Per fine row u: krow[u] = entries whose coarse destination differs from
 // vcmap[u]; cnt[vcmap[u]] += krow[u].  A group of G lanes per row, 4 entries
-// per lane in flight (destinations, then the vcmap gathers).
+// per lane in flight (destinations, then the vcmap gathers); rows longer than
+// kLongRowT are listed for k_build_count_long.
 template <int G>
 __global__ void __launch_bounds__(256) k_build_count(uint32_t n, const uint32_t *__restrict__ rp,
                                                      const uint32_t *__restrict__ col,
                                                      const uint32_t *__restrict__ vcmap,
-                                                     uint32_t *__restrict__ cnt, uint32_t *__restrict__ krow) {
+                                                     uint32_t *__restrict__ cnt, uint32_t *__restrict__ krow,
+                                                     uint32_t *__restrict__ long_list,
+                                                     uint32_t *__restrict__ long_cnt) {
     const unsigned gm = group_mask<G>();
     const uint32_t lane = threadIdx.x & (G - 1);
     const uint64_t gid = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) / G;
@@ -40,6 +67,10 @@ __global__ void __launch_bounds__(256) k_build_count(uint32_t n, const uint32_t 
     for (uint64_t u = gid; u < n; u += ngroups) {
         const uint32_t cu = vcmap[u];
         const uint32_t b = rp[u], e = rp[u + 1];
+        if (e - b > kLongRowT) {   // group-uniform
+            if (lane == 0) list_long_row(long_list, long_cnt, (uint32_t)u);
+            continue;
+        }
         uint32_t c = 0;
         for (uint32_t j0 = b + lane; j0 < e; j0 += 4 * G) {
             uint32_t d[4];
@@ -52,6 +83,37 @@ __global__ void __launch_bounds__(256) k_build_count(uint32_t n, const uint32_t 
 #pragma unroll
         for (int o = G / 2; o > 0; o >>= 1) c += __shfl_xor_sync(gm, c, o);
         if (lane == 0) {
+            krow[u] = c;
+            if (c) atomicAdd(cnt + cu, c);
+        }
+    }
+}
+
+// the long rows of k_build_count, a block per row
+__global__ void __launch_bounds__(kLongThreads) k_build_count_long(const uint32_t *__restrict__ rp,
+                                                                 const uint32_t *__restrict__ col,
+                                                                 const uint32_t *__restrict__ vcmap,
+                                                                 uint32_t *__restrict__ cnt,
+                                                                 uint32_t *__restrict__ krow,
+                                                                 const uint32_t *__restrict__ long_list,
+                                                                 const uint32_t *__restrict__ long_cnt) {
+    __shared__ uint32_t sm[kLongThreads / 32];
+    const uint32_t nl = *long_cnt;
+    for (uint32_t r = blockIdx.x; r < nl; r += gridDim.x) {
+        const uint32_t u = long_list[r];
+        const uint32_t cu = vcmap[u];
+        const uint32_t b = rp[u], e = rp[u + 1];
+        uint32_t c = 0;
+        for (uint32_t j0 = b + threadIdx.x; j0 < e; j0 += 4 * blockDim.x) {
+            uint32_t d[4];
+#pragma unroll
+            for (int q = 0; q < 4; q++) d[q] = j0 + q * blockDim.x < e ? __ldg(col + j0 + q * blockDim.x) : 0u;
+#pragma unroll
+            for (int q = 0; q < 4; q++)
+                if (j0 + q * blockDim.x < e) c += (__ldg(vcmap + d[q]) != cu);
+        }
+        c = block_sum_long(c, sm);
+        if (threadIdx.x == 0) {
             krow[u] = c;
             if (c) atomicAdd(cnt + cu, c);
         }
@@ -82,6 +144,7 @@ __global__ void __launch_bounds__(256) k_build_scatter(uint32_t n, const uint32_
         if (k == 0) continue;   // group-uniform
         const uint32_t cu = vcmap[u];
         const uint32_t b = rp[u], e = rp[u + 1];
+        if (e - b > kLongRowT) continue;   // k_build_scatter_long
         uint32_t base = 0;
         if (lane == 0) base = boff[cu] + atomicAdd(fill + cu, k);
         base = __shfl_sync(gm, base, 0, G);
@@ -108,6 +171,50 @@ __global__ void __launch_bounds__(256) k_build_scatter(uint32_t n, const uint32_
                 base += __popc(bal);
             }
         }
+    }
+}
+
+// The long rows: a block per row reserves the row's slots with one atomic
+// and places its kept entries there in warp order (any order: the dedupe
+// sorts each bucket, and integer weights sum the same either way).
+template <typename WI>
+__global__ void __launch_bounds__(kLongThreads) k_build_scatter_long(
+    const uint32_t *__restrict__ rp, const uint32_t *__restrict__ col, const WI *__restrict__ w,
+    const uint32_t *__restrict__ vcmap, const uint32_t *__restrict__ krow, const uint32_t *__restrict__ boff,
+    uint32_t *__restrict__ fill, uint32_t *__restrict__ bdst, WI *__restrict__ bw,
+    const uint32_t *__restrict__ long_list, const uint32_t *__restrict__ long_cnt) {
+    __shared__ uint32_t s_base, s_pos;
+    const uint32_t nl = *long_cnt;
+    const unsigned lane = threadIdx.x & 31;
+    for (uint32_t r = blockIdx.x; r < nl; r += gridDim.x) {
+        const uint32_t u = long_list[r];
+        const uint32_t k = krow[u];
+        if (k == 0) continue;   // block-uniform
+        const uint32_t cu = vcmap[u];
+        const uint32_t b = rp[u], e = rp[u + 1];
+        if (threadIdx.x == 0) {
+            s_base = boff[cu] + atomicAdd(fill + cu, k);
+            s_pos = 0;
+        }
+        __syncthreads();
+        const uint32_t base = s_base;
+        // whole warps per step (the loop bound is warp-uniform)
+        for (uint32_t j0 = b + (threadIdx.x & ~31u); j0 < e; j0 += blockDim.x) {
+            const uint32_t j = j0 + lane;
+            const uint32_t cv = j < e ? __ldg(vcmap + __ldg(col + j)) : cu;
+            const WI wv = (w && j < e) ? __ldg(w + j) : (WI)0;
+            const bool keep = cv != cu;
+            const unsigned bal = __ballot_sync(0xFFFFFFFFu, keep);
+            uint32_t p0 = 0;
+            if (lane == 0 && bal) p0 = atomicAdd(&s_pos, (uint32_t)__popc(bal));
+            p0 = __shfl_sync(0xFFFFFFFFu, p0, 0);
+            if (keep) {
+                const uint32_t p = base + p0 + __popc(bal & ((1u << lane) - 1u));
+                bdst[p] = cv;
+                if (w) bw[p] = wv;
+            }
+        }
+        __syncthreads();   // s_base / s_pos are rewritten for the next row
     }
 }
 
@@ -727,10 +834,19 @@ static int build_impl(Context &C, const Level &F, const WI *w, const uint32_t *v
     else if (avg <= 16) SGPB_ROWS_LAUNCH(KERNEL_T(16), 16, __VA_ARGS__)                    \
     else SGPB_ROWS_LAUNCH(KERNEL_T(32), 32, __VA_ARGS__)
 
-    uint32_t *krow;
+    uint32_t *krow, *long_list, *long_cnt;
     SGPB_TRY(dalloc_t(C, &krow, (size_t)n + 1));
+    SGPB_TRY(dalloc_t(C, &long_list, F.m / kLongRowT + 1));
+    SGPB_TRY(dalloc_t(C, &long_cnt, 1));
+    SGPB_TRY(dzero(C, long_cnt, sizeof(uint32_t)));
+    uint32_t glong = (uint32_t)(F.m / kLongRowT + 1);
+    if (glong > (uint32_t)C.num_sms * 2) glong = C.num_sms * 2;
 #define K_COUNT(G) k_build_count<G>
-    SGPB_BY_G(K_COUNT, n, F.rp, F.col, vcmap, cnt, krow)
+    SGPB_BY_G(K_COUNT, n, F.rp, F.col, vcmap, cnt, krow, long_list, long_cnt)
+    if (F.m > kLongRowT) {
+        k_build_count_long<<<glong, kLongThreads, 0, C.stream>>>(F.rp, F.col, vcmap, cnt, krow, long_list, long_cnt);
+        C.kernel_launches++;
+    }
     SGPB_TRY(scan_u32(C, cnt, boff, nc, nullptr));
     uint32_t kept = 0;
     SGPB_TRY(read_u32(C, boff + nc, &kept));
@@ -742,6 +858,11 @@ static int build_impl(Context &C, const Level &F, const WI *w, const uint32_t *v
     SGPB_TRY(dalloc_t(C, &tw, (size_t)kept + 1));
 #define K_SCATTER(G) k_build_scatter<G, WI>
     SGPB_BY_G(K_SCATTER, n, F.rp, F.col, w, vcmap, krow, boff, fill, bdst, bw)
+    if (F.m > kLongRowT) {
+        k_build_scatter_long<WI><<<glong, kLongThreads, 0, C.stream>>>(F.rp, F.col, w, vcmap, krow, boff, fill, bdst,
+                                                                      bw, long_list, long_cnt);
+        C.kernel_launches++;
+    }
 #undef K_COUNT
 #undef K_SCATTER
 #undef SGPB_BY_G
@@ -780,7 +901,8 @@ __global__ void __launch_bounds__(256) k_sb_keys(uint32_t n, const uint32_t *__r
                                                  const uint32_t *__restrict__ col,
                                                  const uint32_t *__restrict__ vcmap, int b,
                                                  unsigned long long *__restrict__ keys,
-                                                 unsigned long long *__restrict__ kept) {
+                                                 unsigned long long *__restrict__ kept,
+                                                 uint32_t *__restrict__ long_list, uint32_t *__restrict__ long_cnt) {
     __shared__ unsigned long long wsum[8];
     const uint32_t lane = threadIdx.x & (G - 1);
     const uint64_t gid = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) / G;
@@ -789,6 +911,10 @@ __global__ void __launch_bounds__(256) k_sb_keys(uint32_t n, const uint32_t *__r
     for (uint64_t u = gid; u < n; u += ngroups) {
         const unsigned long long cu = vcmap[u];
         const uint32_t e = rp[u + 1];
+        if (e - rp[u] > kLongRowT) {   // group-uniform: k_sb_keys_long
+            if (lane == 0) list_long_row(long_list, long_cnt, (uint32_t)u);
+            continue;
+        }
         // four entries per lane in flight: destinations, then their vcmap gathers
         for (uint32_t j0 = rp[u] + lane; j0 < e; j0 += 4 * G) {
             uint32_t d[4];
@@ -814,6 +940,41 @@ __global__ void __launch_bounds__(256) k_sb_keys(uint32_t n, const uint32_t *__r
         unsigned long long t = 0;
         for (int k = 0; k < (int)(blockDim.x >> 5); k++) t += wsum[k];
         if (t) atomicAdd(kept, t);
+    }
+}
+
+// the long rows of k_sb_keys, a block per row
+__global__ void __launch_bounds__(kLongThreads) k_sb_keys_long(const uint32_t *__restrict__ rp,
+                                                             const uint32_t *__restrict__ col,
+                                                             const uint32_t *__restrict__ vcmap, int b,
+                                                             unsigned long long *__restrict__ keys,
+                                                             unsigned long long *__restrict__ kept,
+                                                             const uint32_t *__restrict__ long_list,
+                                                             const uint32_t *__restrict__ long_cnt) {
+    __shared__ unsigned long long sm[kLongThreads / 32];
+    const uint32_t nl = *long_cnt;
+    for (uint32_t r = blockIdx.x; r < nl; r += gridDim.x) {
+        const uint32_t u = long_list[r];
+        const unsigned long long cu = vcmap[u];
+        const uint32_t e = rp[u + 1];
+        unsigned long long c = 0;
+        for (uint32_t j0 = rp[u] + threadIdx.x; j0 < e; j0 += 4 * blockDim.x) {
+            uint32_t d[4], cv[4];
+#pragma unroll
+            for (int q = 0; q < 4; q++) d[q] = j0 + q * blockDim.x < e ? __ldg(col + j0 + q * blockDim.x) : 0u;
+#pragma unroll
+            for (int q = 0; q < 4; q++) cv[q] = j0 + q * blockDim.x < e ? __ldg(vcmap + d[q]) : 0u;
+#pragma unroll
+            for (int q = 0; q < 4; q++) {
+                if (j0 + q * blockDim.x < e) {
+                    const bool keep = cv[q] != cu;
+                    keys[j0 + q * blockDim.x] = keep ? (cu << b | cv[q]) : kNoKey;
+                    c += keep;
+                }
+            }
+        }
+        c = block_sum_long(c, sm);
+        if (threadIdx.x == 0 && c) atomicAdd(kept, c);
     }
 }
 
@@ -898,10 +1059,23 @@ static int build_sorted_unit(Context &C, const Level &F, const uint32_t *vcmap, 
         uint32_t g = cdiv((uint64_t)n * G, 256);
         return g > cap ? cap : (g ? g : 1u);
     };
-    if (avg <= 4) k_sb_keys<4><<<rows_grid(4), 256, 0, C.stream>>>(n, F.rp, F.col, vcmap, b, keys, kept);
-    else if (avg <= 16) k_sb_keys<16><<<rows_grid(16), 256, 0, C.stream>>>(n, F.rp, F.col, vcmap, b, keys, kept);
-    else k_sb_keys<32><<<rows_grid(32), 256, 0, C.stream>>>(n, F.rp, F.col, vcmap, b, keys, kept);
+    uint32_t *long_list, *long_cnt;
+    SGPB_TRY(dalloc_t(C, &long_list, F.m / kLongRowT + 1));
+    SGPB_TRY(dalloc_t(C, &long_cnt, 1));
+    SGPB_TRY(dzero(C, long_cnt, sizeof(uint32_t)));
+    if (avg <= 4)
+        k_sb_keys<4><<<rows_grid(4), 256, 0, C.stream>>>(n, F.rp, F.col, vcmap, b, keys, kept, long_list, long_cnt);
+    else if (avg <= 16)
+        k_sb_keys<16><<<rows_grid(16), 256, 0, C.stream>>>(n, F.rp, F.col, vcmap, b, keys, kept, long_list, long_cnt);
+    else
+        k_sb_keys<32><<<rows_grid(32), 256, 0, C.stream>>>(n, F.rp, F.col, vcmap, b, keys, kept, long_list, long_cnt);
     C.kernel_launches++;
+    if (F.m > kLongRowT) {
+        uint32_t gl = (uint32_t)(F.m / kLongRowT + 1);
+        if (gl > (uint32_t)C.num_sms * 2) gl = C.num_sms * 2;
+        k_sb_keys_long<<<gl, kLongThreads, 0, C.stream>>>(F.rp, F.col, vcmap, b, keys, kept, long_list, long_cnt);
+        C.kernel_launches++;
+    }
     bool in_tmp = false;
     SGPB_TRY(radix_sort_keys(C, keys, m, 2 * b, tmp, &in_tmp));
     const unsigned long long *sk = in_tmp ? tmp : keys;

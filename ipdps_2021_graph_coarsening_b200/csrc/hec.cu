@@ -29,11 +29,43 @@ __global__ void k_hn_random(uint32_t n, const uint32_t *__restrict__ rp, const u
 // (weight, tiebreak hash, destination) -- a strict order, so the winner does
 // not depend on the reduction order (the reference's MaxLoc with `>=` at
 // heuristics.h:974-998 takes whichever maximum the reduction meets last).
-// G lanes per row, rows grid-strided.
+// G lanes per row, rows grid-strided.  Rows longer than long_T entries (the
+// hubs of skewed graphs, up to hundreds of thousands of entries) are left to
+// k_hn_heavy_long, a block per row, and listed in long_list: one group would
+// hold its SM for the whole kernel on such a row.
+
+// entries [j0, e) in strides of `s`, four in flight: the running maximum
+template <typename W>
+__device__ __forceinline__ void hn_scan(const uint32_t *__restrict__ col, const W *__restrict__ w, uint64_t seed,
+                                        uint32_t u, uint32_t j0, uint32_t e, uint32_t s, uint64_t &bw, uint64_t &bk,
+                                        bool &have) {
+    for (; j0 < e; j0 += 4 * s) {
+        uint32_t v[4];
+        uint64_t wt[4];
+#pragma unroll
+        for (int q = 0; q < 4; q++) {
+            const uint32_t j = j0 + q * s;
+            v[q] = j < e ? __ldg(col + j) : 0u;
+            wt[q] = j < e ? wload(w, j) : 0ull;
+        }
+#pragma unroll
+        for (int q = 0; q < 4; q++) {
+            if (j0 + q * s >= e) continue;
+            const uint64_t k = ((uint64_t)tiebreak(seed, u, v[q]) << 32) | v[q];
+            if (!have || wt[q] > bw || (wt[q] == bw && k > bk)) { bw = wt[q]; bk = k; have = true; }
+        }
+    }
+}
+
+__device__ __forceinline__ void hn_combine(uint64_t ow, uint64_t ok, int oh, uint64_t &bw, uint64_t &bk, bool &have) {
+    if (oh && (!have || ow > bw || (ow == bw && ok > bk))) { bw = ow; bk = ok; have = true; }
+}
+
 template <int G, typename W>
 __global__ void __launch_bounds__(256) k_hn_heavy(uint32_t n, const uint32_t *__restrict__ rp,
                                                   const uint32_t *__restrict__ col, const W *__restrict__ w,
-                                                  uint64_t seed, uint32_t *__restrict__ hn) {
+                                                  uint64_t seed, uint32_t *__restrict__ hn, uint32_t long_T,
+                                                  uint32_t *__restrict__ long_list, uint32_t *__restrict__ long_cnt) {
     const unsigned gm = group_mask<G>();
     const uint32_t lane = threadIdx.x & (G - 1);
     const uint64_t gid = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) / G;
@@ -41,33 +73,57 @@ __global__ void __launch_bounds__(256) k_hn_heavy(uint32_t n, const uint32_t *__
     for (uint64_t u64 = gid; u64 < n; u64 += ngroups) {
         uint32_t u = (uint32_t)u64;
         uint32_t b = rp[u], e = rp[u + 1];
+        if (e - b > long_T) {   // group-uniform
+            if (lane == 0) long_list[atomicAdd(long_cnt, 1u)] = u;
+            continue;
+        }
         uint64_t bw = 0, bk = 0;   // (weight, tiebreak<<32 | dest); 0 = none
         bool have = false;
-        for (uint32_t j0 = b + lane; j0 < e; j0 += 4 * G) {
-            // four entries per lane in flight, then the lexicographic max
-            uint32_t v[4];
-            uint64_t wt[4];
-#pragma unroll
-            for (int q = 0; q < 4; q++) {
-                const uint32_t j = j0 + q * G;
-                v[q] = j < e ? __ldg(col + j) : 0u;
-                wt[q] = j < e ? wload(w, j) : 0ull;
-            }
-#pragma unroll
-            for (int q = 0; q < 4; q++) {
-                if (j0 + q * G >= e) continue;
-                const uint64_t k = ((uint64_t)tiebreak(seed, u, v[q]) << 32) | v[q];
-                if (!have || wt[q] > bw || (wt[q] == bw && k > bk)) { bw = wt[q]; bk = k; have = true; }
-            }
-        }
+        hn_scan(col, w, seed, u, b + lane, e, G, bw, bk, have);
 #pragma unroll
         for (int o = G / 2; o > 0; o >>= 1) {
             uint64_t ow = __shfl_xor_sync(gm, bw, o);
             uint64_t ok = __shfl_xor_sync(gm, bk, o);
             int oh = __shfl_xor_sync(gm, (int)have, o);
-            if (oh && (!have || ow > bw || (ow == bw && ok > bk))) { bw = ow; bk = ok; have = true; }
+            hn_combine(ow, ok, oh, bw, bk, have);
         }
         if (lane == 0) hn[u] = (e == b) ? (uint32_t)(rand_draw(seed, u) % n) : (uint32_t)(bk & 0xFFFFFFFFu);
+    }
+}
+
+// the rows k_hn_heavy listed as long: a block per row, grid-strided over the list
+constexpr int kHnLongThreads = 1024;
+template <typename W>
+__global__ void __launch_bounds__(kHnLongThreads) k_hn_heavy_long(const uint32_t *__restrict__ rp,
+                                                                  const uint32_t *__restrict__ col,
+                                                                  const W *__restrict__ w, uint64_t seed,
+                                                                  const uint32_t *__restrict__ long_list,
+                                                                  const uint32_t *__restrict__ long_cnt,
+                                                                  uint32_t *__restrict__ hn) {
+    __shared__ uint64_t s_w[kHnLongThreads / 32], s_k[kHnLongThreads / 32];
+    __shared__ int s_h[kHnLongThreads / 32];
+    const unsigned lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    const uint32_t cnt = *long_cnt;
+    for (uint32_t r = blockIdx.x; r < cnt; r += gridDim.x) {
+        const uint32_t u = long_list[r];
+        const uint32_t b = rp[u], e = rp[u + 1];
+        uint64_t bw = 0, bk = 0;
+        bool have = false;
+        hn_scan(col, w, seed, u, b + threadIdx.x, e, blockDim.x, bw, bk, have);
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            uint64_t ow = __shfl_xor_sync(0xFFFFFFFFu, bw, o);
+            uint64_t ok = __shfl_xor_sync(0xFFFFFFFFu, bk, o);
+            int oh = __shfl_xor_sync(0xFFFFFFFFu, (int)have, o);
+            hn_combine(ow, ok, oh, bw, bk, have);
+        }
+        if (lane == 0) { s_w[wid] = bw; s_k[wid] = bk; s_h[wid] = have; }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            for (int k = 1; k < (int)(blockDim.x >> 5); k++) hn_combine(s_w[k], s_k[k], s_h[k], bw, bk, have);
+            hn[u] = (uint32_t)(bk & 0xFFFFFFFFu);   // a long row has entries
+        }
+        __syncthreads();
     }
 }
 
@@ -230,20 +286,35 @@ static int coop_grid(Context &C, const void *kernel, int threads, size_t smem, u
     return SGP_B200_OK;
 }
 
+// rows longer than this go to the block-per-row kernel
+constexpr uint32_t kHnLongT = 8192;
+
 template <typename W>
-static void launch_hn_heavy(Context &C, const Level &L, const W *w, uint64_t seed, uint32_t *hn) {
+static int launch_hn_heavy(Context &C, const Level &L, const W *w, uint64_t seed, uint32_t *hn) {
     double avg = L.n ? (double)L.m / L.n : 0;
     uint32_t blocks_cap = (uint32_t)C.num_sms * 16;
-#define SGPB_HN(G)                                                                         \
-    {                                                                                      \
-        uint32_t blocks = cdiv((uint64_t)L.n * G, 256);                                    \
-        if (blocks > blocks_cap) blocks = blocks_cap;                                      \
-        if (blocks < 1) blocks = 1;                                                        \
-        k_hn_heavy<G, W><<<blocks, 256, 0, C.stream>>>(L.n, L.rp, L.col, w, seed, hn);     \
+    uint32_t *long_list, *long_cnt;
+    SGPB_TRY(dalloc_t(C, &long_list, L.m / kHnLongT + 1));
+    SGPB_TRY(dalloc_t(C, &long_cnt, 1));
+    SGPB_TRY(dzero(C, long_cnt, sizeof(uint32_t)));
+#define SGPB_HN(G)                                                                                      \
+    {                                                                                                   \
+        uint32_t blocks = cdiv((uint64_t)L.n * G, 256);                                                 \
+        if (blocks > blocks_cap) blocks = blocks_cap;                                                   \
+        if (blocks < 1) blocks = 1;                                                                     \
+        k_hn_heavy<G, W><<<blocks, 256, 0, C.stream>>>(L.n, L.rp, L.col, w, seed, hn, kHnLongT, long_list, \
+                                                       long_cnt);                                       \
     }
     if (avg <= 4) SGPB_HN(4) else if (avg <= 8) SGPB_HN(8) else if (avg <= 16) SGPB_HN(16) else SGPB_HN(32)
 #undef SGPB_HN
+    if (L.m > kHnLongT) {
+        uint32_t gl = (uint32_t)(L.m / kHnLongT + 1);
+        if (gl > (uint32_t)C.num_sms * 2) gl = C.num_sms * 2;
+        k_hn_heavy_long<W><<<gl, kHnLongThreads, 0, C.stream>>>(L.rp, L.col, w, seed, long_list, long_cnt, hn);
+        C.kernel_launches++;
+    }
     C.kernel_launches++;
+    return SGP_B200_OK;
 }
 
 // the heavy-neighbour step alone (also used by the HEC_V3 mapping)
@@ -254,9 +325,9 @@ int hec_hn_level(Context &C, const Level &L, int random_level, uint64_t seed, ui
         k_hn_random<<<cdiv(n, 256), 256, 0, C.stream>>>(n, L.rp, L.col, seed, hn);
         C.kernel_launches++;
     } else if (L.wbytes == 8) {
-        launch_hn_heavy<unsigned long long>(C, L, (const unsigned long long *)L.w, seed, hn);
+        SGPB_TRY(launch_hn_heavy<unsigned long long>(C, L, (const unsigned long long *)L.w, seed, hn));
     } else {
-        launch_hn_heavy<uint32_t>(C, L, (const uint32_t *)L.w, seed, hn);
+        SGPB_TRY(launch_hn_heavy<uint32_t>(C, L, (const uint32_t *)L.w, seed, hn));
     }
     SGPB_CUDA(cudaGetLastError());
     return SGP_B200_OK;
