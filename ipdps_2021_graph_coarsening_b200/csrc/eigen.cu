@@ -2038,10 +2038,14 @@ static PIVariant pi_variant(const PIArgs &a) {
 // ascending by destination, in the level's own numbering).  Off by default:
 // on R-MAT levels the per-panel block barriers cost more than the shared-
 // memory gathers save (measured 2x slower than pipelined warp rows).
+// Levels whose layout would need more than kMaxPanels panels (or 2^32
+// panel-row offsets) keep their rule variant.
 static bool panels_wanted(const Level &L, const PIArgs &a) {
     if (a.inv || L.n == 0) return false;
     const char *s = getenv("SGPB_PI_MODE");
-    return s && !strcmp(s, "panel");
+    if (!s || strcmp(s, "panel")) return false;
+    const uint64_t P = cdiv((uint64_t)L.n, (uint64_t)(kPanelBytes / sizeof(double)));
+    return P <= kMaxPanels && P * L.n < 0xFFFFFFFFull;
 }
 
 template <typename W, typename V, int CACHE, bool MX>
@@ -2057,6 +2061,10 @@ static const void *pi_kernel_c(int mode) {
 
 template <typename W, typename V, bool MX>
 static int launch_pi(Context &C, PIArgs &a, uint32_t grid, int mode) {
+    if (mode == 6 && !a.P) {   // column panels need their layout
+        set_error("power iteration: column-panel variant without a panel layout");
+        return SGP_B200_ERR_INVALID;
+    }
     PIVariant var;
     var.mode = a.P ? 6 : mode;
     var.na = true;

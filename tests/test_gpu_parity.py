@@ -238,6 +238,23 @@ def test_power_iter_column_panels(partitioner, weighted, monkeypatch):
     assert 1 - abs(float(np.dot(u_g.cpu().numpy(), u_o))) <= 1e-9
 
 
+def test_power_iter_panels_level_too_wide(partitioner, monkeypatch):
+    """A level wider than the largest panel layout (409,600 vertices: 34 FP64
+    panels of 12,288 entries, more than 31) keeps its rule variant when
+    panels are asked for, and matches the oracle."""
+    monkeypatch.setenv("SGPB_PI_MODE", "panel")
+    g = G.grid2d(640, 640)
+    assert g.n > 31 * 12288
+    x0 = np.random.default_rng(6).random(g.n)
+    cap = 40
+    u_o, it_o, lam_o = O.power_iter(g.row_ptr, g.col, None, x0, 1e-10, cap)
+    u_g, it_g, lam_g, _ = partitioner.power_iter(dev_u32(g.row_ptr), dev_u32(g.col), None,
+                                                 torch.from_numpy(x0).cuda(), None, 1e-10, cap)
+    assert it_g == it_o == cap
+    assert abs(lam_g - lam_o) <= 1e-9 * abs(lam_o)
+    assert 1 - abs(float(np.dot(u_g.cpu().numpy(), u_o))) <= 1e-9
+
+
 def test_power_iter_panels_unsorted_rows(partitioner, monkeypatch):
     """Rows that are not ascending by destination cannot be cut into panel
     segments: the level runs on warp rows and still matches the oracle."""
