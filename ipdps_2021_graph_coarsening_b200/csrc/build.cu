@@ -9,13 +9,16 @@
 //
 // Per-row dedupe is tiered by bucket size:
 //   tier 1 (<= 32 entries)   one warp, bitonic sort in registers
-//   tier 2 (<= kT1 entries)  a 64-thread block, bitonic sort in shared memory
-//   tier 2 (<= kT2 entries)  a kT2Threads block, bitonic sort in shared memory
+//   tier 1b (<= kT1 entries) a 64-thread block, radix sort in shared memory
+//   tier 1c (<= kT1M)        a 128-thread block, radix sort in shared memory
+//   tier 2 (<= kT2 entries)  a 512-thread block, radix sort in shared memory
 //   tier 3 (larger)          dense accumulation over [0, nc): in one block's
 //                            shared memory when nc weights and their bitmap fit
 //                            (a block per row at a time), else in global memory
 //                            (bitmap + weight array, L2-resident); compacted in
 //                            ascending destination order
+#include <type_traits>
+
 #include "common.cuh"
 #include "internal.h"
 
@@ -219,27 +222,29 @@ __global__ void __launch_bounds__(kLongThreads) k_build_scatter_long(
 }
 
 // ------------------------------------------------------------- classify --
-// Bucket sizes 1..32 -> list 0 (one warp), 33..kT1 -> list 1 (small block),
-// ..kT2 -> list 2 (block), larger -> list 3 (dense); one atomic per warp and
-// list.
+// Bucket sizes 1..32 -> list 0 (one warp), 33..kT1 -> list 1 (64 threads),
+// ..kT1M -> list 2 (128 threads), ..kT2 -> list 3 (512 threads), ..kGiant ->
+// list 4 (dense), larger -> list 5 (dense, many blocks a row); one atomic per
+// warp and list.
 constexpr uint32_t kT1 = 256;
-constexpr int kT1Threads = 64;
+constexpr uint32_t kT1M = 1024;
+constexpr int kLists = 6;
 
 // buckets above this many entries are split over many blocks (tier 4)
 constexpr uint32_t kGiant = 1u << 18;
 
 __global__ void k_classify(uint32_t nc, const uint32_t *__restrict__ boff, uint32_t *__restrict__ dcnt,
-                           uint32_t *__restrict__ lists /* 5 x nc */, uint32_t *__restrict__ tcount /* 5 */) {
+                           uint32_t *__restrict__ lists /* kLists x nc */, uint32_t *__restrict__ tcount /* kLists */) {
     const uint32_t c = blockIdx.x * blockDim.x + threadIdx.x;
     const unsigned lane = threadIdx.x & 31;
     int t = -1;
     if (c < nc) {
         const uint32_t sz = boff[c + 1] - boff[c];
         if (sz == 0) dcnt[c] = 0;
-        else t = sz <= 32 ? 0 : sz <= kT1 ? 1 : sz <= (uint32_t)kT2 ? 2 : sz <= kGiant ? 3 : 4;
+        else t = sz <= 32 ? 0 : sz <= kT1 ? 1 : sz <= kT1M ? 2 : sz <= (uint32_t)kT2 ? 3 : sz <= kGiant ? 4 : 5;
     }
 #pragma unroll
-    for (int q = 0; q < 5; q++) {
+    for (int q = 0; q < kLists; q++) {
         const unsigned m = __ballot_sync(0xFFFFFFFFu, t == q);
         if (!m) continue;   // warp-uniform
         const int leader = __ffs(m) - 1;
@@ -304,167 +309,150 @@ __global__ void __launch_bounds__(256) k_dedupe_warp(const uint32_t *__restrict_
     }
 }
 
-// --------------------------------------------------------------- tier 2 --
-constexpr int kT2Threads = 256;
+// ------------------------------------------------------ tiers 1b and 2 --
+// Buckets of 33 .. kT2 entries: a block per bucket at a time sorts the
+// (destination, weight) pairs by an LSD radix sort in shared memory, 8 bits a
+// pass over the low 8 * passes bits of the destinations (all below nc), then
+// merges runs of equal destinations into the bucket's head.  Item q of a
+// bucket is held by warp q / (32 R), round (q / 32) mod R, lane q mod 32; a
+// pass ranks each warp's rounds in order with __match_any_sync against
+// per-warp digit counters, so every pass is stable and the passes compose.
+// A bitonic sort of the same bucket needs O(log^2) compare-exchange stages
+// with a block barrier each; the radix passes need four barriers each.
+template <typename WI, int WARPS, int R>
+struct RadixDedupeCfg {
+    static constexpr int kThreads = WARPS * 32;
+    static constexpr uint32_t kCap = (uint32_t)WARPS * 32 * R;
+    typedef typename std::conditional<sizeof(WI) == 8, unsigned long long, uint32_t>::type VT;
+    static constexpr size_t kSmem = (size_t)kCap * (sizeof(uint32_t) + sizeof(VT));   // dynamic part
+};
 
-template <typename WI, typename WO>
-__global__ void __launch_bounds__(kT2Threads) k_dedupe_block(const uint32_t *__restrict__ list,
+template <typename WI, typename WO, int WARPS, int R>
+__global__ void __launch_bounds__(WARPS * 32) k_dedupe_radix(const uint32_t *__restrict__ list,
                                                              const uint32_t *__restrict__ count,
                                                              const uint32_t *__restrict__ boff,
                                                              uint32_t *__restrict__ bdst, const WI *__restrict__ bw,
                                                              WO *__restrict__ tw, uint32_t *__restrict__ dcnt,
-                                                             uint32_t cap /* largest bucket, even */) {
-    extern __shared__ __align__(16) unsigned char smraw[];
-    uint32_t *skey = (uint32_t *)smraw;                        // cap
-    uint64_t *sw = (uint64_t *)(smraw + cap * sizeof(uint32_t));   // cap
+                                                             int passes) {
+    typedef RadixDedupeCfg<WI, WARPS, R> Cfg;
+    typedef typename Cfg::VT VT;
+    constexpr int kThreads = Cfg::kThreads;
+    constexpr uint32_t kCap = Cfg::kCap;
+    constexpr int kBins = 256;
+    constexpr int kDpt = kBins >= kThreads ? kBins / kThreads : 1;   // digits per thread
+    __shared__ uint32_t wcnt[WARPS][kBins];
+    __shared__ uint32_t dstart[kBins];
     __shared__ uint64_t scan_sm[33];
+    extern __shared__ __align__(16) unsigned char rd_smem[];
+    uint32_t *sk = reinterpret_cast<uint32_t *>(rd_smem);
+    VT *sv = reinterpret_cast<VT *>(rd_smem + kCap * sizeof(uint32_t));
+    const unsigned lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     const uint32_t cntv = *count;
     for (uint32_t k = blockIdx.x; k < cntv; k += gridDim.x) {
         const uint32_t c = list[k];
         const uint32_t b = boff[c], sz = boff[c + 1] - b;
-        uint32_t P = 64;
-        while (P < sz) P <<= 1;
-        for (uint32_t i = threadIdx.x; i < P; i += blockDim.x) {
-            if (i < sz) {
-                skey[i] = bdst[b + i];
-                sw[i] = bw ? (uint64_t)bw[b + i] : 1ull;
-            } else {
-                skey[i] = kSentinel;
-                sw[i] = 0;
-            }
+        uint32_t key[R];
+        VT val[R];
+#pragma unroll
+        for (int r = 0; r < R; r++) {
+            const uint32_t q = (wid * R + r) * 32 + lane;
+            const bool valid = q < sz;
+            key[r] = valid ? bdst[b + q] : 0u;
+            val[r] = valid ? (bw ? (VT)bw[b + q] : (VT)1) : (VT)0;
         }
-        __syncthreads();
-        for (uint32_t kk = 2; kk <= P; kk <<= 1) {
-            for (uint32_t j = kk >> 1; j > 0; j >>= 1) {
-                for (uint32_t t = threadIdx.x; t < P / 2; t += blockDim.x) {
-                    // t-th pair: lower index i has bit j clear
-                    uint32_t i = ((t & ~(j - 1)) << 1) | (t & (j - 1));
-                    uint32_t p = i | j;
-                    bool up = (i & kk) == 0;
-                    uint32_t a = skey[i], bb = skey[p];
-                    if (up ? a > bb : a < bb) {
-                        skey[i] = bb; skey[p] = a;
-                        uint64_t x = sw[i]; sw[i] = sw[p]; sw[p] = x;
-                    }
+        for (int pass = 0; pass < passes; pass++) {
+            const int shift = 8 * pass;
+            for (int d = lane; d < kBins; d += 32) wcnt[wid][d] = 0;
+            __syncwarp();
+            uint32_t rank[R];
+#pragma unroll
+            for (int r = 0; r < R; r++) {
+                if ((wid * R + r) * 32 >= sz) break;   // warp-uniform: rounds past the bucket
+                const uint32_t q = (wid * R + r) * 32 + lane;
+                const bool valid = q < sz;
+                const uint32_t d = (key[r] >> shift) & 0xFFu;
+                const unsigned act = __ballot_sync(0xFFFFFFFFu, valid);
+                rank[r] = 0;
+                if (valid) {
+                    const unsigned peers = __match_any_sync(act, d);
+                    rank[r] = wcnt[wid][d] + __popc(peers & ((1u << lane) - 1u));
+                    __syncwarp(act);
+                    if ((int)lane == __ffs(peers) - 1) wcnt[wid][d] += __popc(peers);
                 }
-                __syncthreads();
-            }
-        }
-        // heads and positions: each thread owns a contiguous segment
-        const uint32_t per = P / blockDim.x > 0 ? P / blockDim.x : 1;
-        const uint32_t s0 = threadIdx.x * per;
-        uint64_t h = 0;
-        for (uint32_t i = s0; i < s0 + per && i < P; i++) {
-            uint32_t key = skey[i];
-            if (key != kSentinel && (i == 0 || skey[i - 1] != key)) h++;
-        }
-        uint64_t tot;
-        uint64_t inc = block_scan_u64(h, scan_sm, &tot);
-        uint64_t pos = inc - h;
-        for (uint32_t i = s0; i < s0 + per && i < P; i++) {
-            uint32_t key = skey[i];
-            if (key != kSentinel && (i == 0 || skey[i - 1] != key)) {
-                uint64_t s = sw[i];
-                for (uint32_t q = i + 1; q < P && skey[q] == key; q++) s += sw[q];
-                bdst[b + pos] = key;
-                tw[b + pos] = (WO)s;
-                pos++;
-            }
-        }
-        if (threadIdx.x == 0) dcnt[c] = (uint32_t)tot;
-        __syncthreads();
-    }
-}
-
-// Tier 2 for 32-bit (or unit) input weights: (destination, weight) packed in
-// one 64-bit word, destination high, so one bitonic sort of words orders the
-// bucket by destination with half the shared-memory traffic of separate
-// key and weight arrays.
-template <typename WI, typename WO>
-__global__ void __launch_bounds__(kT2Threads) k_dedupe_block_packed(const uint32_t *__restrict__ list,
-                                                                    const uint32_t *__restrict__ count,
-                                                                    const uint32_t *__restrict__ boff,
-                                                                    uint32_t *__restrict__ bdst,
-                                                                    const WI *__restrict__ bw, WO *__restrict__ tw,
-                                                                    uint32_t *__restrict__ dcnt) {
-    static_assert(sizeof(WI) == 4, "packed dedupe takes 32-bit input weights");
-    extern __shared__ __align__(16) unsigned char smraw[];
-    unsigned long long *sk = (unsigned long long *)smraw;   // kT2
-    __shared__ uint64_t scan_sm[33];
-    constexpr unsigned long long kNone = ~0ull;
-    const uint32_t cntv = *count;
-    for (uint32_t k = blockIdx.x; k < cntv; k += gridDim.x) {
-        const uint32_t c = list[k];
-        const uint32_t b = boff[c], sz = boff[c + 1] - b;
-        uint32_t P = 64;
-        while (P < sz) P <<= 1;
-        for (uint32_t i = threadIdx.x; i < P; i += blockDim.x)
-            sk[i] = i < sz ? ((unsigned long long)bdst[b + i] << 32) | (bw ? (uint32_t)bw[b + i] : 1u) : kNone;
-        __syncthreads();
-        const unsigned lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
-        for (uint32_t kk = 2; kk <= P; kk <<= 1) {
-            // partners 64 or more apart: pairs through shared memory
-            for (uint32_t j = kk >> 1; j >= 64; j >>= 1) {
-                for (uint32_t t = threadIdx.x; t < P / 2; t += blockDim.x) {
-                    const uint32_t i = ((t & ~(j - 1)) << 1) | (t & (j - 1));
-                    const uint32_t q = i | j;
-                    const bool up = (i & kk) == 0;
-                    const unsigned long long x = sk[i], y = sk[q];
-                    if (up ? x > y : x < y) { sk[i] = y; sk[q] = x; }
-                }
-                __syncthreads();
-            }
-            // partners closer than 64: each warp sorts 64-word chunks in
-            // registers, two consecutive words per lane (the partner of word
-            // q at distance j >= 2 is the same word of lane ^ j/2)
-            for (uint32_t ch = wid; ch < P / 64; ch += nwarps) {
-                const uint32_t q0 = ch * 64 + 2 * lane;
-                const ulonglong2 v = reinterpret_cast<const ulonglong2 *>(sk)[q0 >> 1];
-                unsigned long long x0 = v.x, x1 = v.y;
-                const bool up = (q0 & kk) == 0;   // same for both words: kk > 1
-                for (uint32_t j = (kk >> 1) < 32 ? (kk >> 1) : 32; j >= 2; j >>= 1) {
-                    const unsigned long long y0 = __shfl_xor_sync(0xFFFFFFFFu, x0, j >> 1);
-                    const unsigned long long y1 = __shfl_xor_sync(0xFFFFFFFFu, x1, j >> 1);
-                    const bool lower = (q0 & j) == 0;
-                    // the lower word of a pair keeps the minimum when ascending
-                    const bool keep_min = lower == up;
-                    x0 = keep_min ? (y0 < x0 ? y0 : x0) : (y0 > x0 ? y0 : x0);
-                    x1 = keep_min ? (y1 < x1 ? y1 : x1) : (y1 > x1 ? y1 : x1);
-                }
-                if (up ? x0 > x1 : x0 < x1) {   // j = 1: the lane's own pair
-                    const unsigned long long t = x0;
-                    x0 = x1;
-                    x1 = t;
-                }
-                reinterpret_cast<ulonglong2 *>(sk)[q0 >> 1] = make_ulonglong2(x0, x1);
+                __syncwarp();
             }
             __syncthreads();
+            // per digit: exclusive prefixes over the warps; digit starts from
+            // a block scan of the digit totals (kDpt consecutive digits a thread)
+            const uint32_t d0 = threadIdx.x * kDpt;
+            uint32_t tot[kDpt];
+            uint64_t tsum = 0;
+            if (d0 < kBins) {
+#pragma unroll
+                for (int j = 0; j < kDpt; j++) {
+                    uint32_t t = 0;
+#pragma unroll
+                    for (int w = 0; w < WARPS; w++) {
+                        const uint32_t cw = wcnt[w][d0 + j];
+                        wcnt[w][d0 + j] = t;
+                        t += cw;
+                    }
+                    tot[j] = t;
+                    tsum += t;
+                }
+            }
+            uint64_t all;
+            uint64_t ex = block_scan_u64(d0 < kBins ? tsum : 0, scan_sm, &all) - tsum;
+            if (d0 < kBins) {
+#pragma unroll
+                for (int j = 0; j < kDpt; j++) {
+                    dstart[d0 + j] = (uint32_t)ex;
+                    ex += tot[j];
+                }
+            }
+            __syncthreads();
+#pragma unroll
+            for (int r = 0; r < R; r++) {
+                const uint32_t q = (wid * R + r) * 32 + lane;
+                if (q < sz) {
+                    const uint32_t d = (key[r] >> shift) & 0xFFu;
+                    const uint32_t slot = dstart[d] + wcnt[wid][d] + rank[r];
+                    sk[slot] = key[r];
+                    sv[slot] = val[r];
+                }
+            }
+            __syncthreads();
+#pragma unroll
+            for (int r = 0; r < R; r++) {
+                const uint32_t q = (wid * R + r) * 32 + lane;
+                if (q < sz) {
+                    key[r] = sk[q];
+                    val[r] = sv[q];
+                }
+            }
+            __syncthreads();   // the counters and staging are rewritten next pass
         }
-        // heads of destination runs; each thread owns a contiguous segment
-        const uint32_t per = P / blockDim.x > 0 ? P / blockDim.x : 1;
-        const uint32_t s0 = threadIdx.x * per;
+        // runs of equal destinations: each thread owns a contiguous segment
+        const uint32_t per = (sz + kThreads - 1) / kThreads;
+        const uint32_t s0 = threadIdx.x * per < sz ? threadIdx.x * per : sz;
+        const uint32_t s1 = s0 + per < sz ? s0 + per : sz;
         uint64_t h = 0;
-        for (uint32_t i = s0; i < s0 + per && i < P; i++) {
-            const unsigned long long x = sk[i];
-            if (x != kNone && (i == 0 || (sk[i - 1] >> 32) != (x >> 32))) h++;
-        }
+        for (uint32_t i = s0; i < s1; i++)
+            if (i == 0 || sk[i - 1] != sk[i]) h++;
         uint64_t tot;
-        const uint64_t inc = block_scan_u64(h, scan_sm, &tot);
-        uint64_t pos = inc - h;
-        for (uint32_t i = s0; i < s0 + per && i < P; i++) {
-            const unsigned long long x = sk[i];
-            const uint32_t key = (uint32_t)(x >> 32);
-            if (x != kNone && (i == 0 || (uint32_t)(sk[i - 1] >> 32) != key)) {
-                uint64_t sum = (uint32_t)x;
-                for (uint32_t q = i + 1; q < P && (uint32_t)(sk[q] >> 32) == key && sk[q] != kNone; q++)
-                    sum += (uint32_t)sk[q];
-                bdst[b + pos] = key;
+        uint64_t pos = block_scan_u64(h, scan_sm, &tot) - h;
+        for (uint32_t i = s0; i < s1; i++) {
+            const uint32_t key0 = sk[i];
+            if (i == 0 || sk[i - 1] != key0) {
+                uint64_t sum = sv[i];
+                for (uint32_t q = i + 1; q < sz && sk[q] == key0; q++) sum += sv[q];
+                bdst[b + pos] = key0;
                 tw[b + pos] = (WO)sum;
                 pos++;
             }
         }
         if (threadIdx.x == 0) dcnt[c] = (uint32_t)tot;
-        __syncthreads();
+        __syncthreads();   // the staging arrays are reloaded by the next bucket
     }
 }
 
@@ -717,40 +705,35 @@ template <typename WI, typename WO>
 static int dedupe_buckets(Context &C, uint32_t nc, const uint32_t *boff, uint32_t *bdst, const WI *bw, WO *tw,
                           uint32_t *dcnt) {
     uint32_t *lists, *tcount;
-    SGPB_TRY(dalloc_t(C, &lists, (size_t)5 * nc + 4));
-    SGPB_TRY(dalloc_t(C, &tcount, 5));
-    SGPB_TRY(dzero(C, tcount, sizeof(uint32_t) * 5));
+    SGPB_TRY(dalloc_t(C, &lists, (size_t)kLists * nc + 4));
+    SGPB_TRY(dalloc_t(C, &tcount, kLists));
+    SGPB_TRY(dzero(C, tcount, sizeof(uint32_t) * kLists));
     if (nc) {
         k_classify<<<cdiv(nc, 256), 256, 0, C.stream>>>(nc, boff, dcnt, lists, tcount);
         uint32_t g1 = cdiv(nc, 8);
         if (g1 > (uint32_t)C.num_sms * 16) g1 = C.num_sms * 16;
         k_dedupe_warp<WI, WO><<<g1 ? g1 : 1, 256, 0, C.stream>>>(lists, tcount, boff, bdst, bw, tw, dcnt);
-        // the block kernels size their sort by the bucket: small buckets run
-        // in small blocks, many per SM, large ones in kT2Threads
-        if constexpr (sizeof(WI) == 4) {
-            const size_t sm2 = (size_t)kT2 * sizeof(unsigned long long);
-            SGPB_CUDA(cudaFuncSetAttribute(k_dedupe_block_packed<WI, WO>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                           (int)sm2));
-            k_dedupe_block_packed<WI, WO><<<(uint32_t)C.num_sms * 32, kT1Threads, kT1 * sizeof(unsigned long long),
-                                            C.stream>>>(lists + nc, tcount + 1, boff, bdst, bw, tw, dcnt);
-            const uint32_t g2 = (uint32_t)C.num_sms * 6;
-            k_dedupe_block_packed<WI, WO><<<g2, kT2Threads, sm2, C.stream>>>(lists + 2 * (size_t)nc, tcount + 2,
-                                                                            boff, bdst, bw, tw, dcnt);
-        } else {
-            const size_t sm2 = (size_t)kT2 * (sizeof(uint32_t) + sizeof(uint64_t));
-            SGPB_CUDA(cudaFuncSetAttribute(k_dedupe_block<WI, WO>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                           (int)sm2));
-            k_dedupe_block<WI, WO><<<(uint32_t)C.num_sms * 32, kT1Threads,
-                                     kT1 * (sizeof(uint32_t) + sizeof(uint64_t)), C.stream>>>(
-                lists + nc, tcount + 1, boff, bdst, bw, tw, dcnt, kT1);
-            const uint32_t g2 = (uint32_t)C.num_sms * 4;
-            k_dedupe_block<WI, WO><<<g2, kT2Threads, sm2, C.stream>>>(lists + 2 * (size_t)nc, tcount + 2, boff, bdst,
-                                                                     bw, tw, dcnt, (uint32_t)kT2);
-        }
-        C.kernel_launches += 4;
+        // radix tiers, each block sized for its buckets: 33 .. kT1 entries
+        // in 64 threads, .. kT1M in 128, .. kT2 in 512
+        int bits = 0;
+        while (bits < 32 && (1ull << bits) < (uint64_t)nc) bits++;
+        const int passes = bits > 0 ? (bits + 7) / 8 : 1;
+        typedef RadixDedupeCfg<WI, 2, 4> Cfg1;
+        typedef RadixDedupeCfg<WI, 4, 8> CfgM;
+        typedef RadixDedupeCfg<WI, 16, 8> Cfg2;
+        static_assert(Cfg1::kCap == kT1 && CfgM::kCap == kT1M && Cfg2::kCap == (uint32_t)kT2, "tier sizes");
+        k_dedupe_radix<WI, WO, 2, 4><<<(uint32_t)C.num_sms * 32, Cfg1::kThreads, Cfg1::kSmem, C.stream>>>(
+            lists + nc, tcount + 1, boff, bdst, bw, tw, dcnt, passes);
+        k_dedupe_radix<WI, WO, 4, 8><<<(uint32_t)C.num_sms * 12, CfgM::kThreads, CfgM::kSmem, C.stream>>>(
+            lists + 2 * (size_t)nc, tcount + 2, boff, bdst, bw, tw, dcnt, passes);
+        SGPB_CUDA(cudaFuncSetAttribute(k_dedupe_radix<WI, WO, 16, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)Cfg2::kSmem));
+        k_dedupe_radix<WI, WO, 16, 8><<<(uint32_t)C.num_sms * 2, Cfg2::kThreads, Cfg2::kSmem, C.stream>>>(
+            lists + 3 * (size_t)nc, tcount + 3, boff, bdst, bw, tw, dcnt, passes);
+        C.kernel_launches += 5;
         SGPB_CUDA(cudaGetLastError());
         uint32_t n34[2] = {0, 0};
-        SGPB_TRY(read_u32(C, tcount + 3, n34, 2));
+        SGPB_TRY(read_u32(C, tcount + 4, n34, 2));
         const uint32_t n3 = n34[0], n4 = n34[1];
         // dense accumulation in global memory (L2-resident slots) of the rows
         // of `list`, `per_row` blocks per row
@@ -791,17 +774,17 @@ static int dedupe_buckets(Context &C, uint32_t nc, const uint32_t *boff, uint32_
             SGPB_CUDA(cudaFuncSetAttribute(k_dense_smem<WI, WO>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                            (int)dsm));
             const uint32_t g3 = n3 < (uint32_t)C.num_sms ? n3 : (uint32_t)C.num_sms;
-            k_dense_smem<WI, WO><<<g3, kDenseSmemThreads, dsm, C.stream>>>(lists + 3 * (size_t)nc, tcount + 3, boff,
+            k_dense_smem<WI, WO><<<g3, kDenseSmemThreads, dsm, C.stream>>>(lists + 4 * (size_t)nc, tcount + 4, boff,
                                                                           bdst, bw, tw, dcnt, nc, R);
             C.kernel_launches++;
             SGPB_CUDA(cudaGetLastError());
         } else if (n3) {
-            SGPB_TRY(dense_global(lists + 3 * (size_t)nc, n3, 8));
+            SGPB_TRY(dense_global(lists + 4 * (size_t)nc, n3, 8));
         }
         // tier 4: rows of more than kGiant entries (the hub aggregates of
         // skewed graphs, millions of entries each) on 64 blocks per row, so
         // that one row does not hold one SM for the whole build
-        if (n4) SGPB_TRY(dense_global(lists + 4 * (size_t)nc, n4, 64));
+        if (n4) SGPB_TRY(dense_global(lists + 5 * (size_t)nc, n4, 64));
     }
     return SGP_B200_OK;
 }
@@ -1023,15 +1006,15 @@ __global__ void __launch_bounds__(256) k_sb_weights(uint32_t mc, const uint32_t 
     }
 }
 
-// unit-weight levels with at least this many entries take the sorted build
-// (SGPB_BUILD_SORTED=0 turns it off, =1 forces it for every unit-weight level)
-constexpr uint64_t kSortedBuildMin = 1ull << 22;
-
+// The sorted build runs only when SGPB_BUILD_SORTED=1 asks for it (every
+// unit-weight level then takes it): with the radix-sorted bucket tiers the
+// tiered build is as fast or faster on every family measured (R-MAT 22's
+// coarsening 16.7 ms sorted against 15.9 ms tiered; random geometric, grid,
+// Erdos-Renyi and Chung-Lu graphs of 4M vertices the same or better).
 static bool sorted_build_wanted(const Level &F) {
     if (F.w || F.m == 0) return false;
     const char *e = getenv("SGPB_BUILD_SORTED");
-    if (e && *e) return atoi(e) != 0;
-    return F.m >= kSortedBuildMin;
+    return e && *e && atoi(e) != 0;
 }
 
 template <typename WO>

@@ -50,11 +50,12 @@ def test_sorted_build_matches_oracle_and_tiered(partitioner, monkeypatch, case, 
 
 
 def test_partition_same_with_either_build(partitioner, monkeypatch):
-    """A whole partition of a graph above the size threshold gives the same
-    hierarchy, iterations and partition with either build."""
+    """A whole partition of a large unit-weight graph gives the same
+    hierarchy, iterations and partition with the sorted build (forced) and
+    the default tiered build."""
     g = G.rmat(18, seed=4)
     assert g.m_directed >= 1 << 22
-    monkeypatch.setenv("SGPB_BUILD_SORTED", "0")
+    monkeypatch.setenv("SGPB_BUILD_SORTED", "1")
     a = partitioner.partition(g, rng_state=6)
     monkeypatch.delenv("SGPB_BUILD_SORTED")
     b = partitioner.partition(g, rng_state=6)
