@@ -244,11 +244,13 @@ def batch_leg(p, single_value):
     """The batch configuration (2,048 graphs of 10^3..2.5*10^5 vertices,
     grids with holes and Erdos-Renyi graphs, log-uniform sizes): one batched
     call, host graphs in and host partitions out, FP64 and mixed precision,
-    after one warm-up call on 64 of the graphs; wall clock around the call
-    (it synchronises), phases from sgp_b200_last_timing."""
+    after one untimed warm-up call on the whole batch (the first call of this
+    size grows the memory pool: 11.0 s against 10.6 s for the next ones);
+    wall clock around the call (it synchronises), phases from
+    sgp_b200_last_timing."""
     gs = batch_graphs_cached()
     m_und = sum(g.m_undirected for g in gs)
-    p.partition_batch(gs[:64], workers=16)
+    p.partition_batch(gs, workers=16)
     out = {"workload": "batch2048 (log-uniform 1e3..2.5e5 vertices; grids with 10% holes and ER mean degree 8; "
                        "LCC; unit weights)", "graphs": len(gs), "n": int(sum(g.n for g in gs)),
            "m_undirected": int(m_und), "workers": 16}

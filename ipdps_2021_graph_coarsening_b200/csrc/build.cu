@@ -664,12 +664,17 @@ __global__ void __launch_bounds__(256) k_dense_collect(const uint32_t *__restric
 }
 
 // ---------------------------------------------------------- compaction --
+// Copies the merged buckets into the coarse CSR; with 32-bit weights it also
+// keeps their maximum in *wmax (when given), which decides how narrow the
+// power iteration's copy of the level can store them.
 template <typename WO>
 __global__ void __launch_bounds__(256) k_compact_rows(uint32_t nc, const uint32_t *__restrict__ boff,
                                                      const uint32_t *__restrict__ crp,
                                                      const uint32_t *__restrict__ bdst, const WO *__restrict__ tw,
-                                                     uint32_t *__restrict__ ccol, WO *__restrict__ cw) {
+                                                     uint32_t *__restrict__ ccol, WO *__restrict__ cw,
+                                                     uint32_t *__restrict__ wmax) {
     const unsigned lane = threadIdx.x & 31;
+    uint32_t mx = 0;
     const uint64_t wid = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const uint64_t nw = ((uint64_t)gridDim.x * blockDim.x) >> 5;
     for (uint64_t c = wid; c < nc; c += nw) {
@@ -690,9 +695,14 @@ __global__ void __launch_bounds__(256) k_compact_rows(uint32_t nc, const uint32_
                 if (i < len) {
                     ccol[dst + i] = d[k];
                     cw[dst + i] = x[k];
+                    if constexpr (sizeof(WO) == 4) mx = (uint32_t)x[k] > mx ? (uint32_t)x[k] : mx;
                 }
             }
         }
+    }
+    if constexpr (sizeof(WO) == 4) {
+        mx = warp_max(mx);
+        if (wmax && lane == 0 && mx) atomicMax(wmax, mx);
     }
 }
 
@@ -771,8 +781,11 @@ static int dedupe_buckets(Context &C, uint32_t nc, const uint32_t *boff, uint32_
         while (R > 1 && dense_smem_bytes<WO>(nc, R) > budget) R--;
         const size_t dsm = R ? dense_smem_bytes<WO>(nc, R) : 0;
         if (n3 && R >= 1 && dsm <= budget) {
+            // the limit is a property of the function, shared by every host
+            // thread (batch workers): always the same bound, never this
+            // launch's size, so no thread lowers it under another's launch
             SGPB_CUDA(cudaFuncSetAttribute(k_dense_smem<WI, WO>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                           (int)dsm));
+                                           (int)budget));
             const uint32_t g3 = n3 < (uint32_t)C.num_sms ? n3 : (uint32_t)C.num_sms;
             k_dense_smem<WI, WO><<<g3, kDenseSmemThreads, dsm, C.stream>>>(lists + 4 * (size_t)nc, tcount + 4, boff,
                                                                           bdst, bw, tw, dcnt, nc, R);
@@ -792,7 +805,8 @@ static int dedupe_buckets(Context &C, uint32_t nc, const uint32_t *boff, uint32_
 // ---------------------------------------------------------------- driver --
 template <typename WI, typename WO>
 static int build_impl(Context &C, const Level &F, const WI *w, const uint32_t *vcmap, uint32_t nc,
-                      uint32_t *crp, uint32_t **ccol_io, WO **cw_io, uint64_t *m_c, bool alloc_out) {
+                      uint32_t *crp, uint32_t **ccol_io, WO **cw_io, uint64_t *m_c, bool alloc_out,
+                      uint32_t *wmax = nullptr) {
     const uint32_t n = F.n;
     uint32_t *cnt, *boff, *fill, *dcnt;
     SGPB_TRY(dalloc_t(C, &cnt, (size_t)nc + 1));
@@ -863,7 +877,7 @@ static int build_impl(Context &C, const Level &F, const WI *w, const uint32_t *v
     if (nc) {
         uint32_t g = cdiv(nc, 8);
         if (g > (uint32_t)C.num_sms * 16) g = C.num_sms * 16;
-        k_compact_rows<WO><<<g ? g : 1, 256, 0, C.stream>>>(nc, boff, crp, bdst, tw, *ccol_io, *cw_io);
+        k_compact_rows<WO><<<g ? g : 1, 256, 0, C.stream>>>(nc, boff, crp, bdst, tw, *ccol_io, *cw_io, wmax);
         C.kernel_launches++;
     }
     SGPB_CUDA(cudaGetLastError());
@@ -1149,9 +1163,13 @@ int build_coarse_level(Context &C, const Level &F, const uint32_t *vcmap, uint32
                                                                &mc, true)));
         out->w = cw;
     } else {
-        uint32_t *cw = nullptr;
-        SGPB_TRY((build_impl<uint32_t, uint32_t>(C, F, (const uint32_t *)F.w, vcmap, nc, crp, &ccol, &cw, &mc, true)));
+        uint32_t *cw = nullptr, *wmax = nullptr;
+        SGPB_TRY(dalloc_t(C, &wmax, 1));
+        SGPB_TRY(dzero(C, wmax, sizeof(uint32_t)));
+        SGPB_TRY((build_impl<uint32_t, uint32_t>(C, F, (const uint32_t *)F.w, vcmap, nc, crp, &ccol, &cw, &mc, true,
+                                                 wmax)));
         out->w = cw;
+        out->wmax = wmax;
     }
     out->col = ccol;
     out->m = mc;

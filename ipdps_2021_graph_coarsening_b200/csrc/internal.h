@@ -102,6 +102,7 @@ struct Level {
     int sorted = 0;              // 1: every row ascending by destination (coarse levels)
     uint32_t *vcmap = nullptr;   // this level -> next coarser level
     uint32_t *vtx_w = nullptr;   // vertex weights; null: every vertex weighs 1 (the input level)
+    uint32_t *wmax = nullptr;    // device word: the largest 32-bit weight (tiered builds), null: unknown
     uint32_t max_deg = 0;
     uint32_t seed_hi = 0, seed_lo = 0;
     int hec_rounds = 0;

@@ -36,23 +36,50 @@ __global__ void k_bucket_count(uint32_t n, const uint32_t *rp, uint32_t nb, uint
     for (int k = threadIdx.x; k < kBuckets; k += blockDim.x) cnt[(size_t)k * nb + blockIdx.x] = c[k];
 }
 
-// one thread per tile walks its rows in order: stable, deterministic
-__global__ void k_bucket_scatter(uint32_t n, const uint32_t *rp, uint32_t nb, const uint32_t *off, uint32_t *perm,
-                                 uint32_t *inv) {
-    const uint32_t blk = blockIdx.x * blockDim.x + threadIdx.x;
-    if (blk >= nb) return;
-    uint32_t pos[kBuckets];
-#pragma unroll
-    for (int k = 0; k < kBuckets; k++) pos[k] = off[(size_t)k * nb + blk];
-    const uint64_t t0 = (uint64_t)blk * kPermTile;
-    for (uint64_t i = t0; i < t0 + kPermTile && i < n; i++) {
-        const uint32_t k = deg_key(rp[i + 1] - rp[i]);
-        uint32_t p = 0;
-#pragma unroll
-        for (int q = 0; q < kBuckets; q++)
-            if (q == (int)k) p = pos[q]++;
-        perm[i] = p;
-        inv[p] = (uint32_t)i;
+// A block per tile of kPermTile rows, 256 rows at a time: each warp ranks its
+// rows within their degree class with __match_any_sync, a prefix over the
+// warps per class (and the class's running position in the tile) gives the
+// new ids.  Rows keep their order inside a class: stable, deterministic.
+constexpr int kPermThreads = 256;
+
+__global__ void __launch_bounds__(kPermThreads) k_bucket_scatter(uint32_t n, const uint32_t *rp, uint32_t nb,
+                                                                 const uint32_t *off, uint32_t *perm, uint32_t *inv) {
+    constexpr int kWarps = kPermThreads / 32;
+    __shared__ uint32_t pos[kBuckets];
+    __shared__ uint32_t wc[kWarps][kBuckets];
+    const unsigned lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    if (threadIdx.x < kBuckets) pos[threadIdx.x] = off[(size_t)threadIdx.x * nb + blockIdx.x];
+    const uint64_t t0 = (uint64_t)blockIdx.x * kPermTile;
+    for (uint32_t c0 = 0; c0 < (uint32_t)kPermTile; c0 += kPermThreads) {
+        for (int k = threadIdx.x; k < kWarps * kBuckets; k += kPermThreads) (&wc[0][0])[k] = 0;
+        __syncthreads();
+        const uint64_t i = t0 + c0 + threadIdx.x;
+        const bool valid = i < n;
+        const uint32_t k = valid ? deg_key(rp[i + 1] - rp[i]) : 0u;
+        const unsigned act = __ballot_sync(0xFFFFFFFFu, valid);
+        uint32_t rank = 0;
+        if (valid) {
+            const unsigned peers = __match_any_sync(act, k);
+            rank = __popc(peers & ((1u << lane) - 1u));
+            if ((int)lane == __ffs(peers) - 1) wc[wid][k] = __popc(peers);
+        }
+        __syncthreads();
+        if (threadIdx.x < kBuckets) {
+            uint32_t t = pos[threadIdx.x];
+            for (int w = 0; w < kWarps; w++) {
+                const uint32_t c = wc[w][threadIdx.x];
+                wc[w][threadIdx.x] = t;
+                t += c;
+            }
+            pos[threadIdx.x] = t;
+        }
+        __syncthreads();
+        if (valid) {
+            const uint32_t p = wc[wid][k] + rank;
+            perm[i] = p;
+            inv[p] = (uint32_t)i;
+        }
+        __syncthreads();
     }
 }
 
@@ -135,7 +162,7 @@ int hub_first_copy(Context &C, const Level &L, uint32_t **perm_out, uint32_t **i
     SGPB_TRY(dalloc_t(C, &deg, (size_t)n + 1));
     k_bucket_count<<<nb, 256, 0, C.stream>>>(n, L.rp, nb, cnt);
     SGPB_TRY(scan_u32(C, cnt, off, nb * kBuckets, nullptr));
-    k_bucket_scatter<<<cdiv(nb, 64), 64, 0, C.stream>>>(n, L.rp, nb, off, perm, inv);
+    k_bucket_scatter<<<nb, kPermThreads, 0, C.stream>>>(n, L.rp, nb, off, perm, inv);
     k_perm_degrees<<<cdiv(n, 256), 256, 0, C.stream>>>(n, L.rp, inv, deg);
     C.kernel_launches += 3;
     *out = L;
@@ -148,13 +175,16 @@ int hub_first_copy(Context &C, const Level &L, uint32_t **perm_out, uint32_t **i
     } else if (L.w) {
         // 32-bit weights that all fit 8 or 16 bits are stored narrow: the
         // power iteration streams them every iteration
-        uint32_t *mx, hmx = 0;
-        SGPB_TRY(dalloc_t(C, &mx, 1));
-        SGPB_TRY(dzero(C, mx, 4));
-        uint32_t g = (uint32_t)cdiv(L.m, 256);
-        if (g > (uint32_t)C.num_sms * 8) g = C.num_sms * 8;
-        k_max_u32<<<g ? g : 1, 256, 0, C.stream>>>(L.m, (const uint32_t *)L.w, mx);
-        C.kernel_launches++;
+        // (the tiered build records the maximum; other levels are scanned)
+        uint32_t *mx = L.wmax, hmx = 0;
+        if (!mx) {
+            SGPB_TRY(dalloc_t(C, &mx, 1));
+            SGPB_TRY(dzero(C, mx, 4));
+            uint32_t g = (uint32_t)cdiv(L.m, 256);
+            if (g > (uint32_t)C.num_sms * 8) g = C.num_sms * 8;
+            k_max_u32<<<g ? g : 1, 256, 0, C.stream>>>(L.m, (const uint32_t *)L.w, mx);
+            C.kernel_launches++;
+        }
         SGPB_TRY(read_u32(C, mx, &hmx));
         if (hmx <= 0xFFu) SGPB_TRY((fill_impl<uint32_t, uint8_t>(C, L, perm, inv, out)));
         else if (hmx <= 0xFFFFu) SGPB_TRY((fill_impl<uint32_t, uint16_t>(C, L, perm, inv, out)));
