@@ -1793,6 +1793,16 @@ __global__ void __cluster_dims__(kMidCTAs, 1, 1) __launch_bounds__(kMidThreads, 
 // ----------------------------------------------------------- residual --
 // |L x - lambda x|^2 partial sums per block (x unit-norm FP64 vector).
 // normlap: the random-walk Laplacian I - D^-1 A instead of L = D - A.
+// ||L x - lambda x||^2 and ||x||^2 of the finest level (the reference's
+// eigenvalue log, eigensolve_kokkos.h:60-98, computes the same residual
+// vector): one warp per row with four entries per lane in flight; rows of
+// more than kResLongT entries are left to k_residual_long.
+constexpr uint32_t kResLongT = 8192;
+
+__device__ __forceinline__ double residual_term(int normlap, double xi, double acc, double d, double lambda) {
+    return normlap ? xi - (d > 0 ? acc / d : 0.0) - lambda * xi : d * xi - acc - lambda * xi;
+}
+
 template <typename W>
 __global__ void __launch_bounds__(256) k_residual(uint32_t n, const uint32_t *__restrict__ rp,
                                                  const uint32_t *__restrict__ col, const W *__restrict__ w,
@@ -1804,16 +1814,30 @@ __global__ void __launch_bounds__(256) k_residual(uint32_t n, const uint32_t *__
     const uint64_t wid = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const uint64_t nw = ((uint64_t)gridDim.x * blockDim.x) >> 5;
     for (uint64_t i = wid; i < n; i += nw) {
+        const uint32_t b = rp[i], e = rp[i + 1];
+        if (e - b > kResLongT) continue;   // warp-uniform: k_residual_long
         double acc = 0, d = 0;
-        for (uint32_t j = rp[i] + lane; j < rp[i + 1]; j += 32) {
-            double wt = w ? (double)w[j] : 1.0;
-            acc += wt * x[col[j]];
-            d += wt;
+        for (uint32_t j0 = b + lane; j0 < e; j0 += 128) {
+            uint32_t c[4];
+            double wt[4];
+#pragma unroll
+            for (int k = 0; k < 4; k++) {
+                const uint32_t j = j0 + 32 * k;
+                c[k] = j < e ? col[j] : 0u;
+                wt[k] = j < e ? (w ? (double)w[j] : 1.0) : 0.0;
+            }
+#pragma unroll
+            for (int k = 0; k < 4; k++) {
+                if (j0 + 32 * k < e) {
+                    acc += wt[k] * x[c[k]];
+                    d += wt[k];
+                }
+            }
         }
         acc = warp_sum(acc);
         d = warp_sum(d);
         if (lane == 0) {
-            double r = normlap ? x[i] - (d > 0 ? acc / d : 0.0) - lambda * x[i] : d * x[i] - acc - lambda * x[i];
+            const double r = residual_term(normlap, x[i], acc, d, lambda);
             s[0] += r * r;
             s[1] += x[i] * x[i];
         }
@@ -1822,10 +1846,58 @@ __global__ void __launch_bounds__(256) k_residual(uint32_t n, const uint32_t *__
     if (threadIdx.x == 0) { part[2 * blockIdx.x] = s[0]; part[2 * blockIdx.x + 1] = s[1]; }
 }
 
-__global__ void k_sum_pairs(const double *part, uint32_t nb, double *out) {
+// the rows of more than kResLongT entries (ascending list), a block each;
+// lres[2 r], lres[2 r + 1] = r_i^2, x_i^2 of list entry r
+template <typename W>
+__global__ void __launch_bounds__(1024) k_residual_long(const uint32_t *__restrict__ rp,
+                                                       const uint32_t *__restrict__ col, const W *__restrict__ w,
+                                                       const double *__restrict__ x, double lambda, int normlap,
+                                                       const uint32_t *__restrict__ list,
+                                                       const uint32_t *__restrict__ cnt, double *lres) {
+    __shared__ double sm[96];
+    const uint32_t nl = *cnt;
+    for (uint32_t r = blockIdx.x; r < nl; r += gridDim.x) {
+        const uint32_t i = list[r];
+        const uint32_t b = rp[i], e = rp[i + 1];
+        double v[2] = {0, 0};
+        for (uint32_t j0 = b + threadIdx.x; j0 < e; j0 += 4 * blockDim.x) {
+            uint32_t c[4];
+            double wt[4];
+#pragma unroll
+            for (int k = 0; k < 4; k++) {
+                const uint32_t j = j0 + k * blockDim.x;
+                c[k] = j < e ? col[j] : 0u;
+                wt[k] = j < e ? (w ? (double)w[j] : 1.0) : 0.0;
+            }
+#pragma unroll
+            for (int k = 0; k < 4; k++) {
+                if (j0 + k * blockDim.x < e) {
+                    v[0] += wt[k] * x[c[k]];
+                    v[1] += wt[k];
+                }
+            }
+        }
+        block_sum_d<2>(v, sm);   // ends with a barrier: sm is free for the next row
+        if (threadIdx.x == 0) {
+            const double t = residual_term(normlap, x[i], v[0], v[1], lambda);
+            lres[2 * (size_t)r] = t * t;
+            lres[2 * (size_t)r + 1] = x[i] * x[i];
+        }
+    }
+}
+
+__global__ void k_long_flags(uint32_t n, const uint32_t *rp, uint32_t T, uint8_t *f) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) f[i] = rp[i + 1] - rp[i] > T ? 1 : 0;
+}
+
+// the block partials in block order, then the long rows in ascending order
+__global__ void k_sum_pairs(const double *part, uint32_t nb, const double *lres, const uint32_t *lcnt, double *out) {
     if (threadIdx.x == 0 && blockIdx.x == 0) {
         double a = 0, b = 0;
         for (uint32_t i = 0; i < nb; i++) { a += part[2 * i]; b += part[2 * i + 1]; }
+        const uint32_t nl = lcnt ? *lcnt : 0u;
+        for (uint32_t r = 0; r < nl; r++) { a += lres[2 * (size_t)r]; b += lres[2 * (size_t)r + 1]; }
         out[0] = a; out[1] = b;
     }
 }
@@ -2477,14 +2549,37 @@ int level_residual(Context &C, const Level &L, const double *x, int normlap, Pow
     double *part, *out2;
     SGPB_TRY(dalloc_t(C, &part, 2 * (size_t)nb));
     SGPB_TRY(dalloc_t(C, &out2, 2));
-    if (L.wbytes == 8)
+    // rows of more than kResLongT entries: an ascending list, a block each
+    double *lres = nullptr;
+    uint32_t *lcnt = nullptr, *llist = nullptr;
+    if (L.m > kResLongT && n) {
+        uint8_t *flags;
+        const uint64_t maxl = L.m / kResLongT + 1;
+        SGPB_TRY(dalloc_t(C, &flags, n));
+        SGPB_TRY(dalloc_t(C, &llist, (size_t)n + 1));
+        SGPB_TRY(dalloc_t(C, &lcnt, 1));
+        SGPB_TRY(dalloc_t(C, &lres, 2 * maxl));
+        k_long_flags<<<cdiv(n, 256), 256, 0, C.stream>>>(n, L.rp, kResLongT, flags);
+        C.kernel_launches++;
+        SGPB_TRY(compact_flags(C, flags, n, llist, lcnt));
+    }
+    const uint32_t gl = (uint32_t)(L.m / kResLongT + 1 < (uint64_t)C.num_sms * 2 ? L.m / kResLongT + 1
+                                                                                 : (uint64_t)C.num_sms * 2);
+    if (L.wbytes == 8) {
         k_residual<unsigned long long><<<nb, 256, 0, C.stream>>>(n, L.rp, L.col, (const unsigned long long *)L.w, x,
                                                                  res->lambda, normlap, part);
-    else
+        if (lcnt)
+            k_residual_long<unsigned long long><<<gl, 1024, 0, C.stream>>>(
+                L.rp, L.col, (const unsigned long long *)L.w, x, res->lambda, normlap, llist, lcnt, lres);
+    } else {
         k_residual<uint32_t><<<nb, 256, 0, C.stream>>>(n, L.rp, L.col, (const uint32_t *)L.w, x, res->lambda,
                                                        normlap, part);
-    k_sum_pairs<<<1, 32, 0, C.stream>>>(part, nb, out2);
-    C.kernel_launches += 2;
+        if (lcnt)
+            k_residual_long<uint32_t><<<gl, 1024, 0, C.stream>>>(L.rp, L.col, (const uint32_t *)L.w, x, res->lambda,
+                                                                 normlap, llist, lcnt, lres);
+    }
+    k_sum_pairs<<<1, 32, 0, C.stream>>>(part, nb, lres, lcnt, out2);
+    C.kernel_launches += lcnt ? 3 : 2;
     SGPB_CUDA(cudaGetLastError());
     SGPB_CUDA(cudaMemcpyAsync(C.h_pinned, out2, 2 * sizeof(double), cudaMemcpyDeviceToHost, C.stream));
     SGPB_CUDA(cudaStreamSynchronize(C.stream));

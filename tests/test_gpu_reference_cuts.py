@@ -107,3 +107,26 @@ def test_fiedler_value_against_fp64_eigensolver(partitioner, case):
     if not name.startswith("rmat"):
         assert rel <= 0.05
 
+
+
+def test_residual_with_hub_rows(partitioner):
+    """The reported eigenvalue and residual on a graph whose finest level has
+    rows of more than 8192 entries (R-MAT 18: 19 such hubs, up to 25k
+    entries), which the residual pass gives a block each: both recomputed on
+    the CPU from the eigenvector."""
+    g = G.rmat(18, seed=2)
+    L, d = laplacian(g)
+    assert d.max() > 8192
+    seed = 11
+    r = partitioner.partition(g, rng_state=seed)
+    rng = api.PCG32(state=seed, inc=1)
+    h = partitioner.generate_coarse_graphs(g, rng=rng)
+    try:
+        x = h.eigensolve(rng=rng)
+    finally:
+        h.free()
+    Lx = L @ x
+    lam = float(x @ Lx / (x @ x))
+    res = float(np.linalg.norm(Lx - lam * x) / np.linalg.norm(x) / (2 * d.max()))
+    assert abs(lam - r.lam) <= 1e-9 * lam
+    assert abs(res - r.residual) <= 1e-6 * res + 1e-15
