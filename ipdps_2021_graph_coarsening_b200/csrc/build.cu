@@ -11,7 +11,7 @@
 //   tier 1 (<= 32 entries)   one warp, bitonic sort in registers
 //   tier 1b (<= kT1 entries) a 64-thread block, radix sort in shared memory
 //   tier 1c (<= kT1M)        a 128-thread block, radix sort in shared memory
-//   tier 2 (<= kT2 entries)  a 512-thread block, radix sort in shared memory
+//   tier 2 (<= kT2H / kT2)   a 256- / 512-thread block, radix sort in shared memory
 //   tier 3 (larger)          dense accumulation over [0, nc): in one block's
 //                            shared memory when nc weights and their bitmap fit
 //                            (a block per row at a time), else in global memory
@@ -223,12 +223,13 @@ __global__ void __launch_bounds__(kLongThreads) k_build_scatter_long(
 
 // ------------------------------------------------------------- classify --
 // Bucket sizes 1..32 -> list 0 (one warp), 33..kT1 -> list 1 (64 threads),
-// ..kT1M -> list 2 (128 threads), ..kT2 -> list 3 (512 threads), ..kGiant ->
-// list 4 (dense), larger -> list 5 (dense, many blocks a row); one atomic per
-// warp and list.
+// ..kT1M -> list 2 (128 threads), ..kT2H -> list 3 (256 threads), ..kT2 ->
+// list 4 (512 threads), ..kGiant -> list 5 (dense), larger -> list 6 (dense,
+// many blocks a row); one atomic per warp and list.
 constexpr uint32_t kT1 = 256;
 constexpr uint32_t kT1M = 1024;
-constexpr int kLists = 6;
+constexpr uint32_t kT2H = 2048;
+constexpr int kLists = 7;
 
 // buckets above this many entries are split over many blocks (tier 4)
 constexpr uint32_t kGiant = 1u << 18;
@@ -241,7 +242,7 @@ __global__ void k_classify(uint32_t nc, const uint32_t *__restrict__ boff, uint3
     if (c < nc) {
         const uint32_t sz = boff[c + 1] - boff[c];
         if (sz == 0) dcnt[c] = 0;
-        else t = sz <= 32 ? 0 : sz <= kT1 ? 1 : sz <= kT1M ? 2 : sz <= (uint32_t)kT2 ? 3 : sz <= kGiant ? 4 : 5;
+        else t = sz <= 32 ? 0 : sz <= kT1 ? 1 : sz <= kT1M ? 2 : sz <= kT2H ? 3 : sz <= (uint32_t)kT2 ? 4 : sz <= kGiant ? 5 : 6;
     }
 #pragma unroll
     for (int q = 0; q < kLists; q++) {
@@ -318,7 +319,7 @@ __global__ void __launch_bounds__(256) k_dedupe_warp(const uint32_t *__restrict_
 // pass ranks each warp's rounds in order with __match_any_sync against
 // per-warp digit counters, so every pass is stable and the passes compose.
 // A bitonic sort of the same bucket needs O(log^2) compare-exchange stages
-// with a block barrier each; the radix passes need four barriers each.
+// with a block barrier each; the radix passes need three barriers each.
 template <typename WI, int WARPS, int R>
 struct RadixDedupeCfg {
     static constexpr int kThreads = WARPS * 32;
@@ -422,15 +423,20 @@ __global__ void __launch_bounds__(WARPS * 32) k_dedupe_radix(const uint32_t *__r
                 }
             }
             __syncthreads();
+            // the next pass works on the staged order; its first barrier
+            // (after the ranking) orders these reads before its scatter, and
+            // each warp clears only its own counters, which the other
+            // threads last read before this pass's second barrier
+            if (pass + 1 < passes) {
 #pragma unroll
-            for (int r = 0; r < R; r++) {
-                const uint32_t q = (wid * R + r) * 32 + lane;
-                if (q < sz) {
-                    key[r] = sk[q];
-                    val[r] = sv[q];
+                for (int r = 0; r < R; r++) {
+                    const uint32_t q = (wid * R + r) * 32 + lane;
+                    if (q < sz) {
+                        key[r] = sk[q];
+                        val[r] = sv[q];
+                    }
                 }
             }
-            __syncthreads();   // the counters and staging are rewritten next pass
         }
         // runs of equal destinations: each thread owns a contiguous segment
         const uint32_t per = (sz + kThreads - 1) / kThreads;
@@ -803,26 +809,30 @@ static int dedupe_buckets(Context &C, uint32_t nc, const uint32_t *boff, uint32_
         if (g1 > (uint32_t)C.num_sms * 16) g1 = C.num_sms * 16;
         k_dedupe_warp<WI, WO><<<g1 ? g1 : 1, 256, 0, C.stream>>>(lists, tcount, boff, bdst, bw, tw, dcnt);
         // radix tiers, each block sized for its buckets: 33 .. kT1 entries
-        // in 64 threads, .. kT1M in 128, .. kT2 in 512
+        // in 64 threads, .. kT1M in 128, .. kT2H in 256, .. kT2 in 512
         int bits = 0;
         while (bits < 32 && (1ull << bits) < (uint64_t)nc) bits++;
         const int passes = bits > 0 ? (bits + 7) / 8 : 1;
         typedef RadixDedupeCfg<WI, 2, 4> Cfg1;
         typedef RadixDedupeCfg<WI, 4, 8> CfgM;
+        typedef RadixDedupeCfg<WI, 8, 8> CfgH;
         typedef RadixDedupeCfg<WI, 16, 8> Cfg2;
-        static_assert(Cfg1::kCap == kT1 && CfgM::kCap == kT1M && Cfg2::kCap == (uint32_t)kT2, "tier sizes");
+        static_assert(Cfg1::kCap == kT1 && CfgM::kCap == kT1M && CfgH::kCap == kT2H && Cfg2::kCap == (uint32_t)kT2,
+                      "tier sizes");
         k_dedupe_radix<WI, WO, 2, 4><<<(uint32_t)C.num_sms * 32, Cfg1::kThreads, Cfg1::kSmem, C.stream>>>(
             lists + nc, tcount + 1, boff, bdst, bw, tw, dcnt, passes);
         k_dedupe_radix<WI, WO, 4, 8><<<(uint32_t)C.num_sms * 12, CfgM::kThreads, CfgM::kSmem, C.stream>>>(
             lists + 2 * (size_t)nc, tcount + 2, boff, bdst, bw, tw, dcnt, passes);
+        k_dedupe_radix<WI, WO, 8, 8><<<(uint32_t)C.num_sms * 4, CfgH::kThreads, CfgH::kSmem, C.stream>>>(
+            lists + 3 * (size_t)nc, tcount + 3, boff, bdst, bw, tw, dcnt, passes);
         SGPB_CUDA(cudaFuncSetAttribute(k_dedupe_radix<WI, WO, 16, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        (int)Cfg2::kSmem));
         k_dedupe_radix<WI, WO, 16, 8><<<(uint32_t)C.num_sms * 2, Cfg2::kThreads, Cfg2::kSmem, C.stream>>>(
-            lists + 3 * (size_t)nc, tcount + 3, boff, bdst, bw, tw, dcnt, passes);
-        C.kernel_launches += 5;
+            lists + 4 * (size_t)nc, tcount + 4, boff, bdst, bw, tw, dcnt, passes);
+        C.kernel_launches += 6;
         SGPB_CUDA(cudaGetLastError());
         uint32_t n34[2] = {0, 0};
-        SGPB_TRY(read_u32(C, tcount + 4, n34, 2));
+        SGPB_TRY(read_u32(C, tcount + 5, n34, 2));
         const uint32_t n3 = n34[0], n4 = n34[1];
         // dense accumulation in global memory (L2-resident slots) of the rows
         // of `list`, `per_row` blocks per row
@@ -866,7 +876,7 @@ static int dedupe_buckets(Context &C, uint32_t nc, const uint32_t *boff, uint32_
             SGPB_CUDA(cudaFuncSetAttribute(k_dense_smem<WI, WO>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                            (int)budget));
             const uint32_t g3 = n3 < (uint32_t)C.num_sms ? n3 : (uint32_t)C.num_sms;
-            k_dense_smem<WI, WO><<<g3, kDenseSmemThreads, dsm, C.stream>>>(lists + 4 * (size_t)nc, tcount + 4, boff,
+            k_dense_smem<WI, WO><<<g3, kDenseSmemThreads, dsm, C.stream>>>(lists + 5 * (size_t)nc, tcount + 5, boff,
                                                                           bdst, bw, tw, dcnt, nc, R);
             C.kernel_launches++;
             SGPB_CUDA(cudaGetLastError());
@@ -882,7 +892,7 @@ static int dedupe_buckets(Context &C, uint32_t nc, const uint32_t *boff, uint32_
             const size_t csm = dense_smem_bytes<WO>(Cw, 1);
             SGPB_CUDA(cudaFuncSetAttribute(k_dense_chunked<WI, WO>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                            (int)budget));
-            k_dense_chunked<WI, WO><<<g3, kDenseSmemThreads, csm, C.stream>>>(lists + 4 * (size_t)nc, tcount + 4,
+            k_dense_chunked<WI, WO><<<g3, kDenseSmemThreads, csm, C.stream>>>(lists + 5 * (size_t)nc, tcount + 5,
                                                                              boff, bdst, bw, tw, dcnt, nc, Cw, sdst,
                                                                              scap);
             C.kernel_launches++;
@@ -891,7 +901,7 @@ static int dedupe_buckets(Context &C, uint32_t nc, const uint32_t *boff, uint32_
         // tier 4: rows of more than kGiant entries (the hub aggregates of
         // skewed graphs, millions of entries each) on 64 blocks per row, so
         // that one row does not hold one SM for the whole build
-        if (n4) SGPB_TRY(dense_global(lists + 5 * (size_t)nc, n4, 64));
+        if (n4) SGPB_TRY(dense_global(lists + 6 * (size_t)nc, n4, 64));
     }
     return SGP_B200_OK;
 }
