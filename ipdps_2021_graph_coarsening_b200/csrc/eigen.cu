@@ -101,6 +101,15 @@ constexpr size_t kCacheBytesRows = 96 * 1024;
 constexpr size_t kCacheBytesStream = 48 * 1024;
 // iterate bytes of a relabelled level gathered with L1 evict-last priority
 constexpr size_t kSplitBytes = 128 * 1024;
+// the hub prefix in bytes: kSplitBytes, or SGPB_PI_SPLIT_KB (a tuning knob)
+static size_t split_bytes() {
+    static const size_t v = [] {
+        const char *s = getenv("SGPB_PI_SPLIT_KB");
+        const long kb = s ? atol(s) : 0;
+        return kb > 0 && kb <= 256 ? (size_t)kb * 1024 : kSplitBytes;
+    }();
+    return v;
+}
 // dynamic shared memory for one column panel of the iterate, per block
 constexpr size_t kPanelBytes = 96 * 1024;
 constexpr uint32_t kMaxPanels = 31;
@@ -2146,7 +2155,7 @@ static int launch_pi(Context &C, PIArgs &a, uint32_t grid, int mode) {
     // relabelled copy (L1 policy by hub prefix), 0 = off
     a.kcache = (a.cache_ok == 2 && a.n <= kmax) ? (uint32_t)a.n : 0u;
     const bool split = a.cache_ok == 3 && var.mode != 6;
-    if (split) a.kcache = (uint32_t)(a.n < kSplitBytes / sizeof(V) ? a.n : kSplitBytes / sizeof(V));
+    if (split) a.kcache = (uint32_t)(a.n < split_bytes() / sizeof(V) ? a.n : split_bytes() / sizeof(V));
     if (var.mode == 6) a.kcache = 0;
     const void *k = nullptr;
     if constexpr (sizeof(W) < 4) {
