@@ -174,10 +174,15 @@ typedef struct {
                                    level keeping more than 0.9 of the vertices (sgpar.h:2466-2475) */
     uint32_t cluster_max_log2;  /* power-iteration levels above one block's shared memory and of at
                                    most 2^k cost units (entries + 8 per vertex) run on a cluster of
-                                   8 blocks (one cluster barrier per iteration, several levels at
+                                   blocks (one cluster barrier per iteration, several levels at
                                    once); larger ones on the whole GPU.  0 = the default: 17 for
                                    single partitions, 23 for sgp_b200_partition_batch, whose levels
                                    of many graphs then share the GPU.  Equal values give equal bits. */
+    uint32_t cluster_blocks;    /* blocks per cluster of that kernel: 8 or 2.  0 = the default: 8 for
+                                   single partitions (each level's latency), 2 for
+                                   sgp_b200_partition_batch (twice as many hierarchies iterate at
+                                   once; 2,048 graphs of 10^3..2.5*10^5 vertices: 10.6 -> 8.6 s).
+                                   Equal values (with equal cluster_max_log2) give equal bits. */
 } sgp_b200_options_t;
 
 #define SGP_B200_COARSEN_HEC 0      /* heavy-edge coarsening, heuristics.h:930-1031 (default) */

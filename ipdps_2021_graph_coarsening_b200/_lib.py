@@ -46,7 +46,8 @@ class sgp_b200_options_t(ctypes.Structure):
     _fields_ = [("cutoff", c_u32), ("tol", c_dbl), ("mixed", c_int), ("perc_imbalance", c_int),
                 ("iter_cap", c_u64), ("rng_state", c_u64), ("rng_inc", c_u64), ("part_mem", c_int),
                 ("refine_alg", c_int), ("local_search_alg", c_int), ("fm_passes", c_u32), ("coarsener", c_int),
-                ("cluster_max_log2", c_u32)]
+                ("cluster_max_log2", c_u32),
+                ("cluster_blocks", c_u32)]
 
 
 class sgp_b200_result_t(ctypes.Structure):

@@ -285,7 +285,8 @@ class Partitioner:
     @staticmethod
     def _options(cutoff, tol, mixed, rng_state, rng_inc, iter_cap, perc_imbalance,
                  refine_alg: int = 0, coarsener: int = 0, local_search_alg: int = 0,
-                 fm_passes: int = 0, cluster_max_log2: int = 0) -> L.sgp_b200_options_t:
+                 fm_passes: int = 0, cluster_max_log2: int = 0,
+                 cluster_blocks: int = 0) -> L.sgp_b200_options_t:
         o = L.sgp_b200_options_t()
         L.lib().sgp_b200_default_options(ctypes.byref(o))
         o.cutoff, o.tol, o.mixed, o.perc_imbalance = cutoff, tol, int(mixed), perc_imbalance
@@ -295,6 +296,7 @@ class Partitioner:
         o.local_search_alg = local_search_alg
         o.fm_passes = fm_passes
         o.cluster_max_log2 = cluster_max_log2
+        o.cluster_blocks = cluster_blocks
         return o
 
     @staticmethod
@@ -322,7 +324,8 @@ class Partitioner:
     def partition(self, g, cutoff: int = 50, tol: float = 1e-10, mixed: bool = False,
                   rng_state: int = 0x853C49E6748FEA9B, rng_inc: int = 1, iter_cap: int = 0,
                   perc_imbalance: int = 0, part_out=None, refine_alg: int = 0, coarsener: int = 0,
-                  local_search_alg: int = 0, fm_passes: int = 0, cluster_max_log2: int = 0) -> Result:
+                  local_search_alg: int = 0, fm_passes: int = 0, cluster_max_log2: int = 0,
+                  cluster_blocks: int = 0) -> Result:
         """Partition ``g``: a host :class:`CSR` (numpy) or a dict of CUDA torch
         tensors ``{"row_ptr", "col", "w"}`` (device-resident input).  The
         partition is written to ``part_out`` (numpy or CUDA tensor) when
@@ -330,7 +333,7 @@ class Partitioner:
         keep = []
         dg = self._graph(g, keep)
         o = self._options(cutoff, tol, mixed, rng_state, rng_inc, iter_cap, perc_imbalance, refine_alg, coarsener,
-                          local_search_alg, fm_passes, cluster_max_log2)
+                          local_search_alg, fm_passes, cluster_max_log2, cluster_blocks)
         res = L.sgp_b200_result_t()
         part_out, res.part = self._part_target(dg.n, part_out, o)
         L.check(L.lib().sgp_b200_partition(self._ctx, ctypes.byref(dg), ctypes.byref(o), ctypes.byref(res)),
@@ -354,7 +357,8 @@ class Partitioner:
 
     def partition_batch(self, graphs: list, workers: int = 4, cutoff: int = 50, tol: float = 1e-10,
                         mixed: bool = False, rng_state: int = 0x853C49E6748FEA9B, rng_inc: int = 1,
-                        iter_cap: int = 0, coarsener: int = 0, cluster_max_log2: int = 0) -> list:
+                        iter_cap: int = 0, coarsener: int = 0, cluster_max_log2: int = 0,
+                        cluster_blocks: int = 0) -> list:
         """Partition independent host graphs: ``workers`` host threads on
         separate streams coarsen them (largest first), one launch iterates the
         small coarse levels of every hierarchy (a block per hierarchy at a
@@ -362,14 +366,15 @@ class Partitioner:
         hierarchy at a time; by default every level up to 2^23 cost units),
         and the workers finish the larger levels and the splits.  One
         :class:`Result` per graph, identical to partitioning it alone with the
-        same options and the same ``cluster_max_log2`` (23 by default here)."""
+        same options and the same ``cluster_max_log2`` and ``cluster_blocks``
+        (23 and 2 by default here)."""
         keep = []
         cnt = max(1, len(graphs))
         arr = (L.sgp_b200_graph_t * cnt)()
         for i, g in enumerate(graphs):
             arr[i] = self._graph(g, keep)
         o = self._options(cutoff, tol, mixed, rng_state, rng_inc, iter_cap, 0, 0, coarsener,
-                          cluster_max_log2=cluster_max_log2)
+                          cluster_max_log2=cluster_max_log2, cluster_blocks=cluster_blocks)
         o.part_mem = L.HOST
         res = (L.sgp_b200_result_t * cnt)()
         parts = []

@@ -358,6 +358,12 @@ static int partition_begin(Context &C, const Level &L0, const sgp_b200_options_t
     const uint32_t lg = opt->cluster_max_log2 ? (opt->cluster_max_log2 < 40 ? opt->cluster_max_log2 : 40u)
                                               : (batch ? 23u : 17u);
     S->po.mid_limit = 1ull << lg;
+    // blocks per cluster: 8 for a single partition, 2 in a batch
+    if (opt->cluster_blocks != 0 && opt->cluster_blocks != 2 && opt->cluster_blocks != 8) {
+        set_error("options.cluster_blocks must be 0, 2 or 8 (got %u)", opt->cluster_blocks);
+        return SGP_B200_ERR_INVALID;
+    }
+    S->po.mid_blocks = opt->cluster_blocks ? (int)opt->cluster_blocks : (batch ? 2 : 8);
     SGPB_TRY(eigen_begin(C, S->levels, &S->st, opt->rng_inc, S->po, &S->es));
     return SGP_B200_OK;
 }

@@ -1611,7 +1611,7 @@ __device__ __forceinline__ uint32_t rows_at(const uint32_t *rp, uint32_t lo, uin
 // the first warp reads block r's slot, lane 0 adds them in rank order and
 // broadcasts through shared memory, so every block holds the same totals
 // (and only kMidCTAs remote reads per value and block cross the cluster).
-template <int NV>
+template <int CL, int NV>
 __device__ __forceinline__ void cluster_sum(double (&v)[NV], double (*slot)[8], int buf, double *sm,
                                             cg::cluster_group &cl) {
     block_sum_d<NV>(v, sm);
@@ -1622,13 +1622,13 @@ __device__ __forceinline__ void cluster_sum(double (&v)[NV], double (*slot)[8], 
     if (threadIdx.x < 32) {
         const unsigned lane = threadIdx.x;
         double mine[NV];
-        const double *rs = cl.map_shared_rank(&slot[buf][0], lane < kMidCTAs ? lane : 0u);
+        const double *rs = cl.map_shared_rank(&slot[buf][0], lane < (unsigned)CL ? lane : 0u);
 #pragma unroll
-        for (int k = 0; k < NV; k++) mine[k] = lane < kMidCTAs ? rs[k] : 0.0;
+        for (int k = 0; k < NV; k++) mine[k] = lane < (unsigned)CL ? rs[k] : 0.0;
 #pragma unroll
         for (int k = 0; k < NV; k++) {
             double t = 0;
-            for (int r = 0; r < kMidCTAs; r++) t += __shfl_sync(0xFFFFFFFFu, mine[k], r);
+            for (int r = 0; r < CL; r++) t += __shfl_sync(0xFFFFFFFFu, mine[k], r);
             if (lane == 0) sm[220 + k] = t;
         }
     }
@@ -1638,7 +1638,7 @@ __device__ __forceinline__ void cluster_sum(double (&v)[NV], double (*slot)[8], 
     __syncthreads();   // sm is reused by the next sum
 }
 
-template <typename W, bool MX>
+template <typename W, bool MX, int CL>
 __device__ __forceinline__ void mid_level(const MidLevelDesc &d, cg::cluster_group &cl, double *sm,
                                           double (*slot)[8], uint32_t *win, double *winx, double *wind) {
     typedef typename std::conditional<MX, float, double>::type ACC;
@@ -1649,8 +1649,8 @@ __device__ __forceinline__ void mid_level(const MidLevelDesc &d, cg::cluster_gro
     const unsigned rank = cl.block_rank();
     const unsigned lane = threadIdx.x & 31, wk = threadIdx.x >> 5;
     // rows of this block and of this warp: equal shares of the entries
-    const uint32_t R0 = rank == 0 ? 0u : rows_at(rp, 0, n, m * rank / kMidCTAs);
-    const uint32_t R1 = rank + 1 == kMidCTAs ? n : rows_at(rp, 0, n, m * (rank + 1) / kMidCTAs);
+    const uint32_t R0 = rank == 0 ? 0u : rows_at(rp, 0, n, m * rank / CL);
+    const uint32_t R1 = rank + 1 == (uint32_t)CL ? n : rows_at(rp, 0, n, m * (rank + 1) / CL);
     const uint64_t E0 = rp[R0], E1 = rp[R1];
     const uint32_t w0 = wk == 0 ? R0 : rows_at(rp, R0, R1, E0 + (E1 - E0) * wk / kMidWarps);
     const uint32_t w1 = wk + 1 == kMidWarps ? R1 : rows_at(rp, R0, R1, E0 + (E1 - E0) * (wk + 1) / kMidWarps);
@@ -1690,7 +1690,7 @@ __device__ __forceinline__ void mid_level(const MidLevelDesc &d, cg::cluster_gro
     cl.sync();
     if (threadIdx.x == 0) {
         double a = 0, b = 0, c = 0, mxd = 0;
-        for (int r = 0; r < kMidCTAs; r++) {
+        for (int r = 0; r < CL; r++) {
             const double *rs = cl.map_shared_rank(&slot[1][0], r);
             a += rs[0];
             b += rs[1];
@@ -1710,7 +1710,7 @@ __device__ __forceinline__ void mid_level(const MidLevelDesc &d, cg::cluster_gro
         const double x = d.va[i] - mu;
         q[0] += x * x;
     }
-    cluster_sum<1>(q, slot, 0, sm, cl);
+    cluster_sum<CL, 1>(q, slot, 0, sm, cl);
     double inv_nu = 1.0 / sqrt(q[0]);
     // ---- iterations
     double dot = 0, last = 1;
@@ -1733,7 +1733,7 @@ __device__ __forceinline__ void mid_level(const MidLevelDesc &d, cg::cluster_gro
             for (uint32_t i = w0; i < w1; i++)
                 if (rp[i] == rp[i + 1]) fin(i, (ACC)0, 0.0, src[i]);
         // consecutive exchanges alternate slots (phase 0 used 1, then 0)
-        cluster_sum<kNP>(P, slot, (int)((niter + 1) & 1), sm, cl);
+        cluster_sum<CL, kNP>(P, slot, (int)((niter + 1) & 1), sm, cl);
         const double mu_n = d.normlap ? 0.0 : P[0] / (double)n;
         const double nsq = P[1] - mu_n * P[0];
         const double inv_nu_n = 1.0 / sqrt(nsq);
@@ -1758,7 +1758,9 @@ __device__ __forceinline__ void mid_level(const MidLevelDesc &d, cg::cluster_gro
     }
 }
 
-__global__ void __cluster_dims__(kMidCTAs, 1, 1) __launch_bounds__(kMidThreads, 1)
+// CL blocks per cluster, set at launch (cudaLaunchAttributeClusterDimension)
+template <int CL>
+__global__ void __launch_bounds__(kMidThreads, 1)
     k_power_iter_mid(const MidLevelDesc *__restrict__ lev, const uint2 *__restrict__ chains, uint32_t nchains,
                      uint32_t *next) {
     cg::cluster_group cl = cg::this_cluster();
@@ -1785,11 +1787,11 @@ __global__ void __cluster_dims__(kMidCTAs, 1, 1) __launch_bounds__(kMidThreads, 
             const MidLevelDesc &dsc = lev[ch.x + k];
             const unsigned long long t0 = global_ns();
             if (dsc.wbytes == 8) {
-                if (dsc.mixed) mid_level<unsigned long long, true>(dsc, cl, sm, slot, swin[wk], swinx[wk], swind[wk]);
-                else mid_level<unsigned long long, false>(dsc, cl, sm, slot, swin[wk], swinx[wk], swind[wk]);
+                if (dsc.mixed) mid_level<unsigned long long, true, CL>(dsc, cl, sm, slot, swin[wk], swinx[wk], swind[wk]);
+                else mid_level<unsigned long long, false, CL>(dsc, cl, sm, slot, swin[wk], swinx[wk], swind[wk]);
             } else {
-                if (dsc.mixed) mid_level<uint32_t, true>(dsc, cl, sm, slot, swin[wk], swinx[wk], swind[wk]);
-                else mid_level<uint32_t, false>(dsc, cl, sm, slot, swin[wk], swinx[wk], swind[wk]);
+                if (dsc.mixed) mid_level<uint32_t, true, CL>(dsc, cl, sm, slot, swin[wk], swinx[wk], swind[wk]);
+                else mid_level<uint32_t, false, CL>(dsc, cl, sm, slot, swin[wk], swinx[wk], swind[wk]);
             }
             // every block's part of the result is written before the next
             // level reads it, and every read of another block's slots is done
@@ -2743,19 +2745,44 @@ int power_iter_mid_chains(Context &C, const std::vector<PIChain *> &chains, cons
     SGPB_CUDA(cudaMemcpyAsync(lev_d, h.data(), sizeof(MidLevelDesc) * h.size(), cudaMemcpyHostToDevice, C.stream));
     SGPB_CUDA(cudaMemcpyAsync(ch_d, hc.data(), sizeof(uint2) * hc.size(), cudaMemcpyHostToDevice, C.stream));
     SGPB_TRY(dzero(C, next, 4));
-    // as many clusters as fit at once (the queue balances the rest)
-    cudaLaunchConfig_t cfg;
-    memset(&cfg, 0, sizeof(cfg));
-    cfg.gridDim = dim3(kMidCTAs);
-    cfg.blockDim = dim3(kMidThreads);
-    int max_clusters = 0;
-    SGPB_CUDA(cudaOccupancyMaxActiveClusters(&max_clusters, (const void *)k_power_iter_mid, &cfg));
-    if (max_clusters < 1) {
-        set_error("the mid-size power-iteration cluster does not fit on the device");
-        return SGP_B200_ERR_DEVICE;
+    // as many clusters as fit at once (the queue balances the rest); CL
+    // blocks a cluster: 8 for single partitions (latency of each level), 2
+    // for batches (more hierarchies iterate at once)
+    const int CLn = o.mid_blocks ? o.mid_blocks : kMidCTAs;
+    auto launch = [&](auto tag) -> int {
+        constexpr int CL = decltype(tag)::value;
+        const void *k = (const void *)k_power_iter_mid<CL>;
+        cudaLaunchAttribute attr[1];
+        attr[0].id = cudaLaunchAttributeClusterDimension;
+        attr[0].val.clusterDim.x = CL;
+        attr[0].val.clusterDim.y = 1;
+        attr[0].val.clusterDim.z = 1;
+        cudaLaunchConfig_t cfg;
+        memset(&cfg, 0, sizeof(cfg));
+        cfg.gridDim = dim3(CL);
+        cfg.blockDim = dim3(kMidThreads);
+        cfg.stream = C.stream;
+        cfg.attrs = attr;
+        cfg.numAttrs = 1;
+        int max_clusters = 0;
+        SGPB_CUDA(cudaOccupancyMaxActiveClusters(&max_clusters, k, &cfg));
+        if (max_clusters < 1) {
+            set_error("the mid-size power-iteration cluster does not fit on the device");
+            return SGP_B200_ERR_DEVICE;
+        }
+        const uint32_t nclu = (uint32_t)(hc.size() < (size_t)max_clusters ? hc.size() : (size_t)max_clusters);
+        cfg.gridDim = dim3(nclu * CL);
+        const uint32_t nch = (uint32_t)hc.size();
+        SGPB_CUDA(cudaLaunchKernelEx(&cfg, k_power_iter_mid<CL>, (const MidLevelDesc *)lev_d, (const uint2 *)ch_d, nch,
+                                     next));
+        return SGP_B200_OK;
+    };
+    if (CLn == 2) SGPB_TRY(launch(std::integral_constant<int, 2>()));
+    else if (CLn == 8) SGPB_TRY(launch(std::integral_constant<int, 8>()));
+    else {
+        set_error("cluster_blocks must be 2 or 8 (got %d)", CLn);
+        return SGP_B200_ERR_INVALID;
     }
-    const uint32_t nclu = (uint32_t)(hc.size() < (size_t)max_clusters ? hc.size() : (size_t)max_clusters);
-    k_power_iter_mid<<<nclu * kMidCTAs, kMidThreads, 0, C.stream>>>(lev_d, ch_d, (uint32_t)hc.size(), next);
     C.kernel_launches++;
     SGPB_CUDA(cudaGetLastError());
     std::vector<double> rh(8 * h.size());

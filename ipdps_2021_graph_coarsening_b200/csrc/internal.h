@@ -166,6 +166,7 @@ struct PowerIterOpts {
     int allow_relabel = 1;   // skewed levels may iterate on a hub-first relabelled copy
     int normlap = 0;         // refine_alg 1: normalized-Laplacian (lazy random walk) iteration
     uint64_t mid_limit = 0;  // largest cost (m + 8n) of a level on the cluster kernel; 0 = 2^17
+    int mid_blocks = 0;       // blocks per cluster of the cluster kernel (2 or 8); 0 = 8
 };
 struct PowerIterResult {
     uint64_t niter = 0;

@@ -125,7 +125,7 @@ def test_batch_and_4way_take_the_coarsener(partitioner):
     gs = [CASES["holes"], CASES["er"]]
     many = partitioner.partition_batch(gs, workers=2, rng_state=8, coarsener=L.COARSEN_GOSH)
     for g, r in zip(gs, many):
-        s = partitioner.partition(g, rng_state=8, coarsener=L.COARSEN_GOSH, cluster_max_log2=23)
+        s = partitioner.partition(g, rng_state=8, coarsener=L.COARSEN_GOSH, cluster_max_log2=23, cluster_blocks=2)
         assert np.array_equal(r.part, s.part) and r.level_n == s.level_n
     part4, cut2, cut4, _ = partitioner.partition_4way(CASES["holes"], rng_state=8, coarsener=L.COARSEN_MATCH)
     assert cut4 == cut_of(CASES["holes"], part4) and part4.max() <= 3

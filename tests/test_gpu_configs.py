@@ -11,6 +11,7 @@ in each test.
 import numpy as np
 import pytest
 
+from ipdps_2021_graph_coarsening_b200 import _lib as L
 from ipdps_2021_graph_coarsening_b200 import graphs as G
 from oracle import bindings as O
 
@@ -98,9 +99,11 @@ def batch_graphs(count, seed=17, lo=1000, hi=12000):
     return out
 
 
-# a batch runs levels of up to 2^23 cost units on the cluster kernel (single
-# calls: 2^17); with the same cluster_max_log2 a single call gives equal bits
+# a batch runs levels of up to 2^23 cost units on the cluster kernel in
+# clusters of 2 blocks (single calls: 2^17, 8 blocks); with the same
+# cluster_max_log2 and cluster_blocks a single call gives equal bits
 BATCH_CLUSTER = 23
+BATCH_BLOCKS = 2
 
 
 def test_batch_equals_single_calls(partitioner):
@@ -108,7 +111,7 @@ def test_batch_equals_single_calls(partitioner):
     many = partitioner.partition_batch(gs, workers=4, rng_state=9)
     one = partitioner.partition_batch(gs, workers=1, rng_state=9)
     for g, a, b in zip(gs, many, one):
-        s = partitioner.partition(g, rng_state=9, cluster_max_log2=BATCH_CLUSTER)
+        s = partitioner.partition(g, rng_state=9, cluster_max_log2=BATCH_CLUSTER, cluster_blocks=BATCH_BLOCKS)
         for r in (a, b):
             assert np.array_equal(r.part, s.part)
             assert r.edgecut == s.edgecut == cut_of(g, r.part)
@@ -128,7 +131,8 @@ def test_batch_of_small_hierarchies(partitioner):
     gs = batch_graphs(40, seed=5, lo=40, hi=1500)
     rs = partitioner.partition_batch(gs, workers=3, rng_state=2)
     for g, r in zip(gs, rs):
-        same_result(r, partitioner.partition(g, rng_state=2, cluster_max_log2=BATCH_CLUSTER))
+        same_result(r, partitioner.partition(g, rng_state=2, cluster_max_log2=BATCH_CLUSTER,
+                                             cluster_blocks=BATCH_BLOCKS))
         assert r.edgecut == cut_of(g, r.part)
     for g, r in list(zip(gs, rs))[:6]:
         o = O.partition_graph(g.row_ptr, g.col, None, cutoff=50, tol=1e-10, rng_state=2)
@@ -144,7 +148,8 @@ def test_batch_weighted_and_mixed_equal_single_calls(partitioner, mixed):
     gs += batch_graphs(5, seed=41, lo=2000, hi=20000)
     rs = partitioner.partition_batch(gs, workers=2, rng_state=8, mixed=mixed)
     for g, r in zip(gs, rs):
-        same_result(r, partitioner.partition(g, rng_state=8, mixed=mixed, cluster_max_log2=BATCH_CLUSTER))
+        same_result(r, partitioner.partition(g, rng_state=8, mixed=mixed, cluster_max_log2=BATCH_CLUSTER,
+                                             cluster_blocks=BATCH_BLOCKS))
 
 
 def test_batch_default_and_single_default_agree(partitioner):
@@ -202,7 +207,7 @@ def test_sharded_batch_on_one_rank(partitioner):
     gs = batch_graphs(5, seed=31)
     out = shard.partition_sharded(gs, lambda l: partitioner.partition_batch(l, workers=2, rng_state=6), 0, 1)
     for g, r in zip(gs, out):
-        s = partitioner.partition(g, rng_state=6, cluster_max_log2=BATCH_CLUSTER)
+        s = partitioner.partition(g, rng_state=6, cluster_max_log2=BATCH_CLUSTER, cluster_blocks=BATCH_BLOCKS)
         assert np.array_equal(r.part, s.part) and r.edgecut == s.edgecut
 
 
@@ -258,3 +263,20 @@ def test_refine_alg_out_of_range_is_rejected(partitioner):
     from ipdps_2021_graph_coarsening_b200 import _lib as L
     with pytest.raises(L.SgparError):
         partitioner.partition(G.grid2d(20, 20), refine_alg=2)
+
+
+def test_cluster_blocks_option(partitioner):
+    """Clusters of 2 and 8 blocks for the mid-size levels (the 300 x 300
+    grid's level of 3243 vertices runs there) give the same hierarchy and
+    agree to rounding; other block counts are rejected."""
+    g = G.grid2d(300, 300)
+    a = partitioner.partition(g, rng_state=3, cluster_blocks=2)
+    b = partitioner.partition(g, rng_state=3, cluster_blocks=8)
+    c = partitioner.partition(g, rng_state=3)
+    assert a.level_n == b.level_n == c.level_n and a.rng_state == b.rng_state
+    assert b.lam == c.lam and b.edgecut == c.edgecut   # 8 is the single-call default
+    assert abs(a.lam - b.lam) <= 1e-8 * abs(b.lam)
+    assert abs(a.edgecut - b.edgecut) <= 0.01 * b.edgecut
+    with pytest.raises(L.SgparError) as ei:
+        partitioner.partition(g, rng_state=3, cluster_blocks=3)
+    assert ei.value.code == L.ERR_INVALID and "cluster_blocks" in L.last_error()

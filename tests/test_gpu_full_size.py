@@ -124,6 +124,6 @@ def test_batch2048(partitioner):
         rows = np.repeat(np.arange(g.n), np.diff(g.row_ptr).astype(np.int64))
         assert r.edgecut == int((part[rows] != part[g.col]).sum()) // 2
     for k in (0, 1, 777, 1500, 2047):
-        s = partitioner.partition(gs[k], rng_state=11, cluster_max_log2=23)
+        s = partitioner.partition(gs[k], rng_state=11, cluster_max_log2=23, cluster_blocks=2)
         assert np.array_equal(np.asarray(rs[k].part), np.asarray(s.part)) and rs[k].edgecut == s.edgecut
         assert rs[k].level_iters == s.level_iters
