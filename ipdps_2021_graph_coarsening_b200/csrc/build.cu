@@ -32,6 +32,9 @@ constexpr uint32_t kSentinel = 0xFFFFFFFFu;
 // rows-strided kernel: the count and key kernels list them and leave them to
 // a kernel that gives each such row a block.
 constexpr uint32_t kLongRowT = 8192;
+// levels with at least this many entries keep their entries' coarse
+// destinations from the count for the scatter (k_build_count's cvs)
+constexpr uint64_t kStoreCvMin = 1ull << 20;
 constexpr int kLongThreads = 1024;
 
 __device__ __forceinline__ void list_long_row(uint32_t *long_list, uint32_t *long_cnt, uint32_t u) {
@@ -62,7 +65,7 @@ __global__ void __launch_bounds__(256) k_build_count(uint32_t n, const uint32_t 
                                                      const uint32_t *__restrict__ vcmap,
                                                      uint32_t *__restrict__ cnt, uint32_t *__restrict__ krow,
                                                      uint32_t *__restrict__ long_list,
-                                                     uint32_t *__restrict__ long_cnt) {
+                                                     uint32_t *__restrict__ long_cnt, uint32_t *__restrict__ cvs) {
     const unsigned gm = group_mask<G>();
     const uint32_t lane = threadIdx.x & (G - 1);
     const uint64_t gid = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) / G;
@@ -81,7 +84,11 @@ __global__ void __launch_bounds__(256) k_build_count(uint32_t n, const uint32_t 
             for (int q = 0; q < 4; q++) d[q] = j0 + q * G < e ? __ldg(col + j0 + q * G) : 0u;
 #pragma unroll
             for (int q = 0; q < 4; q++)
-                if (j0 + q * G < e) c += (__ldg(vcmap + d[q]) != cu);
+                if (j0 + q * G < e) {
+                    const uint32_t cv = __ldg(vcmap + d[q]);
+                    if (cvs) cvs[j0 + q * G] = cv;
+                    c += cv != cu;
+                }
         }
 #pragma unroll
         for (int o = G / 2; o > 0; o >>= 1) c += __shfl_xor_sync(gm, c, o);
@@ -99,7 +106,8 @@ __global__ void __launch_bounds__(kLongThreads) k_build_count_long(const uint32_
                                                                  uint32_t *__restrict__ cnt,
                                                                  uint32_t *__restrict__ krow,
                                                                  const uint32_t *__restrict__ long_list,
-                                                                 const uint32_t *__restrict__ long_cnt) {
+                                                                 const uint32_t *__restrict__ long_cnt,
+                                                                 uint32_t *__restrict__ cvs) {
     __shared__ uint32_t sm[kLongThreads / 32];
     const uint32_t nl = *long_cnt;
     for (uint32_t r = blockIdx.x; r < nl; r += gridDim.x) {
@@ -113,7 +121,11 @@ __global__ void __launch_bounds__(kLongThreads) k_build_count_long(const uint32_
             for (int q = 0; q < 4; q++) d[q] = j0 + q * blockDim.x < e ? __ldg(col + j0 + q * blockDim.x) : 0u;
 #pragma unroll
             for (int q = 0; q < 4; q++)
-                if (j0 + q * blockDim.x < e) c += (__ldg(vcmap + d[q]) != cu);
+                if (j0 + q * blockDim.x < e) {
+                    const uint32_t cv = __ldg(vcmap + d[q]);
+                    if (cvs) cvs[j0 + q * blockDim.x] = cv;
+                    c += cv != cu;
+                }
         }
         c = block_sum_long(c, sm);
         if (threadIdx.x == 0) {
@@ -134,7 +146,8 @@ __global__ void __launch_bounds__(256) k_build_scatter(uint32_t n, const uint32_
                                                        const uint32_t *__restrict__ vcmap,
                                                        const uint32_t *__restrict__ krow,
                                                        const uint32_t *__restrict__ boff, uint32_t *__restrict__ fill,
-                                                       uint32_t *__restrict__ bdst, WI *__restrict__ bw) {
+                                                       uint32_t *__restrict__ bdst, WI *__restrict__ bw,
+                                                       const uint32_t *__restrict__ cvs) {
     const unsigned gm = group_mask<G>();
     const uint32_t lane = threadIdx.x & (G - 1);
     const unsigned lane32 = threadIdx.x & 31;
@@ -157,11 +170,15 @@ __global__ void __launch_bounds__(256) k_build_scatter(uint32_t n, const uint32_
 #pragma unroll
             for (int q = 0; q < 4; q++) {
                 const uint32_t j = j0 + q * G + lane;
-                cv[q] = j < e ? __ldg(col + j) : 0u;
+                cv[q] = j < e ? __ldg((cvs ? cvs : col) + j) : 0u;
                 if (w) wv[q] = j < e ? __ldg(w + j) : (WI)0;
             }
+            if (!cvs)
 #pragma unroll
-            for (int q = 0; q < 4; q++) cv[q] = j0 + q * G + lane < e ? __ldg(vcmap + cv[q]) : cu;
+                for (int q = 0; q < 4; q++) cv[q] = j0 + q * G + lane < e ? __ldg(vcmap + cv[q]) : cu;
+            else
+#pragma unroll
+                for (int q = 0; q < 4; q++) cv[q] = j0 + q * G + lane < e ? cv[q] : cu;
 #pragma unroll
             for (int q = 0; q < 4; q++) {
                 const bool keep = cv[q] != cu;
@@ -185,7 +202,7 @@ __global__ void __launch_bounds__(kLongThreads) k_build_scatter_long(
     const uint32_t *__restrict__ rp, const uint32_t *__restrict__ col, const WI *__restrict__ w,
     const uint32_t *__restrict__ vcmap, const uint32_t *__restrict__ krow, const uint32_t *__restrict__ boff,
     uint32_t *__restrict__ fill, uint32_t *__restrict__ bdst, WI *__restrict__ bw,
-    const uint32_t *__restrict__ long_list, const uint32_t *__restrict__ long_cnt) {
+    const uint32_t *__restrict__ long_list, const uint32_t *__restrict__ long_cnt, const uint32_t *__restrict__ cvs) {
     __shared__ uint32_t s_base, s_pos;
     const uint32_t nl = *long_cnt;
     const unsigned lane = threadIdx.x & 31;
@@ -204,7 +221,7 @@ __global__ void __launch_bounds__(kLongThreads) k_build_scatter_long(
         // whole warps per step (the loop bound is warp-uniform)
         for (uint32_t j0 = b + (threadIdx.x & ~31u); j0 < e; j0 += blockDim.x) {
             const uint32_t j = j0 + lane;
-            const uint32_t cv = j < e ? __ldg(vcmap + __ldg(col + j)) : cu;
+            const uint32_t cv = j < e ? (cvs ? __ldg(cvs + j) : __ldg(vcmap + __ldg(col + j))) : cu;
             const WI wv = (w && j < e) ? __ldg(w + j) : (WI)0;
             const bool keep = cv != cu;
             const unsigned bal = __ballot_sync(0xFFFFFFFFu, keep);
@@ -942,10 +959,16 @@ static int build_impl(Context &C, const Level &F, const WI *w, const uint32_t *v
     SGPB_TRY(dzero(C, long_cnt, sizeof(uint32_t)));
     uint32_t glong = (uint32_t)(F.m / kLongRowT + 1);
     if (glong > (uint32_t)C.num_sms * 2) glong = C.num_sms * 2;
+    // large levels: the count keeps each entry's coarse destination, so the
+    // scatter streams it instead of gathering vcmap a second time (the
+    // random gathers, not the bytes, bound both passes)
+    uint32_t *cvs = nullptr;
+    if (F.m >= kStoreCvMin) SGPB_TRY(dalloc_t(C, &cvs, (size_t)F.m + 1));
 #define K_COUNT(G) k_build_count<G>
-    SGPB_BY_G(K_COUNT, n, F.rp, F.col, vcmap, cnt, krow, long_list, long_cnt)
+    SGPB_BY_G(K_COUNT, n, F.rp, F.col, vcmap, cnt, krow, long_list, long_cnt, cvs)
     if (F.m > kLongRowT) {
-        k_build_count_long<<<glong, kLongThreads, 0, C.stream>>>(F.rp, F.col, vcmap, cnt, krow, long_list, long_cnt);
+        k_build_count_long<<<glong, kLongThreads, 0, C.stream>>>(F.rp, F.col, vcmap, cnt, krow, long_list, long_cnt,
+                                                                 cvs);
         C.kernel_launches++;
     }
     SGPB_TRY(scan_u32(C, cnt, boff, nc, nullptr));
@@ -958,10 +981,10 @@ static int build_impl(Context &C, const Level &F, const WI *w, const uint32_t *v
     if (w) SGPB_TRY(dalloc_t(C, &bw, (size_t)kept + 1));
     SGPB_TRY(dalloc_t(C, &tw, (size_t)kept + 1));
 #define K_SCATTER(G) k_build_scatter<G, WI>
-    SGPB_BY_G(K_SCATTER, n, F.rp, F.col, w, vcmap, krow, boff, fill, bdst, bw)
+    SGPB_BY_G(K_SCATTER, n, F.rp, F.col, w, vcmap, krow, boff, fill, bdst, bw, cvs)
     if (F.m > kLongRowT) {
         k_build_scatter_long<WI><<<glong, kLongThreads, 0, C.stream>>>(F.rp, F.col, w, vcmap, krow, boff, fill, bdst,
-                                                                      bw, long_list, long_cnt);
+                                                                      bw, long_list, long_cnt, cvs);
         C.kernel_launches++;
     }
 #undef K_COUNT
