@@ -766,6 +766,7 @@ __global__ void __launch_bounds__(kDenseSmemThreads, 1)
 }
 
 // ---------------------------------------------------------- compaction --
+constexpr int kCompactU = 8;   // entries per lane in flight
 // Copies the merged buckets into the coarse CSR; with 32-bit weights it also
 // keeps their maximum in *wmax (when given), which decides how narrow the
 // power iteration's copy of the level can store them.
@@ -781,18 +782,18 @@ __global__ void __launch_bounds__(256) k_compact_rows(uint32_t nc, const uint32_
     const uint64_t nw = ((uint64_t)gridDim.x * blockDim.x) >> 5;
     for (uint64_t c = wid; c < nc; c += nw) {
         const uint32_t src = boff[c], dst = crp[c], len = crp[c + 1] - dst;
-        // four entries per lane in flight: loads first, then stores
-        for (uint32_t i0 = lane; i0 < len; i0 += 128) {
-            uint32_t d[4];
-            WO x[4];
+        // kCompactU entries per lane in flight: loads first, then stores
+        for (uint32_t i0 = lane; i0 < len; i0 += 32 * kCompactU) {
+            uint32_t d[kCompactU];
+            WO x[kCompactU];
 #pragma unroll
-            for (int k = 0; k < 4; k++) {
+            for (int k = 0; k < kCompactU; k++) {
                 const uint32_t i = i0 + 32 * k;
                 d[k] = i < len ? __ldg(bdst + src + i) : 0u;
                 x[k] = i < len ? __ldg(tw + src + i) : (WO)0;
             }
 #pragma unroll
-            for (int k = 0; k < 4; k++) {
+            for (int k = 0; k < kCompactU; k++) {
                 const uint32_t i = i0 + 32 * k;
                 if (i < len) {
                     ccol[dst + i] = d[k];

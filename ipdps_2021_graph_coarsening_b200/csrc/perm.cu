@@ -103,20 +103,20 @@ __global__ void __launch_bounds__(256) k_perm_fill(uint32_t n, const uint32_t *_
     for (uint64_t i = wid; i < n; i += nwarps) {
         const uint32_t o = inv[i];
         const uint32_t b = rp[o], e = rp[o + 1], d = nrp[i];
-        // four entries per lane in flight: destinations, their new ids, stores
-        for (uint32_t j0 = b + lane; j0 < e; j0 += 128) {
-            uint32_t c[4];
-            WI x[4];
+        // eight entries per lane in flight: destinations, their new ids, stores
+        for (uint32_t j0 = b + lane; j0 < e; j0 += 256) {
+            uint32_t c[8];
+            WI x[8];
 #pragma unroll
-            for (int k = 0; k < 4; k++) {
+            for (int k = 0; k < 8; k++) {
                 const uint32_t j = j0 + 32 * k;
                 c[k] = j < e ? col[j] : 0u;
                 if (w) x[k] = j < e ? w[j] : (WI)0;
             }
 #pragma unroll
-            for (int k = 0; k < 4; k++) c[k] = j0 + 32 * k < e ? perm[c[k]] : 0u;
+            for (int k = 0; k < 8; k++) c[k] = j0 + 32 * k < e ? perm[c[k]] : 0u;
 #pragma unroll
-            for (int k = 0; k < 4; k++) {
+            for (int k = 0; k < 8; k++) {
                 const uint32_t j = j0 + 32 * k;
                 if (j < e) {
                     ncol[d + (j - b)] = c[k];
